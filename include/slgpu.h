@@ -1,0 +1,235 @@
+/*
+ * slgpu.h -- C ABI of the B200 weak-form assembly engine.
+ *
+ * The engine replaces the compute inside sparselizard's
+ *   contribution::generate  (src/formulation/contribution.cpp:20-308)
+ *   rawmat::process         (src/formulation/rawmat.cpp:127-299)
+ * Everything crossing this boundary is plain C: pointers, sizes and int status
+ * codes.  Host arrays passed in are copied (or uploaded) before the call
+ * returns; outputs are written to caller-owned host buffers, following
+ * PETSc's MatCreateSeqAIJWithArrays ownership model that rawmat relies on
+ * (src/formulation/rawmat.cpp:292-296).
+ *
+ * Error convention: every entry point returns SLGPU_OK (0) or a positive
+ * SLGPU_E_* code; slgpu_last_error() gives the message.  sparselizard's
+ * adapter turns a non-zero status into logs::error(), i.e. a thrown
+ * std::runtime_error (src/logs.cpp:9-12).
+ *
+ * One context drives one device.  Calls on a context must be serialised by
+ * the caller (sparselizard's assembly is single-threaded host code).
+ */
+#ifndef SLGPU_H
+#define SLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct slgpu_ctx slgpu_ctx;
+
+enum {
+    SLGPU_OK = 0,
+    SLGPU_E_ARG = 1,          /* invalid argument or inconsistent sizes */
+    SLGPU_E_CUDA = 2,         /* a CUDA call failed */
+    SLGPU_E_UNSUPPORTED = 3,  /* input outside what the engine implements */
+    SLGPU_E_BUDGET = 4,       /* request exceeds the context's HBM budget */
+    SLGPU_E_STATE = 5,        /* call not valid in the current state */
+    SLGPU_E_NODEVICE = 6,     /* no usable CUDA device / extension */
+    SLGPU_E_TIMEOUT = 7       /* a bounded device wait gave up */
+};
+
+/* Context flags. */
+#define SLGPU_CTX_RECORD_ONLY 1u /* no device: groups are recorded for inspection, never executed */
+
+/* Contraction precision (slgpu_matrix_process / slgpu_rhs_assemble). */
+enum {
+    SLGPU_PREC_FP64 = 0,  /* plain FP64 */
+    SLGPU_PREC_SPLIT = 1, /* FP64 operands split into BF16 slices on tensor cores, FP32 accumulation, FP64 recombination */
+    SLGPU_PREC_FP32 = 2   /* FP32 tier */
+};
+
+/*
+ * Context.  hbm_budget bounds the device memory the context may hold
+ * (0 = 150 GB).  Replaces nothing in the reference: sparselizard has no
+ * device; the adapter creates one context per process on first use.
+ */
+int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** out);
+void slgpu_ctx_destroy(slgpu_ctx* ctx);
+int slgpu_last_error(const slgpu_ctx* ctx, char* buf, size_t len);
+/* Bytes of device memory currently held by the context. */
+int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx);
+
+/*
+ * Mesh geometry, resident on the device.  Replaces the node-coordinate and
+ * curved-node gathers of rawfield::getjacterms (src/field/rawfield.cpp:2442-2502).
+ *   xyz   [3*nnodes]                  node coordinates (nodes::getcoordinates)
+ *   conn  [nelem*ncurvednodes]        curved nodes of each element of `elemtype`
+ *                                     (elements::getsubelement(0, type, e, n))
+ */
+int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double* xyz);
+int slgpu_mesh_set_elements(slgpu_ctx* ctx, int mesh, int elemtype, int ncurvednodes, int64_t nelem, const int32_t* conn);
+
+/*
+ * Coefficient program: a DAG evaluated at every (element, Gauss point).  Node
+ * k's value is computed from its operands (earlier nodes).  Lowered from
+ * sparselizard's operation trees (opconstant, opjac, opinvjac, opdetjac,
+ * opparameter, opfield, opsum, opproduct, opinversion, oppower;
+ * src/expression/operation/op*.cpp).
+ */
+enum {
+    SLGPU_OP_CONST = 0,  /* consts[a] */
+    SLGPU_OP_JAC = 1,    /* J(a,b) = d x_b / d ref_a   (jacobian::getjac, src/field/jacobian.cpp:387) */
+    SLGPU_OP_INVJAC = 2, /* inverse of J, entry (a,b)   (jacobian::getinvjac, src/field/jacobian.cpp:396-504) */
+    SLGPU_OP_DETJAC = 3, /* det J (signed)               (src/field/jacobian.cpp:308-349) */
+    SLGPU_OP_ELEM = 4,   /* elemdata[a][e]: one value per element (per-region parameters, ...) */
+    SLGPU_OP_FIELD = 5,  /* sum_f fielddata[a][f*nelem+e] * table b [orient][f][g] (rawfield::interpolate, rawfield.cpp:2632-2686) */
+    SLGPU_OP_COORD = 6,  /* coordinate a (0 x, 1 y, 2 z) interpolated with the Lagrange geometry */
+    SLGPU_OP_ADD = 7,    /* v[a] + v[b] */
+    SLGPU_OP_MUL = 8,    /* v[a] * v[b] */
+    SLGPU_OP_INV = 9,    /* 1 / v[a] */
+    SLGPU_OP_NEG = 10,   /* -v[a] */
+    SLGPU_OP_POW = 11    /* pow(v[a], v[b]) */
+};
+
+typedef struct {
+    int32_t op, a, b, c;
+} slgpu_node;
+
+/* Form-function table: [norient][rows][ngp] values at the Gauss points for one
+ * (derivative, component); hierarchicalformfunctioncontainer::tomatrix
+ * (src/shapefunction/hierarchical/hierarchicalformfunctioncontainer.cpp:78-113)
+ * for each total orientation used by the group. */
+typedef struct {
+    int32_t rows;
+    const double* vals;
+} slgpu_table;
+
+/* One coef*dof*tf term (contribution.cpp:155-249).  dof_table < 0 marks a
+ * right-hand-side term (no dof).  scale is the harmonic product factor of
+ * harmonic::getproduct (src/harmonic.cpp:86-108), relative to the group. */
+typedef struct {
+    int32_t tf_table;
+    int32_t dof_table;
+    int32_t coef_node;
+    int32_t pad;
+    double scale;
+} slgpu_term;
+
+/* Where a group's element matrices go: rows from tfaddr [ntf][nelem], columns
+ * from dofaddr [ndof][nelem] (dofmanager::getaddresses, -1 = not a DOF here,
+ * src/formulation/dofmanager.cpp:846-918), values times multiplier. */
+typedef struct {
+    const int32_t* tfaddr;
+    const int32_t* dofaddr;
+    double multiplier;
+} slgpu_dest;
+
+/* Element types follow sparselizard's numbering (src/element.h): 0 point,
+ * 1 line, 2 triangle, 3 quadrangle, 4 tetrahedron, 5 hexahedron, 6 prism,
+ * 7 pyramid. */
+typedef struct {
+    int32_t mesh, elemtype, elemdim, problemdim;
+    int64_t nelem;
+    const int32_t* elems;   /* [nelem] element numbers within the type */
+    const int32_t* orient;  /* [nelem] orientation variant index in [0, norient) */
+    int32_t norient;
+    int32_t ngp;
+    const double* weights;  /* [ngp] Gauss weights */
+    int32_t ncurvednodes;
+    const double* lagrange; /* [1+elemdim][ncurvednodes][ngp]: Lagrange geometry values then ki/eta/phi derivatives */
+    int32_t ntf, ndof;      /* form functions of the tf and dof fields (ndof = 1 for rhs groups) */
+    int32_t ntables;
+    const slgpu_table* tables;
+    int32_t nnodes;
+    const slgpu_node* nodes;
+    int32_t nconsts;
+    const double* consts;
+    int32_t nelemdata;
+    const double* const* elemdata;  /* each [nelem] */
+    int32_t nfielddata;
+    const double* const* fielddata; /* each [fieldrows[k]][nelem] */
+    const int32_t* fieldrows;
+    int32_t nterms;
+    const slgpu_term* terms;
+    int32_t ndests;
+    const slgpu_dest* dests;
+} slgpu_group;
+
+/*
+ * Matrix assembly (one per sparselizard rawmat).  Groups and raw COO
+ * fragments accumulate; process() builds the A/D CSR split of
+ * rawmat::process (src/formulation/rawmat.cpp:127-299): rows of constrained
+ * DOFs dropped, constrained columns routed to D, both renumbered locally,
+ * duplicates summed in a fixed order.
+ */
+typedef struct {
+    int64_t nA;    /* unconstrained DOFs (rows of A and D) */
+    int64_t nD;    /* constrained DOFs (columns of D) */
+    int64_t nnzA;
+    int64_t nnzD;
+    int64_t ncoo;  /* COO entries generated (before -1 / constrained-row drops) */
+    int32_t pattern_reused; /* 1 if the CSR pattern came from the resident cache */
+    int32_t pad;
+} slgpu_csr_info;
+
+int slgpu_matrix_create(slgpu_ctx* ctx, int64_t ndofs, int* handle);
+int slgpu_matrix_destroy(slgpu_ctx* ctx, int handle);
+/* New matrix sharing the groups and fragments added so far (copy-on-write
+ * support for rawmat::extractaccumulated, src/formulation/rawmat.cpp:328-337). */
+int slgpu_matrix_clone(slgpu_ctx* ctx, int handle, int* new_handle);
+/* Adds a copy of `g`; returns its group index in *index (may be NULL). */
+int slgpu_matrix_add_group(slgpu_ctx* ctx, int handle, const slgpu_group* g, int* index);
+/* Raw fragment as stored by rawmat::accumulate (src/formulation/rawmat.cpp:57-65):
+ * rows [ntr][nc], cols [ndr][nc], vals [nr][nc]; row r of vals uses rows[r/ndr]
+ * and cols[r%ndr] when ntr or ndr differ from nr, else rows[r] and cols[r]. */
+int slgpu_matrix_add_fragment(slgpu_ctx* ctx, int handle, int32_t ntr, int32_t ndr, int32_t nr, int64_t nc,
+                              const int32_t* rows, const int32_t* cols, const double* vals);
+/* Replaces per-element data array `k` of group `gi` (new coefficients on a resident pattern). */
+int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values);
+/* Replaces term scales and destination multipliers of group `gi` (e.g. a new frequency). */
+int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* term_scales, const double* dest_multipliers);
+/* isconstrained [ndofs] (dofmanager::isconstrained, src/formulation/dofmanager.cpp:366-382). */
+int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstrained, int precision, slgpu_csr_info* info);
+/* Copies the processed CSR blocks to host memory: Arows/Drows [nA+1], Acols/Avals [nnzA], Dcols/Dvals [nnzD]. */
+int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* Acols, double* Avals,
+                          int32_t* Drows, int32_t* Dcols, double* Dvals);
+/* Copies only the values (pattern unchanged since the last download). */
+int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, double* Dvals);
+/* Device pointers to the processed CSR arrays (valid until the next process/destroy). */
+int slgpu_matrix_device_csr(slgpu_ctx* ctx, int handle, const int32_t** Arows, const int32_t** Acols, const double** Avals,
+                            const int32_t** Drows, const int32_t** Dcols, const double** Dvals);
+
+/*
+ * Right-hand side (contribution.cpp:293-300 + rawvec::setvalues "add",
+ * src/formulation/rawvec.cpp:216-254): b_accum[addr] += -sum of the group's
+ * element vectors, negative addresses skipped, duplicates summed in a fixed
+ * order.  b_accum is a host array of length ndofs.
+ */
+int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int precision, double* b_accum);
+
+/* Device time (ms) of the phases of the last process()/rhs call:
+ * [0] geometry+coefficients, [1] contraction, [2] pattern (symbolic), [3] CSR values, [4] total. */
+int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5);
+
+/* Record-only contexts: inspect what was recorded for a matrix handle. */
+int slgpu_record_count(const slgpu_ctx* ctx, int handle, int* ngroups, int* nfragments);
+int slgpu_record_group(const slgpu_ctx* ctx, int handle, int gi, slgpu_group* out);
+int slgpu_record_fragment(const slgpu_ctx* ctx, int handle, int fi, int32_t* ntr, int32_t* ndr, int32_t* nr, int64_t* nc,
+                          const int32_t** rows, const int32_t** cols, const double** vals);
+int slgpu_record_constraints(const slgpu_ctx* ctx, int handle, int64_t* ndofs, const uint8_t** isconstrained);
+/* Right-hand-side groups passed to slgpu_rhs_assemble on a record-only context
+ * (which returns SLGPU_E_NODEVICE after recording). */
+int slgpu_record_rhs_count(const slgpu_ctx* ctx, int* ngroups);
+int slgpu_record_rhs_group(const slgpu_ctx* ctx, int gi, slgpu_group* out, int64_t* ndofs);
+/* Mesh arrays given to slgpu_mesh_set_nodes / slgpu_mesh_set_elements. */
+int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nnodes, const double** xyz, int* ncurvednodes,
+                      int64_t* nelem, const int32_t** conn);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,143 @@
+// Replacement for sparselizard's src/formulation/rawmat.cpp (same header,
+// rawmat.h, unchanged).  Element contributions recorded by the GPU
+// contribution::generate and raw fragments passed to accumulate() are turned
+// into the A/D CSR blocks on the device by slgpu_matrix_process, then copied
+// into the rawmat's own Arows/Acols/Avals/Drows/Dcols/Dvals members, which
+// PETSc borrows exactly as in the reference (MatCreateSeqAIJWithArrays).
+#include "rawmat.h"
+
+#include "slgpu_adapter.h"
+
+#include <cstdint>
+#include <vector>
+
+rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr)
+{
+    mydofmanager = dofmngr;
+    mymeshnumber = universe::getrawmesh()->getmeshnumber();
+}
+
+rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr, Mat inA, Mat inD, indexmat inAinds, indexmat inDinds)
+{
+    mydofmanager = dofmngr;
+    Amat = inA;
+    Dmat = inD;
+    Ainds = inAinds;
+    Dinds = inDinds;
+    mymeshnumber = universe::getrawmesh()->getmeshnumber();
+}
+
+rawmat::~rawmat(void)
+{
+    slgpu_adapter::release_matrix(this);
+    // PETSc objects may only be destroyed before PetscFinalize.
+    PetscBool ispetscinitialized;
+    PetscInitialized(&ispetscinitialized);
+    if (ispetscinitialized == PETSC_TRUE) {
+        if (Amat != PETSC_NULLPTR)
+            MatDestroy(&Amat);
+        if (Dmat != PETSC_NULLPTR)
+            MatDestroy(&Dmat);
+        if (isitfactored)
+            KSPDestroy(&myksp);
+    }
+}
+
+long long int rawmat::countrows(void) { return mydofmanager == NULL ? 0 : mydofmanager->countdofs(); }
+
+long long int rawmat::countcolumns(void) { return mydofmanager == NULL ? 0 : mydofmanager->countdofs(); }
+
+void rawmat::accumulate(indexmat rowadresses, indexmat coladresses, densemat vals)
+{
+    // Host fragments (ports, mat(...) constructors) are kept as in the
+    // reference and shipped to the device when the matrix is processed.
+    if (vals.count() > 0) {
+        accumulatedrowindices.push_back(rowadresses);
+        accumulatedcolindices.push_back(coladresses);
+        accumulatedvals.push_back(vals);
+    }
+}
+
+void rawmat::process(std::vector<bool>& isconstrained)
+{
+    const long long ndofs = countrows();
+
+    std::vector<int> renumtolocalindex;
+    gentools::findtruefalse(isconstrained, Dinds, Ainds, renumtolocalindex);
+
+    slgpu_ctx* ctx = slgpu_adapter::context();
+    int handle = slgpu_adapter::matrix_handle(this, ndofs);
+    for (size_t i = 0; i < accumulatedvals.size(); i++) {
+        slgpu_adapter::check(slgpu_matrix_add_fragment(ctx, handle, accumulatedrowindices[i].countrows(),
+                                                       accumulatedcolindices[i].countrows(), accumulatedvals[i].countrows(),
+                                                       accumulatedvals[i].countcolumns(), accumulatedrowindices[i].getvalues(),
+                                                       accumulatedcolindices[i].getvalues(), accumulatedvals[i].getvalues()),
+                             "slgpu_matrix_add_fragment");
+    }
+    std::vector<uint8_t> constr((size_t)ndofs);
+    for (long long i = 0; i < ndofs; i++) constr[i] = isconstrained[i] ? 1 : 0;
+
+    slgpu_csr_info info{};
+    slgpu_adapter::set_last_processed(this);
+    slgpu_adapter::check(slgpu_matrix_process(ctx, handle, constr.data(), slgpu_adapter::precision(), &info), "slgpu_matrix_process");
+    nnzA = info.nnzA;
+    nnzD = info.nnzD;
+
+    Arows = indexmat(Ainds.count() + 1, 1);
+    Acols = indexmat(nnzA, 1);
+    Avals = densemat(nnzA, 1);
+    Drows = indexmat(Ainds.count() + 1, 1);
+    Dcols = indexmat(nnzD, 1);
+    Dvals = densemat(nnzD, 1);
+    slgpu_adapter::check(slgpu_matrix_download(ctx, handle, Arows.getvalues(), Acols.getvalues(), Avals.getvalues(), Drows.getvalues(),
+                                               Dcols.getvalues(), Dvals.getvalues()),
+                         "slgpu_matrix_download");
+
+    MatCreateSeqAIJWithArrays(PETSC_COMM_SELF, Ainds.count(), Ainds.count(), Arows.getvalues(), Acols.getvalues(), Avals.getvalues(), &Amat);
+    MatAssemblyBegin(Amat, MAT_FINAL_ASSEMBLY);
+    MatAssemblyEnd(Amat, MAT_FINAL_ASSEMBLY);
+
+    MatCreateSeqAIJWithArrays(PETSC_COMM_SELF, Ainds.count(), Dinds.count(), Drows.getvalues(), Dcols.getvalues(), Dvals.getvalues(), &Dmat);
+    MatAssemblyBegin(Dmat, MAT_FINAL_ASSEMBLY);
+    MatAssemblyEnd(Dmat, MAT_FINAL_ASSEMBLY);
+}
+
+void rawmat::clearfragments(void)
+{
+    accumulatedrowindices = {};
+    accumulatedcolindices = {};
+    accumulatedvals = {};
+    slgpu_adapter::release_matrix(this);
+}
+
+void rawmat::print(void)
+{
+    std::cout << std::endl;
+    if (mydofmanager == NULL)
+        std::cout << "Undefined matrix" << std::endl;
+    else if (countrows() > 0) {
+        std::cout << "A block " << Ainds.count() << "x" << Ainds.count() << ":" << std::endl << std::endl;
+        MatView(Amat, PETSC_VIEWER_STDOUT_SELF);
+        std::cout << std::endl << "D block " << Ainds.count() << "x" << Dinds.count() << ":" << std::endl << std::endl;
+        MatView(Dmat, PETSC_VIEWER_STDOUT_SELF);
+    } else
+        std::cout << "Empty matrix" << std::endl;
+    std::cout << std::endl;
+}
+
+std::shared_ptr<rawmat> rawmat::extractaccumulated(void)
+{
+    std::shared_ptr<rawmat> output(new rawmat(mydofmanager));
+    output->accumulatedrowindices = accumulatedrowindices;
+    output->accumulatedcolindices = accumulatedcolindices;
+    output->accumulatedvals = accumulatedvals;
+    slgpu_adapter::share_matrix(this, output.get());
+    return output;
+}
+
+indexmat rawmat::getainds(void) { return Ainds; }
+indexmat rawmat::getdinds(void) { return Dinds; }
+Mat rawmat::getapetsc(void) { return Amat; }
+Mat rawmat::getdpetsc(void) { return Dmat; }
+std::shared_ptr<dofmanager> rawmat::getdofmanager(void) { return mydofmanager; }
+KSP* rawmat::getksp(void) { return &myksp; }

@@ -1,0 +1,1375 @@
+// slgpu assembly engine: C ABI implementation, coefficient-program compiler,
+// geometry/coefficient kernel, FP64 contraction kernel and the COO -> CSR
+// builder.  Written for sm_100a (B200); one context per device.
+//
+// Data flow of slgpu_matrix_process (one call = one sparselizard rawmat::process):
+//   1. geometry+coefficients  (per group, thread per (element, Gauss point)):
+//        J, detJ, invJ from the curved nodes and Lagrange derivative tables,
+//        then the group's coefficient program; writes
+//        C[(term, gp)][elem] = coef * scale * w_gp * |detJ|
+//   2. contraction (per group, 64x64 output tiles of (tf*ndof+dof) x elements):
+//        V[p][e] = sum_{term, gp} T_term[i][gp] * D_term[j][gp] * C[(term,gp)][e]
+//      which is contribution.cpp's M = tf (.) dof, K = M * coef^T (:187, :210)
+//      without materialising M.
+//   3. pattern (cached): COO keys (row, col) of every (group, destination, p, e)
+//      and raw fragment, stable radix sort, run detection, A/D split with local
+//      renumbering -> CSR structure plus a sorted-position -> COO map.
+//   4. values: one thread per CSR entry sums its COO contributions in sorted
+//      order (stable sort => insertion order within a (row, col)), so the
+//      result is deterministic; no floating-point atomics.
+#include "engine_internal.h"
+#include "engine_kernels.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+namespace slgpu {
+
+static const char* kNoDevice = "record-only context: nothing is executed";
+
+struct SlgpuException : std::exception {
+    Error e;
+    SlgpuException(int code, std::string msg) : e{code, std::move(msg)} {}
+    const char* what() const noexcept override { return e.msg.c_str(); }
+};
+
+[[noreturn]] static void fail(int code, const std::string& msg) { throw SlgpuException(code, msg); }
+
+static void cuda_check(cudaError_t err, const char* what)
+{
+    if (err != cudaSuccess)
+        fail(SLGPU_E_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+DevBuf& DevBuf::operator=(DevBuf&& o) noexcept
+{
+    if (this != &o) {
+        release();
+        ctx_ = o.ctx_;
+        p_ = o.p_;
+        n_ = o.n_;
+        o.ctx_ = nullptr;
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    return *this;
+}
+
+void DevBuf::alloc(Ctx* ctx, size_t bytes)
+{
+    release();
+    if (bytes == 0)
+        bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    if ((size_t)ctx->in_use + bytes > ctx->budget)
+        fail(SLGPU_E_BUDGET, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget (" +
+                                 std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget) + " in use)");
+    cudaError_t err = cudaMallocAsync(&p_, bytes, ctx->stream);
+    if (err != cudaSuccess) {
+        p_ = nullptr;
+        fail(SLGPU_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(err));
+    }
+    ctx_ = ctx;
+    n_ = bytes;
+    ctx->in_use += (int64_t)bytes;
+}
+
+void DevBuf::release()
+{
+    if (p_ != nullptr && ctx_ != nullptr) {
+        cudaFreeAsync(p_, ctx_->stream);
+        ctx_->in_use -= (int64_t)n_;
+    }
+    p_ = nullptr;
+    n_ = 0;
+    ctx_ = nullptr;
+}
+
+template <class T>
+static void upload(Ctx* ctx, DevBuf& buf, const T* src, size_t count)
+{
+    buf.alloc(ctx, count * sizeof(T));
+    if (count > 0)
+        cuda_check(cudaMemcpyAsync(buf.as<void>(), src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream),
+                   "cudaMemcpyAsync H2D");
+}
+
+template <class T>
+static void upload(Ctx* ctx, DevBuf& buf, const std::vector<T>& v)
+{
+    upload(ctx, buf, v.data(), v.size());
+}
+
+static unsigned grid_for(int64_t n, int block) { return (unsigned)std::max<int64_t>(1, (n + block - 1) / block); }
+
+// ------------------------------------------------------------ program compiler
+// Turns the node DAG into straight-line code over kMaxSlots registers: each
+// node gets a free slot, operand slots are freed after their last use, and a
+// STORE is emitted right after a node that is some term's coefficient.
+static std::vector<Instr> compile_program(const slgpu_group& g, int nterms)
+{
+    const int n = g.nnodes;
+    std::vector<int> last_use(n, -1);
+    std::vector<char> needed(n, 0);
+    for (int t = 0; t < nterms; t++) {
+        int c = g.terms[t].coef_node;
+        if (c < 0 || c >= n)
+            fail(SLGPU_E_ARG, "term coefficient node out of range");
+        needed[c] = 1;
+    }
+    auto is_binary = [](int op) { return op == SLGPU_OP_ADD || op == SLGPU_OP_MUL || op == SLGPU_OP_POW; };
+    auto is_unary = [](int op) { return op == SLGPU_OP_INV || op == SLGPU_OP_NEG; };
+    for (int k = n - 1; k >= 0; k--) {
+        if (!needed[k])
+            continue;
+        const slgpu_node& nd = g.nodes[k];
+        if (is_binary(nd.op) || is_unary(nd.op)) {
+            int ops[2] = {nd.a, is_binary(nd.op) ? nd.b : -1};
+            for (int o : ops) {
+                if (o < 0)
+                    continue;
+                if (o >= k)
+                    fail(SLGPU_E_ARG, "coefficient program operand must precede its node");
+                needed[o] = 1;
+                last_use[o] = std::max(last_use[o], k);
+            }
+        }
+    }
+    std::vector<Instr> prog;
+    std::vector<int> slot_of(n, -1);
+    std::vector<int> free_slots;
+    for (int s = kMaxSlots - 1; s >= 0; s--) free_slots.push_back(s);
+    for (int k = 0; k < n; k++) {
+        if (!needed[k])
+            continue;
+        const slgpu_node& nd = g.nodes[k];
+        Instr in{nd.op, -1, nd.a, nd.b};
+        switch (nd.op) {
+        case SLGPU_OP_CONST:
+            if (nd.a < 0 || nd.a >= g.nconsts) fail(SLGPU_E_ARG, "constant index out of range");
+            break;
+        case SLGPU_OP_JAC:
+        case SLGPU_OP_INVJAC:
+            if (nd.a < 0 || nd.a >= g.problemdim || nd.b < 0 || nd.b >= g.problemdim)
+                fail(SLGPU_E_ARG, "Jacobian entry out of range");
+            break;
+        case SLGPU_OP_DETJAC:
+            break;
+        case SLGPU_OP_ELEM:
+            if (nd.a < 0 || nd.a >= g.nelemdata) fail(SLGPU_E_ARG, "element data index out of range");
+            break;
+        case SLGPU_OP_FIELD:
+            if (nd.a < 0 || nd.a >= g.nfielddata || nd.b < 0 || nd.b >= g.ntables)
+                fail(SLGPU_E_ARG, "field data / table index out of range");
+            if (g.tables[nd.b].rows != g.fieldrows[nd.a])
+                fail(SLGPU_E_ARG, "field coefficient rows do not match its table");
+            break;
+        case SLGPU_OP_COORD:
+            if (nd.a < 0 || nd.a > 2) fail(SLGPU_E_ARG, "coordinate index out of range");
+            break;
+        case SLGPU_OP_ADD:
+        case SLGPU_OP_MUL:
+        case SLGPU_OP_POW:
+            in.a = slot_of[nd.a];
+            in.b = slot_of[nd.b];
+            break;
+        case SLGPU_OP_INV:
+        case SLGPU_OP_NEG:
+            in.a = slot_of[nd.a];
+            break;
+        default:
+            fail(SLGPU_E_UNSUPPORTED, "unknown coefficient program op " + std::to_string(nd.op));
+        }
+        // Free operand slots whose last use is this node (before taking the
+        // destination so that an operand slot can be reused in place).
+        if (is_binary(nd.op) || is_unary(nd.op)) {
+            int ops[2] = {nd.a, is_binary(nd.op) ? nd.b : -1};
+            for (int i = 0; i < 2; i++) {
+                int o = ops[i];
+                if (o < 0 || last_use[o] != k || slot_of[o] < 0)
+                    continue;
+                if (i == 1 && ops[0] == o)
+                    continue;
+                free_slots.push_back(slot_of[o]);
+                slot_of[o] = -2;
+            }
+        }
+        if (free_slots.empty())
+            fail(SLGPU_E_UNSUPPORTED, "coefficient program needs more than " + std::to_string(kMaxSlots) + " live values");
+        in.dst = free_slots.back();
+        free_slots.pop_back();
+        slot_of[k] = in.dst;
+        prog.push_back(in);
+        for (int t = 0; t < nterms; t++)
+            if (g.terms[t].coef_node == k)
+                prog.push_back(Instr{INSTR_STORE, -1, in.dst, t});
+        if (last_use[k] < 0) {  // only stored
+            free_slots.push_back(in.dst);
+            slot_of[k] = -2;
+        }
+    }
+    return prog;
+}
+
+// ------------------------------------------------------------ hashing
+static void hash_device(Ctx* ctx, const int32_t* data, int64_t n, uint64_t salt, uint64_t out[2])
+{
+    if (ctx->hash_acc.empty())
+        ctx->hash_acc.alloc(ctx, 2 * sizeof(unsigned long long));
+    cuda_check(cudaMemsetAsync(ctx->hash_acc.as<void>(), 0, 2 * sizeof(unsigned long long), ctx->stream), "memset");
+    if (n > 0) {
+        unsigned blocks = (unsigned)std::min<int64_t>(148 * 8, grid_for(n, 256));
+        k_hash_i32<<<blocks, 256, 0, ctx->stream>>>(data, n, salt, ctx->hash_acc.as<unsigned long long>());
+        cuda_check(cudaGetLastError(), "k_hash_i32");
+    }
+    unsigned long long h[2];
+    cuda_check(cudaMemcpyAsync(h, ctx->hash_acc.as<void>(), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "D2H hash");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync hash");
+    out[0] = h[0];
+    out[1] = h[1];
+}
+
+static inline uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// ------------------------------------------------------------ group upload
+struct GroupDev::Record {
+    std::vector<int32_t> elems, orient, fieldrows;
+    std::vector<double> weights, lagrange, consts;
+    std::vector<std::vector<double>> tables, elemdata, fielddata;
+    std::vector<slgpu_table> tabdesc;
+    std::vector<slgpu_node> nodes;
+    std::vector<const double*> elemdata_ptr, fielddata_ptr;
+    std::vector<slgpu_term> terms;
+    std::vector<std::vector<int32_t>> tfaddr, dofaddr;
+    std::vector<slgpu_dest> dests;
+    slgpu_group desc{};
+};
+
+static void validate_group(const slgpu_group& g)
+{
+    if (g.nelem < 0 || g.ngp <= 0 || g.ntf <= 0 || g.ndof <= 0 || g.nterms <= 0 || g.ndests <= 0 || g.norient <= 0)
+        fail(SLGPU_E_ARG, "group sizes must be positive");
+    if (g.elemdim != g.problemdim)
+        fail(SLGPU_E_UNSUPPORTED, "only elements of the mesh dimension are supported (element dim " +
+                                      std::to_string(g.elemdim) + ", mesh dim " + std::to_string(g.problemdim) + ")");
+    if (g.problemdim < 1 || g.problemdim > 3)
+        fail(SLGPU_E_ARG, "problem dimension must be 1..3");
+    if (g.ncurvednodes <= 0 || g.ncurvednodes > 64)
+        fail(SLGPU_E_UNSUPPORTED, "curved node count out of range");
+    for (int t = 0; t < g.nterms; t++) {
+        const slgpu_term& tm = g.terms[t];
+        if (tm.tf_table < 0 || tm.tf_table >= g.ntables || g.tables[tm.tf_table].rows != g.ntf)
+            fail(SLGPU_E_ARG, "term tf table invalid or its rows differ from ntf");
+        bool rhs_term = tm.dof_table < 0;
+        if (rhs_term != (g.ndof == 1 && g.terms[0].dof_table < 0))
+            fail(SLGPU_E_ARG, "a group mixes right-hand-side and matrix terms");
+        if (!rhs_term && (tm.dof_table >= g.ntables || g.tables[tm.dof_table].rows != g.ndof))
+            fail(SLGPU_E_ARG, "term dof table invalid or its rows differ from ndof");
+    }
+    for (int d = 0; d < g.ndests; d++) {
+        if (g.dests[d].tfaddr == nullptr)
+            fail(SLGPU_E_ARG, "destination without test-function addresses");
+        if (g.terms[0].dof_table >= 0 && g.dests[d].dofaddr == nullptr)
+            fail(SLGPU_E_ARG, "matrix destination without dof addresses");
+    }
+    if ((int64_t)g.ntf * g.ndof * std::max<int64_t>(g.nelem, 1) >= (int64_t(1) << 40))
+        fail(SLGPU_E_UNSUPPORTED, "group too large");
+}
+
+static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
+{
+    validate_group(g);
+    auto gd = std::make_shared<GroupDev>();
+    gd->mesh = g.mesh;
+    gd->elemtype = g.elemtype;
+    gd->elemdim = g.elemdim;
+    gd->problemdim = g.problemdim;
+    gd->nelem = g.nelem;
+    gd->norient = g.norient;
+    gd->ngp = g.ngp;
+    gd->ncn = g.ncurvednodes;
+    gd->ntf = g.ntf;
+    gd->ndof = g.ndof;
+    gd->nterms = g.nterms;
+    gd->ndests = g.ndests;
+    gd->rhs = g.terms[0].dof_table < 0;
+    gd->prog = compile_program(g, g.nterms);
+    int64_t off = 0;
+    for (int k = 0; k < g.ntables; k++) {
+        gd->tab_off.push_back(off);
+        gd->tab_rows.push_back(g.tables[k].rows);
+        off += (int64_t)g.norient * g.tables[k].rows * g.ngp;
+    }
+    const int64_t tables_total = off;
+    for (int k = 0; k < g.nelemdata; k++) gd->elemdata_off.push_back((int64_t)k * g.nelem);
+    off = 0;
+    for (int k = 0; k < g.nfielddata; k++) {
+        gd->field_off.push_back(off);
+        gd->field_rows.push_back(g.fieldrows[k]);
+        off += (int64_t)g.fieldrows[k] * g.nelem;
+    }
+    const int64_t field_total = off;
+    for (int t = 0; t < g.nterms; t++) {
+        gd->term_scale.push_back(g.terms[t].scale);
+        gd->term_tf.push_back(g.terms[t].tf_table);
+        gd->term_dof.push_back(g.terms[t].dof_table);
+    }
+    for (int d = 0; d < g.ndests; d++) gd->dest_mult.push_back(g.dests[d].multiplier);
+    // Orientation-uniform tiles of at most kTileE elements.
+    for (int64_t e = 0; e < g.nelem;) {
+        int o = g.orient[e];
+        if (o < 0 || o >= g.norient)
+            fail(SLGPU_E_ARG, "orientation index out of range");
+        int64_t e1 = e;
+        while (e1 < g.nelem && g.orient[e1] == o && e1 - e < kTileE) e1++;
+        gd->tiles.push_back(Tile{(int32_t)e, (int32_t)(e1 - e), o, 0});
+        e = e1;
+    }
+    if (g.nelem >= (int64_t(1) << 31))
+        fail(SLGPU_E_UNSUPPORTED, "more than 2^31 elements in a group");
+
+    if (ctx->record_only) {
+        auto r = std::make_shared<GroupDev::Record>();
+        r->elems.assign(g.elems, g.elems + g.nelem);
+        r->orient.assign(g.orient, g.orient + g.nelem);
+        r->weights.assign(g.weights, g.weights + g.ngp);
+        r->lagrange.assign(g.lagrange, g.lagrange + (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp);
+        r->consts.assign(g.consts, g.consts + g.nconsts);
+        for (int k = 0; k < g.ntables; k++)
+            r->tables.emplace_back(g.tables[k].vals, g.tables[k].vals + (size_t)g.norient * g.tables[k].rows * g.ngp);
+        for (int k = 0; k < g.ntables; k++) r->tabdesc.push_back(slgpu_table{g.tables[k].rows, r->tables[k].data()});
+        r->nodes.assign(g.nodes, g.nodes + g.nnodes);
+        for (int k = 0; k < g.nelemdata; k++) r->elemdata.emplace_back(g.elemdata[k], g.elemdata[k] + g.nelem);
+        for (int k = 0; k < g.nfielddata; k++)
+            r->fielddata.emplace_back(g.fielddata[k], g.fielddata[k] + (size_t)g.fieldrows[k] * g.nelem);
+        for (auto& v : r->elemdata) r->elemdata_ptr.push_back(v.data());
+        for (auto& v : r->fielddata) r->fielddata_ptr.push_back(v.data());
+        r->fieldrows.assign(g.fieldrows, g.fieldrows + g.nfielddata);
+        r->terms.assign(g.terms, g.terms + g.nterms);
+        for (int d = 0; d < g.ndests; d++) {
+            r->tfaddr.emplace_back(g.dests[d].tfaddr, g.dests[d].tfaddr + (size_t)g.ntf * g.nelem);
+            if (!gd->rhs)
+                r->dofaddr.emplace_back(g.dests[d].dofaddr, g.dests[d].dofaddr + (size_t)g.ndof * g.nelem);
+            else
+                r->dofaddr.emplace_back();
+        }
+        for (int d = 0; d < g.ndests; d++)
+            r->dests.push_back(slgpu_dest{r->tfaddr[d].data(), gd->rhs ? nullptr : r->dofaddr[d].data(), g.dests[d].multiplier});
+        r->desc = g;
+        r->desc.elems = r->elems.data();
+        r->desc.orient = r->orient.data();
+        r->desc.weights = r->weights.data();
+        r->desc.lagrange = r->lagrange.data();
+        r->desc.tables = r->tabdesc.data();
+        r->desc.nodes = r->nodes.data();
+        r->desc.consts = r->consts.data();
+        r->desc.elemdata = r->elemdata_ptr.data();
+        r->desc.fielddata = r->fielddata_ptr.data();
+        r->desc.fieldrows = r->fieldrows.data();
+        r->desc.terms = r->terms.data();
+        r->desc.dests = r->dests.data();
+        gd->rec = r;
+        return gd;
+    }
+
+    auto mit = ctx->meshes.find(g.mesh);
+    if (mit == ctx->meshes.end() || mit->second.types.count(g.elemtype) == 0)
+        fail(SLGPU_E_STATE, "mesh geometry for this element type was not uploaded");
+    const MeshDev::Type& mt = mit->second.types.at(g.elemtype);
+    if (mt.ncn != g.ncurvednodes)
+        fail(SLGPU_E_ARG, "curved node count differs from the uploaded mesh");
+    for (int64_t e = 0; e < g.nelem; e++)
+        if (g.elems[e] < 0 || g.elems[e] >= mt.nelem)
+            fail(SLGPU_E_ARG, "element number out of range of the uploaded mesh");
+
+    upload(ctx, gd->elems, g.elems, (size_t)g.nelem);
+    upload(ctx, gd->orient, g.orient, (size_t)g.nelem);
+    upload(ctx, gd->weights, g.weights, (size_t)g.ngp);
+    upload(ctx, gd->lagrange, g.lagrange, (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp);
+    gd->tables.alloc(ctx, (size_t)tables_total * sizeof(double));
+    for (int k = 0; k < g.ntables; k++)
+        cuda_check(cudaMemcpyAsync(gd->tables.as<double>() + gd->tab_off[k], g.tables[k].vals,
+                                   (size_t)g.norient * g.tables[k].rows * g.ngp * sizeof(double), cudaMemcpyHostToDevice,
+                                   ctx->stream),
+                   "upload tables");
+    upload(ctx, gd->consts, g.consts, (size_t)g.nconsts);
+    upload(ctx, gd->prog_d, gd->prog);
+    gd->elemdata.alloc(ctx, (size_t)g.nelemdata * g.nelem * sizeof(double));
+    for (int k = 0; k < g.nelemdata; k++)
+        cuda_check(cudaMemcpyAsync(gd->elemdata.as<double>() + gd->elemdata_off[k], g.elemdata[k],
+                                   (size_t)g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                   "upload elemdata");
+    gd->fielddata.alloc(ctx, (size_t)field_total * sizeof(double));
+    for (int k = 0; k < g.nfielddata; k++)
+        cuda_check(cudaMemcpyAsync(gd->fielddata.as<double>() + gd->field_off[k], g.fielddata[k],
+                                   (size_t)g.fieldrows[k] * g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                   "upload fielddata");
+    upload(ctx, gd->field_off_d, gd->field_off);
+    upload(ctx, gd->field_rows_d, gd->field_rows);
+    upload(ctx, gd->tab_off_d, gd->tab_off);
+    upload(ctx, gd->tab_rows_d, gd->tab_rows);
+    upload(ctx, gd->term_scale_d, gd->term_scale);
+    upload(ctx, gd->term_tf_d, gd->term_tf);
+    upload(ctx, gd->term_dof_d, gd->term_dof);
+    upload(ctx, gd->tiles_d, gd->tiles);
+    gd->tfaddr.resize(g.ndests);
+    gd->dofaddr.resize(g.ndests);
+    uint64_t h0 = 0, h1 = 0;
+    for (int d = 0; d < g.ndests; d++) {
+        upload(ctx, gd->tfaddr[d], g.dests[d].tfaddr, (size_t)g.ntf * g.nelem);
+        uint64_t h[2];
+        hash_device(ctx, gd->tfaddr[d].as<int32_t>(), (int64_t)g.ntf * g.nelem, 2 * d + 1, h);
+        h0 = mix64(h0 ^ h[0]);
+        h1 = mix64(h1 ^ h[1]);
+        if (!gd->rhs) {
+            upload(ctx, gd->dofaddr[d], g.dests[d].dofaddr, (size_t)g.ndof * g.nelem);
+            hash_device(ctx, gd->dofaddr[d].as<int32_t>(), (int64_t)g.ndof * g.nelem, 2 * d + 2, h);
+            h0 = mix64(h0 ^ h[0]);
+            h1 = mix64(h1 ^ h[1]);
+        }
+    }
+    gd->addr_hash[0] = mix64(h0 ^ (uint64_t)g.ntf << 40 ^ (uint64_t)g.ndof << 20 ^ (uint64_t)g.nelem);
+    gd->addr_hash[1] = mix64(h1 ^ (uint64_t)g.ndests << 32 ^ (uint64_t)gd->rhs);
+    return gd;
+}
+
+// ------------------------------------------------------------ launches
+static CoefParams coef_params(Ctx* ctx, const GroupDev& g, double* C)
+{
+    const MeshDev& m = ctx->meshes.at(g.mesh);
+    const MeshDev::Type& t = m.types.at(g.elemtype);
+    CoefParams p{};
+    p.xyz = m.xyz.as<double>();
+    p.conn = t.conn.as<int32_t>();
+    p.ncn = g.ncn;
+    p.elems = g.elems.as<int32_t>();
+    p.orient = g.orient.as<int32_t>();
+    p.nelem = g.nelem;
+    p.ngp = g.ngp;
+    p.weights = g.weights.as<double>();
+    p.lagrange = g.lagrange.as<double>();
+    p.dim = g.problemdim;
+    p.prog = g.prog_d.as<Instr>();
+    p.nprog = (int)g.prog.size();
+    p.consts = g.consts.as<double>();
+    p.tables = g.tables.as<double>();
+    p.tab_off = g.tab_off_d.as<int64_t>();
+    p.tab_rows = g.tab_rows_d.as<int32_t>();
+    p.elemdata = g.elemdata.as<double>();
+    p.fielddata = g.fielddata.as<double>();
+    p.field_off = g.field_off_d.as<int64_t>();
+    p.term_scale = g.term_scale_d.as<double>();
+    p.nterms = g.nterms;
+    p.C = C;
+    return p;
+}
+
+// Segments of the COO space: (group, destination) blocks then raw fragments.
+static std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals)
+{
+    std::vector<Segment> segs;
+    int64_t coo = 0, vb = 0;
+    group_val_base->clear();
+    for (auto& g : M.groups) {
+        const int64_t P = (int64_t)g->ntf * g->ndof;
+        group_val_base->push_back(vb);
+        for (int d = 0; d < g->ndests; d++) {
+            segs.push_back(Segment{coo, P * g->nelem, vb, g->dest_mult[d]});
+            coo += P * g->nelem;
+        }
+        vb += P * g->nelem;
+    }
+    for (auto& f : M.frags) {
+        const int64_t n = (int64_t)f->nr * f->nc;
+        segs.push_back(Segment{coo, n, vb, 1.0});
+        coo += n;
+        vb += n;
+    }
+    *total_vals = vb;
+    return segs;
+}
+
+static void ev_record(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->ev[i], ctx->stream), "cudaEventRecord"); }
+
+static float ev_ms(Ctx* ctx, int a, int b)
+{
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+    return ms;
+}
+
+static int bits_for(int64_t n)
+{
+    int b = 1;
+    while ((int64_t(1) << b) <= n) b++;
+    return b;
+}
+
+// Builds (or fetches) the pattern for matrix M with the given constraints.
+static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vector<Segment>& segs, const uint8_t* dconstr,
+                                            bool rhs, uint64_t key0, uint64_t key1, bool* reused)
+{
+    for (auto& p : ctx->patterns) {
+        if (p->key[0] == key0 && p->key[1] == key1 && p->ndofs == M.ndofs) {
+            p->last_use = ++ctx->use_clock;
+            *reused = true;
+            return p;
+        }
+    }
+    *reused = false;
+    auto P = std::make_shared<Pattern>();
+    P->key[0] = key0;
+    P->key[1] = key1;
+    P->ndofs = M.ndofs;
+    int64_t ncoo = segs.empty() ? 0 : segs.back().coo_base + segs.back().count;
+    P->ncoo = ncoo;
+    if (ncoo >= (int64_t)0xFFFFFFFFll)
+        fail(SLGPU_E_UNSUPPORTED, "more than 2^32-1 COO entries in one matrix");
+    const int rowbits = bits_for(M.ndofs);
+    const int colbits = rhs ? 0 : bits_for(M.ndofs);
+    if (rowbits + colbits > 64)
+        fail(SLGPU_E_UNSUPPORTED, "too many DOFs for 64-bit keys");
+    const uint64_t invalid = (rowbits + colbits == 64) ? ~0ull : ((1ull << (rowbits + colbits)) - 1);
+
+    DevBuf keys, keys_alt, idx, idx_alt, counter;
+    keys.alloc(ctx, std::max<int64_t>(ncoo, 1) * 8);
+    keys_alt.alloc(ctx, std::max<int64_t>(ncoo, 1) * 8);
+    idx.alloc(ctx, std::max<int64_t>(ncoo, 1) * 4);
+    idx_alt.alloc(ctx, std::max<int64_t>(ncoo, 1) * 4);
+    counter.alloc(ctx, 16);
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+
+    // Keys in COO order.
+    int si = 0;
+    for (auto& g : M.groups) {
+        for (int d = 0; d < g->ndests; d++, si++) {
+            KeyParams kp{};
+            kp.tfaddr = g->tfaddr[d].as<int32_t>();
+            kp.dofaddr = rhs ? nullptr : g->dofaddr[d].as<int32_t>();
+            kp.ndof = g->ndof;
+            kp.nelem = g->nelem;
+            kp.count = segs[si].count;
+            kp.coo_base = segs[si].coo_base;
+            kp.colbits = colbits;
+            kp.constrained = rhs ? nullptr : dconstr;
+            kp.invalid = invalid;
+            kp.keys = keys.as<unsigned long long>();
+            kp.idx = idx.as<uint32_t>();
+            kp.nvalid = counter.as<unsigned long long>();
+            k_group_keys<<<grid_for(kp.count, 256), 256, 0, ctx->stream>>>(kp);
+            cuda_check(cudaGetLastError(), "k_group_keys");
+        }
+    }
+    for (auto& f : M.frags) {
+        FragKeyParams fp{};
+        fp.rows = f->rows.as<int32_t>();
+        fp.cols = f->cols.as<int32_t>();
+        fp.ntr = f->ntr;
+        fp.ndr = f->ndr;
+        fp.nr = f->nr;
+        fp.nc = f->nc;
+        fp.coo_base = segs[si].coo_base;
+        fp.colbits = colbits;
+        fp.constrained = rhs ? nullptr : dconstr;
+        fp.invalid = invalid;
+        fp.keys = keys.as<unsigned long long>();
+        fp.idx = idx.as<uint32_t>();
+        fp.nvalid = counter.as<unsigned long long>();
+        fp.ndofs = M.ndofs;
+        k_frag_keys<<<grid_for((int64_t)f->nr * f->nc, 256), 256, 0, ctx->stream>>>(fp);
+        cuda_check(cudaGetLastError(), "k_frag_keys");
+        si++;
+    }
+
+    // Stable radix sort on the used key bits.
+    cub::DoubleBuffer<unsigned long long> dk(keys.as<unsigned long long>(), keys_alt.as<unsigned long long>());
+    cub::DoubleBuffer<uint32_t> dv(idx.as<uint32_t>(), idx_alt.as<uint32_t>());
+    size_t temp = 0;
+    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
+               "SortPairs size");
+    DevBuf tmp;
+    tmp.alloc(ctx, temp);
+    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
+               "SortPairs");
+    tmp.release();
+    unsigned long long counts_h[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H nvalid");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync nvalid");
+    if (counts_h[1] != 0)
+        fail(SLGPU_E_ARG, std::to_string(counts_h[1]) + " COO addresses are >= the DOF count");
+    const int64_t nvalid = (int64_t)counts_h[0];
+    P->nvalid = nvalid;
+    const unsigned long long* sk = dk.Current();
+    const uint32_t* sv = dv.Current();
+
+    // Run heads and run indices.
+    DevBuf head, runidx;
+    head.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
+    runidx.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
+    if (nvalid > 0) {
+        k_run_heads<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(sk, nvalid, head.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "k_run_heads");
+        temp = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid,
+                                                 ctx->stream),
+                   "scan size");
+        tmp.alloc(ctx, temp);
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, head.as<uint32_t>(), runidx.as<uint32_t>(),
+                                                 (int64_t)nvalid, ctx->stream),
+                   "scan");
+        tmp.release();
+    }
+    uint32_t last[2] = {0, 0};
+    if (nvalid > 0) {
+        cuda_check(cudaMemcpyAsync(&last[0], runidx.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&last[1], head.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    }
+    const int64_t nruns = nvalid > 0 ? (int64_t)last[0] + last[1] : 0;
+    P->nruns = nruns;
+    P->perm = std::move(idx.as<uint32_t>() == sv ? idx : idx_alt);
+    P->run_start.alloc(ctx, (nruns + 1) * 4);
+    if (nvalid > 0) {
+        k_run_starts<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid,
+                                                                     P->run_start.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "k_run_starts");
+    }
+    uint32_t nv32 = (uint32_t)nvalid;
+    cuda_check(cudaMemcpyAsync(P->run_start.as<uint32_t>() + nruns, &nv32, 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    head.release();
+    runidx.release();
+
+    // Local renumbering of constrained / unconstrained DOFs.
+    DevBuf renum, isA_dof;
+    renum.alloc(ctx, std::max<int64_t>(M.ndofs, 1) * 4);
+    int64_t nA = M.ndofs, nD = 0;
+    if (!rhs) {
+        DevBuf flagsA, scanA, flagsD, scanD;
+        flagsA.alloc(ctx, (M.ndofs + 1) * 4);
+        flagsD.alloc(ctx, (M.ndofs + 1) * 4);
+        scanA.alloc(ctx, (M.ndofs + 1) * 4);
+        scanD.alloc(ctx, (M.ndofs + 1) * 4);
+        k_constraint_flags<<<grid_for(M.ndofs + 1, 256), 256, 0, ctx->stream>>>(dconstr, M.ndofs, flagsA.as<uint32_t>(),
+                                                                                 flagsD.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "k_constraint_flags");
+        temp = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(), (int64_t)M.ndofs + 1,
+                                                 ctx->stream),
+                   "scan size");
+        tmp.alloc(ctx, temp);
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(),
+                                                 (int64_t)M.ndofs + 1, ctx->stream),
+                   "scan");
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsD.as<uint32_t>(), scanD.as<uint32_t>(),
+                                                 (int64_t)M.ndofs + 1, ctx->stream),
+                   "scan");
+        tmp.release();
+        uint32_t tot[2];
+        cuda_check(cudaMemcpyAsync(&tot[0], scanA.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&tot[1], scanD.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        k_renumber<<<grid_for(M.ndofs, 256), 256, 0, ctx->stream>>>(dconstr, M.ndofs, scanA.as<uint32_t>(), scanD.as<uint32_t>(),
+                                                                     renum.as<int32_t>());
+        cuda_check(cudaGetLastError(), "k_renumber");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+        nA = tot[0];
+        nD = tot[1];
+    }
+    P->nA = nA;
+    P->nD = nD;
+
+    // Classify runs into A / D, slots, row counts.
+    P->run_target.alloc(ctx, std::max<int64_t>(nruns, 1) * 4);
+    if (rhs) {
+        P->run_row.alloc(ctx, std::max<int64_t>(nruns, 1) * 4);
+        if (nruns > 0) {
+            k_rhs_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns,
+                                                                      P->run_row.as<int32_t>(), P->run_target.as<int32_t>());
+            cuda_check(cudaGetLastError(), "k_rhs_runs");
+        }
+        P->nnzA = nruns;
+    } else {
+        DevBuf isA, slotA, slotD, isD;
+        isA.alloc(ctx, (nruns + 1) * 4);
+        isD.alloc(ctx, (nruns + 1) * 4);
+        slotA.alloc(ctx, (nruns + 1) * 4);
+        slotD.alloc(ctx, (nruns + 1) * 4);
+        DevBuf rowcA, rowcD;
+        rowcA.alloc(ctx, (nA + 1) * 4);
+        rowcD.alloc(ctx, (nA + 1) * 4);
+        cuda_check(cudaMemsetAsync(rowcA.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
+        cuda_check(cudaMemsetAsync(rowcD.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
+        k_classify_runs<<<grid_for(nruns + 1, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns, colbits, dconstr,
+                                                                            renum.as<int32_t>(), isA.as<uint32_t>(), isD.as<uint32_t>(),
+                                                                            rowcA.as<uint32_t>(), rowcD.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "k_classify_runs");
+        temp = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1,
+                                                 ctx->stream),
+                   "scan size");
+        size_t temp2 = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp2, rowcA.as<uint32_t>(), rowcA.as<uint32_t>(), (int64_t)nA + 1,
+                                                 ctx->stream),
+                   "scan size");
+        temp = std::max(temp, temp2);
+        tmp.alloc(ctx, temp);
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1,
+                                                 ctx->stream),
+                   "scan");
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, isD.as<uint32_t>(), slotD.as<uint32_t>(), (int64_t)nruns + 1,
+                                                 ctx->stream),
+                   "scan");
+        P->Arows.alloc(ctx, (nA + 1) * 4);
+        P->Drows.alloc(ctx, (nA + 1) * 4);
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcA.as<uint32_t>(), P->Arows.as<uint32_t>(), (int64_t)nA + 1,
+                                                 ctx->stream),
+                   "scan");
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcD.as<uint32_t>(), P->Drows.as<uint32_t>(), (int64_t)nA + 1,
+                                                 ctx->stream),
+                   "scan");
+        tmp.release();
+        uint32_t tot[2];
+        cuda_check(cudaMemcpyAsync(&tot[0], slotA.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&tot[1], slotD.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+        P->nnzA = tot[0];
+        P->nnzD = tot[1];
+        if (P->nnzA >= (int64_t(1) << 31) || P->nnzD >= (int64_t(1) << 31))
+            fail(SLGPU_E_UNSUPPORTED, "more than 2^31-1 nonzeros in a CSR block (32-bit PETSc row pointers)");
+        P->Acols.alloc(ctx, std::max<int64_t>(P->nnzA, 1) * 4);
+        P->Dcols.alloc(ctx, std::max<int64_t>(P->nnzD, 1) * 4);
+        if (nruns > 0) {
+            k_fill_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns, colbits, isA.as<uint32_t>(),
+                                                                        slotA.as<uint32_t>(), slotD.as<uint32_t>(), renum.as<int32_t>(),
+                                                                        P->run_target.as<int32_t>(), P->Acols.as<int32_t>(),
+                                                                        P->Dcols.as<int32_t>());
+            cuda_check(cudaGetLastError(), "k_fill_runs");
+        }
+    }
+    keys.release();
+    keys_alt.release();
+    (P->perm.as<uint32_t>() == idx.as<uint32_t>() ? idx_alt : idx).release();
+    P->last_use = ++ctx->use_clock;
+    ctx->patterns.push_back(P);
+    // Keep at most 8 resident patterns (least recently used evicted).
+    while (ctx->patterns.size() > 8) {
+        auto it = std::min_element(ctx->patterns.begin(), ctx->patterns.end(),
+                                   [](const std::shared_ptr<Pattern>& a, const std::shared_ptr<Pattern>& b) { return a->last_use < b->last_use; });
+        ctx->patterns.erase(it);
+    }
+    return P;
+}
+
+static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
+{
+    if (ctx->record_only) {
+        if (isconstrained != nullptr)
+            M.rec_constrained.assign(isconstrained, isconstrained + M.ndofs);
+        fail(SLGPU_E_NODEVICE, kNoDevice);
+    }
+    if (precision != SLGPU_PREC_FP64)
+        fail(SLGPU_E_UNSUPPORTED, "only the FP64 contraction is available in this build");
+    if (M.ndofs <= 0 || M.ndofs >= (int64_t(1) << 31))
+        fail(SLGPU_E_ARG, "DOF count out of range");
+    ev_record(ctx, 0);
+    std::vector<int64_t> gvb;
+    int64_t total_vals = 0;
+    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
+
+    // Constraints on the device (reused buffer keyed by content).
+    DevBuf dconstr;
+    dconstr.alloc(ctx, (M.ndofs + 1));
+    if (!rhs)
+        cuda_check(cudaMemcpyAsync(dconstr.as<void>(), isconstrained, M.ndofs, cudaMemcpyHostToDevice, ctx->stream), "H2D constr");
+    uint64_t ckey[2] = {0, 0};
+    if (!rhs) {
+        // Hash constraints as 32-bit words.
+        std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
+        std::memcpy(packed.data(), isconstrained, M.ndofs);
+        uint64_t a = 0x12345, b = 0x6789;
+        for (size_t i = 0; i < packed.size(); i++) {
+            a = mix64(a ^ (uint64_t)(uint32_t)packed[i] ^ (uint64_t)i << 32);
+            b += mix64((uint64_t)(uint32_t)packed[i] * 0x100000001b3ull + i);
+        }
+        ckey[0] = a;
+        ckey[1] = b;
+    }
+    uint64_t key0 = mix64(ckey[0] ^ (uint64_t)M.ndofs ^ (rhs ? 0xABCDEFull : 0));
+    uint64_t key1 = mix64(ckey[1] ^ (uint64_t)segs.size());
+    for (auto& g : M.groups) {
+        key0 = mix64(key0 ^ g->addr_hash[0]);
+        key1 = mix64(key1 + g->addr_hash[1]);
+    }
+    for (auto& f : M.frags) {
+        key0 = mix64(key0 ^ f->addr_hash[0]);
+        key1 = mix64(key1 + f->addr_hash[1]);
+    }
+
+    // 1+2: geometry, coefficients and contraction into the value buffer.
+    if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
+        M.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
+    int64_t maxC = 0;
+    for (auto& g : M.groups) maxC = std::max<int64_t>(maxC, (int64_t)g->nterms * g->ngp * g->nelem);
+    DevBuf C;
+    C.alloc(ctx, std::max<int64_t>(maxC, 1) * 8);
+    size_t gi = 0;
+    float coef_ms = 0, contract_ms = 0;
+    for (auto& g : M.groups) {
+        if (g->nelem > 0) {
+            CoefParams cp = coef_params(ctx, *g, C.as<double>());
+            int64_t n = g->nelem * (int64_t)g->ngp;
+            ev_record(ctx, 4);
+            k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
+            cuda_check(cudaGetLastError(), "k_geometry_coef");
+            ev_record(ctx, 5);
+            ContractParams kp{};
+            kp.tables = g->tables.as<double>();
+            kp.tab_off = g->tab_off_d.as<int64_t>();
+            kp.term_tf = g->term_tf_d.as<int32_t>();
+            kp.term_dof = g->term_dof_d.as<int32_t>();
+            kp.nterms = g->nterms;
+            kp.ngp = g->ngp;
+            kp.ntf = g->ntf;
+            kp.ndof = g->ndof;
+            kp.nelem = g->nelem;
+            kp.C = C.as<double>();
+            kp.tiles = g->tiles_d.as<Tile>();
+            kp.out = M.vals.as<double>() + gvb[gi];
+            const int64_t P = (int64_t)g->ntf * g->ndof;
+            dim3 grid((unsigned)g->tiles.size(), (unsigned)((P + kTileP - 1) / kTileP));
+            if (grid.y > 65535)
+                fail(SLGPU_E_UNSUPPORTED, "element matrix too large for the contraction grid");
+            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
+            cuda_check(cudaGetLastError(), "k_contract_fp64");
+            ev_record(ctx, 1);
+            cuda_check(cudaEventSynchronize(ctx->ev[1]), "sync");
+            coef_ms += ev_ms(ctx, 4, 5);
+            contract_ms += ev_ms(ctx, 5, 1);
+        }
+        gi++;
+    }
+    C.release();
+    // Fragment values.
+    {
+        int64_t vb = 0;
+        for (auto& g : M.groups) vb += (int64_t)g->ntf * g->ndof * g->nelem;
+        for (auto& f : M.frags) {
+            int64_t n = (int64_t)f->nr * f->nc;
+            if (n > 0)
+                cuda_check(cudaMemcpyAsync(M.vals.as<double>() + vb, f->vals.as<double>(), n * 8, cudaMemcpyDeviceToDevice, ctx->stream),
+                           "D2D fragment values");
+            vb += n;
+        }
+    }
+    ev_record(ctx, 1);
+
+    // 3: pattern.
+    bool reused = false;
+    M.pattern = get_pattern(ctx, M, segs, dconstr.as<uint8_t>(), rhs, key0, key1, &reused);
+    Pattern& P = *M.pattern;
+    ev_record(ctx, 2);
+
+    // 4: values.
+    DevBuf dsegs;
+    upload(ctx, dsegs, segs);
+    if (rhs) {
+        M.Avals.alloc(ctx, (size_t)std::max<int64_t>(M.ndofs, 1) * 8);
+        cuda_check(cudaMemsetAsync(M.Avals.as<void>(), 0, (size_t)M.ndofs * 8, ctx->stream), "memset");
+    } else {
+        M.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
+        M.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
+    }
+    if (P.nruns > 0) {
+        ValueParams vp{};
+        vp.perm = P.perm.as<uint32_t>();
+        vp.run_start = P.run_start.as<uint32_t>();
+        vp.run_target = rhs ? P.run_row.as<int32_t>() : P.run_target.as<int32_t>();
+        vp.nruns = P.nruns;
+        vp.segs = dsegs.as<Segment>();
+        vp.nsegs = (int)segs.size();
+        vp.vals = M.vals.as<double>();
+        vp.Avals = M.Avals.as<double>();
+        vp.Dvals = rhs ? nullptr : M.Dvals.as<double>();
+        vp.negate = rhs ? 1 : 0;
+        k_csr_values<<<grid_for(P.nruns, 256), 256, 0, ctx->stream>>>(vp);
+        cuda_check(cudaGetLastError(), "k_csr_values");
+    }
+    ev_record(ctx, 3);
+    cuda_check(cudaEventSynchronize(ctx->ev[3]), "sync");
+    ctx->timings[0] = coef_ms;
+    ctx->timings[1] = contract_ms;
+    ctx->timings[2] = ev_ms(ctx, 1, 2);
+    ctx->timings[3] = ev_ms(ctx, 2, 3);
+    ctx->timings[4] = ev_ms(ctx, 0, 3);
+    if (info != nullptr) {
+        info->nA = P.nA;
+        info->nD = P.nD;
+        info->nnzA = P.nnzA;
+        info->nnzD = P.nnzD;
+        info->ncoo = P.ncoo;
+        info->pattern_reused = reused ? 1 : 0;
+    }
+    M.info.nA = P.nA;
+    M.info.nD = P.nD;
+    M.info.nnzA = P.nnzA;
+    M.info.nnzD = P.nnzD;
+    M.info.ncoo = P.ncoo;
+    M.info.pattern_reused = reused;
+}
+
+}  // namespace slgpu
+
+using namespace slgpu;
+
+struct slgpu_ctx : public slgpu::Ctx {};
+
+template <class F>
+static int guarded(slgpu_ctx* ctx, F&& f)
+{
+    if (ctx == nullptr)
+        return SLGPU_E_ARG;
+    try {
+        if (!ctx->record_only && ctx->device >= 0)
+            cudaSetDevice(ctx->device);
+        f();
+        return SLGPU_OK;
+    } catch (const SlgpuException& e) {
+        ctx->last_error = e.e.msg;
+        return e.e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->last_error = "host allocation failed";
+        return SLGPU_E_BUDGET;
+    } catch (const std::exception& e) {
+        ctx->last_error = e.what();
+        return SLGPU_E_ARG;
+    }
+}
+
+static Matrix& get_matrix(slgpu_ctx* ctx, int handle)
+{
+    auto it = ctx->matrices.find(handle);
+    if (it == ctx->matrices.end())
+        fail(SLGPU_E_ARG, "unknown matrix handle " + std::to_string(handle));
+    return *it->second;
+}
+
+extern "C" {
+
+int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** out)
+{
+    if (out == nullptr)
+        return SLGPU_E_ARG;
+    *out = nullptr;
+    auto* ctx = new slgpu_ctx();
+    ctx->budget = hbm_budget ? hbm_budget : (size_t)150 * 1000 * 1000 * 1000;
+    ctx->record_only = (flags & SLGPU_CTX_RECORD_ONLY) != 0;
+    if (!ctx->record_only) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+            cudaGetLastError();
+            delete ctx;
+            return SLGPU_E_NODEVICE;
+        }
+        ctx->device = device;
+        if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            delete ctx;
+            return SLGPU_E_CUDA;
+        }
+        for (auto& e : ctx->ev) cudaEventCreate(&e);
+        // Keep freed blocks in the stream-ordered pool between assemblies.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t threshold = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+    }
+    *out = ctx;
+    return SLGPU_OK;
+}
+
+void slgpu_ctx_destroy(slgpu_ctx* ctx)
+{
+    if (ctx == nullptr)
+        return;
+    if (!ctx->record_only)
+        cudaSetDevice(ctx->device);
+    ctx->matrices.clear();
+    ctx->patterns.clear();
+    ctx->meshes.clear();
+    ctx->scratch.release();
+    ctx->hash_acc.release();
+    if (!ctx->record_only) {
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& e : ctx->ev) cudaEventDestroy(e);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+int slgpu_last_error(const slgpu_ctx* ctx, char* buf, size_t len)
+{
+    if (ctx == nullptr || buf == nullptr || len == 0)
+        return SLGPU_E_ARG;
+    std::snprintf(buf, len, "%s", ctx->last_error.c_str());
+    return SLGPU_OK;
+}
+
+int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx) { return ctx ? ctx->in_use : 0; }
+
+int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double* xyz)
+{
+    return guarded(ctx, [&] {
+        if (nnodes < 0 || (nnodes > 0 && xyz == nullptr))
+            fail(SLGPU_E_ARG, "invalid node array");
+        MeshDev& m = ctx->meshes[mesh];
+        m.nnodes = nnodes;
+        if (!ctx->record_only)
+            upload(ctx, m.xyz, xyz, (size_t)3 * nnodes);
+        else
+            m.hxyz.assign(xyz, xyz + 3 * nnodes);
+    });
+}
+
+int slgpu_mesh_set_elements(slgpu_ctx* ctx, int mesh, int elemtype, int ncurvednodes, int64_t nelem, const int32_t* conn)
+{
+    return guarded(ctx, [&] {
+        if (nelem < 0 || ncurvednodes <= 0 || (nelem > 0 && conn == nullptr))
+            fail(SLGPU_E_ARG, "invalid connectivity");
+        MeshDev& m = ctx->meshes[mesh];
+        for (int64_t k = 0; k < nelem * ncurvednodes; k++)
+            if (conn[k] < 0 || conn[k] >= m.nnodes)
+                fail(SLGPU_E_ARG, "connectivity refers to a node outside the uploaded node array");
+        MeshDev::Type& t = m.types[elemtype];
+        t.ncn = ncurvednodes;
+        t.nelem = nelem;
+        if (!ctx->record_only)
+            upload(ctx, t.conn, conn, (size_t)nelem * ncurvednodes);
+        else
+            t.hconn.assign(conn, conn + nelem * ncurvednodes);
+    });
+}
+
+int slgpu_matrix_create(slgpu_ctx* ctx, int64_t ndofs, int* handle)
+{
+    return guarded(ctx, [&] {
+        if (handle == nullptr || ndofs < 0)
+            fail(SLGPU_E_ARG, "invalid matrix arguments");
+        auto m = std::make_unique<Matrix>();
+        m->ndofs = ndofs;
+        *handle = ctx->next_handle++;
+        ctx->matrices[*handle] = std::move(m);
+    });
+}
+
+int slgpu_matrix_destroy(slgpu_ctx* ctx, int handle)
+{
+    return guarded(ctx, [&] {
+        get_matrix(ctx, handle);
+        ctx->matrices.erase(handle);
+    });
+}
+
+int slgpu_matrix_clone(slgpu_ctx* ctx, int handle, int* new_handle)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (new_handle == nullptr)
+            fail(SLGPU_E_ARG, "null handle pointer");
+        auto m = std::make_unique<Matrix>();
+        m->ndofs = M.ndofs;
+        m->groups = M.groups;
+        m->frags = M.frags;
+        m->rec_constrained = M.rec_constrained;
+        *new_handle = ctx->next_handle++;
+        ctx->matrices[*new_handle] = std::move(m);
+    });
+}
+
+int slgpu_matrix_add_group(slgpu_ctx* ctx, int handle, const slgpu_group* g, int* index)
+{
+    return guarded(ctx, [&] {
+        if (g == nullptr)
+            fail(SLGPU_E_ARG, "null group");
+        Matrix& M = get_matrix(ctx, handle);
+        if (g->terms == nullptr || g->nterms <= 0 || g->terms[0].dof_table < 0)
+            fail(SLGPU_E_ARG, "matrix groups need dof tables (use slgpu_rhs_assemble for right-hand sides)");
+        M.groups.push_back(make_group(ctx, *g));
+        if (index)
+            *index = (int)M.groups.size() - 1;
+    });
+}
+
+int slgpu_matrix_add_fragment(slgpu_ctx* ctx, int handle, int32_t ntr, int32_t ndr, int32_t nr, int64_t nc, const int32_t* rows,
+                              const int32_t* cols, const double* vals)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (nr < 0 || nc < 0 || ntr < 0 || ndr < 0)
+            fail(SLGPU_E_ARG, "negative fragment size");
+        if ((int64_t)nr * nc == 0)
+            return;
+        if ((ntr != nr || ndr != nr) && (int64_t)ntr * ndr != nr)
+            fail(SLGPU_E_ARG, "fragment rows must be ntr*ndr when ntr or ndr differ from nr");
+        auto f = std::make_shared<FragmentDev>();
+        f->ntr = ntr;
+        f->ndr = ndr;
+        f->nr = nr;
+        f->nc = nc;
+        if (ctx->record_only) {
+            f->hrows.assign(rows, rows + (size_t)ntr * nc);
+            f->hcols.assign(cols, cols + (size_t)ndr * nc);
+            f->hvals.assign(vals, vals + (size_t)nr * nc);
+        } else {
+            upload(ctx, f->rows, rows, (size_t)ntr * nc);
+            upload(ctx, f->cols, cols, (size_t)ndr * nc);
+            upload(ctx, f->vals, vals, (size_t)nr * nc);
+            uint64_t h[2];
+            hash_device(ctx, f->rows.as<int32_t>(), (int64_t)ntr * nc, 77, h);
+            f->addr_hash[0] = h[0];
+            f->addr_hash[1] = h[1];
+            hash_device(ctx, f->cols.as<int32_t>(), (int64_t)ndr * nc, 78, h);
+            f->addr_hash[0] = mix64(f->addr_hash[0] ^ h[0] ^ (uint64_t)nr << 32 ^ (uint64_t)nc);
+            f->addr_hash[1] = mix64(f->addr_hash[1] ^ h[1] ^ (uint64_t)ntr << 32 ^ (uint64_t)ndr);
+        }
+        M.frags.push_back(std::move(f));
+    });
+}
+
+int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        GroupDev& g = *M.groups[gi];
+        if (k < 0 || k >= (int)g.elemdata_off.size())
+            fail(SLGPU_E_ARG, "element data index out of range");
+        if (ctx->record_only) {
+            std::copy(values, values + g.nelem, g.rec->elemdata[k].begin());
+            return;
+        }
+        cuda_check(cudaMemcpyAsync(g.elemdata.as<double>() + g.elemdata_off[k], values, (size_t)g.nelem * 8, cudaMemcpyHostToDevice,
+                                   ctx->stream),
+                   "upload elemdata");
+    });
+}
+
+int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* term_scales, const double* dest_multipliers)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        GroupDev& g = *M.groups[gi];
+        if (term_scales != nullptr) {
+            g.term_scale.assign(term_scales, term_scales + g.nterms);
+            if (!ctx->record_only)
+                cuda_check(cudaMemcpyAsync(g.term_scale_d.as<void>(), term_scales, (size_t)g.nterms * 8, cudaMemcpyHostToDevice,
+                                           ctx->stream),
+                           "upload scales");
+        }
+        if (dest_multipliers != nullptr)
+            g.dest_mult.assign(dest_multipliers, dest_multipliers + g.ndests);
+    });
+}
+
+int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstrained, int precision, slgpu_csr_info* info)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (isconstrained == nullptr && M.ndofs > 0)
+            fail(SLGPU_E_ARG, "null constraint array");
+        process_matrix(ctx, M, isconstrained, precision, false, info);
+    });
+}
+
+int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* Acols, double* Avals, int32_t* Drows, int32_t* Dcols,
+                          double* Dvals)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (!M.pattern)
+            fail(SLGPU_E_STATE, "matrix not processed");
+        Pattern& P = *M.pattern;
+        auto d2h = [&](void* dst, const void* src, size_t n) {
+            if (n > 0)
+                cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->stream), "D2H csr");
+        };
+        d2h(Arows, P.Arows.as<void>(), (P.nA + 1) * 4);
+        d2h(Acols, P.Acols.as<void>(), P.nnzA * 4);
+        d2h(Avals, M.Avals.as<void>(), P.nnzA * 8);
+        d2h(Drows, P.Drows.as<void>(), (P.nA + 1) * 4);
+        d2h(Dcols, P.Dcols.as<void>(), P.nnzD * 4);
+        d2h(Dvals, M.Dvals.as<void>(), P.nnzD * 8);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync download");
+    });
+}
+
+int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, double* Dvals)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (!M.pattern)
+            fail(SLGPU_E_STATE, "matrix not processed");
+        Pattern& P = *M.pattern;
+        if (P.nnzA > 0)
+            cuda_check(cudaMemcpyAsync(Avals, M.Avals.as<void>(), P.nnzA * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        if (P.nnzD > 0)
+            cuda_check(cudaMemcpyAsync(Dvals, M.Dvals.as<void>(), P.nnzD * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync download");
+    });
+}
+
+int slgpu_matrix_device_csr(slgpu_ctx* ctx, int handle, const int32_t** Arows, const int32_t** Acols, const double** Avals,
+                            const int32_t** Drows, const int32_t** Dcols, const double** Dvals)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (!M.pattern)
+            fail(SLGPU_E_STATE, "matrix not processed");
+        Pattern& P = *M.pattern;
+        *Arows = P.Arows.as<int32_t>();
+        *Acols = P.Acols.as<int32_t>();
+        *Avals = M.Avals.as<double>();
+        *Drows = P.Drows.as<int32_t>();
+        *Dcols = P.Dcols.as<int32_t>();
+        *Dvals = M.Dvals.as<double>();
+    });
+}
+
+int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int precision, double* b_accum)
+{
+    return guarded(ctx, [&] {
+        if (g == nullptr || b_accum == nullptr)
+            fail(SLGPU_E_ARG, "null argument");
+        if (g->terms == nullptr || g->nterms <= 0 || g->terms[0].dof_table >= 0 || g->ndof != 1)
+            fail(SLGPU_E_ARG, "right-hand-side groups have no dof tables and ndof = 1");
+        Matrix M;
+        M.ndofs = ndofs;
+        M.groups.push_back(make_group(ctx, *g));
+        if (ctx->record_only) {
+            ctx->rhs_record.push_back(M.groups.back());
+            ctx->rhs_record_ndofs.push_back(ndofs);
+        }
+        process_matrix(ctx, M, nullptr, precision, true, nullptr);
+        std::vector<double> dense((size_t)ndofs);
+        if (ndofs > 0)
+            cuda_check(cudaMemcpyAsync(dense.data(), M.Avals.as<void>(), (size_t)ndofs * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "sync rhs");
+        for (int64_t i = 0; i < ndofs; i++) b_accum[i] += dense[i];
+    });
+}
+
+int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5)
+{
+    if (ctx == nullptr || ms5 == nullptr)
+        return SLGPU_E_ARG;
+    for (int i = 0; i < 5; i++) ms5[i] = ctx->timings[i];
+    return SLGPU_OK;
+}
+
+int slgpu_record_count(const slgpu_ctx* ctx, int handle, int* ngroups, int* nfragments)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        Matrix& M = get_matrix(c, handle);
+        *ngroups = (int)M.groups.size();
+        *nfragments = (int)M.frags.size();
+    });
+}
+
+int slgpu_record_group(const slgpu_ctx* ctx, int handle, int gi, slgpu_group* out)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        if (!c->record_only)
+            fail(SLGPU_E_STATE, "groups are only kept on record-only contexts");
+        Matrix& M = get_matrix(c, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        *out = M.groups[gi]->rec->desc;
+        out->terms = M.groups[gi]->rec->terms.data();
+    });
+}
+
+int slgpu_record_fragment(const slgpu_ctx* ctx, int handle, int fi, int32_t* ntr, int32_t* ndr, int32_t* nr, int64_t* nc,
+                          const int32_t** rows, const int32_t** cols, const double** vals)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        if (!c->record_only)
+            fail(SLGPU_E_STATE, "fragments are only kept on record-only contexts");
+        Matrix& M = get_matrix(c, handle);
+        if (fi < 0 || fi >= (int)M.frags.size())
+            fail(SLGPU_E_ARG, "fragment index out of range");
+        FragmentDev& f = *M.frags[fi];
+        *ntr = f.ntr;
+        *ndr = f.ndr;
+        *nr = f.nr;
+        *nc = f.nc;
+        *rows = f.hrows.data();
+        *cols = f.hcols.data();
+        *vals = f.hvals.data();
+    });
+}
+
+int slgpu_record_rhs_count(const slgpu_ctx* ctx, int* ngroups)
+{
+    if (ctx == nullptr || ngroups == nullptr)
+        return SLGPU_E_ARG;
+    *ngroups = (int)ctx->rhs_record.size();
+    return SLGPU_OK;
+}
+
+int slgpu_record_rhs_group(const slgpu_ctx* ctx, int gi, slgpu_group* out, int64_t* ndofs)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        if (gi < 0 || gi >= (int)c->rhs_record.size())
+            fail(SLGPU_E_ARG, "rhs group index out of range");
+        *out = c->rhs_record[gi]->rec->desc;
+        *ndofs = c->rhs_record_ndofs[gi];
+    });
+}
+
+int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nnodes, const double** xyz, int* ncurvednodes,
+                      int64_t* nelem, const int32_t** conn)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        if (!c->record_only)
+            fail(SLGPU_E_STATE, "mesh arrays are only kept on record-only contexts");
+        auto it = c->meshes.find(mesh);
+        if (it == c->meshes.end() || it->second.types.count(elemtype) == 0)
+            fail(SLGPU_E_ARG, "no such mesh / element type");
+        *nnodes = it->second.nnodes;
+        *xyz = it->second.hxyz.data();
+        const MeshDev::Type& t = it->second.types.at(elemtype);
+        *ncurvednodes = t.ncn;
+        *nelem = t.nelem;
+        *conn = t.hconn.data();
+    });
+}
+
+int slgpu_record_constraints(const slgpu_ctx* ctx, int handle, int64_t* ndofs, const uint8_t** isconstrained)
+{
+    auto* c = const_cast<slgpu_ctx*>(ctx);
+    return guarded(c, [&] {
+        Matrix& M = get_matrix(c, handle);
+        *ndofs = M.ndofs;
+        *isconstrained = M.rec_constrained.empty() ? nullptr : M.rec_constrained.data();
+    });
+}
+
+}  // extern "C"

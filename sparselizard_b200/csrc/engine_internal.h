@@ -1,0 +1,157 @@
+// Internal declarations of the slgpu assembly engine (not part of the C ABI).
+#pragma once
+
+#include "slgpu.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace slgpu {
+
+struct Ctx;
+
+// Device allocation owned by a context; counts against its HBM budget.
+class DevBuf {
+public:
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+    DevBuf& operator=(DevBuf&& o) noexcept;
+    ~DevBuf() { release(); }
+    void alloc(Ctx* ctx, size_t bytes);  // throws on failure / budget
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(p_); }
+    size_t bytes() const { return n_; }
+    bool empty() const { return p_ == nullptr; }
+
+private:
+    Ctx* ctx_ = nullptr;
+    void* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+// One instruction of a compiled coefficient program (register-allocated DAG).
+struct Instr {
+    int32_t op, dst, a, b;
+};
+enum { INSTR_STORE = 100 };
+constexpr int kMaxSlots = 48;
+
+// Orientation-uniform run of elements processed by one contraction tile row.
+struct Tile {
+    int32_t e0, ne, orient, pad;
+};
+
+struct MeshDev {
+    int64_t nnodes = 0;
+    DevBuf xyz;
+    std::vector<double> hxyz;  // record-only copy
+    struct Type {
+        int ncn = 0;
+        int64_t nelem = 0;
+        DevBuf conn;
+        std::vector<int32_t> hconn;  // record-only copy
+    };
+    std::map<int, Type> types;
+};
+
+// A group after upload: everything a launch needs, plus host-side metadata.
+struct GroupDev {
+    int mesh = 0, elemtype = 0, elemdim = 0, problemdim = 0;
+    int64_t nelem = 0;
+    int norient = 1, ngp = 0, ncn = 0, ntf = 0, ndof = 0, nterms = 0, ndests = 0;
+    bool rhs = false;
+    std::vector<Instr> prog;
+    std::vector<int64_t> tab_off;
+    std::vector<int32_t> tab_rows;
+    std::vector<int64_t> elemdata_off;
+    std::vector<int64_t> field_off;
+    std::vector<int32_t> field_rows;
+    std::vector<double> term_scale;
+    std::vector<int32_t> term_tf, term_dof;
+    std::vector<double> dest_mult;
+    std::vector<Tile> tiles;
+    uint64_t addr_hash[2] = {0, 0};
+
+    DevBuf elems, orient, weights, lagrange, tables, consts, prog_d, elemdata, fielddata, field_off_d, field_rows_d,
+        tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
+    std::vector<DevBuf> tfaddr, dofaddr;  // per destination
+
+    // Record-only copy of the original description (for inspection).
+    struct Record;
+    std::shared_ptr<Record> rec;
+};
+
+struct FragmentDev {
+    int32_t ntr = 0, ndr = 0, nr = 0;
+    int64_t nc = 0;
+    DevBuf rows, cols, vals;
+    uint64_t addr_hash[2] = {0, 0};
+    std::vector<int32_t> hrows, hcols;  // record-only copies
+    std::vector<double> hvals;
+};
+
+// Resident COO -> CSR mapping (pattern), reusable while addresses and
+// constraints are unchanged.
+struct Pattern {
+    uint64_t key[2] = {0, 0};
+    int64_t ndofs = 0, nA = 0, nD = 0, nnzA = 0, nnzD = 0, ncoo = 0, nvalid = 0, nruns = 0;
+    DevBuf perm;       // uint32 [nvalid]: sorted position -> COO index
+    DevBuf run_start;  // uint32 [nruns+1]
+    DevBuf run_target; // int32 [nruns]: >= 0 A slot, < 0 D slot -(s+1)
+    DevBuf Arows, Acols, Drows, Dcols, run_row;  // run_row (rhs): dof per run
+    uint64_t last_use = 0;
+};
+
+struct Segment {
+    int64_t coo_base;
+    int64_t count;
+    int64_t val_base;
+    double mult;
+};
+
+struct Matrix {
+    int64_t ndofs = 0;
+    std::vector<std::shared_ptr<GroupDev>> groups;
+    std::vector<std::shared_ptr<FragmentDev>> frags;
+    std::shared_ptr<Pattern> pattern;
+    DevBuf vals;  // contraction outputs + fragment values
+    DevBuf Avals, Dvals;
+    std::vector<uint8_t> rec_constrained;  // record-only
+    slgpu_csr_info info{};
+};
+
+struct Ctx {
+    int device = -1;
+    bool record_only = false;
+    size_t budget = 0;
+    int64_t in_use = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    double timings[5] = {0, 0, 0, 0, 0};
+    std::string last_error;
+    std::map<int, MeshDev> meshes;
+    std::map<int, std::unique_ptr<Matrix>> matrices;
+    int next_handle = 1;
+    std::vector<std::shared_ptr<Pattern>> patterns;  // resident pattern cache
+    uint64_t use_clock = 0;
+    DevBuf scratch;  // reusable temporary storage (sort, scans)
+    DevBuf hash_acc;
+    std::vector<uint8_t> last_constrained;
+    // Record-only contexts: right-hand-side groups and their DOF counts.
+    std::vector<std::shared_ptr<GroupDev>> rhs_record;
+    std::vector<int64_t> rhs_record_ndofs;
+};
+
+}  // namespace slgpu

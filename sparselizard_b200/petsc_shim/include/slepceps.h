@@ -1,0 +1,2 @@
+// Stand-in header: see slshim_petsc.h.
+#include "slshim_petsc.h"

@@ -1,0 +1,197 @@
+"""Helpers shared by the parity tests.
+
+Each sparselizard build (stock reference, GPU drop-in, record-only lowering)
+runs in its own subprocess so that the two builds' global state never meet
+and a record-only context never leaks into a GPU run.  Results come back as
+.npz files.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GPU_LIB = os.path.join(ROOT, "sparselizard_b200", "_build", "libslz_gpu.so")
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libslz_ref.so")
+
+KEYS = ("Arows", "Acols", "Avals", "Drows", "Dcols", "Dvals", "Ainds", "Dinds", "b")
+
+
+def _child(mode: str, workload: int, msh: str, params, out: str, env_extra=None, reps: int = 1):
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    code = (
+        "import sys; sys.path[:0] = [%r, %r]; import _pipeline; _pipeline._child_main(%r, %d, %r, %r, %r, %d)"
+        % (ROOT, os.path.join(ROOT, "tests"), mode, workload, msh, list(params), out, reps)
+    )
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(f"{mode} run failed (rc={r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+    d = np.load(out, allow_pickle=False)
+    return {k: d[k] for k in d.files}
+
+
+def _child_main(mode, workload, msh, params, out, reps):
+    from sparselizard_b200 import workloads as W
+
+    if mode == "ref":
+        r = W.run(REF_LIB, workload, msh, params, reps=reps)
+    elif mode == "gpu":
+        r = W.run(GPU_LIB, workload, msh, params, reps=reps)
+    elif mode == "record":
+        np.savez(out, **record_oracle_inproc(workload, msh, params))
+        return
+    else:
+        raise ValueError(mode)
+    np.savez(out, ndofs=np.array(r.ndofs), times=r.times, **{k: getattr(r, k) for k in KEYS})
+
+
+def reference(workload, msh, params, reps=1):
+    with tempfile.TemporaryDirectory() as d:
+        return _child("ref", workload, msh, params, os.path.join(d, "o.npz"), reps=reps)
+
+
+def gpu(workload, msh, params, precision="fp64", reps=1):
+    with tempfile.TemporaryDirectory() as d:
+        return _child("gpu", workload, msh, params, os.path.join(d, "o.npz"), {"SLGPU_PRECISION": precision}, reps=reps)
+
+
+def record_oracle(workload, msh, params):
+    """Lowers the workload with the drop-in on a record-only context (no GPU)
+    and assembles the recorded groups with the C restatement oracle."""
+    with tempfile.TemporaryDirectory() as d:
+        return _child("record", workload, msh, params, os.path.join(d, "o.npz"), {"SLGPU_RECORD_ONLY": "1"})
+
+
+def recorded_plan(lib):
+    """Groups, constraints, rhs groups and mesh arrays of the last record-only run."""
+    from sparselizard_b200 import abi
+
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+    h = lib.slgpu_adapter_last_handle()
+    ng, nf = ctypes.c_int(), ctypes.c_int()
+    groups = []
+    if h:
+        assert lib.slgpu_record_count(ctx, h, ctypes.byref(ng), ctypes.byref(nf)) == 0
+        for i in range(ng.value):
+            g = abi.Group()
+            assert lib.slgpu_record_group(ctx, h, i, ctypes.byref(g)) == 0
+            groups.append(g)
+    frags = []
+    for i in range(nf.value):
+        ntr, ndr, nr, nc = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        rp, cp, vp = ctypes.POINTER(ctypes.c_int32)(), ctypes.POINTER(ctypes.c_int32)(), ctypes.POINTER(ctypes.c_double)()
+        lib.slgpu_record_fragment(ctx, h, i, *(ctypes.byref(x) for x in (ntr, ndr, nr, nc, rp, cp, vp)))
+        frags.append((ntr.value, ndr.value, nr.value, nc.value,
+                      np.ctypeslib.as_array(rp, (ntr.value * nc.value,)).copy(),
+                      np.ctypeslib.as_array(cp, (ndr.value * nc.value,)).copy(),
+                      np.ctypeslib.as_array(vp, (nr.value * nc.value,)).copy()))
+    ndofs = ctypes.c_int64()
+    cptr = ctypes.POINTER(ctypes.c_uint8)()
+    con = None
+    if h:
+        lib.slgpu_record_constraints(ctx, h, ctypes.byref(ndofs), ctypes.byref(cptr))
+        if cptr:
+            con = np.ctypeslib.as_array(cptr, (ndofs.value,)).copy()
+    nr = ctypes.c_int()
+    lib.slgpu_record_rhs_count(ctx, ctypes.byref(nr))
+    rhs = []
+    for i in range(nr.value):
+        g = abi.Group()
+        nd = ctypes.c_int64()
+        lib.slgpu_record_rhs_group(ctx, i, ctypes.byref(g), ctypes.byref(nd))
+        rhs.append((g, nd.value))
+
+    def mesh(elemtype):
+        nn, xp, ncn, ne, cp2 = ctypes.c_int64(), ctypes.POINTER(ctypes.c_double)(), ctypes.c_int(), ctypes.c_int64(), ctypes.POINTER(ctypes.c_int32)()
+        assert lib.slgpu_record_mesh(ctx, 0, elemtype, *(ctypes.byref(x) for x in (nn, xp, ncn, ne, cp2))) == 0
+        return (np.ctypeslib.as_array(xp, (3 * nn.value,)).copy(), np.ctypeslib.as_array(cp2, (ne.value * ncn.value,)).copy())
+
+    return dict(groups=groups, frags=frags, ndofs=ndofs.value, constrained=con, rhs=rhs, mesh=mesh)
+
+
+def record_oracle_inproc(workload, msh, params):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import slref
+
+    from sparselizard_b200 import workloads as W
+
+    assert os.environ.get("SLGPU_RECORD_ONLY") == "1"
+    lib = W.load(GPU_LIB)
+    try:
+        W.run(GPU_LIB, workload, msh, params)
+        raise AssertionError("a record-only run must not assemble")
+    except RuntimeError as e:
+        assert "record-only" in str(e), str(e)
+    plan = recorded_plan(lib)
+    out = {}
+    if plan["groups"] or plan["frags"]:
+        xyz = None
+        conns = []
+        for g in plan["groups"]:
+            xyz, conn = plan["mesh"](g.elemtype)
+            conns.append(conn)
+        if xyz is None:
+            xyz = np.zeros(3)
+        res = slref.matrix(plan["groups"], xyz, conns, plan["ndofs"], plan["constrained"], plan["frags"])
+        out.update({k: res[k] for k in ("Arows", "Acols", "Avals", "Drows", "Dcols", "Dvals")})
+    b = None
+    for g, nd in plan["rhs"]:
+        xyz, conn = plan["mesh"](g.elemtype)
+        bb = slref.rhs(g, xyz, conn, nd)
+        b = bb if b is None else b + bb
+    if b is not None:
+        out["b_raw"] = b
+    out["ngroups"] = np.array(len(plan["groups"]))
+    return out
+
+
+def check_pattern(ref, other):
+    for k in ("Arows", "Acols", "Drows", "Dcols"):
+        a, b = np.asarray(ref[k]), np.asarray(other[k])
+        assert a.shape == b.shape and np.array_equal(a, b), f"{k} differs from the reference"
+
+
+def rowwise_rel_err(rows, ref_vals, vals):
+    """max over rows of max|vals - ref| / max|ref| within the row (0 for empty rows)."""
+    rows = np.asarray(rows, np.int64)
+    if ref_vals.size == 0:
+        return 0.0
+    diff = np.abs(np.asarray(vals) - np.asarray(ref_vals))
+    mag = np.abs(np.asarray(ref_vals))
+    nz = np.diff(rows) > 0
+    starts = rows[:-1][nz]
+    dmax = np.maximum.reduceat(diff, starts)
+    mmax = np.maximum.reduceat(mag, starts)
+    floor = mag.max() * 1e-300 + 1e-300
+    return float(np.max(dmax / np.maximum(mmax, floor)))
+
+
+def check_values(ref, other, tol):
+    """Row-wise relative error of A and D values (each row against its own
+    largest entry) must not exceed tol; returns the errors."""
+    ea = rowwise_rel_err(ref["Arows"], ref["Avals"], other["Avals"])
+    ed = rowwise_rel_err(ref["Drows"], ref["Dvals"], other["Dvals"])
+    assert ea <= tol, f"A values: row-relative error {ea:.3e} > {tol:g}"
+    assert ed <= tol, f"D values: row-relative error {ed:.3e} > {tol:g}"
+    return ea, ed
+
+
+def check_rhs(ref, b, tol, unconstrained_only=False):
+    rb = np.asarray(ref["b"])
+    b = np.asarray(b)
+    mask = np.ones(rb.size, bool)
+    if unconstrained_only:
+        mask[np.asarray(ref["Dinds"])] = False
+    scale = max(np.abs(rb[mask]).max() if mask.any() else 0.0, 1e-300)
+    err = float(np.abs(rb[mask] - b[mask]).max() / scale) if mask.any() else 0.0
+    assert err <= tol, f"b: relative error {err:.3e} > {tol:g}"
+    return err
