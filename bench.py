@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Assembly benchmark: nnz/s of sparselizard's generate()/A()/b() path on B200.
+
+A step is one assembly pass over the workload on its resident pattern:
+geometry + coefficients + element contraction for every element group, then
+the A/D CSR values (duplicates summed in a fixed order).  The first
+generate()/A()/b() through the drop-in (lowering, upload, pattern build) is
+reported separately as `first_assembly`.
+
+value  : device throughput, inputs already in HBM (CUDA events on the engine's
+         stream, summed over the K steps; max over ranks).
+e2e    : the same metric through the C ABI with host buffers: every step
+         uploads the mesh node coordinates from pinned memory, assembles and
+         downloads the CSR values to pinned memory (host clock around
+         synchronised calls).
+--impl reference times stock sparselizard (built from its sources, CPU, all
+host threads) on a bounded sample of the same workload.
+
+Multi-GPU: element assembly of independent requests does not shard inside
+one matrix without an exchange step, so N ranks run N independent replicas
+(weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from sparselizard_b200 import abi, meshgen, workloads as W  # noqa: E402
+
+GPU_LIB = os.path.join(ROOT, "sparselizard_b200", "_build", "libslz_gpu.so")
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libslz_ref.so")
+SIGMAS = [1e3, 5.0e5, 2.0e6, 6.0e7]
+
+# Workloads: the elasticity case is the headline (64^3 hexahedra, order-2
+# vector field); the others are selectable with --workload.
+WORKLOADS = {
+    "c1": dict(kind=W.POISSON_QUAD, mesh="quad", n=256, params=[1], ref_n=256,
+               name="poisson_q4_256x256_h1_order1"),
+    "c2": dict(kind=W.ELASTICITY_HEX, mesh="hex", n=64, params=[2, -2], ref_n=16,
+               name="elasticity_hex_64^3_h1xyz_order2"),
+    "c3": dict(kind=W.HELMHOLTZ_TET, mesh="tet_orders", n=32, params=[], ref_n=8,
+               name="helmholtz_tet_32^3x6_orders1to5"),
+    "c4": dict(kind=W.EDDY_TET, mesh="tet_sigma", n=24, params=[2, 1.0e3] + SIGMAS, ref_n=8,
+               name="eddy_hcurl_tet_24^3x6_order2_harmonics23"),
+}
+
+
+def write_mesh(spec, n, path):
+    if spec["mesh"] == "quad":
+        meshgen.quad_mesh(path, n, jitter=0.2, seed=1)
+    elif spec["mesh"] == "hex":
+        meshgen.hex_mesh(path, n, jitter=0.15, seed=1)
+    elif spec["mesh"] == "tet_orders":
+        rng = np.random.Generator(np.random.PCG64(1))
+        tags = meshgen.ORDER_REGION_BASE + rng.integers(1, 6, size=6 * n ** 3)
+        meshgen.tet_mesh(path, n, jitter=0.1, seed=1, element_tags=tags)
+    elif spec["mesh"] == "tet_sigma":
+        rng = np.random.Generator(np.random.PCG64(1))
+        tags = meshgen.MATERIAL_REGION_BASE + rng.integers(0, 4, size=6 * n ** 3)
+        meshgen.tet_mesh(path, n, jitter=0.1, seed=1, element_tags=tags)
+    else:
+        raise ValueError(spec["mesh"])
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def allreduce(vals, op):
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized():
+        return vals
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=op)
+    return t.tolist()
+
+
+def cpu_reference_run(spec, n, reps, warmup, threads):
+    with tempfile.TemporaryDirectory() as d:
+        msh = os.path.join(d, "m.msh")
+        write_mesh(spec, n, msh)
+        r = W.run(REF_LIB, spec["kind"], msh, spec["params"], reps=warmup + reps, threads=threads)
+    per = r.times[warmup:].sum(axis=1)
+    return r.nnz, per
+
+
+def run_reference(args, spec):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(threads))
+    nnz, per = cpu_reference_run(spec, spec["ref_n"], args.steps, args.warmup, threads)
+    value = nnz / float(np.mean(per))
+    sample = f"{spec['name']} at n={spec['ref_n']} ({nnz} nnz), generate()+A()+b() per step"
+    line = {
+        "impl": "reference", "metric": "assembled_nnz_per_s", "value": value, "unit": "nnz/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(per)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded jittered mesh)",
+        "config": {"workload": spec["name"], "sample_n": spec["ref_n"], "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "nnz/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, spec):
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    os.environ["SLGPU_DEVICE"] = str(local)
+    os.environ["SLGPU_PRECISION"] = args.precision
+    prec = {"fp64": abi.PREC_FP64, "split": abi.PREC_SPLIT, "fp32": abi.PREC_FP32}[args.precision]
+    tmpd = tempfile.mkdtemp(prefix=f"slbench{rank}_")
+    msh = os.path.join(tmpd, "m.msh")
+    n = args.n or spec["n"]
+    write_mesh(spec, n, msh)
+
+    lib = W.load(GPU_LIB)
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    lib.slz_bench_prepare.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+    lib.slz_bench_constraints.restype = ctypes.POINTER(ctypes.c_uint8)
+    lib.slz_bench_nodes.argtypes = [ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
+    lib.slz_bench_nodes.restype = ctypes.c_longlong
+    params = (ctypes.c_double * max(1, len(spec["params"])))(*spec["params"])
+    t3 = (ctypes.c_double * 3)()
+    info4 = (ctypes.c_longlong * 4)()
+    rc = lib.slz_bench_prepare(spec["kind"], msh.encode(), params, t3, info4)
+    if rc != 0:
+        raise RuntimeError("prepare failed: " + lib.slz_last_error().decode(errors="replace"))
+    first = dict(generate_s=t3[0], A_s=t3[1], b_s=t3[2])
+    handle = int(info4[0])
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+    ndofs = int(info4[1])
+    cons = lib.slz_bench_constraints()
+    info = abi.CsrInfo()
+
+    def process():
+        st = lib.slgpu_matrix_process(ctx, handle, cons, prec, ctypes.byref(info))
+        if st != 0:
+            buf = ctypes.create_string_buffer(2048)
+            lib.slgpu_last_error(ctx, buf, 2048)
+            raise RuntimeError(f"process failed ({st}): {buf.value.decode()}")
+        ms = np.zeros(5)
+        lib.slgpu_last_timings(ctx, abi.f64p(ms))
+        return ms
+
+    work = abi.Work()
+    nnz = info4[2]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        process()
+    lib.slgpu_matrix_work(ctx, handle, ctypes.byref(work))
+    nnz = int(work.nnz)
+    l2_rule = "inputs larger than L2" if work.nvalid * 8 > 126e6 else "L2 flushed between steps"
+
+    # ---- device-resident steps
+    phase = np.zeros(5)
+    launches0 = lib.slgpu_kernel_launches(ctx)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            phase += process()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+    launches = lib.slgpu_kernel_launches(ctx) - launches0
+    dev_ms = phase[4] / args.steps
+    dev_ms_max, = allreduce([dev_ms], torch.distributed.ReduceOp.MAX) if world > 1 else [dev_ms]
+    total_nnz, = allreduce([float(nnz)], torch.distributed.ReduceOp.SUM) if world > 1 else [float(nnz)]
+    value = total_nnz / (dev_ms_max * 1e-3)
+
+    # ---- end-to-end steps through the C ABI with pinned host buffers
+    xyzp = ctypes.POINTER(ctypes.c_double)()
+    nnodes = lib.slz_bench_nodes(ctypes.byref(xyzp))
+    host_xyz = torch.empty(3 * nnodes, dtype=torch.float64).pin_memory()
+    host_xyz.numpy()[:] = np.ctypeslib.as_array(xyzp, (3 * nnodes,))
+    avals = torch.empty(max(1, info.nnzA), dtype=torch.float64).pin_memory()
+    dvals = torch.empty(max(1, info.nnzD), dtype=torch.float64).pin_memory()
+    e2e_t = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = lib.slgpu_mesh_set_nodes(ctx, 0, nnodes, ctypes.cast(host_xyz.data_ptr(), ctypes.POINTER(ctypes.c_double)))
+        assert st == 0
+        process()
+        st = lib.slgpu_matrix_download_values(ctx, handle, ctypes.cast(avals.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                              ctypes.cast(dvals.data_ptr(), ctypes.POINTER(ctypes.c_double)))
+        assert st == 0
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_t))
+    e2e_s_max, = allreduce([e2e_s], torch.distributed.ReduceOp.MAX) if world > 1 else [e2e_s]
+    e2e_value = total_nnz / e2e_s_max
+
+    # ---- roofline of the dominant kernel
+    hbm, bf16, peak_kind = peaks()
+    ph = phase / args.steps
+    dominant = int(np.argmax([ph[0], ph[1], ph[3]]))
+    if dominant == 1:
+        flops = work.contraction_flops
+        achieved = flops / (ph[1] * 1e-3) / 1e12
+        roof = {"kernel": "k_contract_fp64", "bound": "fp64", "achieved": achieved, "unit": "TFLOP/s",
+                "peak": 40.0, "peak_kind": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+                "frac": achieved / 40.0, "traffic": None}
+    elif dominant == 2:
+        byts = 8.0 * work.nvalid + 4.0 * work.nvalid + 8.0 * nnz
+        achieved = byts / (ph[3] * 1e-3) / 1e9
+        roof = {"kernel": "k_csr_values", "bound": "hbm", "achieved": achieved, "unit": "GB/s", "peak": hbm,
+                "peak_kind": peak_kind, "frac": achieved / hbm, "traffic": None}
+    else:
+        byts = 8.0 * work.coef_points * max(1, work.ngroups)
+        achieved = byts / (ph[0] * 1e-3) / 1e9
+        roof = {"kernel": "k_geometry_coef", "bound": "hbm", "achieved": achieved, "unit": "GB/s", "peak": hbm,
+                "peak_kind": peak_kind, "frac": achieved / hbm, "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        threads = os.cpu_count() or 1
+        cnnz, per = cpu_reference_run(spec, spec["ref_n"], 2, 1, threads)
+        cpu = {"value": cnnz / float(np.mean(per)), "unit": "nnz/s", "cores": threads, "kind": "reference",
+               "sample": f"stock sparselizard generate()+A()+b(), {spec['name']} at n={spec['ref_n']} ({cnnz} nnz), "
+                         f"mean of 2 after 1 warm-up"}
+
+    if rank == 0:
+        line = {
+            "metric": "assembled_nnz_per_s", "value": value, "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered mesh)",
+            "config": {"workload": spec["name"], "n": n, "precision": args.precision, "ndofs": ndofs, "nnz": nnz,
+                       "ncoo": int(work.ncoo), "groups": int(work.ngroups), "l2": l2_rule,
+                       "parallelism": f"replicas{world}"},
+            "phases_ms": {"geometry_coef": ph[0], "contraction": ph[1], "values": ph[3], "total": ph[4]},
+            "first_assembly": first,
+            "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_s_max * 1e3,
+                    "h2d_bytes_per_step": int(24 * nnodes), "d2h_bytes_per_step": int(8 * (info.nnzA + info.nnzD))},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    lib.slz_bench_release()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split", "fp32"])
+    ap.add_argument("--n", type=int, default=0, help="override the mesh size (elements per side)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, spec)
+    else:
+        run_ours(args, spec)
+
+
+if __name__ == "__main__":
+    main()

@@ -189,6 +189,8 @@ int slgpu_matrix_add_fragment(slgpu_ctx* ctx, int handle, int32_t ntr, int32_t n
                               const int32_t* rows, const int32_t* cols, const double* vals);
 /* Replaces per-element data array `k` of group `gi` (new coefficients on a resident pattern). */
 int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values);
+/* Replaces field coefficient array `k` ([rows][nelem]) of group `gi`. */
+int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values);
 /* Replaces term scales and destination multipliers of group `gi` (e.g. a new frequency). */
 int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* term_scales, const double* dest_multipliers);
 /* isconstrained [ndofs] (dofmanager::isconstrained, src/formulation/dofmanager.cpp:366-382). */
@@ -213,6 +215,25 @@ int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int 
 /* Device time (ms) of the phases of the last process()/rhs call:
  * [0] geometry+coefficients, [1] contraction, [2] pattern (symbolic), [3] CSR values, [4] total. */
 int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5);
+/* Number of kernels this context has launched so far. */
+int64_t slgpu_kernel_launches(const slgpu_ctx* ctx);
+
+/* Algorithmic work of one process() of a matrix, for roofline accounting:
+ * contraction_flops = sum over groups of nelem * sum over terms of
+ * 2*ntf*ndof*ngp (the reference's K = M * coef^T counted once per term);
+ * coef_points = sum of nelem*ngp; ncoo / nvalid = COO entries generated / kept;
+ * nnz = nnzA + nnzD. */
+typedef struct {
+    double contraction_flops;
+    int64_t coef_points;
+    int64_t ncoo;
+    int64_t nvalid;
+    int64_t nnz;
+    int64_t nA;
+    int32_t ngroups;
+    int32_t pad;
+} slgpu_work;
+int slgpu_matrix_work(slgpu_ctx* ctx, int handle, slgpu_work* out);
 
 /* Record-only contexts: inspect what was recorded for a matrix handle. */
 int slgpu_record_count(const slgpu_ctx* ctx, int handle, int* ngroups, int* nfragments);

@@ -87,6 +87,13 @@ static void eval_nodes(const slgpu_group* g, int64_t e, int gp, int o, double J[
     }
 }
 
+/* Magnitude mode: every product and every summand replaced by its absolute
+ * value, giving sum |terms| for each entry -- the scale of the standard
+ * floating-point error bound |fl(sum) - sum| <= gamma_n * sum |terms|. */
+static int g_absmode = 0;
+
+void slref_set_absmode(int on) { g_absmode = on; }
+
 int slref_element_matrices(const slgpu_group* g, const double* xyz, const int32_t* conn, double* K)
 {
     const int ngp = g->ngp, ntf = g->ntf, ndof = g->ndof, nterms = g->nterms, ndests = g->ndests;
@@ -122,12 +129,15 @@ int slref_element_matrices(const slgpu_group* g, const double* xyz, const int32_
                         for (int gp = 0; gp < ngp; gp++) {
                             double m = T[(int64_t)i * ngp + gp] * g->weights[gp];
                             if (D) m *= D[(int64_t)j * ngp + gp];
-                            s += m * coefdet[(int64_t)t * ngp + gp];
+                            if (g_absmode)
+                                s += fabs(m) * fabs(coefdet[(int64_t)t * ngp + gp]);
+                            else
+                                s += m * coefdet[(int64_t)t * ngp + gp];
                         }
                         Kt[(int64_t)i * ndof + j] = s;
                     }
                 /* Harmonic folding: stiffness += factor * K_term (contribution.cpp:220-246). */
-                const double factor = tm.scale * g->dests[d].multiplier;
+                const double factor = g_absmode ? fabs(tm.scale * g->dests[d].multiplier) : tm.scale * g->dests[d].multiplier;
                 for (int64_t p = 0; p < P; p++) Kd[p] += factor * Kt[p];
             }
             for (int64_t p = 0; p < P; p++) K[((int64_t)d * P + p) * nelem + e] = Kd[p];
@@ -198,7 +208,7 @@ int slref_matrix(const slgpu_group* groups, int ngroups, const double* xyz, cons
                 for (int64_t c = 0; c < f->nc; c++, idx++) {                                                        \
                     const int32_t cr = f->rows[ctr * f->nc + c];                                                    \
                     const int32_t cc = f->cols[cdr * f->nc + c];                                                    \
-                    const double cv = f->vals[r * f->nc + c];                                                       \
+                    const double cv = g_absmode ? fabs(f->vals[r * f->nc + c]) : f->vals[r * f->nc + c];            \
                     BODY                                                                                            \
                 }                                                                                                   \
             }                                                                                                       \

@@ -53,6 +53,12 @@ int slref_rhs(const slgpu_group* g, const double* xyz, const int32_t* conn, int6
 
 void slref_free(slref_csr* c);
 
+/* on != 0: the functions above return sum |terms| instead of sum terms (every
+ * product, factor and summand taken in absolute value), the scale against
+ * which rounding differences between two correct summation orders are
+ * judged. */
+void slref_set_absmode(int on);
+
 #ifdef __cplusplus
 }
 #endif

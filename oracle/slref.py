@@ -43,13 +43,16 @@ def lib():
         l.slref_rhs.argtypes = [POINTER(abi.Group), POINTER(c_double), POINTER(c_int32), c_int64, POINTER(c_double)]
         l.slref_rhs.restype = c_int
         l.slref_free.argtypes = [POINTER(Csr)]
+        l.slref_set_absmode.argtypes = [c_int]
         _lib = l
     return _lib
 
 
-def matrix(groups, xyz, conns, ndofs, isconstrained, frags=()):
-    """rawmat::process of the groups' element matrices + fragments -> dict of CSR arrays."""
+def matrix(groups, xyz, conns, ndofs, isconstrained, frags=(), absmode=False):
+    """rawmat::process of the groups' element matrices + fragments -> dict of CSR arrays.
+    absmode: values are sum |terms| (the rounding-error scale) instead of sum terms."""
     l = lib()
+    l.slref_set_absmode(1 if absmode else 0)
     G = (abi.Group * max(1, len(groups)))(*groups)
     C = (POINTER(c_int32) * max(1, len(conns)))(*[abi.i32p(c) for c in conns])
     F = (Fragment * max(1, len(frags)))()
@@ -64,6 +67,7 @@ def matrix(groups, xyz, conns, ndofs, isconstrained, frags=()):
     xyz = np.ascontiguousarray(xyz, np.float64)
     st = l.slref_matrix(G, len(groups), abi.f64p(xyz), C, F, len(frags), ndofs,
                         con.ctypes.data_as(POINTER(c_uint8)), ctypes.byref(out))
+    l.slref_set_absmode(0)
     if st != 0:
         raise RuntimeError("slref_matrix failed")
     nA, nnzA, nnzD = out.nA, out.nnzA, out.nnzD
@@ -80,14 +84,16 @@ def matrix(groups, xyz, conns, ndofs, isconstrained, frags=()):
     return res
 
 
-def rhs(group, xyz, conn, ndofs):
+def rhs(group, xyz, conn, ndofs, absmode=False):
     l = lib()
+    l.slref_set_absmode(1 if absmode else 0)
     b = np.zeros(ndofs)
     xyz = np.ascontiguousarray(xyz, np.float64)
     conn = np.ascontiguousarray(conn, np.int32)
     if l.slref_rhs(ctypes.byref(group), abi.f64p(xyz), abi.i32p(conn), ndofs, abi.f64p(b)) != 0:
         raise RuntimeError("slref_rhs failed")
-    return b
+    l.slref_set_absmode(0)
+    return np.abs(b) if absmode else b
 
 
 def element_matrices(group, xyz, conn):

@@ -63,6 +63,11 @@ class CsrInfo(ctypes.Structure):
                 ("pattern_reused", c_int32), ("pad", c_int32)]
 
 
+class Work(ctypes.Structure):
+    _fields_ = [("contraction_flops", c_double), ("coef_points", c_int64), ("ncoo", c_int64), ("nvalid", c_int64),
+                ("nnz", c_int64), ("nA", c_int64), ("ngroups", c_int32), ("pad", c_int32)]
+
+
 # Every exported symbol with (restype, argtypes); the tests check that the
 # library exports each of them.
 SIGNATURES = {
@@ -79,7 +84,10 @@ SIGNATURES = {
     "slgpu_matrix_add_fragment": (c_int, [c_void_p, c_int, c_int32, c_int32, c_int32, c_int64, POINTER(c_int32),
                                           POINTER(c_int32), POINTER(c_double)]),
     "slgpu_matrix_set_elemdata": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double)]),
+    "slgpu_matrix_set_fielddata": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double)]),
     "slgpu_matrix_set_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
+    "slgpu_kernel_launches": (c_int64, [c_void_p]),
+    "slgpu_matrix_work": (c_int, [c_void_p, c_int, c_void_p]),
     "slgpu_matrix_process": (c_int, [c_void_p, c_int, POINTER(c_uint8), c_int, POINTER(CsrInfo)]),
     "slgpu_matrix_download": (c_int, [c_void_p, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_double),
                                       POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),

@@ -29,7 +29,7 @@ rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr, Mat inA, Mat inD, indexmat i
 
 rawmat::~rawmat(void)
 {
-    slgpu_adapter::release_matrix(this);
+    slgpu_adapter::forget_matrix(this);
     // PETSc objects may only be destroyed before PetscFinalize.
     PetscBool ispetscinitialized;
     PetscInitialized(&ispetscinitialized);

@@ -33,6 +33,7 @@ struct MatEntry {
 };
 std::map<rawmat*, std::shared_ptr<MatEntry>> g_mats;
 std::shared_ptr<MatEntry> g_last_entry;
+std::map<rawmat*, std::shared_ptr<MatEntry>> g_processed;
 
 struct MeshState {
     int rawmeshnumber = -1;
@@ -46,6 +47,7 @@ struct CtxGuard {
     ~CtxGuard()
     {
         g_mats.clear();
+        g_processed.clear();
         g_last_entry.reset();
         if (g_ctx != nullptr)
             slgpu_ctx_destroy(g_ctx);
@@ -75,7 +77,10 @@ slgpu_ctx* context(void)
     size_t budget = 0;
     if (const char* b = std::getenv("SLGPU_HBM_BUDGET_GB"))
         budget = (size_t)(std::atof(b) * 1e9);
-    int st = slgpu_ctx_create(0, budget, flags, &g_ctx);
+    int device = 0;
+    if (const char* d = std::getenv("SLGPU_DEVICE"))
+        device = std::atoi(d);
+    int st = slgpu_ctx_create(device, budget, flags, &g_ctx);
     if (st != SLGPU_OK) {
         g_ctx = nullptr;
         g_ctx_failed = true;
@@ -142,6 +147,9 @@ int ensure_mesh(int elemtype)
 
 int find_matrix_handle(rawmat* m)
 {
+    auto p = g_processed.find(m);
+    if (p != g_processed.end())
+        return p->second->handle;
     auto it = g_mats.find(m);
     return it == g_mats.end() ? 0 : it->second->handle;
 }
@@ -174,6 +182,12 @@ void share_matrix(rawmat* from, rawmat* to)
 
 void release_matrix(rawmat* m) { g_mats.erase(m); }
 
+void forget_matrix(rawmat* m)
+{
+    g_mats.erase(m);
+    g_processed.erase(m);
+}
+
 bool record_only(void)
 {
     context();
@@ -187,6 +201,10 @@ void set_last_processed(rawmat* m)
     auto it = g_mats.find(m);
     g_last_entry = it == g_mats.end() ? nullptr : it->second;
     g_last_handle = g_last_entry ? g_last_entry->handle : 0;
+    // The processed engine matrix (resident pattern and values) stays with
+    // the rawmat until it is destroyed, even after clearfragments().
+    if (g_last_entry)
+        g_processed[m] = g_last_entry;
 }
 
 }  // namespace slgpu_adapter

@@ -39,6 +39,8 @@ int find_matrix_handle(rawmat* m);
 void share_matrix(rawmat* from, rawmat* to);
 // Forgets a rawmat's engine matrix (destroying it when no other rawmat uses it).
 void release_matrix(rawmat* m);
+// Drops every engine matrix tied to a rawmat (its destructor).
+void forget_matrix(rawmat* m);
 
 // True on a record-only context (SLGPU_RECORD_ONLY=1): groups are recorded for
 // inspection and every assembly request ends in an error.

@@ -561,6 +561,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
             kp.nelem = g->nelem;
             kp.count = segs[si].count;
             kp.coo_base = segs[si].coo_base;
+            kp.ndofs = M.ndofs;
             kp.colbits = colbits;
             kp.constrained = rhs ? nullptr : dconstr;
             kp.invalid = invalid;
@@ -787,22 +788,31 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
 
     // Constraints on the device (reused buffer keyed by content).
-    DevBuf dconstr;
-    dconstr.alloc(ctx, (M.ndofs + 1));
-    if (!rhs)
-        cuda_check(cudaMemcpyAsync(dconstr.as<void>(), isconstrained, M.ndofs, cudaMemcpyHostToDevice, ctx->stream), "H2D constr");
+    // Constraints: device copy and content key, both reused while the array
+    // is byte-identical to the previous call's.
     uint64_t ckey[2] = {0, 0};
+    const uint8_t* dconstr_ptr = nullptr;
     if (!rhs) {
-        // Hash constraints as 32-bit words.
-        std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
-        std::memcpy(packed.data(), isconstrained, M.ndofs);
-        uint64_t a = 0x12345, b = 0x6789;
-        for (size_t i = 0; i < packed.size(); i++) {
-            a = mix64(a ^ (uint64_t)(uint32_t)packed[i] ^ (uint64_t)i << 32);
-            b += mix64((uint64_t)(uint32_t)packed[i] * 0x100000001b3ull + i);
+        const bool same = ctx->constr_host.size() == (size_t)M.ndofs &&
+                          std::memcmp(ctx->constr_host.data(), isconstrained, (size_t)M.ndofs) == 0;
+        if (!same) {
+            ctx->constr_host.assign(isconstrained, isconstrained + M.ndofs);
+            ctx->constr_dev.alloc(ctx, (size_t)M.ndofs + 1);
+            cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), isconstrained, M.ndofs, cudaMemcpyHostToDevice, ctx->stream),
+                       "H2D constr");
+            std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
+            std::memcpy(packed.data(), isconstrained, M.ndofs);
+            uint64_t a = 0x12345, b = 0x6789;
+            for (size_t i = 0; i < packed.size(); i++) {
+                a = mix64(a ^ (uint64_t)(uint32_t)packed[i] ^ (uint64_t)i << 32);
+                b += mix64((uint64_t)(uint32_t)packed[i] * 0x100000001b3ull + i);
+            }
+            ctx->constr_key[0] = a;
+            ctx->constr_key[1] = b;
         }
-        ckey[0] = a;
-        ckey[1] = b;
+        ckey[0] = ctx->constr_key[0];
+        ckey[1] = ctx->constr_key[1];
+        dconstr_ptr = ctx->constr_dev.as<uint8_t>();
     }
     uint64_t key0 = mix64(ckey[0] ^ (uint64_t)M.ndofs ^ (rhs ? 0xABCDEFull : 0));
     uint64_t key1 = mix64(ckey[1] ^ (uint64_t)segs.size());
@@ -823,15 +833,20 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     DevBuf C;
     C.alloc(ctx, std::max<int64_t>(maxC, 1) * 8);
     size_t gi = 0;
-    float coef_ms = 0, contract_ms = 0;
+    while (ctx->evpool.size() < 3 * M.groups.size()) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        ctx->evpool.push_back(e);
+    }
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
             CoefParams cp = coef_params(ctx, *g, C.as<double>());
             int64_t n = g->nelem * (int64_t)g->ngp;
-            ev_record(ctx, 4);
+            cuda_check(cudaEventRecord(ctx->evpool[3 * gi], ctx->stream), "cudaEventRecord");
             k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
             cuda_check(cudaGetLastError(), "k_geometry_coef");
-            ev_record(ctx, 5);
+            ctx->launches++;
+            cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 1], ctx->stream), "cudaEventRecord");
             ContractParams kp{};
             kp.tables = g->tables.as<double>();
             kp.tab_off = g->tab_off_d.as<int64_t>();
@@ -851,10 +866,8 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
                 fail(SLGPU_E_UNSUPPORTED, "element matrix too large for the contraction grid");
             k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
-            ev_record(ctx, 1);
-            cuda_check(cudaEventSynchronize(ctx->ev[1]), "sync");
-            coef_ms += ev_ms(ctx, 4, 5);
-            contract_ms += ev_ms(ctx, 5, 1);
+            ctx->launches++;
+            cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 2], ctx->stream), "cudaEventRecord");
         }
         gi++;
     }
@@ -875,7 +888,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
 
     // 3: pattern.
     bool reused = false;
-    M.pattern = get_pattern(ctx, M, segs, dconstr.as<uint8_t>(), rhs, key0, key1, &reused);
+    M.pattern = get_pattern(ctx, M, segs, dconstr_ptr, rhs, key0, key1, &reused);
     Pattern& P = *M.pattern;
     ev_record(ctx, 2);
 
@@ -903,9 +916,20 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         vp.negate = rhs ? 1 : 0;
         k_csr_values<<<grid_for(P.nruns, 256), 256, 0, ctx->stream>>>(vp);
         cuda_check(cudaGetLastError(), "k_csr_values");
+        ctx->launches++;
     }
     ev_record(ctx, 3);
     cuda_check(cudaEventSynchronize(ctx->ev[3]), "sync");
+    float coef_ms = 0, contract_ms = 0;
+    for (size_t k = 0; k < M.groups.size(); k++) {
+        if (M.groups[k]->nelem == 0)
+            continue;
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->evpool[3 * k], ctx->evpool[3 * k + 1]);
+        cudaEventElapsedTime(&b, ctx->evpool[3 * k + 1], ctx->evpool[3 * k + 2]);
+        coef_ms += a;
+        contract_ms += b;
+    }
     ctx->timings[0] = coef_ms;
     ctx->timings[1] = contract_ms;
     ctx->timings[2] = ev_ms(ctx, 1, 2);
@@ -1009,9 +1033,11 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
     ctx->meshes.clear();
     ctx->scratch.release();
     ctx->hash_acc.release();
+    ctx->constr_dev.release();
     if (!ctx->record_only) {
         cudaStreamSynchronize(ctx->stream);
         for (auto& e : ctx->ev) cudaEventDestroy(e);
+        for (auto& e : ctx->evpool) cudaEventDestroy(e);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -1162,6 +1188,49 @@ int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const d
         cuda_check(cudaMemcpyAsync(g.elemdata.as<double>() + g.elemdata_off[k], values, (size_t)g.nelem * 8, cudaMemcpyHostToDevice,
                                    ctx->stream),
                    "upload elemdata");
+    });
+}
+
+int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        GroupDev& g = *M.groups[gi];
+        if (k < 0 || k >= (int)g.field_off.size())
+            fail(SLGPU_E_ARG, "field data index out of range");
+        const size_t n = (size_t)g.field_rows[k] * g.nelem;
+        if (ctx->record_only) {
+            std::copy(values, values + n, g.rec->fielddata[k].begin());
+            return;
+        }
+        cuda_check(cudaMemcpyAsync(g.fielddata.as<double>() + g.field_off[k], values, n * 8, cudaMemcpyHostToDevice, ctx->stream),
+                   "upload fielddata");
+    });
+}
+
+int64_t slgpu_kernel_launches(const slgpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int slgpu_matrix_work(slgpu_ctx* ctx, int handle, slgpu_work* out)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (out == nullptr)
+            fail(SLGPU_E_ARG, "null output");
+        slgpu_work w{};
+        for (auto& g : M.groups) {
+            w.contraction_flops += (double)g->nelem * g->nterms * 2.0 * g->ntf * g->ndof * g->ngp;
+            w.coef_points += g->nelem * (int64_t)g->ngp;
+        }
+        w.ngroups = (int32_t)M.groups.size();
+        if (M.pattern) {
+            w.ncoo = M.pattern->ncoo;
+            w.nvalid = M.pattern->nvalid;
+            w.nnz = M.pattern->nnzA + M.pattern->nnzD;
+            w.nA = M.pattern->nA;
+        }
+        *out = w;
     });
 }
 

@@ -148,7 +148,11 @@ struct Ctx {
     uint64_t use_clock = 0;
     DevBuf scratch;  // reusable temporary storage (sort, scans)
     DevBuf hash_acc;
-    std::vector<uint8_t> last_constrained;
+    std::vector<uint8_t> constr_host;  // last constraint array seen by process()
+    DevBuf constr_dev;
+    uint64_t constr_key[2] = {0, 0};
+    std::vector<cudaEvent_t> evpool;   // per-group phase events
+    int64_t launches = 0;              // kernels launched by this context
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;

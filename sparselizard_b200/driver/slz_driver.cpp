@@ -11,6 +11,8 @@
 #include "sparselizard.h"
 
 #include <chrono>
+#include <memory>
+#include <stdexcept>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -110,18 +112,24 @@ void run_reps(formulation& f, int reps, double* times)
     }
 }
 
+struct Problem {
+    mesh m;
+    std::vector<field> fields;
+    std::vector<parameter> params;  // created after the mesh
+    formulation f;
+};
+
 // Poisson on quadrangles: integral(vol, -grad(dof(v))*grad(tf(v)), -2) +
 // integral(vol, 1*tf(v), -2), v = 0 on the boundary.
-void poisson_quad(const char* msh, int order, int reps, double* times)
+void poisson_quad(Problem& P, const char* msh, int order)
 {
-    mesh m(msh, 0);
+    P.m = mesh(msh, 0);
     field v("h1");
     v.setorder(VOL, order);
     v.setconstraint(BOUNDARY);
-    formulation f;
-    f += integral(VOL, -grad(dof(v)) * grad(tf(v)), -2);
-    f += integral(VOL, 1 * tf(v), -2);
-    run_reps(f, reps, times);
+    P.f += integral(VOL, -grad(dof(v)) * grad(tf(v)), -2);
+    P.f += integral(VOL, 1 * tf(v), -2);
+    P.fields = {v};
 }
 
 // Sets a "one" field to one value per element of region `reg` (element order of
@@ -142,9 +150,9 @@ void set_per_element(field& E, int reg, const std::vector<double>& values)
 
 // 3D linear elasticity, vector h1 field, per-element lognormal E, nu = 0.3,
 // bottom face clamped: integral(vol, predefinedelasticity(dof(u), tf(u), E, nu), delta).
-void elasticity_hex(const char* msh, int order, int delta, int reps, double* times)
+void elasticity_hex(Problem& P, const char* msh, int order, int delta)
 {
-    mesh m(msh, 0);
+    P.m = mesh(msh, 0);
     field u("h1xyz"), E("one");
     u.setorder(VOL, order);
     u.setconstraint(CLAMP);
@@ -152,31 +160,29 @@ void elasticity_hex(const char* msh, int order, int delta, int reps, double* tim
     std::vector<double> evals(1 << 22);
     for (double& e : evals) e = 150e9 * std::exp(0.3 * rng.draw());
     set_per_element(E, VOL, evals);
-    formulation f;
-    f += integral(VOL, predefinedelasticity(dof(u), tf(u), E, 0.3), delta);
-    run_reps(f, reps, times);
+    P.f += integral(VOL, predefinedelasticity(dof(u), tf(u), E, 0.3), delta);
+    P.fields = {u, E};
 }
 
 // p-adaptive scalar Helmholtz on tets: region ORDER_REGION_BASE+p holds the
 // order-p elements (p = 1..5); orders are set in descending order.
-void helmholtz_tet(const char* msh, int reps, double* times)
+void helmholtz_tet(Problem& P, const char* msh)
 {
-    mesh m(msh, 0);
+    P.m = mesh(msh, 0);
     int vol = selectunion({ORDER_REGION_BASE + 1, ORDER_REGION_BASE + 2, ORDER_REGION_BASE + 3, ORDER_REGION_BASE + 4, ORDER_REGION_BASE + 5});
     field p("h1");
     for (int ord = 5; ord >= 1; ord--)
         p.setorder(ORDER_REGION_BASE + ord, ord);
-    formulation f;
-    f += integral(vol, grad(dof(p)) * grad(tf(p)) - 400.0 * dof(p) * tf(p));
-    run_reps(f, reps, times);
+    P.f += integral(vol, grad(dof(p)) * grad(tf(p)) - 400.0 * dof(p) * tf(p));
+    P.fields = {p};
 }
 
 // Harmonic eddy currents on tets, hcurl order 2 with harmonics {2,3}:
 // integral(vol, curl(dof(a))*curl(tf(a))/mu + sigma*dt(dof(a))*tf(a)),
 // sigma per material region, at fundamental frequency `freq`.
-void eddy_tet(const char* msh, int order, const double* sigmas, double freq, int reps, double* times)
+void eddy_tet(Problem& P, const char* msh, int order, const double* sigmas, double freq)
 {
-    mesh m(msh, 0);
+    P.m = mesh(msh, 0);
     int vol = selectunion({MATERIAL_REGION_BASE, MATERIAL_REGION_BASE + 1, MATERIAL_REGION_BASE + 2, MATERIAL_REGION_BASE + 3});
     setfundamentalfrequency(freq);
     field a("hcurl", {2, 3});
@@ -185,9 +191,22 @@ void eddy_tet(const char* msh, int order, const double* sigmas, double freq, int
     for (int r = 0; r < 4; r++)
         sigma.setvalue(MATERIAL_REGION_BASE + r, sigmas[r]);
     double mu = 4.0 * 3.141592653589793 * 1e-7;
-    formulation f;
-    f += integral(vol, curl(dof(a)) * curl(tf(a)) / mu + sigma * dt(dof(a)) * tf(a));
-    run_reps(f, reps, times);
+    P.f += integral(vol, curl(dof(a)) * curl(tf(a)) / mu + sigma * dt(dof(a)) * tf(a));
+    P.params = {sigma};
+    P.fields = {a};
+}
+
+std::unique_ptr<Problem> build(int workload, const char* msh, const double* params)
+{
+    auto P = std::make_unique<Problem>();
+    switch (workload) {
+    case 1: poisson_quad(*P, msh, (int)params[0]); break;
+    case 2: elasticity_hex(*P, msh, (int)params[0], (int)params[1]); break;
+    case 3: helmholtz_tet(*P, msh); break;
+    case 4: eddy_tet(*P, msh, (int)params[0], params + 2, params[1]); break;
+    default: throw std::runtime_error("unknown workload");
+    }
+    return P;
 }
 
 } // namespace
@@ -202,23 +221,8 @@ int slz_run(int workload, const char* msh, const double* params, int reps, doubl
 {
     g_error.clear();
     try {
-        switch (workload) {
-        case 1:
-            poisson_quad(msh, (int)params[0], reps, times);
-            break;
-        case 2:
-            elasticity_hex(msh, (int)params[0], (int)params[1], reps, times);
-            break;
-        case 3:
-            helmholtz_tet(msh, reps, times);
-            break;
-        case 4:
-            eddy_tet(msh, (int)params[0], params + 2, params[1], reps, times);
-            break;
-        default:
-            g_error = "unknown workload";
-            return 1;
-        }
+        std::unique_ptr<Problem> P = build(workload, msh, params);
+        run_reps(P->f, reps, times);
     } catch (const std::exception& e) {
         g_error = e.what();
         if (g_error.empty())
@@ -264,3 +268,69 @@ void slz_result_copy(int* Arows, int* Acols, double* Avals, int* Drows, int* Dco
 void slz_set_threads(int n) { setmaxnumthreads(n); }
 
 }
+
+#ifdef SLZ_GPU_BUILD
+// Benchmark support (GPU drop-in build only): keeps one problem resident after
+// a first generate()/A()/b() so that the engine matrix it produced can be
+// re-assembled on its resident pattern through the C ABI.
+#include "slgpu_adapter.h"
+
+namespace {
+struct BenchState {
+    std::unique_ptr<Problem> P;
+    mat A;
+    vec b;
+    std::vector<unsigned char> constrained;
+};
+std::unique_ptr<BenchState> g_bench;
+}  // namespace
+
+extern "C" {
+
+// times3: generate / A / b wall seconds of the first assembly; info4: engine
+// matrix handle, ndofs, nnzA, nnzD.
+int slz_bench_prepare(int workload, const char* msh, const double* params, double* times3, long long* info4)
+{
+    g_error.clear();
+    try {
+        g_bench.reset();
+        auto B = std::make_unique<BenchState>();
+        B->P = build(workload, msh, params);
+        double t0 = now_s();
+        B->P->f.generate();
+        double t1 = now_s();
+        B->A = B->P->f.A();
+        double t2 = now_s();
+        B->b = B->P->f.b();
+        double t3 = now_s();
+        times3[0] = t1 - t0;
+        times3[1] = t2 - t1;
+        times3[2] = t3 - t2;
+        std::shared_ptr<rawmat> raw = B->A.getpointer();
+        std::vector<bool> c = raw->getdofmanager()->isconstrained();
+        B->constrained.assign(c.begin(), c.end());
+        info4[0] = slgpu_adapter::find_matrix_handle(raw.get());
+        info4[1] = raw->countrows();
+        info4[2] = raw->countnnz();
+        info4[3] = B->A.getdinds().count();
+        g_bench = std::move(B);
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+    return 0;
+}
+
+const unsigned char* slz_bench_constraints(void) { return g_bench ? g_bench->constrained.data() : nullptr; }
+
+// Node coordinates of the resident mesh in sparselizard's numbering.
+long long slz_bench_nodes(const double** xyz)
+{
+    std::vector<double>* c = universe::getrawmesh()->getnodes()->getcoordinates();
+    *xyz = c->data();
+    return (long long)c->size() / 3;
+}
+
+void slz_bench_release(void) { g_bench.reset(); }
+}
+#endif

@@ -143,13 +143,19 @@ def record_oracle_inproc(workload, msh, params):
             xyz = np.zeros(3)
         res = slref.matrix(plan["groups"], xyz, conns, plan["ndofs"], plan["constrained"], plan["frags"])
         out.update({k: res[k] for k in ("Arows", "Acols", "Avals", "Drows", "Dcols", "Dvals")})
+        mag = slref.matrix(plan["groups"], xyz, conns, plan["ndofs"], plan["constrained"], plan["frags"], absmode=True)
+        out["Aabs"], out["Dabs"] = mag["Avals"], mag["Dvals"]
     b = None
+    babs = None
     for g, nd in plan["rhs"]:
         xyz, conn = plan["mesh"](g.elemtype)
         bb = slref.rhs(g, xyz, conn, nd)
+        ba = slref.rhs(g, xyz, conn, nd, absmode=True)
         b = bb if b is None else b + bb
+        babs = ba if babs is None else babs + ba
     if b is not None:
         out["b_raw"] = b
+        out["b_abs"] = babs
     out["ngroups"] = np.array(len(plan["groups"]))
     return out
 
@@ -175,23 +181,83 @@ def rowwise_rel_err(rows, ref_vals, vals):
     return float(np.max(dmax / np.maximum(mmax, floor)))
 
 
-def check_values(ref, other, tol):
-    """Row-wise relative error of A and D values (each row against its own
-    largest entry) must not exceed tol; returns the errors."""
-    ea = rowwise_rel_err(ref["Arows"], ref["Avals"], other["Avals"])
-    ed = rowwise_rel_err(ref["Drows"], ref["Dvals"], other["Dvals"])
-    assert ea <= tol, f"A values: row-relative error {ea:.3e} > {tol:g}"
-    assert ed <= tol, f"D values: row-relative error {ed:.3e} > {tol:g}"
+def scaled_errors(ref, other):
+    """Entry-wise errors |a_ij - b_ij| / sqrt(S_i S_j), S = largest magnitude in
+    each DOF's row/column of the reference (A and D together).  This is the
+    error of the symmetrically scaled matrix D^-1/2 A D^-1/2: an entry that is
+    exactly zero in exact arithmetic (e.g. curl-curl of a gradient form
+    function) is judged against the scale of the terms that cancel in it, not
+    against its own rounding noise.  Also returns the Frobenius-relative error."""
+    Arows, Drows = np.asarray(ref["Arows"], np.int64), np.asarray(ref["Drows"], np.int64)
+    Acols, Dcols = np.asarray(ref["Acols"], np.int64), np.asarray(ref["Dcols"], np.int64)
+    Av, Dv = np.abs(np.asarray(ref["Avals"])), np.abs(np.asarray(ref["Dvals"]))
+    nA = Arows.size - 1
+    rowA = np.repeat(np.arange(nA), np.diff(Arows))
+    rowD = np.repeat(np.arange(nA), np.diff(Drows))
+    S = np.zeros(max(nA, 1))
+    if Av.size:
+        np.maximum.at(S, rowA, Av)
+        np.maximum.at(S, Acols, Av)
+    if Dv.size:
+        np.maximum.at(S, rowD, Dv)
+    Cd = np.zeros(int(Dcols.max()) + 1 if Dcols.size else 1)
+    if Dv.size:
+        np.maximum.at(Cd, Dcols, Dv)
+    floor = 1e-300
+    eA = np.abs(np.asarray(other["Avals"]) - np.asarray(ref["Avals"])) / np.maximum(np.sqrt(S[rowA] * S[Acols]), floor) if Av.size else np.zeros(1)
+    eD = np.abs(np.asarray(other["Dvals"]) - np.asarray(ref["Dvals"])) / np.maximum(np.sqrt(S[rowD] * Cd[Dcols]), floor) if Dv.size else np.zeros(1)
+    allref = np.concatenate([np.asarray(ref["Avals"]), np.asarray(ref["Dvals"])])
+    alloth = np.concatenate([np.asarray(other["Avals"]), np.asarray(other["Dvals"])])
+    fro = float(np.linalg.norm(alloth - allref) / max(np.linalg.norm(allref), floor))
+    return float(eA.max()), float(eD.max()), fro
+
+
+def magnitude_errors(ref, other, mag):
+    """max |a_ij - b_ij| / S_ij with S_ij = sum of |terms| summed into entry
+    (i,j) (oracle magnitude mode): the relative error of each entry against
+    the size of what was added up to form it, i.e. the quantity the standard
+    floating-point bound |fl(sum) - sum| <= gamma_n * sum|terms| controls."""
+    out = []
+    for v, s in (("Avals", "Aabs"), ("Dvals", "Dabs")):
+        a, b, S = np.asarray(ref[v]), np.asarray(other[v]), np.asarray(mag[s])
+        if a.size == 0:
+            out.append(0.0)
+            continue
+        floor = max(S.max(), 1e-300) * 1e-300
+        out.append(float((np.abs(a - b) / np.maximum(S, floor)).max()))
+    return out
+
+
+def check_values(ref, other, tol, mag=None):
+    """Values of A and D within tol.  With `mag` (oracle magnitude-mode
+    output for the same plan) each entry is judged against the sum of the
+    magnitudes of its terms; without it, against the symmetric row/column
+    scale (scaled_errors).  The Frobenius-relative error must also be <= tol."""
+    ea, ed, fro = scaled_errors(ref, other)
+    if mag is not None:
+        ea, ed = magnitude_errors(ref, other, mag)
+    detail = f"(A {ea:.3e}, D {ed:.3e}, Frobenius {fro:.3e})"
+    assert ea <= tol, f"A values: entry-wise error {ea:.3e} > {tol:g} {detail}"
+    assert ed <= tol, f"D values: entry-wise error {ed:.3e} > {tol:g} {detail}"
+    assert fro <= tol, f"Frobenius-relative error {fro:.3e} > {tol:g} {detail}"
     return ea, ed
 
 
-def check_rhs(ref, b, tol, unconstrained_only=False):
+def check_rhs(ref, b, tol, unconstrained_only=False, babs=None):
+    """b within tol: against the magnitude sums `babs` entry by entry when
+    given, else against max |b|."""
     rb = np.asarray(ref["b"])
     b = np.asarray(b)
     mask = np.ones(rb.size, bool)
     if unconstrained_only:
         mask[np.asarray(ref["Dinds"])] = False
-    scale = max(np.abs(rb[mask]).max() if mask.any() else 0.0, 1e-300)
-    err = float(np.abs(rb[mask] - b[mask]).max() / scale) if mask.any() else 0.0
+    if not mask.any():
+        return 0.0
+    if babs is not None:
+        babs = np.asarray(babs)[mask]
+        scale = np.maximum(babs, max(babs.max(), 1e-300) * 1e-300)
+    else:
+        scale = max(np.abs(rb[mask]).max(), 1e-300)
+    err = float((np.abs(rb[mask] - b[mask]) / scale).max())
     assert err <= tol, f"b: relative error {err:.3e} > {tol:g}"
     return err

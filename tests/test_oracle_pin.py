@@ -25,9 +25,9 @@ def tmp(tmp_path_factory):
 
 def _pin(ref, rec):
     P.check_pattern(ref, rec)
-    errs = P.check_values(ref, rec, TOL)
+    errs = P.check_values(ref, rec, TOL, mag=rec)
     if "b_raw" in rec:
-        P.check_rhs(ref, rec["b_raw"], TOL, unconstrained_only=True)
+        P.check_rhs(ref, rec["b_raw"], TOL, unconstrained_only=True, babs=rec["b_abs"])
     return errs
 
 
