@@ -249,6 +249,36 @@ int slgpu_record_rhs_group(const slgpu_ctx* ctx, int gi, slgpu_group* out, int64
 int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nnodes, const double** xyz, int* ncurvednodes,
                       int64_t* nelem, const int32_t** conn);
 
+/*
+ * Element matrices of one group without allocating device memory.
+ * This entry point has no counterpart in the reference: it exists for
+ * callers that cannot allocate GPU memory themselves -- a host application
+ * whose own allocator owns the whole device heap, or a latency-critical loop
+ * that must not pay for cudaMalloc/cudaFree -- and already hold the mesh and
+ * output buffers on the device.
+ *   g          group description in host memory, as for slgpu_matrix_add_group
+ *              (destinations are not used: no assembly happens here)
+ *   xyz        device pointer, [3*nnodes] node coordinates
+ *   conn       device pointer, [mesh_nelem*ncurvednodes] curved-node
+ *              connectivity of g->elemtype; every entry must index xyz
+ *   K          device pointer, [ntf*ndof][nelem] output: K[(i*ndof+j)*nelem+e]
+ *              = sum over terms of scale * element matrix entry (i, j) of
+ *              element e (no destination multiplier)
+ *   stream     cudaStream_t the work is queued on (0 = legacy default stream);
+ *              the call returns once the work is queued
+ *   err/errlen optional buffer for the error message
+ * Working memory is a 32 MiB array compiled into this library's device image
+ * (held on every GPU that loads the library until the process exits).
+ * Groups needing more (program, tables, per-element data and
+ * nterms*ngp*nelem doubles of coefficients) are rejected with SLGPU_E_BUDGET.
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that may run at the same time on the GPU race and must be ordered
+ * by the caller (same stream, or events).
+ */
+int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, const int32_t* conn, int64_t mesh_nelem,
+                                   double* K, void* stream, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

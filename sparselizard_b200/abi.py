@@ -88,6 +88,8 @@ SIGNATURES = {
     "slgpu_matrix_set_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
     "slgpu_matrix_work": (c_int, [c_void_p, c_int, c_void_p]),
+    "slgpu_element_matrices_noalloc": (c_int, [POINTER(Group), c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
+                                               c_char_p, c_size_t]),
     "slgpu_matrix_process": (c_int, [c_void_p, c_int, POINTER(c_uint8), c_int, POINTER(CsrInfo)]),
     "slgpu_matrix_download": (c_int, [c_void_p, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_double),
                                       POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),

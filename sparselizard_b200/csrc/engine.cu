@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 
 namespace slgpu {
@@ -1442,3 +1443,213 @@ int slgpu_record_constraints(const slgpu_ctx* ctx, int handle, int64_t* ndofs, c
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Element matrices without any device allocation.
+//
+// Some callers cannot allocate device memory: a host application whose own
+// memory manager owns the whole device heap (allocations behind its back
+// break its accounting or fail outright), or a latency-critical loop where
+// cudaMalloc/cudaFree and the device-wide synchronisation they can imply are
+// not acceptable.  For them slgpu_element_matrices_noalloc computes one
+// group's element matrices using only the caller's input/output buffers and a
+// fixed scratch array that lives in this library's device image.
+//
+// The scratch array below is file-scope and statically sized: every GPU that
+// loads this library holds kNoAllocScratchBytes of it until the process
+// exits.  All calls share it and it keeps whatever the last call left there;
+// calls whose work overlaps on the GPU (different streams, or different host
+// threads without ordering) race on it and must be serialised by the caller.
+// Nothing in it has to start at zero: every byte a call reads was written by
+// that same call first.
+namespace slgpu {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[256] = {};  // device address of the scratch, per device
+
+// Device address of the scratch array on the current device.  In host code
+// the name g_noalloc_scratch is only a host-side stand-in, not a device
+// address, so the address is looked up once per device (with that device
+// current) and kept.
+static void* noalloc_scratch_address(int* status, std::string* msg)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        cudaGetLastError();
+        *status = SLGPU_E_NODEVICE;
+        *msg = "no current CUDA device";
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (err != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            *status = SLGPU_E_CUDA;
+            *msg = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(err);
+            return nullptr;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    return g_noalloc_addr[dev];
+}
+}  // namespace slgpu
+
+extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, const int32_t* conn, int64_t mesh_nelem,
+                                              double* K, void* stream, char* err, size_t errlen)
+{
+    auto report = [&](int code, const std::string& m) {
+        if (err != nullptr && errlen > 0)
+            std::snprintf(err, errlen, "%s", m.c_str());
+        return code;
+    };
+    if (g == nullptr || xyz == nullptr || conn == nullptr || K == nullptr)
+        return report(SLGPU_E_ARG, "null argument");
+    try {
+        validate_group(*g);
+        for (int64_t e = 0; e < g->nelem; e++)
+            if (g->elems[e] < 0 || g->elems[e] >= mesh_nelem)
+                return report(SLGPU_E_ARG, "element number outside the mesh");
+        std::vector<Instr> prog = compile_program(*g, g->nterms);
+        std::vector<Tile> tiles;
+        for (int64_t e = 0; e < g->nelem;) {
+            const int o = g->orient[e];
+            if (o < 0 || o >= g->norient)
+                return report(SLGPU_E_ARG, "orientation index out of range");
+            int64_t e1 = e;
+            while (e1 < g->nelem && g->orient[e1] == o && e1 - e < kTileE) e1++;
+            tiles.push_back(Tile{(int32_t)e, (int32_t)(e1 - e), o, 0});
+            e = e1;
+        }
+        // Scratch layout: each block 256-byte aligned.
+        struct Block {
+            const void* src;
+            size_t bytes;
+            size_t off;
+        };
+        std::vector<Block> blocks;
+        size_t top = 0;
+        auto place = [&](const void* src, size_t bytes) {
+            top = (top + 255) & ~size_t(255);
+            blocks.push_back(Block{src, bytes, top});
+            top += bytes;
+            return blocks.size() - 1;
+        };
+        std::vector<int64_t> tab_off(g->ntables), field_off(g->nfielddata);
+        std::vector<int32_t> tab_rows(g->ntables);
+        int64_t tot = 0;
+        for (int k = 0; k < g->ntables; k++) {
+            tab_off[k] = tot;
+            tab_rows[k] = g->tables[k].rows;
+            tot += (int64_t)g->norient * g->tables[k].rows * g->ngp;
+        }
+        const int64_t tables_total = tot;
+        tot = 0;
+        for (int k = 0; k < g->nfielddata; k++) {
+            field_off[k] = tot;
+            tot += (int64_t)g->fieldrows[k] * g->nelem;
+        }
+        const int64_t field_total = tot;
+        std::vector<double> term_scale(g->nterms);
+        std::vector<int32_t> term_tf(g->nterms), term_dof(g->nterms);
+        for (int t = 0; t < g->nterms; t++) {
+            term_scale[t] = g->terms[t].scale;
+            term_tf[t] = g->terms[t].tf_table;
+            term_dof[t] = g->terms[t].dof_table;
+        }
+        const size_t b_prog = place(prog.data(), prog.size() * sizeof(Instr));
+        const size_t b_consts = place(g->consts, (size_t)g->nconsts * 8);
+        const size_t b_tables = place(nullptr, (size_t)tables_total * 8);
+        const size_t b_weights = place(g->weights, (size_t)g->ngp * 8);
+        const size_t b_lag = place(g->lagrange, (size_t)(1 + g->elemdim) * g->ncurvednodes * g->ngp * 8);
+        const size_t b_elems = place(g->elems, (size_t)g->nelem * 4);
+        const size_t b_orient = place(g->orient, (size_t)g->nelem * 4);
+        const size_t b_elemdata = place(nullptr, (size_t)g->nelemdata * g->nelem * 8);
+        const size_t b_field = place(nullptr, (size_t)field_total * 8);
+        const size_t b_fieldoff = place(field_off.data(), field_off.size() * 8);
+        const size_t b_taboff = place(tab_off.data(), tab_off.size() * 8);
+        const size_t b_tabrows = place(tab_rows.data(), tab_rows.size() * 4);
+        const size_t b_scale = place(term_scale.data(), term_scale.size() * 8);
+        const size_t b_ttf = place(term_tf.data(), term_tf.size() * 4);
+        const size_t b_tdof = place(term_dof.data(), term_dof.size() * 4);
+        const size_t b_tiles = place(tiles.data(), tiles.size() * sizeof(Tile));
+        const size_t b_C = place(nullptr, (size_t)g->nterms * g->ngp * g->nelem * 8);
+        if (top > kNoAllocScratchBytes)
+            return report(SLGPU_E_BUDGET, "group needs " + std::to_string(top) + " bytes of scratch; the allocation-free path has " +
+                                              std::to_string(kNoAllocScratchBytes) + " (use slgpu_matrix_* for larger groups)");
+        int status = SLGPU_OK;
+        std::string msg;
+        unsigned char* base = static_cast<unsigned char*>(noalloc_scratch_address(&status, &msg));
+        if (base == nullptr)
+            return report(status, msg);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        auto h2d = [&](size_t off, const void* src, size_t bytes) {
+            if (bytes > 0)
+                cuda_check(cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync to scratch");
+        };
+        for (const Block& b : blocks)
+            if (b.src != nullptr)
+                h2d(b.off, b.src, b.bytes);
+        for (int k = 0; k < g->ntables; k++)
+            h2d(blocks[b_tables].off + (size_t)tab_off[k] * 8, g->tables[k].vals, (size_t)g->norient * g->tables[k].rows * g->ngp * 8);
+        for (int k = 0; k < g->nelemdata; k++)
+            h2d(blocks[b_elemdata].off + (size_t)k * g->nelem * 8, g->elemdata[k], (size_t)g->nelem * 8);
+        for (int k = 0; k < g->nfielddata; k++)
+            h2d(blocks[b_field].off + (size_t)field_off[k] * 8, g->fielddata[k], (size_t)g->fieldrows[k] * g->nelem * 8);
+        if (g->nelem == 0)
+            return report(SLGPU_OK, "");
+        auto at = [&](size_t b) { return (void*)(base + blocks[b].off); };
+        CoefParams cp{};
+        cp.xyz = xyz;
+        cp.conn = conn;
+        cp.ncn = g->ncurvednodes;
+        cp.elems = (const int32_t*)at(b_elems);
+        cp.orient = (const int32_t*)at(b_orient);
+        cp.nelem = g->nelem;
+        cp.ngp = g->ngp;
+        cp.weights = (const double*)at(b_weights);
+        cp.lagrange = (const double*)at(b_lag);
+        cp.dim = g->problemdim;
+        cp.prog = (const Instr*)at(b_prog);
+        cp.nprog = (int)prog.size();
+        cp.consts = (const double*)at(b_consts);
+        cp.tables = (const double*)at(b_tables);
+        cp.tab_off = (const int64_t*)at(b_taboff);
+        cp.tab_rows = (const int32_t*)at(b_tabrows);
+        cp.elemdata = (const double*)at(b_elemdata);
+        cp.fielddata = (const double*)at(b_field);
+        cp.field_off = (const int64_t*)at(b_fieldoff);
+        cp.term_scale = (const double*)at(b_scale);
+        cp.nterms = g->nterms;
+        cp.C = (double*)at(b_C);
+        const int64_t n = g->nelem * (int64_t)g->ngp;
+        k_geometry_coef<<<grid_for(n, 128), 128, 0, s>>>(cp);
+        cuda_check(cudaGetLastError(), "k_geometry_coef");
+        ContractParams kp{};
+        kp.tables = cp.tables;
+        kp.tab_off = cp.tab_off;
+        kp.term_tf = (const int32_t*)at(b_ttf);
+        kp.term_dof = (const int32_t*)at(b_tdof);
+        kp.nterms = g->nterms;
+        kp.ngp = g->ngp;
+        kp.ntf = g->ntf;
+        kp.ndof = g->ndof;
+        kp.nelem = g->nelem;
+        kp.C = cp.C;
+        kp.tiles = (const Tile*)at(b_tiles);
+        kp.out = K;
+        const int64_t P = (int64_t)g->ntf * g->ndof;
+        dim3 grid((unsigned)tiles.size(), (unsigned)((P + kTileP - 1) / kTileP));
+        if (grid.y > 65535)
+            return report(SLGPU_E_UNSUPPORTED, "element matrix too large for the contraction grid");
+        k_contract_fp64<<<grid, dim3(16, 16), 0, s>>>(kp);
+        cuda_check(cudaGetLastError(), "k_contract_fp64");
+        return report(SLGPU_OK, "");
+    } catch (const SlgpuException& e) {
+        return report(e.e.code, e.e.msg);
+    } catch (const std::exception& e) {
+        return report(SLGPU_E_ARG, e.what());
+    }
+}
