@@ -261,7 +261,7 @@ int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nno
  *   xyz        device pointer, [3*nnodes] node coordinates
  *   conn       device pointer, [mesh_nelem*ncurvednodes] curved-node
  *              connectivity of g->elemtype; every entry must index xyz
- *   K          device pointer, [ntf*ndof][nelem] output: K[(i*ndof+j)*nelem+e]
+ *   K          device pointer, [nelem][ntf*ndof] output: K[e*ntf*ndof+i*ndof+j]
  *              = sum over terms of scale * element matrix entry (i, j) of
  *              element e (no destination multiplier)
  *   stream     cudaStream_t the work is queued on (0 = legacy default stream);

@@ -517,7 +517,8 @@ static int bits_for(int64_t n)
     return b;
 }
 
-// Builds (or fetches) the pattern for matrix M with the given constraints.
+// Builds (or fetches) the pattern for matrix M with the given constraints
+// (all-zero constraints for a right-hand side, which has one column).
 static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vector<Segment>& segs, const uint8_t* dconstr,
                                             bool rhs, uint64_t key0, uint64_t key1, bool* reused)
 {
@@ -533,7 +534,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     P->key[0] = key0;
     P->key[1] = key1;
     P->ndofs = M.ndofs;
-    int64_t ncoo = segs.empty() ? 0 : segs.back().coo_base + segs.back().count;
+    const int64_t ncoo = segs.empty() ? 0 : segs.back().coo_base + segs.back().count;
     P->ncoo = ncoo;
     if (ncoo >= (int64_t)0xFFFFFFFFll)
         fail(SLGPU_E_UNSUPPORTED, "more than 2^32-1 COO entries in one matrix");
@@ -542,7 +543,10 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     if (rowbits + colbits > 64)
         fail(SLGPU_E_UNSUPPORTED, "too many DOFs for 64-bit keys");
     const uint64_t invalid = (rowbits + colbits == 64) ? ~0ull : ((1ull << (rowbits + colbits)) - 1);
+    size_t temp = 0;
+    DevBuf tmp;
 
+    // ---- COO keys in COO order, stable radix sort on the used bits.
     DevBuf keys, keys_alt, idx, idx_alt, counter;
     keys.alloc(ctx, std::max<int64_t>(ncoo, 1) * 8);
     keys_alt.alloc(ctx, std::max<int64_t>(ncoo, 1) * 8);
@@ -550,8 +554,6 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     idx_alt.alloc(ctx, std::max<int64_t>(ncoo, 1) * 4);
     counter.alloc(ctx, 16);
     cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
-
-    // Keys in COO order.
     int si = 0;
     for (auto& g : M.groups) {
         for (int d = 0; d < g->ndests; d++, si++) {
@@ -559,18 +561,21 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
             kp.tfaddr = g->tfaddr[d].as<int32_t>();
             kp.dofaddr = rhs ? nullptr : g->dofaddr[d].as<int32_t>();
             kp.ndof = g->ndof;
+            kp.ntf = g->ntf;
             kp.nelem = g->nelem;
             kp.count = segs[si].count;
             kp.coo_base = segs[si].coo_base;
             kp.ndofs = M.ndofs;
             kp.colbits = colbits;
-            kp.constrained = rhs ? nullptr : dconstr;
+            kp.constrained = dconstr;
             kp.invalid = invalid;
             kp.keys = keys.as<unsigned long long>();
             kp.idx = idx.as<uint32_t>();
             kp.nvalid = counter.as<unsigned long long>();
-            k_group_keys<<<grid_for(kp.count, 256), 256, 0, ctx->stream>>>(kp);
-            cuda_check(cudaGetLastError(), "k_group_keys");
+            if (kp.count > 0) {
+                k_group_keys<<<grid_for(kp.count, 256), 256, 0, ctx->stream>>>(kp);
+                cuda_check(cudaGetLastError(), "k_group_keys");
+            }
         }
     }
     for (auto& f : M.frags) {
@@ -583,7 +588,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         fp.nc = f->nc;
         fp.coo_base = segs[si].coo_base;
         fp.colbits = colbits;
-        fp.constrained = rhs ? nullptr : dconstr;
+        fp.constrained = dconstr;
         fp.invalid = invalid;
         fp.keys = keys.as<unsigned long long>();
         fp.idx = idx.as<uint32_t>();
@@ -593,14 +598,10 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         cuda_check(cudaGetLastError(), "k_frag_keys");
         si++;
     }
-
-    // Stable radix sort on the used key bits.
     cub::DoubleBuffer<unsigned long long> dk(keys.as<unsigned long long>(), keys_alt.as<unsigned long long>());
     cub::DoubleBuffer<uint32_t> dv(idx.as<uint32_t>(), idx_alt.as<uint32_t>());
-    size_t temp = 0;
     cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
                "SortPairs size");
-    DevBuf tmp;
     tmp.alloc(ctx, temp);
     cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
                "SortPairs");
@@ -613,9 +614,9 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     const int64_t nvalid = (int64_t)counts_h[0];
     P->nvalid = nvalid;
     const unsigned long long* sk = dk.Current();
-    const uint32_t* sv = dv.Current();
+    const uint32_t* perm = dv.Current();
 
-    // Run heads and run indices.
+    // ---- runs (one per CSR entry).
     DevBuf head, runidx;
     head.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
     runidx.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
@@ -623,12 +624,11 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         k_run_heads<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(sk, nvalid, head.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_run_heads");
         temp = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid,
-                                                 ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid, ctx->stream),
                    "scan size");
         tmp.alloc(ctx, temp);
-        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, head.as<uint32_t>(), runidx.as<uint32_t>(),
-                                                 (int64_t)nvalid, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid,
+                                                 ctx->stream),
                    "scan");
         tmp.release();
     }
@@ -639,24 +639,19 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
     }
     const int64_t nruns = nvalid > 0 ? (int64_t)last[0] + last[1] : 0;
-    P->nruns = nruns;
-    P->perm = std::move(idx.as<uint32_t>() == sv ? idx : idx_alt);
-    P->run_start.alloc(ctx, (nruns + 1) * 4);
+    DevBuf run_start;
+    run_start.alloc(ctx, (nruns + 1) * 4);
     if (nvalid > 0) {
         k_run_starts<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid,
-                                                                     P->run_start.as<uint32_t>());
+                                                                     run_start.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_run_starts");
     }
-    uint32_t nv32 = (uint32_t)nvalid;
-    cuda_check(cudaMemcpyAsync(P->run_start.as<uint32_t>() + nruns, &nv32, 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
-    head.release();
-    runidx.release();
 
-    // Local renumbering of constrained / unconstrained DOFs.
-    DevBuf renum, isA_dof;
+    // ---- local renumbering of constrained / unconstrained DOFs.
+    DevBuf renum;
     renum.alloc(ctx, std::max<int64_t>(M.ndofs, 1) * 4);
-    int64_t nA = M.ndofs, nD = 0;
-    if (!rhs) {
+    int64_t nA = 0, nD = 0;
+    {
         DevBuf flagsA, scanA, flagsD, scanD;
         flagsA.alloc(ctx, (M.ndofs + 1) * 4);
         flagsD.alloc(ctx, (M.ndofs + 1) * 4);
@@ -670,11 +665,11 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
                                                  ctx->stream),
                    "scan size");
         tmp.alloc(ctx, temp);
-        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(),
-                                                 (int64_t)M.ndofs + 1, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(), (int64_t)M.ndofs + 1,
+                                                 ctx->stream),
                    "scan");
-        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsD.as<uint32_t>(), scanD.as<uint32_t>(),
-                                                 (int64_t)M.ndofs + 1, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsD.as<uint32_t>(), scanD.as<uint32_t>(), (int64_t)M.ndofs + 1,
+                                                 ctx->stream),
                    "scan");
         tmp.release();
         uint32_t tot[2];
@@ -690,38 +685,28 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     P->nA = nA;
     P->nD = nD;
 
-    // Classify runs into A / D, slots, row counts.
-    P->run_target.alloc(ctx, std::max<int64_t>(nruns, 1) * 4);
-    if (rhs) {
-        P->run_row.alloc(ctx, std::max<int64_t>(nruns, 1) * 4);
-        if (nruns > 0) {
-            k_rhs_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns,
-                                                                      P->run_row.as<int32_t>(), P->run_target.as<int32_t>());
-            cuda_check(cudaGetLastError(), "k_rhs_runs");
-        }
-        P->nnzA = nruns;
-    } else {
-        DevBuf isA, slotA, slotD, isD;
+    // ---- A / D classification, CSR structure, slot of every run.
+    DevBuf run_target;
+    run_target.alloc(ctx, std::max<int64_t>(nruns, 1) * 4);
+    {
+        DevBuf isA, slotA, slotD, isD, rowcA, rowcD;
         isA.alloc(ctx, (nruns + 1) * 4);
         isD.alloc(ctx, (nruns + 1) * 4);
         slotA.alloc(ctx, (nruns + 1) * 4);
         slotD.alloc(ctx, (nruns + 1) * 4);
-        DevBuf rowcA, rowcD;
         rowcA.alloc(ctx, (nA + 1) * 4);
         rowcD.alloc(ctx, (nA + 1) * 4);
         cuda_check(cudaMemsetAsync(rowcA.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
         cuda_check(cudaMemsetAsync(rowcD.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
-        k_classify_runs<<<grid_for(nruns + 1, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns, colbits, dconstr,
+        k_classify_runs<<<grid_for(nruns + 1, 256), 256, 0, ctx->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, dconstr,
                                                                             renum.as<int32_t>(), isA.as<uint32_t>(), isD.as<uint32_t>(),
                                                                             rowcA.as<uint32_t>(), rowcD.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_classify_runs");
         temp = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1,
-                                                 ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1, ctx->stream),
                    "scan size");
         size_t temp2 = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp2, rowcA.as<uint32_t>(), rowcA.as<uint32_t>(), (int64_t)nA + 1,
-                                                 ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp2, rowcA.as<uint32_t>(), rowcA.as<uint32_t>(), (int64_t)nA + 1, ctx->stream),
                    "scan size");
         temp = std::max(temp, temp2);
         tmp.alloc(ctx, temp);
@@ -751,16 +736,149 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         P->Acols.alloc(ctx, std::max<int64_t>(P->nnzA, 1) * 4);
         P->Dcols.alloc(ctx, std::max<int64_t>(P->nnzD, 1) * 4);
         if (nruns > 0) {
-            k_fill_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, P->run_start.as<uint32_t>(), nruns, colbits, isA.as<uint32_t>(),
+            k_fill_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, isA.as<uint32_t>(),
                                                                         slotA.as<uint32_t>(), slotD.as<uint32_t>(), renum.as<int32_t>(),
-                                                                        P->run_target.as<int32_t>(), P->Acols.as<int32_t>(),
+                                                                        run_target.as<int32_t>(), P->Acols.as<int32_t>(),
                                                                         P->Dcols.as<int32_t>());
             cuda_check(cudaGetLastError(), "k_fill_runs");
         }
     }
+    run_start.release();
+
+    // ---- slot map: position of each kept COO entry inside its row segment.
+    P->slotmap.alloc(ctx, std::max<int64_t>(ncoo, 1) * 2);
+    cuda_check(cudaMemsetAsync(P->slotmap.as<void>(), 0xFF, std::max<int64_t>(ncoo, 1) * 2, ctx->stream), "memset slotmap");
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+    std::vector<CooSeg> csegs;
+    {
+        size_t s = 0;
+        for (auto& g : M.groups)
+            for (int d = 0; d < g->ndests; d++, s++) csegs.push_back(CooSeg{segs[s].coo_base, (int64_t)std::max(1, g->ndof)});
+        for (size_t f = 0; f < M.frags.size(); f++, s++) csegs.push_back(CooSeg{segs[s].coo_base, 1});
+    }
+    DevBuf dcsegs, dup;
+    upload(ctx, dcsegs, csegs);
+    dup.alloc(ctx, std::max<int64_t>(ncoo, 1));
+    cuda_check(cudaMemsetAsync(dup.as<void>(), 0, std::max<int64_t>(ncoo, 1), ctx->stream), "memset dup");
+    if (nvalid > 0) {
+        k_slotmap<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(sk, perm, head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid, colbits,
+                                                                  run_target.as<int32_t>(), renum.as<int32_t>(), P->Arows.as<uint32_t>(),
+                                                                  P->Drows.as<uint32_t>(), P->slotmap.as<int16_t>(),
+                                                                  counter.as<unsigned long long>(), dcsegs.as<CooSeg>(), (int)csegs.size(),
+                                                                  dup.as<uint8_t>());
+        cuda_check(cudaGetLastError(), "k_slotmap");
+    }
+    head.release();
+    runidx.release();
+    run_target.release();
     keys.release();
     keys_alt.release();
-    (P->perm.as<uint32_t>() == idx.as<uint32_t>() ? idx_alt : idx).release();
+    idx.release();
+    idx_alt.release();
+
+    // ---- incidences: element-matrix rows (or fragment entries) grouped by row.
+    std::vector<IncSeg> isegs;
+    int64_t ninc_total = 0;
+    si = 0;
+    for (auto& g : M.groups) {
+        for (int d = 0; d < g->ndests; d++, si++) {
+            IncSeg s{};
+            s.inc_base = ninc_total;
+            s.count = g->nelem * (int64_t)g->ntf;
+            s.coo_base = segs[si].coo_base;
+            s.val_base = segs[si].val_base;
+            s.mult = segs[si].mult;
+            s.width = g->ndof;
+            s.ntf = g->ntf;
+            s.kind = 0;
+            s.nelem = g->nelem;
+            s.rows = g->tfaddr[d].as<int32_t>();
+            isegs.push_back(s);
+            ninc_total += s.count;
+        }
+    }
+    for (auto& f : M.frags) {
+        IncSeg s{};
+        s.inc_base = ninc_total;
+        s.count = (int64_t)f->nr * f->nc;
+        s.coo_base = segs[si].coo_base;
+        s.val_base = segs[si].val_base;
+        s.mult = 1.0;
+        s.width = 1;
+        s.kind = 1;
+        s.ntr = f->ntr;
+        s.ndr = f->ndr;
+        s.nr = f->nr;
+        s.nc = f->nc;
+        s.rows = f->rows.as<int32_t>();
+        s.cols = f->cols.as<int32_t>();
+        isegs.push_back(s);
+        ninc_total += s.count;
+        si++;
+    }
+    if (ninc_total >= (int64_t)0xFFFFFFFFll)
+        fail(SLGPU_E_UNSUPPORTED, "more than 2^32-1 element-matrix rows in one matrix");
+    DevBuf disegs;
+    upload(ctx, disegs, isegs);
+    DevBuf ikeys, ikeys_alt, iids, iids_alt;
+    ikeys.alloc(ctx, std::max<int64_t>(ninc_total, 1) * 4);
+    ikeys_alt.alloc(ctx, std::max<int64_t>(ninc_total, 1) * 4);
+    iids.alloc(ctx, std::max<int64_t>(ninc_total, 1) * 4);
+    iids_alt.alloc(ctx, std::max<int64_t>(ninc_total, 1) * 4);
+    for (size_t s = 0; s < isegs.size(); s++) {
+        if (isegs[s].count == 0)
+            continue;
+        k_inc_keys<<<grid_for(isegs[s].count, 256), 256, 0, ctx->stream>>>(disegs.as<IncSeg>(), (int)s, dconstr, M.ndofs,
+                                                                          ikeys.as<uint32_t>(), iids.as<uint32_t>(),
+                                                                          counter.as<unsigned long long>() + 1);
+        cuda_check(cudaGetLastError(), "k_inc_keys");
+    }
+    cub::DoubleBuffer<uint32_t> ik(ikeys.as<uint32_t>(), ikeys_alt.as<uint32_t>());
+    cub::DoubleBuffer<uint32_t> iv(iids.as<uint32_t>(), iids_alt.as<uint32_t>());
+    temp = 0;
+    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->stream), "SortPairs size");
+    tmp.alloc(ctx, temp);
+    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->stream), "SortPairs");
+    tmp.release();
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    if (counts_h[0] != 0)
+        fail(SLGPU_E_UNSUPPORTED, "a CSR row is longer than 32767 entries");
+    const int64_t ninc = (int64_t)counts_h[1];
+    P->ninc = ninc;
+    P->inc.alloc(ctx, std::max<int64_t>(ninc, 1) * 8);
+    DevBuf rowcount;
+    rowcount.alloc(ctx, (nA + 1) * 4);
+    cuda_check(cudaMemsetAsync(rowcount.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
+    if (isegs.size() >= (size_t(1) << 23))
+        fail(SLGPU_E_UNSUPPORTED, "too many element groups and fragments in one matrix");
+    if (ninc > 0) {
+        k_inc_finalize<<<grid_for(ninc, 256), 256, 0, ctx->stream>>>(ik.Current(), iv.Current(), ninc, disegs.as<IncSeg>(),
+                                                                     (int)isegs.size(), renum.as<int32_t>(), dup.as<uint8_t>(),
+                                                                     P->inc.as<unsigned long long>(), rowcount.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "k_inc_finalize");
+    }
+    dup.release();
+    P->inc_ptr.alloc(ctx, (nA + 1) * 4);
+    temp = 0;
+    cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, rowcount.as<uint32_t>(), P->inc_ptr.as<uint32_t>(), (int64_t)nA + 1, ctx->stream),
+               "scan size");
+    tmp.alloc(ctx, temp);
+    cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcount.as<uint32_t>(), P->inc_ptr.as<uint32_t>(), (int64_t)nA + 1,
+                                             ctx->stream),
+               "scan");
+    tmp.release();
+    // Longest row.
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+    if (nA > 0) {
+        k_max_rowlen<<<grid_for(nA, 256), 256, 0, ctx->stream>>>(P->Arows.as<uint32_t>(), P->Drows.as<uint32_t>(), nA,
+                                                                   counter.as<unsigned long long>());
+        cuda_check(cudaGetLastError(), "k_max_rowlen");
+    }
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    P->lmax = (int)counts_h[0];
+
     P->last_use = ++ctx->use_clock;
     ctx->patterns.push_back(P);
     // Keep at most 8 resident patterns (least recently used evicted).
@@ -788,35 +906,34 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     int64_t total_vals = 0;
     std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
 
-    // Constraints on the device (reused buffer keyed by content).
     // Constraints: device copy and content key, both reused while the array
-    // is byte-identical to the previous call's.
-    uint64_t ckey[2] = {0, 0};
-    const uint8_t* dconstr_ptr = nullptr;
-    if (!rhs) {
-        const bool same = ctx->constr_host.size() == (size_t)M.ndofs &&
-                          std::memcmp(ctx->constr_host.data(), isconstrained, (size_t)M.ndofs) == 0;
-        if (!same) {
-            ctx->constr_host.assign(isconstrained, isconstrained + M.ndofs);
-            ctx->constr_dev.alloc(ctx, (size_t)M.ndofs + 1);
-            cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), isconstrained, M.ndofs, cudaMemcpyHostToDevice, ctx->stream),
-                       "H2D constr");
-            std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
-            std::memcpy(packed.data(), isconstrained, M.ndofs);
-            uint64_t a = 0x12345, b = 0x6789;
-            for (size_t i = 0; i < packed.size(); i++) {
-                a = mix64(a ^ (uint64_t)(uint32_t)packed[i] ^ (uint64_t)i << 32);
-                b += mix64((uint64_t)(uint32_t)packed[i] * 0x100000001b3ull + i);
-            }
-            ctx->constr_key[0] = a;
-            ctx->constr_key[1] = b;
-        }
-        ckey[0] = ctx->constr_key[0];
-        ckey[1] = ctx->constr_key[1];
-        dconstr_ptr = ctx->constr_dev.as<uint8_t>();
+    // is byte-identical to the previous call's.  A right-hand side uses an
+    // all-zero array (every row kept).
+    const uint8_t* hconstr = isconstrained;
+    std::vector<uint8_t> zeros;
+    if (rhs) {
+        zeros.assign((size_t)M.ndofs, 0);
+        hconstr = zeros.data();
     }
-    uint64_t key0 = mix64(ckey[0] ^ (uint64_t)M.ndofs ^ (rhs ? 0xABCDEFull : 0));
-    uint64_t key1 = mix64(ckey[1] ^ (uint64_t)segs.size());
+    const bool same = ctx->constr_host.size() == (size_t)M.ndofs &&
+                      std::memcmp(ctx->constr_host.data(), hconstr, (size_t)M.ndofs) == 0;
+    if (!same) {
+        ctx->constr_host.assign(hconstr, hconstr + M.ndofs);
+        ctx->constr_dev.alloc(ctx, (size_t)M.ndofs + 1);
+        cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), hconstr, M.ndofs, cudaMemcpyHostToDevice, ctx->stream), "H2D constr");
+        std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
+        std::memcpy(packed.data(), hconstr, M.ndofs);
+        uint64_t a = 0x12345, b = 0x6789;
+        for (size_t i = 0; i < packed.size(); i++) {
+            a = mix64(a ^ (uint64_t)(uint32_t)packed[i] ^ (uint64_t)i << 32);
+            b += mix64((uint64_t)(uint32_t)packed[i] * 0x100000001b3ull + i);
+        }
+        ctx->constr_key[0] = a;
+        ctx->constr_key[1] = b;
+    }
+    const uint8_t* dconstr = ctx->constr_dev.as<uint8_t>();
+    uint64_t key0 = mix64(ctx->constr_key[0] ^ (uint64_t)M.ndofs ^ (rhs ? 0xABCDEFull : 0));
+    uint64_t key1 = mix64(ctx->constr_key[1] ^ (uint64_t)segs.size());
     for (auto& g : M.groups) {
         key0 = mix64(key0 ^ g->addr_hash[0]);
         key1 = mix64(key1 + g->addr_hash[1]);
@@ -833,12 +950,12 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     for (auto& g : M.groups) maxC = std::max<int64_t>(maxC, (int64_t)g->nterms * g->ngp * g->nelem);
     DevBuf C;
     C.alloc(ctx, std::max<int64_t>(maxC, 1) * 8);
-    size_t gi = 0;
     while (ctx->evpool.size() < 3 * M.groups.size()) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         ctx->evpool.push_back(e);
     }
+    size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
             CoefParams cp = coef_params(ctx, *g, C.as<double>());
@@ -862,9 +979,9 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             kp.tiles = g->tiles_d.as<Tile>();
             kp.out = M.vals.as<double>() + gvb[gi];
             const int64_t P = (int64_t)g->ntf * g->ndof;
-            dim3 grid((unsigned)g->tiles.size(), (unsigned)((P + kTileP - 1) / kTileP));
+            dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
             if (grid.y > 65535)
-                fail(SLGPU_E_UNSUPPORTED, "element matrix too large for the contraction grid");
+                fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
             k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
             ctx->launches++;
@@ -873,7 +990,6 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         gi++;
     }
     C.release();
-    // Fragment values.
     {
         int64_t vb = 0;
         for (auto& g : M.groups) vb += (int64_t)g->ntf * g->ndof * g->nelem;
@@ -889,34 +1005,50 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
 
     // 3: pattern.
     bool reused = false;
-    M.pattern = get_pattern(ctx, M, segs, dconstr_ptr, rhs, key0, key1, &reused);
+    M.pattern = get_pattern(ctx, M, segs, dconstr, rhs, key0, key1, &reused);
     Pattern& P = *M.pattern;
     ev_record(ctx, 2);
 
-    // 4: values.
-    DevBuf dsegs;
-    upload(ctx, dsegs, segs);
+    // 4: values, one warp per row.
+    std::vector<RowSeg> rsegs(segs.size());
+    {
+        size_t s = 0;
+        for (auto& g : M.groups)
+            for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
+        for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
+    }
+    DevBuf drsegs;
+    upload(ctx, drsegs, rsegs);
     if (rhs) {
         M.Avals.alloc(ctx, (size_t)std::max<int64_t>(M.ndofs, 1) * 8);
-        cuda_check(cudaMemsetAsync(M.Avals.as<void>(), 0, (size_t)M.ndofs * 8, ctx->stream), "memset");
     } else {
         M.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
         M.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
     }
-    if (P.nruns > 0) {
-        ValueParams vp{};
-        vp.perm = P.perm.as<uint32_t>();
-        vp.run_start = P.run_start.as<uint32_t>();
-        vp.run_target = rhs ? P.run_row.as<int32_t>() : P.run_target.as<int32_t>();
-        vp.nruns = P.nruns;
-        vp.segs = dsegs.as<Segment>();
-        vp.nsegs = (int)segs.size();
-        vp.vals = M.vals.as<double>();
-        vp.Avals = M.Avals.as<double>();
-        vp.Dvals = rhs ? nullptr : M.Dvals.as<double>();
-        vp.negate = rhs ? 1 : 0;
-        k_csr_values<<<grid_for(P.nruns, 256), 256, 0, ctx->stream>>>(vp);
-        cuda_check(cudaGetLastError(), "k_csr_values");
+    if (P.nA > 0) {
+        RowParams rp{};
+        rp.inc_ptr = P.inc_ptr.as<uint32_t>();
+        rp.inc = P.inc.as<unsigned long long>();
+        rp.segs = drsegs.as<RowSeg>();
+        rp.slotmap = P.slotmap.as<int16_t>();
+        rp.vals = M.vals.as<double>();
+        rp.Arows = P.Arows.as<uint32_t>();
+        rp.Drows = P.Drows.as<uint32_t>();
+        rp.nrows = P.nA;
+        rp.lmax = std::max(1, P.lmax);
+        rp.Avals = M.Avals.as<double>();
+        rp.Dvals = rhs ? nullptr : M.Dvals.as<double>();
+        rp.dense = rhs ? M.Avals.as<double>() : nullptr;
+        const size_t per_warp = (size_t)rp.lmax * 8;
+        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
+        size_t smem = per_warp * wpb;
+        if (smem > 48 * 1024) {
+            if (smem > 227 * 1024)
+                fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
+            cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        }
+        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->stream>>>(rp);
+        cuda_check(cudaGetLastError(), "k_row_values");
         ctx->launches++;
     }
     ev_record(ctx, 3);
@@ -1641,9 +1773,9 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
         kp.tiles = (const Tile*)at(b_tiles);
         kp.out = K;
         const int64_t P = (int64_t)g->ntf * g->ndof;
-        dim3 grid((unsigned)tiles.size(), (unsigned)((P + kTileP - 1) / kTileP));
+        dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)tiles.size());
         if (grid.y > 65535)
-            return report(SLGPU_E_UNSUPPORTED, "element matrix too large for the contraction grid");
+            return report(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
         k_contract_fp64<<<grid, dim3(16, 16), 0, s>>>(kp);
         cuda_check(cudaGetLastError(), "k_contract_fp64");
         return report(SLGPU_OK, "");

@@ -103,14 +103,16 @@ struct FragmentDev {
 };
 
 // Resident COO -> CSR mapping (pattern), reusable while addresses and
-// constraints are unchanged.
+// constraints are unchanged.  The numeric phase only needs the CSR structure,
+// the per-row incidence lists and the slot map.
 struct Pattern {
     uint64_t key[2] = {0, 0};
-    int64_t ndofs = 0, nA = 0, nD = 0, nnzA = 0, nnzD = 0, ncoo = 0, nvalid = 0, nruns = 0;
-    DevBuf perm;       // uint32 [nvalid]: sorted position -> COO index
-    DevBuf run_start;  // uint32 [nruns+1]
-    DevBuf run_target; // int32 [nruns]: >= 0 A slot, < 0 D slot -(s+1)
-    DevBuf Arows, Acols, Drows, Dcols, run_row;  // run_row (rhs): dof per run
+    int64_t ndofs = 0, nA = 0, nD = 0, nnzA = 0, nnzD = 0, ncoo = 0, nvalid = 0, ninc = 0;
+    int lmax = 0;          // longest row (A and D entries)
+    DevBuf Arows, Acols, Drows, Dcols;
+    DevBuf slotmap;        // int16 [ncoo]: position in the row's [A | D] segment, -1 = dropped
+    DevBuf inc_ptr;        // uint32 [nA+1]: incidences of each row
+    DevBuf inc;            // uint64 [ninc]: segment << 40 | COO index of the incidence's first entry
     uint64_t last_use = 0;
 };
 

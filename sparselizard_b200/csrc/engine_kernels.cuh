@@ -161,19 +161,22 @@ struct ContractParams {
     int64_t nelem;
     const double* C;
     const Tile* tiles;
-    double* out;  // [ntf*ndof][nelem]
+    double* out;  // [nelem][ntf*ndof]
 };
 
-// FP64 contraction: out[p][e] = sum_q M[p][q] C[q][e] with
+// FP64 contraction: out[e][p] = sum_q M[p][q] C[q][e] with
 // M[(i,j)][(t,g)] = T_t[o][i][g] * D_t[o][j][g] built in shared memory per
 // tile (o = the tile's orientation).  Block 16x16 threads, 64 p x 64 e tile,
-// each thread 4 x 4 outputs strided by 16.
+// each thread 4 x 4 outputs strided by 16; the tile is transposed through
+// shared memory so that the element-major output rows are written whole.
+// Grid: x = p tiles (adjacent blocks share the C columns in L2), y = tiles.
 __global__ void __launch_bounds__(256) k_contract_fp64(ContractParams p)
 {
-    __shared__ double Ms[kTileQ][kTileP];
-    __shared__ double Cs[kTileQ][kTileE];
-    const Tile tile = p.tiles[blockIdx.x];
-    const int p0 = blockIdx.y * kTileP;
+    __shared__ double sm[kTileE * (kTileP + 1)];
+    double(*Ms)[kTileP] = reinterpret_cast<double(*)[kTileP]>(sm);
+    double(*Cs)[kTileE] = reinterpret_cast<double(*)[kTileE]>(sm + kTileQ * kTileP);
+    const Tile tile = p.tiles[blockIdx.y];
+    const int p0 = blockIdx.x * kTileP;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 16 + tx;
     const int P = p.ntf * p.ndof;
     const int Q = p.nterms * p.ngp;
@@ -222,27 +225,28 @@ __global__ void __launch_bounds__(256) k_contract_fp64(ContractParams p)
         }
         __syncthreads();
     }
+    // Transpose through shared memory: Out[e][p].
+    double(*Out)[kTileP + 1] = reinterpret_cast<double(*)[kTileP + 1]>(sm);
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int pe = p0 + ty + 16 * i;
-        if (pe >= P)
-            continue;
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int ee = tx + 16 * j;
-            if (ee < tile.ne)
-                p.out[(int64_t)pe * p.nelem + tile.e0 + ee] = acc[i][j];
-        }
+        for (int j = 0; j < 4; j++) Out[tx + 16 * j][ty + 16 * i] = acc[i][j];
+    __syncthreads();
+    const int pw = min(kTileP, P - p0);
+    for (int idx = tid; idx < kTileE * kTileP; idx += 256) {
+        const int ee = idx / kTileP, pp = idx % kTileP;
+        if (ee < tile.ne && pp < pw)
+            p.out[(int64_t)(tile.e0 + ee) * P + p0 + pp] = Out[ee][pp];
     }
 }
 
 struct KeyParams {
     const int32_t* tfaddr;
     const int32_t* dofaddr;  // null: right-hand side (column 0)
-    int ndof;
+    int ndof, ntf;
     int64_t nelem, count, coo_base, ndofs;
     int colbits;
-    const uint8_t* constrained;  // null: keep constrained rows
+    const uint8_t* constrained;
     unsigned long long invalid;
     unsigned long long* keys;
     uint32_t* idx;
@@ -256,15 +260,17 @@ __device__ __forceinline__ void count_valid(unsigned long long* ctr, bool valid)
         atomicAdd(ctr, (unsigned long long)__popc(mask));
 }
 
-// COO keys of one (group, destination) block in COO order (p-major, element
-// minor), with the drop rules of rawmat::process (src/formulation/rawmat.cpp:162):
-// negative row or column address, or a constrained row.
+// COO keys of one (group, destination) block in COO order (element-major:
+// e, then i*ndof+j), with the drop rules of rawmat::process
+// (src/formulation/rawmat.cpp:162): negative row or column address, or a
+// constrained row.
 __global__ void k_group_keys(KeyParams p)
 {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     bool valid = false;
     if (k < p.count) {
-        const int64_t pe = k / p.nelem, e = k - pe * p.nelem;
+        const int64_t P = (int64_t)p.ntf * p.ndof;
+        const int64_t e = k / P, pe = k - e * P;
         const int64_t i = pe / p.ndof, j = pe - i * p.ndof;
         const int row = p.tfaddr[i * p.nelem + e];
         const int col = p.dofaddr ? p.dofaddr[j * p.nelem + e] : 0;
@@ -291,18 +297,26 @@ struct FragKeyParams {
     unsigned long long* nvalid;
 };
 
+__device__ __forceinline__ void frag_decode(int64_t k, int ntr, int ndr, int nr, int64_t nc, int64_t* ctr, int64_t* cdr, int64_t* c)
+{
+    const int64_t r = k / nc;
+    *c = k - r * nc;
+    *ctr = r;
+    *cdr = r;
+    if (ntr != nr || ndr != nr) {
+        *ctr = r / ndr;
+        *cdr = r % ndr;
+    }
+}
+
 // Raw fragments decode rows as rawmat::process does (rawmat.cpp:150-155).
 __global__ void k_frag_keys(FragKeyParams p)
 {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     bool valid = false;
     if (k < (int64_t)p.nr * p.nc) {
-        const int64_t r = k / p.nc, c = k - r * p.nc;
-        int64_t ctr = r, cdr = r;
-        if (p.ntr != p.nr || p.ndr != p.nr) {
-            ctr = r / p.ndr;
-            cdr = r % p.ndr;
-        }
+        int64_t ctr, cdr, c;
+        frag_decode(k, p.ntr, p.ndr, p.nr, p.nc, &ctr, &cdr, &c);
         const int row = p.rows[ctr * p.nc + c];
         const int col = p.cols[cdr * p.nc + c];
         bool bad = row >= p.ndofs || col >= p.ndofs;
@@ -348,15 +362,6 @@ __global__ void k_renumber(const uint8_t* c, int64_t ndofs, const uint32_t* sA, 
         renum[i] = c[i] ? (int32_t)sD[i] : (int32_t)sA[i];
 }
 
-__global__ void k_rhs_runs(const unsigned long long* sk, const uint32_t* run_start, int64_t nruns, int32_t* run_row, int32_t* run_target)
-{
-    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r < nruns) {
-        run_row[r] = (int32_t)sk[run_start[r]];
-        run_target[r] = (int32_t)r;
-    }
-}
-
 __global__ void k_classify_runs(const unsigned long long* sk, const uint32_t* run_start, int64_t nruns, int colbits, const uint8_t* c,
                                 const int32_t* renum, uint32_t* isA, uint32_t* isD, uint32_t* rowcA, uint32_t* rowcD)
 {
@@ -397,48 +402,226 @@ __global__ void k_fill_runs(const unsigned long long* sk, const uint32_t* run_st
     }
 }
 
-struct ValueParams {
-    const uint32_t* perm;
-    const uint32_t* run_start;
-    const int32_t* run_target;
-    int64_t nruns;
-    const Segment* segs;
-    int nsegs;
-    const double* vals;
-    double* Avals;
-    double* Dvals;
-    int negate;
+// Position of every kept COO entry inside its row's value segment
+// ([A part | D part]); entries that are dropped keep -1.
+// runidx is the exclusive scan of the run heads, so position k belongs to
+// run runidx[k] + head[k] - 1 (a head starts its own run; any other
+// position's exclusive count already includes its run's head).
+// COO segment bounds used to tell which incidence (element-matrix row) a COO
+// entry belongs to.
+struct CooSeg {
+    int64_t coo_base;
+    int64_t width;
 };
 
-// One CSR entry per thread: its COO contributions in sorted order (stable
-// sort keeps COO order within a (row, col)), summed in FP64.
-__global__ void k_csr_values(ValueParams p)
+__device__ __forceinline__ int64_t incidence_of(const CooSeg* segs, int nsegs, int64_t coo, int* seg)
+{
+    int lo = 0, hi = nsegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].coo_base <= coo)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    *seg = lo;
+    return (coo - segs[lo].coo_base) / segs[lo].width;
+}
+
+// Also flags (dup[coo] = 1) an entry that falls on the same CSR entry as the
+// previous entry of its own incidence -- two dof functions of one element
+// with the same address.  Within a run entries keep COO order and the
+// entries of one incidence are contiguous in COO order, so such pairs are
+// adjacent.
+__global__ void k_slotmap(const unsigned long long* sk, const uint32_t* perm, const uint32_t* head, const uint32_t* runidx, int64_t nvalid,
+                          int colbits, const int32_t* run_target, const int32_t* renum, const uint32_t* Arows, const uint32_t* Drows,
+                          int16_t* slotmap, unsigned long long* overflow, const CooSeg* csegs, int ncsegs, uint8_t* dup)
+{
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= nvalid)
+        return;
+    if (k > 0 && head[k] == 0) {
+        int sa, sb;
+        const int64_t ia = incidence_of(csegs, ncsegs, perm[k], &sa);
+        const int64_t ib = incidence_of(csegs, ncsegs, perm[k - 1], &sb);
+        if (sa == sb && ia == ib)
+            dup[perm[k]] = 1;
+    }
+    const int64_t row = (int64_t)(sk[k] >> colbits);
+    const int32_t lr = renum[row];
+    const int32_t t = run_target[(int64_t)runidx[k] + head[k] - 1];
+    int64_t off;
+    if (t >= 0)
+        off = (int64_t)t - Arows[lr];
+    else
+        off = (int64_t)(Arows[lr + 1] - Arows[lr]) + (-(int64_t)t - 1 - Drows[lr]);
+    if (off > 32767) {
+        atomicAdd(overflow, 1ull);
+        off = -1;
+    }
+    slotmap[perm[k]] = (int16_t)off;
+}
+
+// One incidence = one (segment, element, test function) row of an element
+// matrix (width ndof), or one raw fragment entry (width 1).
+struct IncSeg {
+    int64_t inc_base;  // first incidence id of the segment
+    int64_t count;     // incidences in the segment
+    int64_t coo_base;  // first COO index of the segment
+    int64_t val_base;  // first value of the segment in the value buffer
+    double mult;       // destination multiplier
+    int32_t width;     // entries per incidence (ndof, or 1 for fragments)
+    int32_t ntf;       // group segments: test functions per element
+    int32_t kind;      // 0 group, 1 fragment
+    int32_t ntr, ndr, nr;
+    int64_t nelem, nc;
+    const int32_t* rows;  // group: tfaddr [ntf][nelem]; fragment: rows
+    const int32_t* cols;  // fragment: cols
+};
+
+__global__ void k_inc_keys(const IncSeg* segs, int s, const uint8_t* constrained, int64_t ndofs, uint32_t* keys, uint32_t* ids,
+                           unsigned long long* nvalid)
+{
+    const IncSeg sg = segs[s];
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool valid = false;
+    if (k < sg.count) {
+        int row;
+        if (sg.kind == 0) {
+            const int64_t e = k / sg.ntf, i = k - e * sg.ntf;
+            row = sg.rows[i * sg.nelem + e];
+        } else {
+            int64_t ctr, cdr, c;
+            frag_decode(k, sg.ntr, sg.ndr, sg.nr, sg.nc, &ctr, &cdr, &c);
+            row = sg.rows[ctr * sg.nc + c];
+            if (sg.cols[cdr * sg.nc + c] < 0)
+                row = -1;
+        }
+        valid = row >= 0 && row < ndofs && !constrained[row];
+        keys[sg.inc_base + k] = valid ? (uint32_t)row : 0xFFFFFFFFu;
+        ids[sg.inc_base + k] = (uint32_t)(sg.inc_base + k);
+    }
+    count_valid(nvalid, valid);
+}
+
+// inc[k] = (serial << 63) | (segment << 40) | COO index of the incidence's
+// first entry; serial marks an incidence with repeated addresses, whose
+// entries must be added one after the other.
+__global__ void k_inc_finalize(const uint32_t* skeys, const uint32_t* sids, int64_t ninc, const IncSeg* segs, int nsegs,
+                               const int32_t* renum, const uint8_t* dup, unsigned long long* inc, uint32_t* rowcount)
+{
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= ninc)
+        return;
+    const int64_t id = sids[k];
+    int lo = 0, hi = nsegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].inc_base <= id)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const IncSeg& sg = segs[lo];
+    const int64_t local = id - sg.inc_base;
+    int64_t coo;
+    if (sg.kind == 0) {
+        const int64_t e = local / sg.ntf, i = local - e * sg.ntf;
+        coo = sg.coo_base + e * (int64_t)sg.ntf * sg.width + i * sg.width;
+    } else {
+        coo = sg.coo_base + local;
+    }
+    unsigned long long serial = 0;
+    for (int j = 0; j < sg.width; j++) serial |= dup[coo + j];
+    inc[k] = (serial << 63) | ((unsigned long long)lo << 40) | (unsigned long long)coo;
+    atomicAdd(&rowcount[renum[skeys[k]]], 1u);
+}
+
+__global__ void k_max_rowlen(const uint32_t* Arows, const uint32_t* Drows, int64_t nrows, unsigned long long* out)
 {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r >= p.nruns)
+    unsigned long long len = 0;
+    if (r < nrows)
+        len = (unsigned long long)(Arows[r + 1] - Arows[r]) + (unsigned long long)(Drows[r + 1] - Drows[r]);
+    for (int off = 16; off > 0; off >>= 1) len = max(len, __shfl_down_sync(0xffffffffu, len, off));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(out, len);
+}
+
+struct RowSeg {
+    int64_t coo_base;
+    int64_t val_base;
+    double mult;
+    int32_t width, pad;
+};
+
+struct RowParams {
+    const uint32_t* inc_ptr;
+    const unsigned long long* inc;
+    const RowSeg* segs;
+    const int16_t* slotmap;
+    const double* vals;
+    const uint32_t* Arows;
+    const uint32_t* Drows;
+    int64_t nrows;
+    int lmax;
+    double* Avals;
+    double* Dvals;
+    double* dense;  // right-hand side: dense[row] = -value (Avals unused)
+};
+
+// CSR values, one warp per row: the row's incidences are visited in a fixed
+// order and each adds its element-matrix row (contiguous in the element-major
+// value buffer) into a shared-memory copy of the row through the slot map.
+// Within one incidence every lane hits a different slot, so the sum of each
+// CSR entry is formed in incidence order: deterministic, no atomics.
+__global__ void k_row_values(RowParams p)
+{
+    extern __shared__ double rowbuf[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (r >= p.nrows)
         return;
-    const uint32_t s = p.run_start[r], t = p.run_start[r + 1];
-    double acc = 0;
-    for (uint32_t k = s; k < t; k++) {
-        const int64_t coo = p.perm[k];
-        int lo = 0, hi = p.nsegs - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (p.segs[mid].coo_base <= coo)
-                lo = mid;
-            else
-                hi = mid - 1;
+    double* buf = rowbuf + (int64_t)warp * p.lmax;
+    const int la = (int)(p.Arows[r + 1] - p.Arows[r]);
+    const int ld = p.Drows ? (int)(p.Drows[r + 1] - p.Drows[r]) : 0;
+    const int L = la + ld;
+    for (int s = lane; s < L; s += 32) buf[s] = 0.0;
+    __syncwarp();
+    const uint32_t k1 = p.inc_ptr[r + 1];
+    for (uint32_t k = p.inc_ptr[r]; k < k1; k++) {
+        const unsigned long long pk = p.inc[k];
+        const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+        const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
+        const double* v = p.vals + sg.val_base + (coo - sg.coo_base);
+        const int16_t* sm = p.slotmap + coo;
+        if (pk >> 63) {
+            if (lane == 0)
+                for (int j = 0; j < sg.width; j++) {
+                    const int s = sm[j];
+                    if (s >= 0)
+                        buf[s] += v[j] * sg.mult;
+                }
+        } else {
+            for (int j = lane; j < sg.width; j += 32) {
+                const int s = sm[j];
+                if (s >= 0)
+                    buf[s] += v[j] * sg.mult;
+            }
         }
-        const Segment sg = p.segs[lo];
-        acc += p.vals[sg.val_base + (coo - sg.coo_base)] * sg.mult;
+        __syncwarp();
     }
-    const int32_t target = p.run_target[r];
-    if (p.Dvals == nullptr)
-        p.Avals[target] = p.negate ? -acc : acc;
-    else if (target >= 0)
-        p.Avals[target] = acc;
-    else
-        p.Dvals[-target - 1] = acc;
+    if (p.dense != nullptr) {
+        if (lane == 0)
+            p.dense[r] = L > 0 ? -buf[0] : 0.0;
+        return;
+    }
+    for (int s = lane; s < L; s += 32) {
+        if (s < la)
+            p.Avals[p.Arows[r] + s] = buf[s];
+        else
+            p.Dvals[p.Drows[r] + (s - la)] = buf[s];
+    }
 }
 
 }  // namespace slgpu

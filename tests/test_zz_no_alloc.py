@@ -49,8 +49,7 @@ def _regular_element_matrices(ctx, gb, xyz, conn):
                                       abi.i32p(d2), abi.f64p(np.zeros(1))))
     ctx.check(L.slgpu_matrix_destroy(ctx.h, h))
     assert np.array_equal(cols.reshape(ndofs, ndof), np.tile(np.arange(ndof), (ndofs, 1)))
-    K = vals.reshape(nelem, ntf, ndof).transpose(1, 2, 0).reshape(ntf * ndof, nelem)
-    return K
+    return vals.reshape(nelem, ntf * ndof)
 
 
 def _noalloc(gb, xyz_dev, conn_dev, mesh_nelem, out_dev, stream):
@@ -73,7 +72,7 @@ def test_noalloc_matches_regular_path_twice():
         xyz_dev = torch.from_numpy(xyz).cuda()
         conn_dev = torch.from_numpy(conn).cuda()
         g = gb.g
-        out = torch.full((g.ntf * g.ndof, g.nelem), float("nan"), dtype=torch.float64, device="cuda")
+        out = torch.full((g.nelem, g.ntf * g.ndof), float("nan"), dtype=torch.float64, device="cuda")
         st, msg = _noalloc(gb, xyz_dev, conn_dev, conn.size // 4, out, stream)
         assert st == abi.OK, msg
         torch.cuda.synchronize()
