@@ -19,6 +19,9 @@
 //      result is deterministic; no floating-point atomics.
 #include "engine_internal.h"
 #include "engine_kernels.cuh"
+#include "split_tc.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <cub/cub.cuh>
 
@@ -890,6 +893,131 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     return P;
 }
 
+// ------------------------------------------------------------ split precision (host side)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (fn == nullptr) {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cuda_check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+        if (q != cudaDriverEntryPointSuccess || ptr == nullptr)
+            fail(SLGPU_E_CUDA, "cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }
+    return fn;
+}
+
+// 3D TMA map over an interleaved slice array [outer][rows][16 bytes]; one box
+// is kSplitKStage chunks of box_rows rows.
+static CUtensorMap slice_map(void* base, uint64_t rows, uint64_t outer, uint32_t box_rows)
+{
+    CUtensorMap m;
+    cuuint64_t dims[3] = {16, rows, outer};
+    cuuint64_t strides[2] = {16, rows * 16};
+    cuuint32_t box[3] = {16, box_rows, (cuuint32_t)kSplitKStage};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        fail(SLGPU_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+// Tier 0: 7 slices, levels <= 8 (28 INT8 products; about 1e-12 relative per
+// element matrix, well inside 1e-10); tier 1: 5 slices, levels <= 6 (15
+// products; about 1e-8, inside the FP32-level 1e-6).
+static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
+{
+    std::unique_ptr<GroupDev::Split>& sp = g.split[tier];
+    if (sp)
+        return *sp;
+    sp.reset(new GroupDev::Split());
+    sp->S = tier == 0 ? 7 : 5;
+    sp->L = tier == 0 ? 8 : 6;
+    const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+    sp->Qpad = (Q + 127) / 128 * 128;
+    sp->Ppad = (P + 127) / 128 * 128;
+    sp->slices.alloc(ctx, (size_t)sp->S * g.norient * sp->Qpad * sp->Ppad);
+    sp->rowexp.alloc(ctx, (size_t)g.norient * sp->Ppad * 4);
+    RowSliceParams rp{};
+    rp.tables = g.tables.as<double>();
+    rp.tab_off = g.tab_off_d.as<int64_t>();
+    rp.term_tf = g.term_tf_d.as<int32_t>();
+    rp.term_dof = g.term_dof_d.as<int32_t>();
+    rp.nterms = g.nterms;
+    rp.ngp = g.ngp;
+    rp.ntf = g.ntf;
+    rp.ndof = g.ndof;
+    rp.norient = g.norient;
+    rp.S = sp->S;
+    rp.Qpad = sp->Qpad;
+    rp.Ppad = sp->Ppad;
+    rp.slices = sp->slices.as<int8_t>();
+    rp.rowexp = sp->rowexp.as<int32_t>();
+    if (g.norient > 65535)
+        fail(SLGPU_E_UNSUPPORTED, "too many orientation variants");
+    k_slice_rows<<<dim3((unsigned)sp->Ppad, (unsigned)g.norient), 256, 0, ctx->stream>>>(rp);
+    cuda_check(cudaGetLastError(), "k_slice_rows");
+    ctx->launches++;
+    sp->mapA = slice_map(sp->slices.as<void>(), (uint64_t)sp->Ppad, (uint64_t)sp->S * g.norient * (sp->Qpad / 16), kSplitM);
+    return *sp;
+}
+
+// Split contraction of one group: column slices of C, then the tcgen05 kernel.
+static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, double* out)
+{
+    GroupDev::Split& sp = ensure_split(ctx, g, tier);
+    const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+    const int64_t Epad = (g.nelem + kSplitN - 1) / kSplitN * kSplitN;
+    const size_t colbytes = (size_t)sp.S * sp.Qpad * Epad;
+    if (ctx->split_cols.bytes() < colbytes)
+        ctx->split_cols.alloc(ctx, colbytes);
+    if (ctx->split_colexp.bytes() < (size_t)g.nelem * 4)
+        ctx->split_colexp.alloc(ctx, (size_t)g.nelem * 4);
+    ColSliceParams cs{};
+    cs.C = C;
+    cs.Q = Q;
+    cs.Qpad = sp.Qpad;
+    cs.S = sp.S;
+    cs.nelem = g.nelem;
+    cs.Epad = Epad;
+    cs.slices = ctx->split_cols.as<int8_t>();
+    cs.colexp = ctx->split_colexp.as<int32_t>();
+    k_slice_cols<<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+    cuda_check(cudaGetLastError(), "k_slice_cols");
+    ctx->launches++;
+    const CUtensorMap mapB = slice_map(ctx->split_cols.as<void>(), (uint64_t)Epad, (uint64_t)sp.S * (sp.Qpad / 16), kSplitN);
+    SplitParams p{};
+    p.S = sp.S;
+    p.L = sp.L;
+    p.nchunkA = sp.Qpad / 16;
+    p.nkstage = sp.Qpad / 128;
+    p.P = P;
+    p.Ppad = sp.Ppad;
+    p.norient = g.norient;
+    p.nelem = g.nelem;
+    p.Epad = Epad;
+    p.tiles = g.tiles_d.as<Tile>();
+    p.rowexp = sp.rowexp.as<int32_t>();
+    p.colexp = ctx->split_colexp.as<int32_t>();
+    p.out = out;
+    p.error = ctx->split_error.as<unsigned int>();
+    // One CTA per SM: the kernel holds all 512 TMEM columns.
+    const size_t smem = std::max<size_t>(kSplitSmemBytes, 120 * 1024);
+    static bool attr = false;
+    if (!attr) {
+        cuda_check(cudaFuncSetAttribute(k_contract_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        attr = true;
+    }
+    dim3 grid((unsigned)(sp.Ppad / kSplitM), (unsigned)g.tiles.size());
+    if (grid.y > 65535)
+        fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
+    k_contract_split<<<grid, 128, smem, ctx->stream>>>(sp.mapA, mapB, p);
+    cuda_check(cudaGetLastError(), "k_contract_split");
+    ctx->launches++;
+}
+
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
 {
     if (ctx->record_only) {
@@ -897,8 +1025,8 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             M.rec_constrained.assign(isconstrained, isconstrained + M.ndofs);
         fail(SLGPU_E_NODEVICE, kNoDevice);
     }
-    if (precision != SLGPU_PREC_FP64)
-        fail(SLGPU_E_UNSUPPORTED, "only the FP64 contraction is available in this build");
+    if (precision != SLGPU_PREC_FP64 && precision != SLGPU_PREC_SPLIT && precision != SLGPU_PREC_FP32)
+        fail(SLGPU_E_ARG, "unknown precision mode");
     if (M.ndofs <= 0 || M.ndofs >= (int64_t(1) << 31))
         fail(SLGPU_E_ARG, "DOF count out of range");
     ev_record(ctx, 0);
@@ -950,6 +1078,11 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     for (auto& g : M.groups) maxC = std::max<int64_t>(maxC, (int64_t)g->nterms * g->ngp * g->nelem);
     DevBuf C;
     C.alloc(ctx, std::max<int64_t>(maxC, 1) * 8);
+    if (precision != SLGPU_PREC_FP64) {
+        if (ctx->split_error.empty())
+            ctx->split_error.alloc(ctx, 16);
+        cuda_check(cudaMemsetAsync(ctx->split_error.as<void>(), 0, 16, ctx->stream), "memset");
+    }
     while (ctx->evpool.size() < 3 * M.groups.size()) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
@@ -965,6 +1098,14 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             cuda_check(cudaGetLastError(), "k_geometry_coef");
             ctx->launches++;
             cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 1], ctx->stream), "cudaEventRecord");
+            // Split precision for the larger element matrices (order >= 2);
+            // right-hand sides and small matrices stay in FP64.
+            if (precision != SLGPU_PREC_FP64 && !g->rhs && (int64_t)g->ntf * g->ndof >= 64) {
+                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, C.as<double>(), M.vals.as<double>() + gvb[gi]);
+                cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 2], ctx->stream), "cudaEventRecord");
+                gi++;
+                continue;
+            }
             ContractParams kp{};
             kp.tables = g->tables.as<double>();
             kp.tab_off = g->tab_off_d.as<int64_t>();
@@ -1053,6 +1194,12 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     }
     ev_record(ctx, 3);
     cuda_check(cudaEventSynchronize(ctx->ev[3]), "sync");
+    if (precision != SLGPU_PREC_FP64) {
+        unsigned int err = 0;
+        cuda_check(cudaMemcpy(&err, ctx->split_error.as<void>(), 4, cudaMemcpyDeviceToHost), "D2H split error");
+        if (err != 0)
+            fail(SLGPU_E_TIMEOUT, "a split-precision contraction tile timed out waiting for its data");
+    }
     float coef_ms = 0, contract_ms = 0;
     for (size_t k = 0; k < M.groups.size(); k++) {
         if (M.groups[k]->nelem == 0)
@@ -1167,6 +1314,12 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
     ctx->scratch.release();
     ctx->hash_acc.release();
     ctx->constr_dev.release();
+    // Every device buffer the context owns is freed on its stream, so all of
+    // them must go before the stream does.
+    ctx->split_cols.release();
+    ctx->split_colexp.release();
+    ctx->split_error.release();
+    ctx->rhs_record.clear();
     if (!ctx->record_only) {
         cudaStreamSynchronize(ctx->stream);
         for (auto& e : ctx->ev) cudaEventDestroy(e);

@@ -3,6 +3,7 @@
 
 #include "slgpu.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -88,6 +89,14 @@ struct GroupDev {
         tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
     std::vector<DevBuf> tfaddr, dofaddr;  // per destination
 
+    // Split-precision operand A (row slices of M), built on first use per tier.
+    struct Split {
+        int S = 0, L = 0, Qpad = 0, Ppad = 0;
+        DevBuf slices, rowexp;
+        CUtensorMap mapA;
+    };
+    std::unique_ptr<Split> split[2];
+
     // Record-only copy of the original description (for inspection).
     struct Record;
     std::shared_ptr<Record> rec;
@@ -155,6 +164,8 @@ struct Ctx {
     uint64_t constr_key[2] = {0, 0};
     std::vector<cudaEvent_t> evpool;   // per-group phase events
     int64_t launches = 0;              // kernels launched by this context
+    DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
+    DevBuf split_error;                // device flag set by a timed-out wait
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;

@@ -1,0 +1,74 @@
+"""Split-precision (Ozaki INT8 slices on tcgen05 tensor cores) contraction.
+
+Element matrices from the split path are compared with the FP64 path on the
+same inputs: relative Frobenius error per element matrix <= 1e-10 for the
+split tier and <= 1e-6 for the FP32-level tier.  The drop-in check runs a
+small elasticity problem through sparselizard with SLGPU_PRECISION=split.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import _pipeline as P
+import _synthetic as S
+from sparselizard_b200 import abi, meshgen, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _element_matrices(ctx, gb, xyz, conn, precision):
+    """Element matrices through slgpu_matrix_* with one row per (element, tf)."""
+    g = gb.g
+    nelem, ntf, ndof = g.nelem, g.ntf, g.ndof
+    tfaddr = (np.arange(nelem)[None, :] * ntf + np.arange(ntf)[:, None]).astype(np.int32)
+    dofaddr = np.repeat(np.arange(ndof, dtype=np.int32)[:, None], nelem, axis=1)
+    dest = (abi.Dest * 1)()
+    dest[0].tfaddr, dest[0].dofaddr, dest[0].multiplier = abi.i32p(tfaddr), abi.i32p(dofaddr), 1.0
+    g.ndests, g.dests = 1, dest
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, 0, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, 0, 3, 4, conn.size // 4, abi.i32p(conn)))
+    ndofs = nelem * ntf
+    h = ctypes.c_int()
+    ctx.check(L.slgpu_matrix_create(ctx.h, ndofs, ctypes.byref(h)))
+    ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g), None))
+    info = abi.CsrInfo()
+    con = np.zeros(ndofs, np.uint8)
+    ctx.check(L.slgpu_matrix_process(ctx.h, h, con.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), precision,
+                                     ctypes.byref(info)))
+    rows, cols = np.zeros(ndofs + 1, np.int32), np.zeros(info.nnzA, np.int32)
+    vals = np.zeros(info.nnzA)
+    ctx.check(L.slgpu_matrix_download(ctx.h, h, abi.i32p(rows), abi.i32p(cols), abi.f64p(vals),
+                                      abi.i32p(np.zeros(ndofs + 1, np.int32)), abi.i32p(np.zeros(1, np.int32)),
+                                      abi.f64p(np.zeros(1))))
+    ctx.check(L.slgpu_matrix_destroy(ctx.h, h))
+    return vals.reshape(nelem, ntf * ndof)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = abi.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("seed,norient,nterms,ngp1", [(0, 1, 3, 3), (1, 3, 4, 4), (2, 2, 9, 3), (3, 2, 9, 4)])
+def test_split_element_matrices(ctx, seed, norient, nterms, ngp1):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gb, xyz, conn = S.group(rng, nelem_grid=14, ntf=9, ndof=9, nterms=nterms, ngp1=ngp1, norient=norient, ndests=1)
+    ref = _element_matrices(ctx, gb, xyz, conn, abi.PREC_FP64)
+    for prec, tol in ((abi.PREC_SPLIT, 1e-10), (abi.PREC_FP32, 1e-6)):
+        got = _element_matrices(ctx, gb, xyz, conn, prec)
+        err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert err.max() <= tol, f"precision {prec}: per-element Frobenius error {err.max():.3e} > {tol:g}"
+
+
+def test_split_dropin_elasticity(ref_lib, gpu_lib, tmp_path):
+    msh = str(tmp_path / "h.msh")
+    meshgen.hex_mesh(msh, 4, jitter=0.15, seed=1)
+    ref = P.reference(W.ELASTICITY_HEX, msh, [2, -2])
+    got = P.gpu(W.ELASTICITY_HEX, msh, [2, -2], precision="split")
+    P.check_pattern(ref, got)
+    _, _, fro = P.scaled_errors(ref, got)
+    assert fro <= 1e-10, f"assembled Frobenius-relative error {fro:.3e}"
