@@ -47,8 +47,9 @@ enum {
 /* Contraction precision (slgpu_matrix_process / slgpu_rhs_assemble). */
 enum {
     SLGPU_PREC_FP64 = 0,  /* plain FP64 */
-    SLGPU_PREC_SPLIT = 1, /* FP64 operands split into BF16 slices on tensor cores, FP32 accumulation, FP64 recombination */
-    SLGPU_PREC_FP32 = 2   /* FP32 tier */
+    SLGPU_PREC_SPLIT = 1, /* FP64 operands split into 7 INT8 slices on the tensor cores (tcgen05 kind::i8), exact INT32
+                             accumulation, FP64 recombination; <= 1e-10 relative per element matrix */
+    SLGPU_PREC_FP32 = 2   /* same with 5 slices: FP32-level tier, <= 1e-6 */
 };
 
 /*
@@ -215,6 +216,10 @@ int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int 
 /* Device time (ms) of the phases of the last process()/rhs call:
  * [0] geometry+coefficients, [1] contraction, [2] pattern (symbolic), [3] CSR values, [4] total. */
 int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5);
+/* Compiles (host only, no device needed) the runtime-generated geometry and
+ * coefficient kernels the matrix's groups would use, returning SLGPU_E_CUDA
+ * with the compiler log in `log` if one does not compile. */
+int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_t len);
 /* Number of kernels this context has launched so far. */
 int64_t slgpu_kernel_launches(const slgpu_ctx* ctx);
 

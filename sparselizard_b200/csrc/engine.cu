@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -309,6 +310,29 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     gd->ndests = g.ndests;
     gd->rhs = g.terms[0].dof_table < 0;
     gd->prog = compile_program(g, g.nterms);
+    gd->nodes.assign(g.nodes, g.nodes + g.nnodes);
+    for (int t = 0; t < g.nterms; t++) gd->term_node.push_back(g.terms[t].coef_node);
+    gd->hconsts.assign(g.consts, g.consts + g.nconsts);
+    {
+        // Geometry key: groups with the same key share elements, orientations,
+        // Gauss points and Lagrange tables, so one kernel evaluates them all.
+        uint64_t h = mix64((uint64_t)g.mesh ^ (uint64_t)g.elemtype << 8 ^ (uint64_t)g.ngp << 16 ^ (uint64_t)g.ncurvednodes << 32 ^
+                           (uint64_t)g.problemdim << 48);
+        h = mix64(h ^ (uint64_t)g.nelem);
+        for (int64_t e = 0; e < g.nelem; e++) h = mix64(h ^ ((uint64_t)(uint32_t)g.elems[e] << 8 | (uint64_t)(uint32_t)g.orient[e] << 40));
+        const size_t nl = (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp;
+        for (size_t k = 0; k < nl; k++) {
+            uint64_t w;
+            std::memcpy(&w, &g.lagrange[k], 8);
+            h = mix64(h ^ w);
+        }
+        for (int k = 0; k < g.ngp; k++) {
+            uint64_t w;
+            std::memcpy(&w, &g.weights[k], 8);
+            h = mix64(h ^ w);
+        }
+        gd->geom_hash = h;
+    }
     int64_t off = 0;
     for (int k = 0; k < g.ntables; k++) {
         gd->tab_off.push_back(off);
@@ -936,7 +960,7 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
     sp->S = tier == 0 ? 7 : 5;
     sp->L = tier == 0 ? 8 : 6;
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
-    sp->Qpad = (Q + 127) / 128 * 128;
+    sp->Qpad = (Q + 16 * kSplitKStage - 1) / (16 * kSplitKStage) * (16 * kSplitKStage);
     sp->Ppad = (P + 127) / 128 * 128;
     sp->slices.alloc(ctx, (size_t)sp->S * g.norient * sp->Qpad * sp->Ppad);
     sp->rowexp.alloc(ctx, (size_t)g.norient * sp->Ppad * 4);
@@ -984,7 +1008,12 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     cs.Epad = Epad;
     cs.slices = ctx->split_cols.as<int8_t>();
     cs.colexp = ctx->split_colexp.as<int32_t>();
-    k_slice_cols<<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+    if (sp.S == 7)
+        k_slice_cols<7><<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+    else if (sp.S == 5)
+        k_slice_cols<5><<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+    else
+        fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
     cuda_check(cudaGetLastError(), "k_slice_cols");
     ctx->launches++;
     const CUtensorMap mapB = slice_map(ctx->split_cols.as<void>(), (uint64_t)Epad, (uint64_t)sp.S * (sp.Qpad / 16), kSplitN);
@@ -992,7 +1021,7 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     p.S = sp.S;
     p.L = sp.L;
     p.nchunkA = sp.Qpad / 16;
-    p.nkstage = sp.Qpad / 128;
+    p.nkstage = sp.Qpad / (16 * kSplitKStage);
     p.P = P;
     p.Ppad = sp.Ppad;
     p.norient = g.norient;
@@ -1004,7 +1033,7 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     p.out = out;
     p.error = ctx->split_error.as<unsigned int>();
     // One CTA per SM: the kernel holds all 512 TMEM columns.
-    const size_t smem = std::max<size_t>(kSplitSmemBytes, 120 * 1024);
+    const size_t smem = kSplitSmemBytes;
     static bool attr = false;
     if (!attr) {
         cuda_check(cudaFuncSetAttribute(k_contract_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
@@ -1016,6 +1045,89 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     k_contract_split<<<grid, 128, smem, ctx->stream>>>(sp.mapA, mapB, p);
     cuda_check(cudaGetLastError(), "k_contract_split");
     ctx->launches++;
+}
+
+// Host mirror of the runtime-compiled kernel's parameter structs (coef_jit.cu).
+struct JitGeom {
+    const double* xyz;
+    const int32_t* conn;
+    const int32_t* elems;
+    const int32_t* orient;
+    long long nelem;
+    const double* weights;
+    const double* lagrange;
+};
+struct JitGroup {
+    const double* tables;
+    const double* elemdata;
+    const double* fielddata;
+    const double* term_scale;
+    double* C;
+};
+
+// Geometry + coefficients of every group into C (offsets coff).  Consecutive
+// groups with the same geometry key run as one runtime-compiled kernel; the
+// interpreter kernel is used when SLGPU_COEF_INTERPRETER=1 or when a kernel
+// cannot be compiled.
+static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vector<int64_t>& coff)
+{
+    static const bool interp_only = [] {
+        const char* v = std::getenv("SLGPU_COEF_INTERPRETER");
+        return v != nullptr && std::strcmp(v, "1") == 0;
+    }();
+    const size_t ng = M.groups.size();
+    size_t k = 0;
+    while (k < ng) {
+        GroupDev& g0 = *M.groups[k];
+        size_t k1 = k + 1;
+        while (k1 < ng && M.groups[k1]->geom_hash == g0.geom_hash) k1++;
+        if (g0.nelem == 0) {
+            k = k1;
+            continue;
+        }
+        bool done = false;
+        if (!interp_only && !ctx->jit_broken) {
+            try {
+                std::vector<const GroupDev*> batch;
+                for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
+                cudaKernel_t kern = jit_coef_kernel(ctx, jit_coef_source(batch));
+                std::vector<JitGroup> jg;
+                for (size_t j = k; j < k1; j++) {
+                    GroupDev& G = *M.groups[j];
+                    jg.push_back(JitGroup{G.tables.as<double>(), G.elemdata.as<double>(), G.fielddata.as<double>(),
+                                          G.term_scale_d.as<double>(), C + coff[j]});
+                }
+                DevBuf djg;
+                upload(ctx, djg, jg);
+                const MeshDev& m = ctx->meshes.at(g0.mesh);
+                JitGeom geom{m.xyz.as<double>(), m.types.at(g0.elemtype).conn.as<int32_t>(), g0.elems.as<int32_t>(), g0.orient.as<int32_t>(),
+                             (long long)g0.nelem, g0.weights.as<double>(), g0.lagrange.as<double>()};
+                const JitGroup* gp = djg.as<JitGroup>();
+                void* args[] = {&geom, &gp};
+                const int64_t n = g0.nelem * (int64_t)g0.ngp;
+                cuda_check(cudaLaunchKernel((const void*)kern, dim3(grid_for(n, 128)), dim3(128), args, 0, ctx->stream),
+                           "coefficient kernel launch");
+                ctx->launches++;
+                done = true;
+            } catch (const SlgpuException&) {
+                throw;
+            } catch (const std::exception& e) {
+                ctx->jit_broken = true;
+                ctx->jit_error = e.what();
+            }
+        }
+        if (!done) {
+            for (size_t j = k; j < k1; j++) {
+                GroupDev& G = *M.groups[j];
+                CoefParams cp = coef_params(ctx, G, C + coff[j]);
+                const int64_t n = G.nelem * (int64_t)G.ngp;
+                k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
+                cuda_check(cudaGetLastError(), "k_geometry_coef");
+                ctx->launches++;
+            }
+        }
+        k = k1;
+    }
 }
 
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
@@ -1074,35 +1186,37 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     // 1+2: geometry, coefficients and contraction into the value buffer.
     if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
         M.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
-    int64_t maxC = 0;
-    for (auto& g : M.groups) maxC = std::max<int64_t>(maxC, (int64_t)g->nterms * g->ngp * g->nelem);
+    // Coefficients of every group coexist ([term][gp][element] per group) so
+    // that groups sharing geometry are evaluated by one kernel.
+    std::vector<int64_t> coff(M.groups.size());
+    int64_t ctot = 0;
+    for (size_t k = 0; k < M.groups.size(); k++) {
+        coff[k] = ctot;
+        ctot += (int64_t)M.groups[k]->nterms * M.groups[k]->ngp * M.groups[k]->nelem;
+    }
     DevBuf C;
-    C.alloc(ctx, std::max<int64_t>(maxC, 1) * 8);
+    C.alloc(ctx, std::max<int64_t>(ctot, 1) * 8);
     if (precision != SLGPU_PREC_FP64) {
         if (ctx->split_error.empty())
             ctx->split_error.alloc(ctx, 16);
         cuda_check(cudaMemsetAsync(ctx->split_error.as<void>(), 0, 16, ctx->stream), "memset");
     }
-    while (ctx->evpool.size() < 3 * M.groups.size()) {
+    while (ctx->evpool.size() < 3) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         ctx->evpool.push_back(e);
     }
+    cuda_check(cudaEventRecord(ctx->evpool[0], ctx->stream), "cudaEventRecord");
+    launch_coefficients(ctx, M, C.as<double>(), coff);
+    cuda_check(cudaEventRecord(ctx->evpool[1], ctx->stream), "cudaEventRecord");
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
-            CoefParams cp = coef_params(ctx, *g, C.as<double>());
-            int64_t n = g->nelem * (int64_t)g->ngp;
-            cuda_check(cudaEventRecord(ctx->evpool[3 * gi], ctx->stream), "cudaEventRecord");
-            k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
-            cuda_check(cudaGetLastError(), "k_geometry_coef");
-            ctx->launches++;
-            cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 1], ctx->stream), "cudaEventRecord");
+            double* Cg = C.as<double>() + coff[gi];
             // Split precision for the larger element matrices (order >= 2);
             // right-hand sides and small matrices stay in FP64.
             if (precision != SLGPU_PREC_FP64 && !g->rhs && (int64_t)g->ntf * g->ndof >= 64) {
-                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, C.as<double>(), M.vals.as<double>() + gvb[gi]);
-                cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 2], ctx->stream), "cudaEventRecord");
+                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, M.vals.as<double>() + gvb[gi]);
                 gi++;
                 continue;
             }
@@ -1116,7 +1230,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             kp.ntf = g->ntf;
             kp.ndof = g->ndof;
             kp.nelem = g->nelem;
-            kp.C = C.as<double>();
+            kp.C = Cg;
             kp.tiles = g->tiles_d.as<Tile>();
             kp.out = M.vals.as<double>() + gvb[gi];
             const int64_t P = (int64_t)g->ntf * g->ndof;
@@ -1126,10 +1240,10 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
             ctx->launches++;
-            cuda_check(cudaEventRecord(ctx->evpool[3 * gi + 2], ctx->stream), "cudaEventRecord");
         }
         gi++;
     }
+    cuda_check(cudaEventRecord(ctx->evpool[2], ctx->stream), "cudaEventRecord");
     C.release();
     {
         int64_t vb = 0;
@@ -1201,15 +1315,8 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             fail(SLGPU_E_TIMEOUT, "a split-precision contraction tile timed out waiting for its data");
     }
     float coef_ms = 0, contract_ms = 0;
-    for (size_t k = 0; k < M.groups.size(); k++) {
-        if (M.groups[k]->nelem == 0)
-            continue;
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, ctx->evpool[3 * k], ctx->evpool[3 * k + 1]);
-        cudaEventElapsedTime(&b, ctx->evpool[3 * k + 1], ctx->evpool[3 * k + 2]);
-        coef_ms += a;
-        contract_ms += b;
-    }
+    cudaEventElapsedTime(&coef_ms, ctx->evpool[0], ctx->evpool[1]);
+    cudaEventElapsedTime(&contract_ms, ctx->evpool[1], ctx->evpool[2]);
     ctx->timings[0] = coef_ms;
     ctx->timings[1] = contract_ms;
     ctx->timings[2] = ev_ms(ctx, 1, 2);
@@ -1320,6 +1427,9 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
     ctx->split_colexp.release();
     ctx->split_error.release();
     ctx->rhs_record.clear();
+    for (cudaLibrary_t lib : ctx->jit_libs) cudaLibraryUnload(lib);
+    ctx->jit_libs.clear();
+    ctx->jit_kernels.clear();
     if (!ctx->record_only) {
         cudaStreamSynchronize(ctx->stream);
         for (auto& e : ctx->ev) cudaEventDestroy(e);
@@ -1497,6 +1607,29 @@ int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const 
 }
 
 int64_t slgpu_kernel_launches(const slgpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_t len)
+{
+    int st = guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        size_t k = 0;
+        while (k < M.groups.size()) {
+            size_t k1 = k + 1;
+            while (k1 < M.groups.size() && M.groups[k1]->geom_hash == M.groups[k]->geom_hash) k1++;
+            std::vector<const GroupDev*> batch;
+            for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
+            try {
+                jit_compile(jit_coef_source(batch));
+            } catch (const std::exception& e) {
+                fail(SLGPU_E_CUDA, e.what());
+            }
+            k = k1;
+        }
+    });
+    if (log != nullptr && len > 0)
+        std::snprintf(log, len, "%s", st == SLGPU_OK ? "" : ctx->last_error.c_str());
+    return st;
+}
 
 int slgpu_matrix_work(slgpu_ctx* ctx, int handle, slgpu_work* out)
 {

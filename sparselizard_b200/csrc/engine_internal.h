@@ -84,6 +84,12 @@ struct GroupDev {
     std::vector<double> dest_mult;
     std::vector<Tile> tiles;
     uint64_t addr_hash[2] = {0, 0};
+    // Coefficient program as given (for the runtime-compiled kernel) and a
+    // hash of the geometry inputs (groups with equal hashes share J, detJ).
+    std::vector<slgpu_node> nodes;
+    std::vector<int> term_node;
+    std::vector<double> hconsts;
+    uint64_t geom_hash = 0;
 
     DevBuf elems, orient, weights, lagrange, tables, consts, prog_d, elemdata, fielddata, field_off_d, field_rows_d,
         tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
@@ -166,9 +172,18 @@ struct Ctx {
     int64_t launches = 0;              // kernels launched by this context
     DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
     DevBuf split_error;                // device flag set by a timed-out wait
+    std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source
+    std::vector<cudaLibrary_t> jit_libs;
+    bool jit_broken = false;  // a coefficient kernel failed to compile: interpreter from then on
+    std::string jit_error;
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;
 };
+
+// Runtime-compiled coefficient kernels (coef_jit.cu).
+std::string jit_coef_source(const std::vector<const GroupDev*>& batch);
+cudaKernel_t jit_coef_kernel(Ctx* ctx, const std::string& src);
+std::vector<char> jit_compile(const std::string& src);  // NVRTC only, no device needed
 
 }  // namespace slgpu

@@ -26,7 +26,7 @@ namespace slgpu {
 
 constexpr int kSplitM = 128;     // element-matrix entries per tile (TMEM lanes)
 constexpr int kSplitN = 64;      // elements per tile (= kTileE)
-constexpr int kSplitKStage = 8;  // 16-byte K chunks per pipeline stage (128 bytes of K)
+constexpr int kSplitKStage = 4;  // 16-byte K chunks per pipeline stage (64 bytes of K)
 constexpr int kSplitMaxS = 7;    // slices per operand (levels 2..8 fit 448 TMEM columns)
 
 struct SplitParams {
@@ -119,6 +119,7 @@ struct ColSliceParams {
     int32_t* colexp;  // [nelem]
 };
 
+template <int S>
 __global__ void k_slice_cols(ColSliceParams p)
 {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -131,20 +132,27 @@ __global__ void k_slice_cols(ColSliceParams p)
         frexp(mx, &ex);
     p.colexp[e] = ex;
     const int nchunk = p.Qpad / 16;
+    uint4* out = reinterpret_cast<uint4*>(p.slices);
     for (int c = 0; c < nchunk; c++) {
-        int8_t sl[kSplitMaxS][16];
+        uint32_t w[S][4];
+#pragma unroll
+        for (int s = 0; s < S; s++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[s][k] = 0;
+#pragma unroll
         for (int k = 0; k < 16; k++) {
             const int q = c * 16 + k;
-            const double v = q < p.Q ? ldexp(p.C[(int64_t)q * p.nelem + e], -ex) : 0.0;
-            int8_t tmp[kSplitMaxS];
-            split7(v, p.S, tmp);
-            for (int s = 0; s < p.S; s++) sl[s][k] = tmp[s];
+            double x = q < p.Q ? ldexp(p.C[(int64_t)q * p.nelem + e], -ex) : 0.0;
+#pragma unroll
+            for (int s = 0; s < S; s++) {
+                const double y = x * 128.0;
+                const double m = trunc(y);
+                w[s][k >> 2] |= (uint32_t)(uint8_t)(int8_t)m << (8 * (k & 3));
+                x = y - m;
+            }
         }
-        for (int s = 0; s < p.S; s++) {
-            uint4 w;
-            memcpy(&w, sl[s], 16);
-            reinterpret_cast<uint4*>(p.slices)[((int64_t)s * nchunk + c) * p.Epad + e] = w;
-        }
+#pragma unroll
+        for (int s = 0; s < S; s++) out[((int64_t)s * nchunk + c) * p.Epad + e] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
     }
 }
 
@@ -235,14 +243,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r)
 
 // ---------------------------------------------------------------- contraction
 
-// Shared memory: B stage (all S slices, 64 rows x 128 bytes each = 8 KB per
-// slice), two A stages (128 rows x 128 bytes = 16 KB), barriers, TMEM address.
+// Shared memory: two pipeline stages; each holds every A slice (128 rows x
+// 64 bytes = 8 KB) and every B slice (64 rows x 64 bytes = 4 KB) of one
+// 64-byte K stage, plus barriers and the TMEM address.
 struct SplitSmem {
-    alignas(1024) int8_t B[kSplitMaxS][kSplitKStage][kSplitN][16];
-    alignas(1024) int8_t A[2][kSplitKStage][kSplitM][16];
-    alignas(8) uint64_t bar_b;
-    uint64_t bar_a[2];
-    uint64_t bar_mma[2];
+    alignas(1024) int8_t A[2][kSplitMaxS][kSplitKStage][kSplitM][16];
+    alignas(1024) int8_t B[2][kSplitMaxS][kSplitKStage][kSplitN][16];
+    alignas(8) uint64_t full[2];
+    uint64_t mma_done[2];
     uint32_t tmem;
     int failed;
     int colexp[kSplitN];
@@ -253,12 +261,11 @@ constexpr size_t kSplitSmemBytes = sizeof(SplitSmem) + 1024;
 // Thread 0 issues TMA and MMA; warp 0 owns the TMEM allocation; all warps
 // run the epilogue (warp w reads TMEM lanes 32w..32w+31).
 //
-// Pipeline per K stage (128 bytes of K): all B slices are loaded once; A
-// slices stream through two buffers.  A buffer is refilled only after the
-// MMAs that read it have completed (tcgen05.commit on bar_mma[buffer]); B is
-// refilled only after every outstanding MMA has completed.  Every wait is
-// bounded: on timeout the CTA records the failure, skips its epilogue, frees
-// its TMEM and returns.
+// Pipeline: stage ks (64 bytes of K) loads all S A slices and S B slices into
+// buffer ks&1 under one barrier; stage ks+1 is loaded while the MMAs of stage
+// ks run, once the MMAs that last read its buffer (stage ks-1) have completed
+// (tcgen05.commit on mma_done[buffer]).  Every wait is bounded: on timeout the
+// CTA records the failure, skips its epilogue, frees its TMEM and returns.
 __global__ void __launch_bounds__(128, 1) k_contract_split(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                                                            SplitParams p)
 {
@@ -275,11 +282,10 @@ __global__ void __launch_bounds__(128, 1) k_contract_split(const __grid_constant
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(&sm.bar_b, 1);
-        mbar_init(&sm.bar_a[0], 1);
-        mbar_init(&sm.bar_a[1], 1);
-        mbar_init(&sm.bar_mma[0], 1);
-        mbar_init(&sm.bar_mma[1], 1);
+        mbar_init(&sm.full[0], 1);
+        mbar_init(&sm.full[1], 1);
+        mbar_init(&sm.mma_done[0], 1);
+        mbar_init(&sm.mma_done[1], 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -296,60 +302,55 @@ __global__ void __launch_bounds__(128, 1) k_contract_split(const __grid_constant
         const uint32_t idesc = umma_idesc_i8(kSplitM, kSplitN);
         const uint32_t lboA = kSplitM * 16, lboB = kSplitN * 16, sbo = 128;
         const int amax = min(p.S, p.L - 1);
-        const uint32_t bytesA = kSplitKStage * kSplitM * 16, bytesB = (uint32_t)(p.S * kSplitKStage * kSplitN * 16);
-        uint32_t ph_b = 0, ph_a[2] = {0, 0}, ph_mma[2] = {0, 0};
+        const uint32_t stage_bytes = (uint32_t)(p.S * kSplitKStage * (kSplitM + kSplitN) * 16);
+        uint32_t ph_full[2] = {0, 0}, ph_mma[2] = {0, 0};
         bool pending[2] = {false, false};
         bool ok = true;
-        int cur = 0;
+        auto issue = [&](int ks) {
+            const int buf = ks & 1;
+            mbar_expect_tx(&sm.full[buf], stage_bytes);
+            for (int s = 0; s < p.S; s++) {
+                tma_load_3d(&sm.A[buf][s][0][0][0], &mapA, &sm.full[buf], 0, p0,
+                            (s * p.norient + tile.orient) * p.nchunkA + ks * kSplitKStage);
+                tma_load_3d(&sm.B[buf][s][0][0][0], &mapB, &sm.full[buf], 0, tile.e0, s * p.nchunkA + ks * kSplitKStage);
+            }
+        };
         auto drain = [&](int i) {
             if (pending[i] && ok) {
-                ok = mbar_wait(&sm.bar_mma[i], ph_mma[i]);
+                ok = mbar_wait(&sm.mma_done[i], ph_mma[i]);
                 ph_mma[i] ^= 1;
                 pending[i] = false;
             }
         };
+        issue(0);
         for (int ks = 0; ks < p.nkstage && ok; ks++) {
-            drain(0);
-            drain(1);
-            if (!ok)
-                break;
-            mbar_expect_tx(&sm.bar_b, bytesB);
-            for (int b = 0; b < p.S; b++)
-                tma_load_3d(&sm.B[b][0][0][0], &mapB, &sm.bar_b, 0, tile.e0, b * p.nchunkA + ks * kSplitKStage);
-            mbar_expect_tx(&sm.bar_a[cur], bytesA);
-            tma_load_3d(&sm.A[cur][0][0][0], &mapA, &sm.bar_a[cur], 0, p0, (0 * p.norient + tile.orient) * p.nchunkA + ks * kSplitKStage);
-            ok = mbar_wait(&sm.bar_b, ph_b);
-            ph_b ^= 1;
-            for (int a = 1; a <= amax && ok; a++) {
-                const int nxt = cur ^ 1;
-                if (a < amax) {
-                    drain(nxt);
-                    if (!ok)
-                        break;
-                    mbar_expect_tx(&sm.bar_a[nxt], bytesA);
-                    tma_load_3d(&sm.A[nxt][0][0][0], &mapA, &sm.bar_a[nxt], 0, p0,
-                                (a * p.norient + tile.orient) * p.nchunkA + ks * kSplitKStage);
-                }
-                ok = mbar_wait(&sm.bar_a[cur], ph_a[cur]);
-                ph_a[cur] ^= 1;
+            const int buf = ks & 1;
+            if (ks + 1 < p.nkstage) {
+                drain(buf ^ 1);
                 if (!ok)
                     break;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                issue(ks + 1);
+            }
+            ok = mbar_wait(&sm.full[buf], ph_full[buf]);
+            ph_full[buf] ^= 1;
+            if (!ok)
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int a = 1; a <= amax; a++) {
                 for (int b = 1; b <= p.S && a + b <= p.L; b++) {
                     const int level = a + b;
                     const uint32_t dcol = tmem + (uint32_t)((level - 2) * kSplitN);
                     const int afirst = max(1, level - p.S);
                     for (int k = 0; k < kSplitKStage / 2; k++) {
-                        const uint64_t ad = umma_desc(smem_u32(&sm.A[cur][2 * k][0][0]), lboA, sbo);
-                        const uint64_t bd = umma_desc(smem_u32(&sm.B[b - 1][2 * k][0][0]), lboB, sbo);
+                        const uint64_t ad = umma_desc(smem_u32(&sm.A[buf][a - 1][2 * k][0][0]), lboA, sbo);
+                        const uint64_t bd = umma_desc(smem_u32(&sm.B[buf][b - 1][2 * k][0][0]), lboB, sbo);
                         const uint32_t acc = (ks == 0 && k == 0 && a == afirst) ? 0u : 1u;
                         umma_i8(dcol, ad, bd, idesc, acc);
                     }
                 }
-                umma_commit(&sm.bar_mma[cur]);
-                pending[cur] = true;
-                cur = nxt;
             }
+            umma_commit(&sm.mma_done[buf]);
+            pending[buf] = true;
         }
         drain(0);
         drain(1);

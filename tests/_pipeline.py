@@ -133,6 +133,14 @@ def record_oracle_inproc(workload, msh, params):
         assert "record-only" in str(e), str(e)
     plan = recorded_plan(lib)
     out = {}
+    # The runtime-generated coefficient kernels of the recorded groups must
+    # compile (NVRTC runs on the host, no device needed).
+    h = lib.slgpu_adapter_last_handle()
+    if h:
+        log = ctypes.create_string_buffer(4096)
+        ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+        st = lib.slgpu_check_coefficient_kernels(ctx, h, log, 4096)
+        assert st == 0, "coefficient kernel does not compile: " + log.value.decode(errors="replace")
     if plan["groups"] or plan["frags"]:
         xyz = None
         conns = []
