@@ -220,6 +220,19 @@ int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5);
  * coefficient kernels the matrix's groups would use, returning SLGPU_E_CUDA
  * with the compiler log in `log` if one does not compile. */
 int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_t len);
+/* Per kernel family, for the last process(): summed device time in ms (CUDA
+ * events around each launch on the context's stream), number of launches and
+ * algorithmic work of those launches.  Families and work units:
+ *   "coefficients"        bytes of coefficients written (8 per term, point, element)
+ *   "contract_fp64"       FLOPs, 2*ntf*ndof*nterms*ngp per element
+ *   "slice_cols"          bytes: coefficients read, slices and exponents written
+ *   "contract_split"      INT8 tensor operations, 2*pairs*ntf*ndof*nterms*ngp per
+ *   "contract_split_fp32" element (pairs = 28 for the split tier, 15 for FP32)
+ *   "row_values"          bytes: kept element values + slots, incidences, row
+ *                         pointers read; A and D values written
+ * A family that did not run reports zeros.  No counterpart in the reference
+ * (a measurement hook). */
+int slgpu_kernel_stats(const slgpu_ctx* ctx, const char* family, double* total_ms, int64_t* launches, double* work);
 /* Number of kernels this context has launched so far. */
 int64_t slgpu_kernel_launches(const slgpu_ctx* ctx);
 

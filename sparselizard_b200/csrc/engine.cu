@@ -528,6 +528,37 @@ static std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>
     return segs;
 }
 
+// Kernel-family timers: kstat_start/kstat_stop bracket launches with an
+// event pair; kstat_collect sums them once the stream has been synchronised.
+static int kstat_start(Ctx* ctx, const char* family, double work)
+{
+    const size_t i = ctx->kev_tag.size();
+    while (ctx->kev.size() < 2 * (i + 1)) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        ctx->kev.push_back(e);
+    }
+    cuda_check(cudaEventRecord(ctx->kev[2 * i], ctx->stream), "cudaEventRecord");
+    ctx->kev_tag.emplace_back(family, work);
+    return (int)i;
+}
+
+static void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->kev[2 * i + 1], ctx->stream), "cudaEventRecord"); }
+
+static void kstat_collect(Ctx* ctx)
+{
+    ctx->kstats.clear();
+    for (size_t i = 0; i < ctx->kev_tag.size(); i++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]);
+        Ctx::KernelStat& k = ctx->kstats[ctx->kev_tag[i].first];
+        k.ms += ms;
+        k.work += ctx->kev_tag[i].second;
+        k.launches++;
+    }
+    ctx->kev_tag.clear();
+}
+
 static void ev_record(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->ev[i], ctx->stream), "cudaEventRecord"); }
 
 static float ev_ms(Ctx* ctx, int a, int b)
@@ -918,35 +949,6 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 }
 
 // ------------------------------------------------------------ split precision (host side)
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (fn == nullptr) {
-        void* ptr = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        cuda_check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
-        if (q != cudaDriverEntryPointSuccess || ptr == nullptr)
-            fail(SLGPU_E_CUDA, "cuTensorMapEncodeTiled is not available");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-    }
-    return fn;
-}
-
-// 3D TMA map over an interleaved slice array [outer][rows][16 bytes]; one box
-// is kSplitKStage chunks of box_rows rows.
-static CUtensorMap slice_map(void* base, uint64_t rows, uint64_t outer, uint32_t box_rows)
-{
-    CUtensorMap m;
-    cuuint64_t dims[3] = {16, rows, outer};
-    cuuint64_t strides[2] = {16, rows * 16};
-    cuuint32_t box[3] = {16, box_rows, (cuuint32_t)kSplitKStage};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS)
-        fail(SLGPU_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-    return m;
-}
 
 // Tier 0: 7 slices, levels <= 8 (28 INT8 products; about 1e-12 relative per
 // element matrix, well inside 1e-10); tier 1: 5 slices, levels <= 6 (15
@@ -960,8 +962,8 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
     sp->S = tier == 0 ? 7 : 5;
     sp->L = tier == 0 ? 8 : 6;
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
-    sp->Qpad = (Q + 16 * kSplitKStage - 1) / (16 * kSplitKStage) * (16 * kSplitKStage);
-    sp->Ppad = (P + 127) / 128 * 128;
+    sp->Qpad = std::max(kSplitKStep, (Q + kSplitKStep - 1) / kSplitKStep * kSplitKStep);
+    sp->Ppad = (P + kSplitM - 1) / kSplitM * kSplitM;
     sp->slices.alloc(ctx, (size_t)sp->S * g.norient * sp->Qpad * sp->Ppad);
     sp->rowexp.alloc(ctx, (size_t)g.norient * sp->Ppad * 4);
     RowSliceParams rp{};
@@ -984,8 +986,29 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
     k_slice_rows<<<dim3((unsigned)sp->Ppad, (unsigned)g.norient), 256, 0, ctx->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_slice_rows");
     ctx->launches++;
-    sp->mapA = slice_map(sp->slices.as<void>(), (uint64_t)sp->Ppad, (uint64_t)sp->S * g.norient * (sp->Qpad / 16), kSplitM);
     return *sp;
+}
+
+// Whether a group's contraction can take the split path: level sums stay
+// below 2^31 (at most 7 * Qpad * 127^2) and the integer recombination stays
+// exact in FP64.
+static bool split_supported(const GroupDev& g)
+{
+    const int64_t Q = (int64_t)g.nterms * g.ngp;
+    return Q > 0 && Q <= 16384;
+}
+
+template <int S, int L>
+static void launch_split(Ctx* ctx, const SplitParams& p)
+{
+    static bool attr = false;
+    if (!attr) {
+        cuda_check(cudaFuncSetAttribute(k_contract_split<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemBytes),
+                   "smem attribute");
+        attr = true;
+    }
+    const int64_t grid = std::min<int64_t>(p.nwork, std::max(ctx->nsm, 1));
+    k_contract_split<S, L><<<(unsigned)grid, kSplitThreads, kSplitSmemBytes, ctx->stream>>>(p);
 }
 
 // Split contraction of one group: column slices of C, then the tcgen05 kernel.
@@ -993,56 +1016,55 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
 {
     GroupDev::Split& sp = ensure_split(ctx, g, tier);
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
-    const int64_t Epad = (g.nelem + kSplitN - 1) / kSplitN * kSplitN;
-    const size_t colbytes = (size_t)sp.S * sp.Qpad * Epad;
+    const int64_t ntiles = (int64_t)g.tiles.size();
+    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * kSplitN;
     if (ctx->split_cols.bytes() < colbytes)
         ctx->split_cols.alloc(ctx, colbytes);
-    if (ctx->split_colexp.bytes() < (size_t)g.nelem * 4)
-        ctx->split_colexp.alloc(ctx, (size_t)g.nelem * 4);
+    if (ctx->split_colexp.bytes() < (size_t)ntiles * kSplitN * 4)
+        ctx->split_colexp.alloc(ctx, (size_t)ntiles * kSplitN * 4);
     ColSliceParams cs{};
     cs.C = C;
+    cs.tiles = g.tiles_d.as<Tile>();
     cs.Q = Q;
     cs.Qpad = sp.Qpad;
-    cs.S = sp.S;
     cs.nelem = g.nelem;
-    cs.Epad = Epad;
+    cs.ntiles = ntiles;
     cs.slices = ctx->split_cols.as<int8_t>();
     cs.colexp = ctx->split_colexp.as<int32_t>();
+    const dim3 cgrid = grid_for(ntiles * kSplitN, 128);
+    const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + (double)colbytes + 4.0 * ntiles * kSplitN);
     if (sp.S == 7)
-        k_slice_cols<7><<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<7><<<cgrid, 128, 0, ctx->stream>>>(cs);
     else if (sp.S == 5)
-        k_slice_cols<5><<<grid_for(g.nelem, 128), 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<5><<<cgrid, 128, 0, ctx->stream>>>(cs);
     else
         fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
+    kstat_stop(ctx, kt);
     cuda_check(cudaGetLastError(), "k_slice_cols");
     ctx->launches++;
-    const CUtensorMap mapB = slice_map(ctx->split_cols.as<void>(), (uint64_t)Epad, (uint64_t)sp.S * (sp.Qpad / 16), kSplitN);
     SplitParams p{};
-    p.S = sp.S;
-    p.L = sp.L;
-    p.nchunkA = sp.Qpad / 16;
-    p.nkstage = sp.Qpad / (16 * kSplitKStage);
     p.P = P;
     p.Ppad = sp.Ppad;
-    p.norient = g.norient;
-    p.nelem = g.nelem;
-    p.Epad = Epad;
+    p.ntp = sp.Ppad / kSplitM;
+    p.nk = sp.Qpad / kSplitKStep;
+    p.nwork = (int64_t)p.ntp * ntiles;
     p.tiles = g.tiles_d.as<Tile>();
+    p.A = sp.slices.as<int8_t>();
+    p.B = ctx->split_cols.as<int8_t>();
     p.rowexp = sp.rowexp.as<int32_t>();
     p.colexp = ctx->split_colexp.as<int32_t>();
     p.out = out;
     p.error = ctx->split_error.as<unsigned int>();
-    // One CTA per SM: the kernel holds all 512 TMEM columns.
-    const size_t smem = kSplitSmemBytes;
-    static bool attr = false;
-    if (!attr) {
-        cuda_check(cudaFuncSetAttribute(k_contract_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-        attr = true;
-    }
-    dim3 grid((unsigned)(sp.Ppad / kSplitM), (unsigned)g.tiles.size());
-    if (grid.y > 65535)
-        fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
-    k_contract_split<<<grid, 128, smem, ctx->stream>>>(sp.mapA, mapB, p);
+    // Algorithmic INT8 operations: 2 per product, pairs (a, b) with a + b <= L.
+    int pairs = 0;
+    for (int a = 1; a <= sp.S; a++)
+        for (int b = 1; b <= sp.S; b++) pairs += (a + b <= sp.L);
+    const int kc = kstat_start(ctx, sp.S == 7 ? "contract_split" : "contract_split_fp32", 2.0 * pairs * P * Q * g.nelem);
+    if (sp.S == 7)
+        launch_split<7, 8>(ctx, p);
+    else
+        launch_split<5, 6>(ctx, p);
+    kstat_stop(ctx, kc);
     cuda_check(cudaGetLastError(), "k_contract_split");
     ctx->launches++;
 }
@@ -1105,8 +1127,12 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 const JitGroup* gp = djg.as<JitGroup>();
                 void* args[] = {&geom, &gp};
                 const int64_t n = g0.nelem * (int64_t)g0.ngp;
+                double cbytes = 0;
+                for (size_t j = k; j < k1; j++) cbytes += 8.0 * M.groups[j]->nterms * M.groups[j]->ngp * M.groups[j]->nelem;
+                const int kt = kstat_start(ctx, "coefficients", cbytes);
                 cuda_check(cudaLaunchKernel((const void*)kern, dim3(grid_for(n, 128)), dim3(128), args, 0, ctx->stream),
                            "coefficient kernel launch");
+                kstat_stop(ctx, kt);
                 ctx->launches++;
                 done = true;
             } catch (const SlgpuException&) {
@@ -1121,7 +1147,9 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 GroupDev& G = *M.groups[j];
                 CoefParams cp = coef_params(ctx, G, C + coff[j]);
                 const int64_t n = G.nelem * (int64_t)G.ngp;
+                const int kt = kstat_start(ctx, "coefficients", 8.0 * G.nterms * G.ngp * G.nelem);
                 k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
+                kstat_stop(ctx, kt);
                 cuda_check(cudaGetLastError(), "k_geometry_coef");
                 ctx->launches++;
             }
@@ -1132,6 +1160,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
 
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
 {
+    ctx->kev_tag.clear();
     if (ctx->record_only) {
         if (isconstrained != nullptr)
             M.rec_constrained.assign(isconstrained, isconstrained + M.ndofs);
@@ -1215,7 +1244,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             double* Cg = C.as<double>() + coff[gi];
             // Split precision for the larger element matrices (order >= 2);
             // right-hand sides and small matrices stay in FP64.
-            if (precision != SLGPU_PREC_FP64 && !g->rhs && (int64_t)g->ntf * g->ndof >= 64) {
+            if (precision != SLGPU_PREC_FP64 && !g->rhs && (int64_t)g->ntf * g->ndof >= 64 && split_supported(*g)) {
                 contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, M.vals.as<double>() + gvb[gi]);
                 gi++;
                 continue;
@@ -1237,7 +1266,9 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
             if (grid.y > 65535)
                 fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
+            const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
             k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
+            kstat_stop(ctx, kt);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
             ctx->launches++;
         }
@@ -1302,12 +1333,18 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
                 fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
             cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
         }
+        // Bytes: kept element values and their slots, incidences, row
+        // pointers read; A and D values written.
+        const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
+        const int kt = kstat_start(ctx, "row_values", rbytes);
         k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->stream>>>(rp);
+        kstat_stop(ctx, kt);
         cuda_check(cudaGetLastError(), "k_row_values");
         ctx->launches++;
     }
     ev_record(ctx, 3);
     cuda_check(cudaEventSynchronize(ctx->ev[3]), "sync");
+    kstat_collect(ctx);
     if (precision != SLGPU_PREC_FP64) {
         unsigned int err = 0;
         cuda_check(cudaMemcpy(&err, ctx->split_error.as<void>(), 4, cudaMemcpyDeviceToHost), "D2H split error");
@@ -1398,6 +1435,7 @@ int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** 
             return SLGPU_E_CUDA;
         }
         for (auto& e : ctx->ev) cudaEventCreate(&e);
+        cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
         // Keep freed blocks in the stream-ordered pool between assemblies.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -1434,6 +1472,7 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
         cudaStreamSynchronize(ctx->stream);
         for (auto& e : ctx->ev) cudaEventDestroy(e);
         for (auto& e : ctx->evpool) cudaEventDestroy(e);
+        for (auto& e : ctx->kev) cudaEventDestroy(e);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -1764,6 +1803,22 @@ int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5)
     if (ctx == nullptr || ms5 == nullptr)
         return SLGPU_E_ARG;
     for (int i = 0; i < 5; i++) ms5[i] = ctx->timings[i];
+    return SLGPU_OK;
+}
+
+int slgpu_kernel_stats(const slgpu_ctx* ctx, const char* family, double* total_ms, int64_t* launches, double* work)
+{
+    if (ctx == nullptr || family == nullptr)
+        return SLGPU_E_ARG;
+    auto it = ctx->kstats.find(family);
+    const Ctx::KernelStat none{};
+    const Ctx::KernelStat& k = it == ctx->kstats.end() ? none : it->second;
+    if (total_ms != nullptr)
+        *total_ms = k.ms;
+    if (launches != nullptr)
+        *launches = k.launches;
+    if (work != nullptr)
+        *work = k.work;
     return SLGPU_OK;
 }
 

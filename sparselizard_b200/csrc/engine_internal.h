@@ -3,7 +3,6 @@
 
 #include "slgpu.h"
 
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -99,7 +98,6 @@ struct GroupDev {
     struct Split {
         int S = 0, L = 0, Qpad = 0, Ppad = 0;
         DevBuf slices, rowexp;
-        CUtensorMap mapA;
     };
     std::unique_ptr<Split> split[2];
 
@@ -151,6 +149,7 @@ struct Matrix {
 
 struct Ctx {
     int device = -1;
+    int nsm = 0;  // multiprocessors of the device
     bool record_only = false;
     size_t budget = 0;
     int64_t in_use = 0;
@@ -170,6 +169,15 @@ struct Ctx {
     uint64_t constr_key[2] = {0, 0};
     std::vector<cudaEvent_t> evpool;   // per-group phase events
     int64_t launches = 0;              // kernels launched by this context
+    // Per kernel family: device time (CUDA events around each launch on the
+    // stream), launches and algorithmic work of the last process().
+    struct KernelStat {
+        double ms = 0, work = 0;
+        int64_t launches = 0;
+    };
+    std::map<std::string, KernelStat> kstats;
+    std::vector<cudaEvent_t> kev;                          // start/stop pairs
+    std::vector<std::pair<std::string, double>> kev_tag;   // family, work of each pair
     DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
     DevBuf split_error;                // device flag set by a timed-out wait
     std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source

@@ -8,14 +8,21 @@
 // Each sum_q m_a c_b is an INT8 x INT8 product summed exactly in INT32 by
 // tcgen05.mma (kind::i8); all pairs with the same level l = a+b accumulate
 // in the same TMEM accumulator (still exact: at most S products of
-// |m c| <= 127^2 per q).  The epilogue recombines the levels in FP64.
+// |m c| <= 127^2 per q).  The epilogue recombines the levels.
 //
-// Operands live in global memory in the interleaved K-major layout that the
-// UMMA "no swizzle" canonical form expects, so that one 3D TMA box lands in
-// shared memory ready for the descriptors:
-//   slices[s][chunk][row][16 bytes],  chunk = q / 16.
+// Level accumulators sit side by side in TMEM (level l at columns
+// 64(l-2) .. 64(l-2)+63), and the column slices of one K step sit side by side
+// in shared memory, so A slice a times the concatenation [c_1 | ... | c_k]
+// (N = 64k <= 256) writes every pair (a, b) straight into level a+b's
+// columns: 10 MMAs per K step for S = 7 instead of 28.
+//
+// Operands live in global memory already in the interleaved K-major layout
+// that the UMMA "no swizzle" canonical form expects, blocked so that one K
+// step of one tile is a single contiguous range (one bulk copy per operand):
+//   A (rows of M):    [orient][ptile][kstep][slice][2][128][16 bytes]
+//   B (columns of C): [etile][kstep][2][slice][64][16 bytes]
 // A core matrix (8 rows x 16 bytes) is 128 contiguous bytes; 8-row groups are
-// SBO = 128 bytes apart and 16-byte K chunks LBO = rows*16 bytes apart.
+// SBO = 128 bytes apart, the two 16-byte K chunks of a step LBO bytes apart.
 #pragma once
 
 #include "engine_internal.h"
@@ -26,19 +33,21 @@ namespace slgpu {
 
 constexpr int kSplitM = 128;     // element-matrix entries per tile (TMEM lanes)
 constexpr int kSplitN = 64;      // elements per tile (= kTileE)
-constexpr int kSplitKStage = 4;  // 16-byte K chunks per pipeline stage (64 bytes of K)
+constexpr int kSplitKStep = 32;  // bytes of K per pipeline stage (one MMA K)
+constexpr int kSplitStages = 4;  // shared-memory pipeline depth
 constexpr int kSplitMaxS = 7;    // slices per operand (levels 2..8 fit 448 TMEM columns)
+constexpr int kSplitThreads = 192;
+constexpr int kSplitABytes = 2 * kSplitM * 16;  // one slice of one K step of A
+constexpr int kSplitBBytes = 2 * kSplitN * 16;  // one slice of one K step of B
 
 struct SplitParams {
-    int S;          // slices per operand
-    int L;          // highest level kept (pairs with a + b <= L)
-    int nchunkA;    // Qpad / 16
-    int nkstage;    // Qpad / 128
-    int P, Ppad, norient;
-    int64_t nelem, Epad;
+    int P, Ppad, ntp, nk;   // entries, padded entries, row tiles, K steps
+    int64_t nwork;          // row tiles x element tiles
     const Tile* tiles;
+    const int8_t* A;        // row slices
+    const int8_t* B;        // column slices
     const int32_t* rowexp;  // [norient][Ppad]
-    const int32_t* colexp;  // [nelem]
+    const int32_t* colexp;  // [ntiles][64]
     double* out;            // [nelem][P]
     unsigned int* error;    // set on a timed-out wait
 };
@@ -53,7 +62,7 @@ struct RowSliceParams {
     const int32_t* term_tf;
     const int32_t* term_dof;
     int nterms, ngp, ntf, ndof, norient, S, Qpad, Ppad;
-    int8_t* slices;   // [S][norient][Qpad/16][Ppad][16]
+    int8_t* slices;   // [orient][ptile][kstep][S][2][128][16]
     int32_t* rowexp;  // [norient][Ppad]
 };
 
@@ -100,39 +109,49 @@ __global__ void k_slice_rows(RowSliceParams p)
         frexp(red[0], &ex);  // red[0] = f * 2^ex, f in [0.5, 1)
     if (threadIdx.x == 0)
         p.rowexp[(int64_t)o * p.Ppad + pe] = ex;
-    const int nchunk = p.Qpad / 16;
+    const int ntp = p.Ppad / kSplitM, nk = p.Qpad / kSplitKStep;
+    const int pt = pe / kSplitM, r = pe % kSplitM;
     for (int q = threadIdx.x; q < p.Qpad; q += blockDim.x) {
         int8_t sl[kSplitMaxS];
         split7(ldexp(m_entry(p, o, pe, q), -ex), p.S, sl);
+        const int ks = q / kSplitKStep, c = (q / 16) & 1;
         for (int s = 0; s < p.S; s++)
-            p.slices[((((int64_t)s * p.norient + o) * nchunk + q / 16) * p.Ppad + pe) * 16 + (q & 15)] = sl[s];
+            p.slices[(((((int64_t)o * ntp + pt) * nk + ks) * p.S + s) * 2 + c) * (kSplitM * 16) + r * 16 + (q & 15)] = sl[s];
     }
 }
 
-// Column slices of C: thread per element; C[q][e] read coalesced over e,
-// 16-byte chunks written coalesced over e.
+// Column slices of C: thread per (element tile, slot); C[q][e] is read
+// coalesced over the tile's consecutive elements and 16-byte chunks are
+// written coalesced over slots.  Empty slots get zero slices.
 struct ColSliceParams {
     const double* C;  // [Q][nelem]
-    int Q, Qpad, S;
-    int64_t nelem, Epad;
-    int8_t* slices;   // [S][Qpad/16][Epad][16]
-    int32_t* colexp;  // [nelem]
+    const Tile* tiles;
+    int Q, Qpad;
+    int64_t nelem, ntiles;
+    int8_t* slices;   // [etile][kstep][2][S][64][16]
+    int32_t* colexp;  // [etile][64]
 };
 
 template <int S>
 __global__ void k_slice_cols(ColSliceParams p)
 {
-    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= p.nelem)
+    const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t t = gt / kSplitN;
+    const int slot = (int)(gt % kSplitN);
+    if (t >= p.ntiles)
         return;
+    const Tile tile = p.tiles[t];
+    const bool valid = slot < tile.ne;
+    const int64_t e = tile.e0 + slot;
     double mx = 0;
-    for (int q = 0; q < p.Q; q++) mx = fmax(mx, fabs(p.C[(int64_t)q * p.nelem + e]));
+    if (valid)
+        for (int q = 0; q < p.Q; q++) mx = fmax(mx, fabs(p.C[(int64_t)q * p.nelem + e]));
     int ex = 0;
     if (mx > 0)
         frexp(mx, &ex);
-    p.colexp[e] = ex;
+    p.colexp[t * kSplitN + slot] = ex;
     const int nchunk = p.Qpad / 16;
-    uint4* out = reinterpret_cast<uint4*>(p.slices);
+    uint4* out = reinterpret_cast<uint4*>(p.slices) + t * (int64_t)nchunk * S * kSplitN + slot;
     for (int c = 0; c < nchunk; c++) {
         uint32_t w[S][4];
 #pragma unroll
@@ -142,7 +161,7 @@ __global__ void k_slice_cols(ColSliceParams p)
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             const int q = c * 16 + k;
-            double x = q < p.Q ? ldexp(p.C[(int64_t)q * p.nelem + e], -ex) : 0.0;
+            double x = (valid && q < p.Q) ? ldexp(p.C[(int64_t)q * p.nelem + e], -ex) : 0.0;
 #pragma unroll
             for (int s = 0; s < S; s++) {
                 const double y = x * 128.0;
@@ -151,8 +170,9 @@ __global__ void k_slice_cols(ColSliceParams p)
                 x = y - m;
             }
         }
+        // chunk c of K step c/2 lands at [kstep][c&1][s][slot]: (c*S + s) * 64.
 #pragma unroll
-        for (int s = 0; s < S; s++) out[((int64_t)s * nchunk + c) * p.Epad + e] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+        for (int s = 0; s < S; s++) out[((int64_t)c * S + s) * kSplitN] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
     }
 }
 
@@ -170,8 +190,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait for the phase with the given parity.  Gives up (false) after
+// 2^22 polls, or early once another role of the CTA has recorded a failure.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* failed)
 {
     const uint32_t a = smem_u32(bar);
     for (uint32_t it = 0; it < (1u << 22); it++) {
@@ -185,17 +211,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
             : "memory");
         if (done)
             return true;
+        if ((it & 255) == 255 && *failed)
+            return false;
     }
     return false;
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2)
+// Contiguous global -> shared copy completing on an mbarrier (16-byte
+// aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // UMMA shared-memory descriptor, K-major, no swizzle (layout type 0), version 1.
@@ -231,167 +259,229 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r)
+// 16 consecutive 32-bit TMEM columns of this thread's lane (no wait).
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, int32_t* r)
 {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
           "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 2^s as a double for a normal exponent, else ldexp (exact either way).
+__device__ __forceinline__ double scale2(double x, int s)
+{
+    if (s >= -1022 && s <= 1023)
+        return x * __longlong_as_double((long long)(s + 1023) << 52);
+    return ldexp(x, s);
 }
 
 // ---------------------------------------------------------------- contraction
 
-// Shared memory: two pipeline stages; each holds every A slice (128 rows x
-// 64 bytes = 8 KB) and every B slice (64 rows x 64 bytes = 4 KB) of one
-// 64-byte K stage, plus barriers and the TMEM address.
+// Shared memory: kSplitStages pipeline stages, each one K step (32 bytes) of
+// every A slice (128 rows) and every B slice (64 rows), plus barriers.
 struct SplitSmem {
-    alignas(1024) int8_t A[2][kSplitMaxS][kSplitKStage][kSplitM][16];
-    alignas(1024) int8_t B[2][kSplitMaxS][kSplitKStage][kSplitN][16];
-    alignas(8) uint64_t full[2];
-    uint64_t mma_done[2];
+    alignas(1024) int8_t A[kSplitStages][kSplitMaxS * kSplitABytes];
+    alignas(1024) int8_t B[kSplitStages][kSplitMaxS * kSplitBBytes];
+    alignas(8) uint64_t full[kSplitStages];
+    uint64_t empty[kSplitStages];
+    uint64_t tmem_full, tmem_empty, drain;
     uint32_t tmem;
     int failed;
-    int colexp[kSplitN];
 };
 constexpr size_t kSplitSmemBytes = sizeof(SplitSmem) + 1024;
 
-// One CTA = one (128 entries x 64 elements) tile; 128 threads (4 warps).
-// Thread 0 issues TMA and MMA; warp 0 owns the TMEM allocation; all warps
-// run the epilogue (warp w reads TMEM lanes 32w..32w+31).
-//
-// Pipeline: stage ks (64 bytes of K) loads all S A slices and S B slices into
-// buffer ks&1 under one barrier; stage ks+1 is loaded while the MMAs of stage
-// ks run, once the MMAs that last read its buffer (stage ks-1) have completed
-// (tcgen05.commit on mma_done[buffer]).  Every wait is bounded: on timeout the
-// CTA records the failure, skips its epilogue, frees its TMEM and returns.
-__global__ void __launch_bounds__(128, 1) k_contract_split(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                                                           SplitParams p)
+// Persistent, warp-specialised kernel; one CTA per SM holds all 512 TMEM
+// columns.  Work item w = (row tile w % ntp, element tile w / ntp), so the
+// CTAs working at the same time share element tiles (B is read from L2 once
+// per tile).
+//   warp 0 (one thread): bulk copies of each K step into the stage ring;
+//   warp 1 (one thread): MMAs; owns the TMEM allocation;
+//   warps 2-5: epilogue, warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31.
+// Barriers: full/empty per stage (copies -> MMA -> copies), tmem_full (MMAs of
+// a tile done -> epilogue) and tmem_empty (epilogue has read the accumulators
+// -> next tile's MMAs).  Every wait is bounded: on timeout the CTA records
+// the failure, the roles stop, outstanding copies and MMAs are waited for
+// (bounded), the TMEM is freed and the CTA returns.
+template <int S, int L>
+__global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams p)
 {
+    static_assert(S <= kSplitMaxS && L - 1 <= S && L >= 6 && L <= 8, "level layout");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     SplitSmem& sm = *reinterpret_cast<SplitSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const Tile tile = p.tiles[blockIdx.y];
-    const int p0 = blockIdx.x * kSplitM;
-    const uint32_t ncols = 512;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr uint32_t kCols = 512;
+    volatile int* failed = &sm.failed;
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)), "r"(ncols)
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)), "r"(kCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(&sm.full[0], 1);
-        mbar_init(&sm.full[1], 1);
-        mbar_init(&sm.mma_done[0], 1);
-        mbar_init(&sm.mma_done[1], 1);
+        for (int s = 0; s < kSplitStages; s++) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        mbar_init(&sm.tmem_full, 1);
+        mbar_init(&sm.tmem_empty, 4);
+        mbar_init(&sm.drain, 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (tid < kSplitN) {
-        const int64_t e = tile.e0 + tid;
-        sm.colexp[tid] = (tid < tile.ne && e < p.nelem) ? p.colexp[e] : 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
+    constexpr uint32_t kABytes = S * kSplitABytes, kBBytes = S * kSplitBBytes;
 
-    if (tid == 0) {
-        const uint32_t idesc = umma_idesc_i8(kSplitM, kSplitN);
-        const uint32_t lboA = kSplitM * 16, lboB = kSplitN * 16, sbo = 128;
-        const int amax = min(p.S, p.L - 1);
-        const uint32_t stage_bytes = (uint32_t)(p.S * kSplitKStage * (kSplitM + kSplitN) * 16);
-        uint32_t ph_full[2] = {0, 0}, ph_mma[2] = {0, 0};
-        bool pending[2] = {false, false};
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------ producer
+        int stage = 0;
+        uint32_t phase = 0;
+        uint32_t used = 0, last_parity = 0;  // per-stage bit sets
         bool ok = true;
-        auto issue = [&](int ks) {
-            const int buf = ks & 1;
-            mbar_expect_tx(&sm.full[buf], stage_bytes);
-            for (int s = 0; s < p.S; s++) {
-                tma_load_3d(&sm.A[buf][s][0][0][0], &mapA, &sm.full[buf], 0, p0,
-                            (s * p.norient + tile.orient) * p.nchunkA + ks * kSplitKStage);
-                tma_load_3d(&sm.B[buf][s][0][0][0], &mapB, &sm.full[buf], 0, tile.e0, s * p.nchunkA + ks * kSplitKStage);
-            }
-        };
-        auto drain = [&](int i) {
-            if (pending[i] && ok) {
-                ok = mbar_wait(&sm.mma_done[i], ph_mma[i]);
-                ph_mma[i] ^= 1;
-                pending[i] = false;
-            }
-        };
-        issue(0);
-        for (int ks = 0; ks < p.nkstage && ok; ks++) {
-            const int buf = ks & 1;
-            if (ks + 1 < p.nkstage) {
-                drain(buf ^ 1);
-                if (!ok)
+        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
+            const int pt = (int)(w % p.ntp);
+            const int64_t t = w / p.ntp;
+            const int orient = p.tiles[t].orient;
+            const int8_t* srcA = p.A + ((int64_t)orient * p.ntp + pt) * p.nk * kABytes;
+            const int8_t* srcB = p.B + t * p.nk * kBBytes;
+            for (int ks = 0; ks < p.nk; ks++) {
+                if (!mbar_wait(&sm.empty[stage], phase ^ 1, failed)) {
+                    ok = false;
                     break;
-                issue(ks + 1);
+                }
+                mbar_expect_tx(&sm.full[stage], kABytes + kBBytes);
+                bulk_load(sm.A[stage], srcA + (int64_t)ks * kABytes, kABytes, &sm.full[stage]);
+                bulk_load(sm.B[stage], srcB + (int64_t)ks * kBBytes, kBBytes, &sm.full[stage]);
+                used |= 1u << stage;
+                last_parity = (last_parity & ~(1u << stage)) | (phase << stage);
+                if (++stage == kSplitStages) {
+                    stage = 0;
+                    phase ^= 1;
+                }
             }
-            ok = mbar_wait(&sm.full[buf], ph_full[buf]);
-            ph_full[buf] ^= 1;
-            if (!ok)
+        }
+        if (!ok) {
+            *failed = 1;
+            atomicOr(p.error, 1u);
+        }
+        // No copy may still be in flight when the CTA leaves.
+        const int zero = 0;
+        for (int s = 0; s < kSplitStages; s++)
+            if (used & (1u << s))
+                if (!mbar_wait(&sm.full[s], (last_parity >> s) & 1, &zero))
+                    atomicOr(p.error, 2u);
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------ MMA issuer
+        int stage = 0;
+        uint32_t phase = 0;
+        bool ok = true;
+        int64_t i = 0;
+        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x, i++) {
+            if (i > 0 && !mbar_wait(&sm.tmem_empty, (uint32_t)((i - 1) & 1), failed)) {
+                ok = false;
                 break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            for (int a = 1; a <= amax; a++) {
-                for (int b = 1; b <= p.S && a + b <= p.L; b++) {
-                    const int level = a + b;
-                    const uint32_t dcol = tmem + (uint32_t)((level - 2) * kSplitN);
-                    const int afirst = max(1, level - p.S);
-                    for (int k = 0; k < kSplitKStage / 2; k++) {
-                        const uint64_t ad = umma_desc(smem_u32(&sm.A[buf][a - 1][2 * k][0][0]), lboA, sbo);
-                        const uint64_t bd = umma_desc(smem_u32(&sm.B[buf][b - 1][2 * k][0][0]), lboB, sbo);
-                        const uint32_t acc = (ks == 0 && k == 0 && a == afirst) ? 0u : 1u;
-                        umma_i8(dcol, ad, bd, idesc, acc);
+            for (int ks = 0; ks < p.nk; ks++) {
+                if (!mbar_wait(&sm.full[stage], phase, failed)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_base = smem_u32(sm.A[stage]), b_base = smem_u32(sm.B[stage]);
+#pragma unroll
+                for (int a0 = 0; a0 < S; a0++) {
+                    const int nbt = (S < L - 1 - a0) ? S : L - 1 - a0;  // b = 1 .. min(S, L - a)
+                    const uint64_t ad = umma_desc(a_base + a0 * kSplitABytes, kSplitM * 16, 128);
+#pragma unroll
+                    for (int b0 = 0; b0 < nbt; b0 += 4) {
+                        const int nb = (nbt - b0) < 4 ? (nbt - b0) : 4;
+                        const uint64_t bd = umma_desc(b_base + b0 * kSplitN * 16, S * kSplitN * 16, 128);
+                        umma_i8(tmem + (uint32_t)(kSplitN * (a0 + b0)), ad, bd, umma_idesc_i8(kSplitM, kSplitN * nb),
+                                (ks > 0 || a0 > 0) ? 1u : 0u);
+                    }
+                }
+                umma_commit(&sm.empty[stage]);
+                if (++stage == kSplitStages) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+            if (ok)
+                umma_commit(&sm.tmem_full);
+        }
+        if (!ok) {
+            *failed = 1;
+            atomicOr(p.error, 1u);
+        }
+        // Every MMA issued by this thread completes before the TMEM is freed.
+        const int zero = 0;
+        umma_commit(&sm.drain);
+        if (!mbar_wait(&sm.drain, 0, &zero))
+            atomicOr(p.error, 2u);
+    } else if (warp >= 2) {
+        // ------------------------------------------------ epilogue
+        const int quarter = warp & 3;
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+        int64_t i = 0;
+        for (int64_t w = blockIdx.x; w < p.nwork; w += gridDim.x, i++) {
+            if (!mbar_wait(&sm.tmem_full, (uint32_t)(i & 1), failed)) {
+                *failed = 1;
+                atomicOr(p.error, 1u);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int pt = (int)(w % p.ntp);
+            const int64_t t = w / p.ntp;
+            const Tile tile = p.tiles[t];
+            const int pe = pt * kSplitM + quarter * 32 + lane;
+            const int rex = p.rowexp[(int64_t)tile.orient * p.Ppad + pe] - 35;
+            const int32_t* ce = p.colexp + t * kSplitN;
+            double* outp = p.out + (int64_t)tile.e0 * p.P + pe;
+#pragma unroll 1
+            for (int c0 = 0; c0 < kSplitN; c0 += 16) {
+                int32_t r[L - 1][16];
+#pragma unroll
+                for (int l = 0; l < L - 1; l++) tmem_ld16_nowait(lane_base + (uint32_t)(l * kSplitN + c0), r[l]);
+                tmem_ld_wait();
+                if (c0 + 16 == kSplitN) {
+                    // All accumulators are in registers: release the TMEM.
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0)
+                        mbar_arrive(&sm.tmem_empty);
+                }
+                if (pe < p.P) {
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        // V = 2^-35 (H + 2^-21 Lo): H = sum_{l<=5} r_l 2^(7(5-l)),
+                        // Lo = sum_{l>=6} r_l 2^(7(8-l)); both exact in int64.
+                        long long H = 0, Lo = 0;
+#pragma unroll
+                        for (int l = 2; l <= 5; l++) H = H * 128 + r[l - 2][j];
+#pragma unroll
+                        for (int l = 6; l <= L; l++) Lo = Lo * 128 + r[l - 2][j];
+                        Lo <<= 7 * (8 - L);
+                        const double d = fma((double)Lo, 0x1p-21, (double)H);
+                        const int ee = c0 + j;
+                        if (ee < tile.ne)
+                            outp[(int64_t)ee * p.P] = scale2(d, rex + ce[ee]);
                     }
                 }
             }
-            umma_commit(&sm.mma_done[buf]);
-            pending[buf] = true;
-        }
-        drain(0);
-        drain(1);
-        if (!ok) {
-            sm.failed = 1;
-            atomicOr(p.error, 1u);
         }
     }
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    if (!sm.failed) {
-        // Epilogue: thread t owns TMEM lane (row) t = entry p0 + t.
-        const int pe = p0 + tid;
-        const int rex = p.rowexp[(int64_t)tile.orient * p.Ppad + min(pe, p.Ppad - 1)];
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-        for (int c0 = 0; c0 < kSplitN; c0 += 16) {
-            double v[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) v[i] = 0.0;
-            for (int level = p.L; level >= 2; level--) {
-                uint32_t r[16];
-                tmem_ld16(tmem + lane_base + (uint32_t)((level - 2) * kSplitN + c0), r);
-                const double sc = ldexp(1.0, -7 * level);
-#pragma unroll
-                for (int i = 0; i < 16; i++) v[i] += (double)(int32_t)r[i] * sc;
-            }
-            if (pe < p.P) {
-#pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const int ee = c0 + i;
-                    if (ee < tile.ne)
-                        p.out[(int64_t)(tile.e0 + ee) * p.P + pe] = ldexp(v[i], rex + sm.colexp[ee]);
-                }
-            }
-        }
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 }  // namespace slgpu

@@ -64,6 +64,19 @@ def test_split_element_matrices(ctx, seed, norient, nterms, ngp1):
         assert err.max() <= tol, f"precision {prec}: per-element Frobenius error {err.max():.3e} > {tol:g}"
 
 
+@pytest.mark.parametrize("seed,grid,ntf,ndof,norient,nterms,ngp1", [(4, 100, 20, 20, 3, 5, 4), (5, 40, 27, 27, 1, 9, 3)])
+def test_split_many_tiles(ctx, seed, grid, ntf, ndof, norient, nterms, ngp1):
+    """Several row tiles and more work items than multiprocessors, so that
+    every CTA of the persistent kernel reuses its stages and accumulators."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gb, xyz, conn = S.group(rng, nelem_grid=grid, ntf=ntf, ndof=ndof, nterms=nterms, ngp1=ngp1, norient=norient, ndests=1)
+    ref = _element_matrices(ctx, gb, xyz, conn, abi.PREC_FP64)
+    for prec, tol in ((abi.PREC_SPLIT, 1e-10), (abi.PREC_FP32, 1e-6)):
+        got = _element_matrices(ctx, gb, xyz, conn, prec)
+        err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert err.max() <= tol, f"precision {prec}: per-element Frobenius error {err.max():.3e} > {tol:g}"
+
+
 def test_split_dropin_elasticity(ref_lib, gpu_lib, tmp_path):
     msh = str(tmp_path / "h.msh")
     meshgen.hex_mesh(msh, 4, jitter=0.15, seed=1)
