@@ -126,6 +126,37 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+# DRAM bytes (read + write) per launch of the dominant kernels, from ncu
+# captures of a smaller case of the same workload, per element of the
+# launch's group (traffic grows in proportion to the elements).  Summaries
+# and the commands that made them are under profiles/.
+TRAFFIC_PER_ELEMENT = {}
+
+
+def traffic_per_launch(workload, family, n, launches):
+    per = TRAFFIC_PER_ELEMENT.get((workload, family))
+    if per is None:
+        return None
+    nelem = {"c2": n ** 3, "c1": n * n}.get(workload)
+    return None if nelem is None else per * nelem
+
+
+FAMILIES = ("coefficients", "contract_fp64", "slice_cols", "contract_split", "contract_split_fp32", "row_values")
+
+
+def kernel_stats(lib, ctx, acc):
+    """Adds the per-kernel-family event times of the last process() to acc."""
+    for fam in FAMILIES:
+        ms, nl, wk = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+        lib.slgpu_kernel_stats(ctx, fam.encode(), ctypes.byref(ms), ctypes.byref(nl), ctypes.byref(wk))
+        if nl.value > 0:
+            a = acc.setdefault(fam, {"ms": 0.0, "launches": 0, "work": 0.0})
+            a["ms"] += ms.value
+            a["launches"] += nl.value
+            a["work"] += wk.value
+    return acc
+
+
 def dist_setup(n_gpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -237,6 +268,7 @@ def run_ours(args, spec):
 
     # ---- device-resident steps
     phase = np.zeros(5)
+    stats = {}
     launches0 = lib.slgpu_kernel_launches(ctx)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
@@ -247,6 +279,7 @@ def run_ours(args, spec):
             flush.zero_()
             torch.cuda.synchronize()
             phase += process()
+            kernel_stats(lib, ctx, stats)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -281,26 +314,61 @@ def run_ours(args, spec):
     e2e_s_max, = allreduce([e2e_s], torch.distributed.ReduceOp.MAX) if world > 1 else [e2e_s]
     e2e_value = total_nnz / e2e_s_max
 
-    # ---- roofline of the dominant kernel
+    # ---- the plain FP64 GPU path on the same resident pattern, and the
+    # split path's error against it on the assembled matrix
+    fp64 = None
+    if prec != abi.PREC_FP64:
+        split_vals = avals.numpy()[: info.nnzA].copy()
+        prec_run = prec
+        prec = abi.PREC_FP64
+        for _ in range(args.warmup):
+            process()
+        ph64 = np.zeros(5)
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ph64 += process()
+        st = lib.slgpu_matrix_download_values(ctx, handle, ctypes.cast(avals.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                              ctypes.cast(dvals.data_ptr(), ctypes.POINTER(ctypes.c_double)))
+        assert st == 0
+        ref = avals.numpy()[: info.nnzA]
+        num = den = 0.0
+        for a in range(0, ref.size, 1 << 26):
+            d = split_vals[a:a + (1 << 26)] - ref[a:a + (1 << 26)]
+            num += float(d @ d)
+            den += float(ref[a:a + (1 << 26)] @ ref[a:a + (1 << 26)])
+        del split_vals
+        ms64 = ph64[4] / args.steps
+        ms64_max, = allreduce([ms64], torch.distributed.ReduceOp.MAX) if world > 1 else [ms64]
+        fp64 = {"value": total_nnz / (ms64_max * 1e-3), "ms_per_step": ms64_max,
+                "contraction_ms": ph64[1] / args.steps,
+                "rel_fro_err_vs_fp64": (num / den) ** 0.5 if den > 0 else 0.0,
+                "speedup": ms64_max / dev_ms_max}
+        prec = prec_run
+
+    # ---- roofline of the dominant kernel (per-kernel events over the timed steps)
     hbm, bf16, peak_kind = peaks()
     ph = phase / args.steps
-    dominant = int(np.argmax([ph[0], ph[1], ph[3]]))
-    if dominant == 1:
-        flops = work.contraction_flops
-        achieved = flops / (ph[1] * 1e-3) / 1e12
-        roof = {"kernel": "k_contract_fp64", "bound": "fp64", "achieved": achieved, "unit": "TFLOP/s",
-                "peak": 40.0, "peak_kind": "nominal B200 FP64 (no measured FP64 peak on this pool)",
-                "frac": achieved / 40.0, "traffic": None}
-    elif dominant == 2:
-        byts = 8.0 * work.nvalid + 4.0 * work.nvalid + 8.0 * nnz
-        achieved = byts / (ph[3] * 1e-3) / 1e9
-        roof = {"kernel": "k_csr_values", "bound": "hbm", "achieved": achieved, "unit": "GB/s", "peak": hbm,
-                "peak_kind": peak_kind, "frac": achieved / hbm, "traffic": None}
+    dom = max(stats, key=lambda f: stats[f]["ms"])
+    k = stats[dom]
+    rate = k["work"] / (k["ms"] * 1e-3)
+    kernel_names = {"coefficients": "slgpu_coef (runtime-compiled)", "contract_fp64": "k_contract_fp64",
+                    "slice_cols": "k_slice_cols", "contract_split": "k_contract_split<7,8>",
+                    "contract_split_fp32": "k_contract_split<5,6>", "row_values": "k_row_values"}
+    if dom.startswith("contract_split"):
+        peak = 2.0 * bf16
+        roof = {"kernel": kernel_names[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_kind": f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops",
+                "frac": rate / 1e12 / peak}
+    elif dom == "contract_fp64":
+        roof = {"kernel": kernel_names[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": 40.0, "unit": "TFLOP/s",
+                "peak_kind": "nominal B200 FP64 40 TFLOP/s (FP64 vector and tensor rates are equal; not measured here)",
+                "frac": rate / 1e12 / 40.0}
     else:
-        byts = 8.0 * work.coef_points * max(1, work.ngroups)
-        achieved = byts / (ph[0] * 1e-3) / 1e9
-        roof = {"kernel": "k_geometry_coef", "bound": "hbm", "achieved": achieved, "unit": "GB/s", "peak": hbm,
-                "peak_kind": peak_kind, "frac": achieved / hbm, "traffic": None}
+        roof = {"kernel": kernel_names[dom], "bound": "hbm", "achieved": rate / 1e9, "peak": hbm, "unit": "GB/s",
+                "peak_kind": peak_kind, "frac": rate / 1e9 / hbm}
+    roof["ms_per_launch"] = k["ms"] / k["launches"]
+    roof["traffic"] = traffic_per_launch(args.workload, dom, n, k["launches"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
@@ -319,6 +387,8 @@ def run_ours(args, spec):
                        "ncoo": int(work.ncoo), "groups": int(work.ngroups), "l2": l2_rule,
                        "parallelism": f"replicas{world}"},
             "phases_ms": {"geometry_coef": ph[0], "contraction": ph[1], "values": ph[3], "total": ph[4]},
+            "kernels": stats,
+            "fp64_gpu": fp64,
             "first_assembly": first,
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_s_max * 1e3,
                     "h2d_bytes_per_step": int(24 * nnodes), "d2h_bytes_per_step": int(8 * (info.nnzA + info.nnzD))},
@@ -340,7 +410,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split", "fp32"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split", "fp32"])
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (elements per side)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -38,6 +38,7 @@ struct JitGroup {
     const double* fielddata;
     const double* term_scale;
     double* C;
+    int* elemexp;
 };
 )";
 
@@ -134,10 +135,14 @@ std::string jit_coef_source(const std::vector<const GroupDev*>& batch)
             }
             s << ";\n";
         }
+        s << "    double cmax = 0;\n";
         for (int t = 0; t < G.nterms; t++) {
             const int c = G.term_node[t];
-            s << "    q.C[((i64)" << t << " * " << ngp << " + g) * p.nelem + e] = v" << c << " * q.term_scale[" << t << "] * wdet;\n";
+            s << "    { const double c = v" << c << " * q.term_scale[" << t << "] * wdet; q.C[((i64)" << t << " * " << ngp
+              << " + g) * p.nelem + e] = c; cmax = fmax(cmax, fabs(c)); }\n";
         }
+        // Exponent of the element's largest coefficient for split precision.
+        s << "    if (q.elemexp != nullptr && cmax > 0) { int ex; frexp(cmax, &ex); atomicMax(q.elemexp + e, ex); }\n";
         s << "  }\n";
     }
     s << "}\n";

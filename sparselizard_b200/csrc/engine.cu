@@ -998,32 +998,46 @@ static bool split_supported(const GroupDev& g)
     return Q > 0 && Q <= 16384;
 }
 
-template <int S, int L>
+template <int S, int L, int NE>
 static void launch_split(Ctx* ctx, const SplitParams& p)
 {
     static bool attr = false;
+    constexpr size_t smem = split_smem_bytes<NE>();
     if (!attr) {
-        cuda_check(cudaFuncSetAttribute(k_contract_split<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemBytes),
+        cuda_check(cudaFuncSetAttribute(k_contract_split<S, L, NE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                    "smem attribute");
         attr = true;
     }
     const int64_t grid = std::min<int64_t>(p.nwork, std::max(ctx->nsm, 1));
-    k_contract_split<S, L><<<(unsigned)grid, kSplitThreads, kSplitSmemBytes, ctx->stream>>>(p);
+    k_contract_split<S, L, NE><<<(unsigned)grid, kSplitThreads, smem, ctx->stream>>>(p);
 }
 
-// Split contraction of one group: column slices of C, then the tcgen05 kernel.
-static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, double* out)
+// Element-tile width of the split kernel: SLGPU_SPLIT_TILE=32 or 64 (default 64).
+static int split_tile_width()
+{
+    static const int ne = [] {
+        const char* v = std::getenv("SLGPU_SPLIT_TILE");
+        return (v != nullptr && std::strcmp(v, "32") == 0) ? 32 : 64;
+    }();
+    return ne;
+}
+
+// Split contraction of one group: column slices of C (exponents per element
+// from the coefficient kernel), then the tcgen05 kernel.
+static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out)
 {
     GroupDev::Split& sp = ensure_split(ctx, g, tier);
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+    const int NE = split_tile_width();
     const int64_t ntiles = (int64_t)g.tiles.size();
-    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * kSplitN;
+    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
     if (ctx->split_cols.bytes() < colbytes)
         ctx->split_cols.alloc(ctx, colbytes);
-    if (ctx->split_colexp.bytes() < (size_t)ntiles * kSplitN * 4)
-        ctx->split_colexp.alloc(ctx, (size_t)ntiles * kSplitN * 4);
+    if (ctx->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
+        ctx->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
     ColSliceParams cs{};
     cs.C = C;
+    cs.elemexp = elemexp;
     cs.tiles = g.tiles_d.as<Tile>();
     cs.Q = Q;
     cs.Qpad = sp.Qpad;
@@ -1031,12 +1045,16 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     cs.ntiles = ntiles;
     cs.slices = ctx->split_cols.as<int8_t>();
     cs.colexp = ctx->split_colexp.as<int32_t>();
-    const dim3 cgrid = grid_for(ntiles * kSplitN, 128);
-    const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + (double)colbytes + 4.0 * ntiles * kSplitN);
-    if (sp.S == 7)
-        k_slice_cols<7><<<cgrid, 128, 0, ctx->stream>>>(cs);
+    const dim3 cgrid = grid_for(ntiles * 64, 128);
+    const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + 4.0 * g.nelem + (double)colbytes + 4.0 * ntiles * 64);
+    if (sp.S == 7 && NE == 64)
+        k_slice_cols<7, 64><<<cgrid, 128, 0, ctx->stream>>>(cs);
+    else if (sp.S == 7)
+        k_slice_cols<7, 32><<<cgrid, 128, 0, ctx->stream>>>(cs);
+    else if (sp.S == 5 && NE == 64)
+        k_slice_cols<5, 64><<<cgrid, 128, 0, ctx->stream>>>(cs);
     else if (sp.S == 5)
-        k_slice_cols<5><<<cgrid, 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<5, 32><<<cgrid, 128, 0, ctx->stream>>>(cs);
     else
         fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
     kstat_stop(ctx, kt);
@@ -1047,7 +1065,7 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     p.Ppad = sp.Ppad;
     p.ntp = sp.Ppad / kSplitM;
     p.nk = sp.Qpad / kSplitKStep;
-    p.nwork = (int64_t)p.ntp * ntiles;
+    p.nwork = (int64_t)p.ntp * ntiles * (64 / NE);
     p.tiles = g.tiles_d.as<Tile>();
     p.A = sp.slices.as<int8_t>();
     p.B = ctx->split_cols.as<int8_t>();
@@ -1060,13 +1078,25 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, dou
     for (int a = 1; a <= sp.S; a++)
         for (int b = 1; b <= sp.S; b++) pairs += (a + b <= sp.L);
     const int kc = kstat_start(ctx, sp.S == 7 ? "contract_split" : "contract_split_fp32", 2.0 * pairs * P * Q * g.nelem);
-    if (sp.S == 7)
-        launch_split<7, 8>(ctx, p);
+    if (sp.S == 7 && NE == 64)
+        launch_split<7, 8, 64>(ctx, p);
+    else if (sp.S == 7)
+        launch_split<7, 8, 32>(ctx, p);
+    else if (NE == 64)
+        launch_split<5, 6, 64>(ctx, p);
     else
-        launch_split<5, 6>(ctx, p);
+        launch_split<5, 6, 32>(ctx, p);
     kstat_stop(ctx, kc);
     cuda_check(cudaGetLastError(), "k_contract_split");
     ctx->launches++;
+}
+
+// Whether a group's contraction runs in split precision: element matrices
+// with at least 64 entries (order >= 2 in practice); right-hand sides and
+// small matrices stay in FP64.
+static bool uses_split(const GroupDev& g, int precision)
+{
+    return precision != SLGPU_PREC_FP64 && !g.rhs && (int64_t)g.ntf * g.ndof >= 64 && split_supported(g);
 }
 
 // Host mirror of the runtime-compiled kernel's parameter structs (coef_jit.cu).
@@ -1085,13 +1115,15 @@ struct JitGroup {
     const double* fielddata;
     const double* term_scale;
     double* C;
+    int32_t* elemexp;  // nullptr, or per element: atomicMax of frexp exponents of |C|
 };
 
 // Geometry + coefficients of every group into C (offsets coff).  Consecutive
 // groups with the same geometry key run as one runtime-compiled kernel; the
 // interpreter kernel is used when SLGPU_COEF_INTERPRETER=1 or when a kernel
 // cannot be compiled.
-static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vector<int64_t>& coff)
+static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vector<int64_t>& coff, int32_t* elemexp,
+                                const std::vector<int64_t>& eoff)
 {
     static const bool interp_only = [] {
         const char* v = std::getenv("SLGPU_COEF_INTERPRETER");
@@ -1117,7 +1149,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 for (size_t j = k; j < k1; j++) {
                     GroupDev& G = *M.groups[j];
                     jg.push_back(JitGroup{G.tables.as<double>(), G.elemdata.as<double>(), G.fielddata.as<double>(),
-                                          G.term_scale_d.as<double>(), C + coff[j]});
+                                          G.term_scale_d.as<double>(), C + coff[j], eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
                 }
                 DevBuf djg;
                 upload(ctx, djg, jg);
@@ -1146,6 +1178,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
             for (size_t j = k; j < k1; j++) {
                 GroupDev& G = *M.groups[j];
                 CoefParams cp = coef_params(ctx, G, C + coff[j]);
+                cp.elemexp = eoff[j] >= 0 ? elemexp + eoff[j] : nullptr;
                 const int64_t n = G.nelem * (int64_t)G.ngp;
                 const int kt = kstat_start(ctx, "coefficients", 8.0 * G.nterms * G.ngp * G.nelem);
                 k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
@@ -1235,8 +1268,22 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         ctx->evpool.push_back(e);
     }
+    // Split-precision groups: per-element exponents of the coefficients,
+    // gathered by the coefficient kernels (atomicMax from a very negative start).
+    std::vector<int64_t> eoff(M.groups.size(), -1);
+    int64_t etot = 0;
+    for (size_t k = 0; k < M.groups.size(); k++)
+        if (uses_split(*M.groups[k], precision)) {
+            eoff[k] = etot;
+            etot += M.groups[k]->nelem;
+        }
+    DevBuf E;
+    if (etot > 0) {
+        E.alloc(ctx, (size_t)etot * 4);
+        cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->stream), "memset");
+    }
     cuda_check(cudaEventRecord(ctx->evpool[0], ctx->stream), "cudaEventRecord");
-    launch_coefficients(ctx, M, C.as<double>(), coff);
+    launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff);
     cuda_check(cudaEventRecord(ctx->evpool[1], ctx->stream), "cudaEventRecord");
     size_t gi = 0;
     for (auto& g : M.groups) {
@@ -1244,8 +1291,8 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             double* Cg = C.as<double>() + coff[gi];
             // Split precision for the larger element matrices (order >= 2);
             // right-hand sides and small matrices stay in FP64.
-            if (precision != SLGPU_PREC_FP64 && !g->rhs && (int64_t)g->ntf * g->ndof >= 64 && split_supported(*g)) {
-                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, M.vals.as<double>() + gvb[gi]);
+            if (uses_split(*g, precision)) {
+                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], M.vals.as<double>() + gvb[gi]);
                 gi++;
                 continue;
             }

@@ -62,6 +62,7 @@ struct CoefParams {
     const double* term_scale;
     int nterms;
     double* C;  // [nterms][ngp][nelem]
+    int32_t* elemexp;  // nullptr, or [nelem]: atomicMax of the frexp exponents of |C|
 };
 
 // Geometry (J, detJ, invJ; src/field/jacobian.cpp:248-349 and :396-504 for
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
         inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
     }
     const double wdet = p.weights[g] * fabs(det);
+    double cmax = 0;
 
     double s[kMaxSlots];
     for (int k = 0; k < p.nprog; k++) {
@@ -144,11 +146,19 @@ __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
         case SLGPU_OP_INV: v = 1.0 / s[in.a]; break;
         case SLGPU_OP_NEG: v = -s[in.a]; break;
         case SLGPU_OP_POW: v = pow(s[in.a], s[in.b]); break;
-        case INSTR_STORE:
-            p.C[((int64_t)in.b * p.ngp + g) * p.nelem + e] = s[in.a] * p.term_scale[in.b] * wdet;
+        case INSTR_STORE: {
+            const double c = s[in.a] * p.term_scale[in.b] * wdet;
+            p.C[((int64_t)in.b * p.ngp + g) * p.nelem + e] = c;
+            cmax = fmax(cmax, fabs(c));
             continue;
         }
+        }
         s[in.dst] = v;
+    }
+    if (p.elemexp != nullptr && cmax > 0) {
+        int ex;
+        frexp(cmax, &ex);
+        atomicMax(p.elemexp + e, ex);
     }
 }
 
@@ -575,6 +585,33 @@ struct RowParams {
 // value buffer) into a shared-memory copy of the row through the slot map.
 // Within one incidence every lane hits a different slot, so the sum of each
 // CSR entry is formed in incidence order: deterministic, no atomics.
+//
+// The loads of kRowBatch incidences are issued before any of them is added
+// (lane j holds entry j of each), so a warp keeps that many element-matrix
+// rows in flight instead of one; the additions still run in incidence order.
+// Incidences flagged serial (duplicate addresses) or wider than a warp are
+// added by their own loop at their place in the order.
+constexpr int kRowBatch = 8;
+
+__device__ __forceinline__ void row_add_generic(double* buf, const RowSeg& sg, const double* v, const int16_t* sm, bool serial,
+                                                int lane)
+{
+    if (serial) {
+        if (lane == 0)
+            for (int j = 0; j < sg.width; j++) {
+                const int s = sm[j];
+                if (s >= 0)
+                    buf[s] += v[j] * sg.mult;
+            }
+    } else {
+        for (int j = lane; j < sg.width; j += 32) {
+            const int s = sm[j];
+            if (s >= 0)
+                buf[s] += v[j] * sg.mult;
+        }
+    }
+}
+
 __global__ void k_row_values(RowParams p)
 {
     extern __shared__ double rowbuf[];
@@ -588,28 +625,42 @@ __global__ void k_row_values(RowParams p)
     const int L = la + ld;
     for (int s = lane; s < L; s += 32) buf[s] = 0.0;
     __syncwarp();
-    const uint32_t k1 = p.inc_ptr[r + 1];
-    for (uint32_t k = p.inc_ptr[r]; k < k1; k++) {
-        const unsigned long long pk = p.inc[k];
-        const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-        const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
-        const double* v = p.vals + sg.val_base + (coo - sg.coo_base);
-        const int16_t* sm = p.slotmap + coo;
-        if (pk >> 63) {
-            if (lane == 0)
-                for (int j = 0; j < sg.width; j++) {
-                    const int s = sm[j];
-                    if (s >= 0)
-                        buf[s] += v[j] * sg.mult;
+    const uint32_t k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+    for (uint32_t kb = k0; kb < k1; kb += 32) {
+        const int nkb = (int)min(32u, k1 - kb);
+        const unsigned long long mine = lane < nkb ? p.inc[kb + lane] : 0ull;
+        for (int u = 0; u < nkb; u += kRowBatch) {
+            double val[kRowBatch];
+            int slot[kRowBatch];
+#pragma unroll
+            for (int x = 0; x < kRowBatch; x++) {
+                slot[x] = -1;
+                val[x] = 0.0;
+                const unsigned long long pk = __shfl_sync(0xffffffffu, mine, (u + x) & 31);
+                if (u + x < nkb) {
+                    const RowSeg& sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+                    const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
+                    if (!(pk >> 63) && sg.width <= 32 && lane < sg.width) {
+                        slot[x] = p.slotmap[coo + lane];
+                        val[x] = p.vals[sg.val_base + (coo - sg.coo_base) + lane];
+                    }
                 }
-        } else {
-            for (int j = lane; j < sg.width; j += 32) {
-                const int s = sm[j];
-                if (s >= 0)
-                    buf[s] += v[j] * sg.mult;
+            }
+#pragma unroll
+            for (int x = 0; x < kRowBatch; x++) {
+                const unsigned long long pk = __shfl_sync(0xffffffffu, mine, (u + x) & 31);
+                if (u + x < nkb) {
+                    const RowSeg& sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+                    if ((pk >> 63) || sg.width > 32) {
+                        const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
+                        row_add_generic(buf, sg, p.vals + sg.val_base + (coo - sg.coo_base), p.slotmap + coo, (pk >> 63) != 0, lane);
+                    } else if (slot[x] >= 0) {
+                        buf[slot[x]] += val[x] * sg.mult;
+                    }
+                }
+                __syncwarp();
             }
         }
-        __syncwarp();
     }
     if (p.dense != nullptr) {
         if (lane == 0)

@@ -11,16 +11,17 @@
 // |m c| <= 127^2 per q).  The epilogue recombines the levels.
 //
 // Level accumulators sit side by side in TMEM (level l at columns
-// 64(l-2) .. 64(l-2)+63), and the column slices of one K step sit side by side
-// in shared memory, so A slice a times the concatenation [c_1 | ... | c_k]
-// (N = 64k <= 256) writes every pair (a, b) straight into level a+b's
-// columns: 10 MMAs per K step for S = 7 instead of 28.
+// NE(l-2) .. NE(l-2)+NE-1 for an element tile of NE columns), and the column
+// slices of one K step sit side by side in shared memory, so A slice a times
+// the concatenation [c_1 | ... | c_k] (N = NE k <= 256) writes every pair
+// (a, b) straight into level a+b's columns: for S = 7, 10 MMAs per K step
+// (NE = 64) or 7 (NE = 32) instead of 28.
 //
 // Operands live in global memory already in the interleaved K-major layout
 // that the UMMA "no swizzle" canonical form expects, blocked so that one K
 // step of one tile is a single contiguous range (one bulk copy per operand):
 //   A (rows of M):    [orient][ptile][kstep][slice][2][128][16 bytes]
-//   B (columns of C): [etile][kstep][2][slice][64][16 bytes]
+//   B (columns of C): [unit][kstep][2][slice][NE][16 bytes]
 // A core matrix (8 rows x 16 bytes) is 128 contiguous bytes; 8-row groups are
 // SBO = 128 bytes apart, the two 16-byte K chunks of a step LBO bytes apart.
 #pragma once
@@ -32,25 +33,48 @@
 namespace slgpu {
 
 constexpr int kSplitM = 128;     // element-matrix entries per tile (TMEM lanes)
-constexpr int kSplitN = 64;      // elements per tile (= kTileE)
 constexpr int kSplitKStep = 32;  // bytes of K per pipeline stage (one MMA K)
-constexpr int kSplitStages = 4;  // shared-memory pipeline depth
-constexpr int kSplitMaxS = 7;    // slices per operand (levels 2..8 fit 448 TMEM columns)
-constexpr int kSplitThreads = 192;
+constexpr int kSplitMaxS = 7;    // slices per operand (levels 2..8)
+constexpr int kSplitEpiWarps = 8;
+constexpr int kSplitThreads = 64 + 32 * kSplitEpiWarps;
 constexpr int kSplitABytes = 2 * kSplitM * 16;  // one slice of one K step of A
-constexpr int kSplitBBytes = 2 * kSplitN * 16;  // one slice of one K step of B
+
+// Element-tile width NE (columns of one accumulator level) and what follows
+// from it.  NE = 64: one accumulator (7 levels x 64 = 448 TMEM columns), the
+// epilogue of a tile runs between its MMAs and the next tile's.  NE = 32: two
+// accumulators (2 x 224 columns), the epilogue of one tile overlaps the MMAs
+// of the next; A (the rows of M) is read twice as often per element.
+template <int NE>
+struct SplitShape {
+    static constexpr int kUnits = 64 / NE;               // element tiles per 64-element tile
+    static constexpr int kBufs = NE == 32 ? 2 : 1;       // TMEM accumulators
+    static constexpr int kStages = NE == 32 ? 6 : 4;     // shared-memory pipeline depth
+    static constexpr int kBBytes = 2 * NE * 16;          // one slice of one K step of B
+    static constexpr int kGroup = 256 / NE;              // B slices per MMA (N <= 256)
+};
 
 struct SplitParams {
     int P, Ppad, ntp, nk;   // entries, padded entries, row tiles, K steps
-    int64_t nwork;          // row tiles x element tiles
-    const Tile* tiles;
+    int64_t nwork;          // row tiles x element units
+    const Tile* tiles;      // 64-element tiles; unit u = tile u / kUnits, part u % kUnits
     const int8_t* A;        // row slices
     const int8_t* B;        // column slices
     const int32_t* rowexp;  // [norient][Ppad]
-    const int32_t* colexp;  // [ntiles][64]
+    const int32_t* colexp;  // [ntiles][64]: exponent of each slot
     double* out;            // [nelem][P]
     unsigned int* error;    // set on a timed-out wait
 };
+
+// Elements [e0, e0 + ne) and orientation of element unit u (ne <= 0: empty).
+template <int NE>
+__device__ __forceinline__ Tile split_unit(const Tile* tiles, int64_t u)
+{
+    Tile t = tiles[u / SplitShape<NE>::kUnits];
+    const int part = (int)(u % SplitShape<NE>::kUnits) * NE;
+    t.e0 += part;
+    t.ne = min(t.ne - part, NE);
+    return t;
+}
 
 // ---------------------------------------------------------------- slicing
 
@@ -120,39 +144,47 @@ __global__ void k_slice_rows(RowSliceParams p)
     }
 }
 
-// Column slices of C: thread per (element tile, slot); C[q][e] is read
-// coalesced over the tile's consecutive elements and 16-byte chunks are
-// written coalesced over slots.  Empty slots get zero slices.
+// Column slices of C: thread per (64-element tile, slot); C[q][e] is read
+// once, coalesced over the tile's consecutive elements, and 16-byte chunks
+// are written coalesced over slots.  The exponent of each element (largest
+// |C[q][e]| = f 2^ex, f in [0.5, 1)) comes from the coefficient kernel.
+// Empty slots get zero slices.
 struct ColSliceParams {
     const double* C;  // [Q][nelem]
+    const int32_t* elemexp;  // [nelem]; below -1100: the column is zero
     const Tile* tiles;
     int Q, Qpad;
     int64_t nelem, ntiles;
-    int8_t* slices;   // [etile][kstep][2][S][64][16]
-    int32_t* colexp;  // [etile][64]
+    int8_t* slices;   // [unit][kstep][2][S][NE][16]
+    int32_t* colexp;  // [ntiles][64]
 };
 
-template <int S>
+template <int S, int NE>
 __global__ void k_slice_cols(ColSliceParams p)
 {
     const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t t = gt / kSplitN;
-    const int slot = (int)(gt % kSplitN);
+    const int64_t t = gt / 64;
+    const int slot = (int)(gt % 64);
     if (t >= p.ntiles)
         return;
     const Tile tile = p.tiles[t];
     const bool valid = slot < tile.ne;
     const int64_t e = tile.e0 + slot;
-    double mx = 0;
-    if (valid)
-        for (int q = 0; q < p.Q; q++) mx = fmax(mx, fabs(p.C[(int64_t)q * p.nelem + e]));
-    int ex = 0;
-    if (mx > 0)
-        frexp(mx, &ex);
-    p.colexp[t * kSplitN + slot] = ex;
+    int ex = valid ? p.elemexp[e] : 0;
+    if (ex < -1100)
+        ex = 0;
+    p.colexp[t * 64 + slot] = ex;
     const int nchunk = p.Qpad / 16;
-    uint4* out = reinterpret_cast<uint4*>(p.slices) + t * (int64_t)nchunk * S * kSplitN + slot;
+    const int64_t unit = t * SplitShape<NE>::kUnits + slot / NE;
+    uint4* out = reinterpret_cast<uint4*>(p.slices) + unit * (int64_t)nchunk * S * NE + slot % NE;
+    const double* col = p.C + e;
     for (int c = 0; c < nchunk; c++) {
+        double x[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int q = c * 16 + k;
+            x[k] = (valid && q < p.Q) ? ldexp(col[(int64_t)q * p.nelem], -ex) : 0.0;
+        }
         uint32_t w[S][4];
 #pragma unroll
         for (int s = 0; s < S; s++)
@@ -160,19 +192,18 @@ __global__ void k_slice_cols(ColSliceParams p)
             for (int k = 0; k < 4; k++) w[s][k] = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            const int q = c * 16 + k;
-            double x = (valid && q < p.Q) ? ldexp(p.C[(int64_t)q * p.nelem + e], -ex) : 0.0;
+            double y = x[k];
 #pragma unroll
             for (int s = 0; s < S; s++) {
-                const double y = x * 128.0;
-                const double m = trunc(y);
+                const double z = y * 128.0;
+                const double m = trunc(z);
                 w[s][k >> 2] |= (uint32_t)(uint8_t)(int8_t)m << (8 * (k & 3));
-                x = y - m;
+                y = z - m;
             }
         }
-        // chunk c of K step c/2 lands at [kstep][c&1][s][slot]: (c*S + s) * 64.
+        // chunk c of K step c/2 lands at [kstep][c&1][s][slot]: (c*S + s) * NE.
 #pragma unroll
-        for (int s = 0; s < S; s++) out[((int64_t)c * S + s) * kSplitN] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+        for (int s = 0; s < S; s++) out[((int64_t)c * S + s) * NE] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
     }
 }
 
@@ -281,37 +312,45 @@ __device__ __forceinline__ double scale2(double x, int s)
 
 // ---------------------------------------------------------------- contraction
 
-// Shared memory: kSplitStages pipeline stages, each one K step (32 bytes) of
-// every A slice (128 rows) and every B slice (64 rows), plus barriers.
+// Shared memory: pipeline stages, each one K step (32 bytes) of every A slice
+// (128 rows) and every B slice (NE rows), plus barriers.
+template <int NE>
 struct SplitSmem {
-    alignas(1024) int8_t A[kSplitStages][kSplitMaxS * kSplitABytes];
-    alignas(1024) int8_t B[kSplitStages][kSplitMaxS * kSplitBBytes];
-    alignas(8) uint64_t full[kSplitStages];
-    uint64_t empty[kSplitStages];
-    uint64_t tmem_full, tmem_empty, drain;
+    static constexpr int kSt = SplitShape<NE>::kStages;
+    alignas(1024) int8_t A[kSt][kSplitMaxS * kSplitABytes];
+    alignas(1024) int8_t B[kSt][kSplitMaxS * SplitShape<NE>::kBBytes];
+    alignas(8) uint64_t full[kSt];
+    uint64_t empty[kSt];
+    uint64_t tmem_full[2], tmem_empty[2], drain;
     uint32_t tmem;
     int failed;
 };
-constexpr size_t kSplitSmemBytes = sizeof(SplitSmem) + 1024;
+template <int NE>
+constexpr size_t split_smem_bytes() { return sizeof(SplitSmem<NE>) + 1024; }
 
 // Persistent, warp-specialised kernel; one CTA per SM holds all 512 TMEM
-// columns.  Work item w = (row tile w % ntp, element tile w / ntp), so the
-// CTAs working at the same time share element tiles (B is read from L2 once
-// per tile).
+// columns.  Work item w = (row tile w % ntp, element unit w / ntp), so the
+// CTAs working at the same time share element units (B is read from L2 once
+// per unit).  Empty units (past the end of a short tile) are skipped by every
+// role alike.
 //   warp 0 (one thread): bulk copies of each K step into the stage ring;
 //   warp 1 (one thread): MMAs; owns the TMEM allocation;
-//   warps 2-5: epilogue, warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31.
-// Barriers: full/empty per stage (copies -> MMA -> copies), tmem_full (MMAs of
-// a tile done -> epilogue) and tmem_empty (epilogue has read the accumulators
-// -> next tile's MMAs).  Every wait is bounded: on timeout the CTA records
-// the failure, the roles stop, outstanding copies and MMAs are waited for
-// (bounded), the TMEM is freed and the CTA returns.
-template <int S, int L>
+//   warps 2-9: epilogue; warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31 and
+//              half of the NE columns.
+// Barriers: full/empty per stage (copies -> MMA -> copies), tmem_full[b] (MMAs
+// of a tile done -> epilogue) and tmem_empty[b] (epilogue has read
+// accumulator b -> MMAs of the next tile using it).  Every wait is bounded: on
+// timeout the CTA records the failure, the roles stop, outstanding copies and
+// MMAs are waited for (bounded), the TMEM is freed and the CTA returns.
+template <int S, int L, int NE>
 __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams p)
 {
     static_assert(S <= kSplitMaxS && L - 1 <= S && L >= 6 && L <= 8, "level layout");
+    using Sh = SplitShape<NE>;
+    static_assert(Sh::kBufs == 1 ? (L - 1) * NE <= 512 : (L - 1) * NE <= 256, "accumulators fit the 512 TMEM columns");
+    constexpr int kSt = Sh::kStages;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    SplitSmem& sm = *reinterpret_cast<SplitSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    SplitSmem<NE>& sm = *reinterpret_cast<SplitSmem<NE>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr uint32_t kCols = 512;
     volatile int* failed = &sm.failed;
@@ -322,12 +361,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < kSplitStages; s++) {
+        for (int s = 0; s < kSt; s++) {
             mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 1);
         }
-        mbar_init(&sm.tmem_full, 1);
-        mbar_init(&sm.tmem_empty, 4);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&sm.tmem_full[b], 1);
+            mbar_init(&sm.tmem_empty[b], kSplitEpiWarps);
+        }
         mbar_init(&sm.drain, 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -336,7 +377,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
-    constexpr uint32_t kABytes = S * kSplitABytes, kBBytes = S * kSplitBBytes;
+    constexpr uint32_t kABytes = S * kSplitABytes, kBBytes = S * Sh::kBBytes;
 
     if (warp == 0 && lane == 0) {
         // ------------------------------------------------ producer
@@ -346,10 +387,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         bool ok = true;
         for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
             const int pt = (int)(w % p.ntp);
-            const int64_t t = w / p.ntp;
-            const int orient = p.tiles[t].orient;
-            const int8_t* srcA = p.A + ((int64_t)orient * p.ntp + pt) * p.nk * kABytes;
-            const int8_t* srcB = p.B + t * p.nk * kBBytes;
+            const int64_t u = w / p.ntp;
+            const Tile unit = split_unit<NE>(p.tiles, u);
+            if (unit.ne <= 0)
+                continue;
+            const int8_t* srcA = p.A + ((int64_t)unit.orient * p.ntp + pt) * p.nk * kABytes;
+            const int8_t* srcB = p.B + u * p.nk * kBBytes;
             for (int ks = 0; ks < p.nk; ks++) {
                 if (!mbar_wait(&sm.empty[stage], phase ^ 1, failed)) {
                     ok = false;
@@ -360,7 +403,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                 bulk_load(sm.B[stage], srcB + (int64_t)ks * kBBytes, kBBytes, &sm.full[stage]);
                 used |= 1u << stage;
                 last_parity = (last_parity & ~(1u << stage)) | (phase << stage);
-                if (++stage == kSplitStages) {
+                if (++stage == kSt) {
                     stage = 0;
                     phase ^= 1;
                 }
@@ -372,7 +415,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         }
         // No copy may still be in flight when the CTA leaves.
         const int zero = 0;
-        for (int s = 0; s < kSplitStages; s++)
+        for (int s = 0; s < kSt; s++)
             if (used & (1u << s))
                 if (!mbar_wait(&sm.full[s], (last_parity >> s) & 1, &zero))
                     atomicOr(p.error, 2u);
@@ -381,13 +424,18 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         int stage = 0;
         uint32_t phase = 0;
         bool ok = true;
-        int64_t i = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x, i++) {
-            if (i > 0 && !mbar_wait(&sm.tmem_empty, (uint32_t)((i - 1) & 1), failed)) {
+        int64_t i = 0;  // units processed by this CTA
+        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
+            if (split_unit<NE>(p.tiles, w / p.ntp).ne <= 0)
+                continue;
+            const int buf = (int)(i % Sh::kBufs);
+            const int64_t use = i / Sh::kBufs;
+            if (use > 0 && !mbar_wait(&sm.tmem_empty[buf], (uint32_t)((use - 1) & 1), failed)) {
                 ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dbase = tmem + (uint32_t)(buf * 256);
             for (int ks = 0; ks < p.nk; ks++) {
                 if (!mbar_wait(&sm.full[stage], phase, failed)) {
                     ok = false;
@@ -400,21 +448,23 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                     const int nbt = (S < L - 1 - a0) ? S : L - 1 - a0;  // b = 1 .. min(S, L - a)
                     const uint64_t ad = umma_desc(a_base + a0 * kSplitABytes, kSplitM * 16, 128);
 #pragma unroll
-                    for (int b0 = 0; b0 < nbt; b0 += 4) {
-                        const int nb = (nbt - b0) < 4 ? (nbt - b0) : 4;
-                        const uint64_t bd = umma_desc(b_base + b0 * kSplitN * 16, S * kSplitN * 16, 128);
-                        umma_i8(tmem + (uint32_t)(kSplitN * (a0 + b0)), ad, bd, umma_idesc_i8(kSplitM, kSplitN * nb),
+                    for (int b0 = 0; b0 < nbt; b0 += Sh::kGroup) {
+                        const int nb = (nbt - b0) < Sh::kGroup ? (nbt - b0) : Sh::kGroup;
+                        const uint64_t bd = umma_desc(b_base + b0 * NE * 16, S * NE * 16, 128);
+                        umma_i8(dbase + (uint32_t)(NE * (a0 + b0)), ad, bd, umma_idesc_i8(kSplitM, NE * nb),
                                 (ks > 0 || a0 > 0) ? 1u : 0u);
                     }
                 }
                 umma_commit(&sm.empty[stage]);
-                if (++stage == kSplitStages) {
+                if (++stage == kSt) {
                     stage = 0;
                     phase ^= 1;
                 }
             }
-            if (ok)
-                umma_commit(&sm.tmem_full);
+            if (!ok)
+                break;
+            umma_commit(&sm.tmem_full[buf]);
+            i++;
         }
         if (!ok) {
             *failed = 1;
@@ -428,34 +478,47 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
     } else if (warp >= 2) {
         // ------------------------------------------------ epilogue
         const int quarter = warp & 3;
+        const int cbeg = ((warp - 2) / 4) * (NE / 2);  // this warp's half of the columns
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         int64_t i = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork; w += gridDim.x, i++) {
-            if (!mbar_wait(&sm.tmem_full, (uint32_t)(i & 1), failed)) {
+        for (int64_t w = blockIdx.x; w < p.nwork; w += gridDim.x) {
+            const int pt = (int)(w % p.ntp);
+            const int64_t u = w / p.ntp;
+            const Tile unit = split_unit<NE>(p.tiles, u);
+            if (unit.ne <= 0)
+                continue;
+            const int buf = (int)(i % Sh::kBufs);
+            if (!mbar_wait(&sm.tmem_full[buf], (uint32_t)((i / Sh::kBufs) & 1), failed)) {
                 *failed = 1;
                 atomicOr(p.error, 1u);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int pt = (int)(w % p.ntp);
-            const int64_t t = w / p.ntp;
-            const Tile tile = p.tiles[t];
             const int pe = pt * kSplitM + quarter * 32 + lane;
-            const int rex = p.rowexp[(int64_t)tile.orient * p.Ppad + pe] - 35;
-            const int32_t* ce = p.colexp + t * kSplitN;
-            double* outp = p.out + (int64_t)tile.e0 * p.P + pe;
+            const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
+            const int32_t* ce = p.colexp + u * NE;
+            double* outp = p.out + (int64_t)unit.e0 * p.P + pe;
 #pragma unroll 1
-            for (int c0 = 0; c0 < kSplitN; c0 += 16) {
+            for (int c0 = cbeg; c0 < cbeg + NE / 2; c0 += 16) {
                 int32_t r[L - 1][16];
 #pragma unroll
-                for (int l = 0; l < L - 1; l++) tmem_ld16_nowait(lane_base + (uint32_t)(l * kSplitN + c0), r[l]);
+                for (int l = 0; l < L - 1; l++) tmem_ld16_nowait(lane_base + (uint32_t)(buf * 256 + l * NE + c0), r[l]);
                 tmem_ld_wait();
-                if (c0 + 16 == kSplitN) {
-                    // All accumulators are in registers: release the TMEM.
+                if (c0 + 16 == cbeg + NE / 2) {
+                    // All of this warp's accumulators are in registers: release.
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                     __syncwarp();
                     if (lane == 0)
-                        mbar_arrive(&sm.tmem_empty);
+                        mbar_arrive(&sm.tmem_empty[buf]);
+                }
+                int cx[16];
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    const int4 c4 = *reinterpret_cast<const int4*>(ce + c0 + j);
+                    cx[j] = c4.x;
+                    cx[j + 1] = c4.y;
+                    cx[j + 2] = c4.z;
+                    cx[j + 3] = c4.w;
                 }
                 if (pe < p.P) {
 #pragma unroll
@@ -469,12 +532,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                         for (int l = 6; l <= L; l++) Lo = Lo * 128 + r[l - 2][j];
                         Lo <<= 7 * (8 - L);
                         const double d = fma((double)Lo, 0x1p-21, (double)H);
-                        const int ee = c0 + j;
-                        if (ee < tile.ne)
-                            outp[(int64_t)ee * p.P] = scale2(d, rex + ce[ee]);
+                        if (c0 + j < unit.ne)
+                            outp[(int64_t)(c0 + j) * p.P] = scale2(d, rex + cx[j]);
                     }
                 }
             }
+            i++;
         }
     }
     __syncthreads();
