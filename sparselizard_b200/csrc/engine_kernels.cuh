@@ -586,33 +586,35 @@ struct RowParams {
 // Within one incidence every lane hits a different slot, so the sum of each
 // CSR entry is formed in incidence order: deterministic, no atomics.
 //
-// The loads of kRowBatch incidences are issued before any of them is added
-// (lane j holds entry j of each), so a warp keeps that many element-matrix
-// rows in flight instead of one; the additions still run in incidence order.
-// Incidences flagged serial (duplicate addresses) or wider than a warp are
-// added by their own loop at their place in the order.
+// Lane l decodes incidence l of each group of 32 (segment lookup, value and
+// slot offsets) once; the other lanes receive it by shuffle.  The loads of
+// kRowBatch incidences are issued before any of them is added (lane j holds
+// entry j of each), so a warp keeps that many element-matrix rows in flight;
+// the additions still run in incidence order.  Incidences flagged serial
+// (duplicate addresses) or wider than a warp are added by their own loop at
+// their place in the order.
 constexpr int kRowBatch = 8;
 
-__device__ __forceinline__ void row_add_generic(double* buf, const RowSeg& sg, const double* v, const int16_t* sm, bool serial,
+__device__ __forceinline__ void row_add_generic(double* buf, int width, double mult, const double* v, const int16_t* sm, bool serial,
                                                 int lane)
 {
     if (serial) {
         if (lane == 0)
-            for (int j = 0; j < sg.width; j++) {
+            for (int j = 0; j < width; j++) {
                 const int s = sm[j];
                 if (s >= 0)
-                    buf[s] += v[j] * sg.mult;
+                    buf[s] = fma(v[j], mult, buf[s]);
             }
     } else {
-        for (int j = lane; j < sg.width; j += 32) {
+        for (int j = lane; j < width; j += 32) {
             const int s = sm[j];
             if (s >= 0)
-                buf[s] += v[j] * sg.mult;
+                buf[s] = fma(v[j], mult, buf[s]);
         }
     }
 }
 
-__global__ void k_row_values(RowParams p)
+__global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
 {
     extern __shared__ double rowbuf[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -626,36 +628,49 @@ __global__ void k_row_values(RowParams p)
     for (int s = lane; s < L; s += 32) buf[s] = 0.0;
     __syncwarp();
     const uint32_t k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+    constexpr int kGeneric = 1 << 17, kSerial = 1 << 16;
     for (uint32_t kb = k0; kb < k1; kb += 32) {
         const int nkb = (int)min(32u, k1 - kb);
-        const unsigned long long mine = lane < nkb ? p.inc[kb + lane] : 0ull;
+        long long voff = 0, coo = 0;
+        double mult = 0.0;
+        int info = 0;  // width | kSerial | kGeneric
+        if (lane < nkb) {
+            const unsigned long long pk = p.inc[kb + lane];
+            const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+            coo = (long long)(pk & ((1ull << 40) - 1));
+            voff = sg.val_base + (coo - sg.coo_base);
+            mult = sg.mult;
+            const bool serial = (pk >> 63) != 0;
+            info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
+        }
         for (int u = 0; u < nkb; u += kRowBatch) {
             double val[kRowBatch];
             int slot[kRowBatch];
 #pragma unroll
             for (int x = 0; x < kRowBatch; x++) {
+                const int src = (u + x) & 31;
+                const long long vo = __shfl_sync(0xffffffffu, voff, src);
+                const long long co = __shfl_sync(0xffffffffu, coo, src);
+                const int inf = __shfl_sync(0xffffffffu, info, src);
                 slot[x] = -1;
                 val[x] = 0.0;
-                const unsigned long long pk = __shfl_sync(0xffffffffu, mine, (u + x) & 31);
-                if (u + x < nkb) {
-                    const RowSeg& sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-                    const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
-                    if (!(pk >> 63) && sg.width <= 32 && lane < sg.width) {
-                        slot[x] = p.slotmap[coo + lane];
-                        val[x] = p.vals[sg.val_base + (coo - sg.coo_base) + lane];
-                    }
+                if (u + x < nkb && !(inf & kGeneric) && lane < (inf & 0xffff)) {
+                    slot[x] = p.slotmap[co + lane];
+                    val[x] = p.vals[vo + lane];
                 }
             }
 #pragma unroll
             for (int x = 0; x < kRowBatch; x++) {
-                const unsigned long long pk = __shfl_sync(0xffffffffu, mine, (u + x) & 31);
                 if (u + x < nkb) {
-                    const RowSeg& sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-                    if ((pk >> 63) || sg.width > 32) {
-                        const int64_t coo = (int64_t)(pk & ((1ull << 40) - 1));
-                        row_add_generic(buf, sg, p.vals + sg.val_base + (coo - sg.coo_base), p.slotmap + coo, (pk >> 63) != 0, lane);
+                    const int src = (u + x) & 31;
+                    const double m = __shfl_sync(0xffffffffu, mult, src);
+                    const int inf = __shfl_sync(0xffffffffu, info, src);
+                    if (inf & kGeneric) {
+                        const long long vo = __shfl_sync(0xffffffffu, voff, src);
+                        const long long co = __shfl_sync(0xffffffffu, coo, src);
+                        row_add_generic(buf, inf & 0xffff, m, p.vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
                     } else if (slot[x] >= 0) {
-                        buf[slot[x]] += val[x] * sg.mult;
+                        buf[slot[x]] = fma(val[x], m, buf[slot[x]]);
                     }
                 }
                 __syncwarp();

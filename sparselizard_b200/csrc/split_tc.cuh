@@ -178,12 +178,16 @@ __global__ void k_slice_cols(ColSliceParams p)
     const int64_t unit = t * SplitShape<NE>::kUnits + slot / NE;
     uint4* out = reinterpret_cast<uint4*>(p.slices) + unit * (int64_t)nchunk * S * NE + slot % NE;
     const double* col = p.C + e;
+    // |C| 2^(7S - ex) < 2^(7S): its integer part holds the S 7-bit slices
+    // (the same digits repeated truncation of C 2^-ex by 128 produces).
+    const bool fast = 7 * S - ex <= 1023;
+    const double scale = fast ? __longlong_as_double((long long)(7 * S - ex + 1023) << 52) : 0.0;
     for (int c = 0; c < nchunk; c++) {
         double x[16];
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             const int q = c * 16 + k;
-            x[k] = (valid && q < p.Q) ? ldexp(col[(int64_t)q * p.nelem], -ex) : 0.0;
+            x[k] = (valid && q < p.Q) ? col[(int64_t)q * p.nelem] : 0.0;
         }
         uint32_t w[S][4];
 #pragma unroll
@@ -192,13 +196,13 @@ __global__ void k_slice_cols(ColSliceParams p)
             for (int k = 0; k < 4; k++) w[s][k] = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            double y = x[k];
+            const double ax = fast ? fabs(x[k]) * scale : ldexp(fabs(x[k]), 7 * S - ex);
+            const unsigned long long mag = __double2ull_rz(ax);
+            const bool neg = x[k] < 0;
 #pragma unroll
             for (int s = 0; s < S; s++) {
-                const double z = y * 128.0;
-                const double m = trunc(z);
-                w[s][k >> 2] |= (uint32_t)(uint8_t)(int8_t)m << (8 * (k & 3));
-                y = z - m;
+                const int d = (int)((mag >> (7 * (S - 1 - s))) & 127);
+                w[s][k >> 2] |= (uint32_t)(uint8_t)(int8_t)(neg ? -d : d) << (8 * (k & 3));
             }
         }
         // chunk c of K step c/2 lands at [kstep][c&1][s][slot]: (c*S + s) * NE.
