@@ -56,6 +56,7 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept
     if (this != &o) {
         release();
         ctx_ = o.ctx_;
+        s_ = o.s_;
         p_ = o.p_;
         n_ = o.n_;
         o.ctx_ = nullptr;
@@ -74,12 +75,13 @@ void DevBuf::alloc(Ctx* ctx, size_t bytes)
     if ((size_t)ctx->in_use + bytes > ctx->budget)
         fail(SLGPU_E_BUDGET, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget (" +
                                  std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget) + " in use)");
-    cudaError_t err = cudaMallocAsync(&p_, bytes, ctx->stream);
+    cudaError_t err = cudaMallocAsync(&p_, bytes, ctx->x->stream);
     if (err != cudaSuccess) {
         p_ = nullptr;
         fail(SLGPU_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(err));
     }
     ctx_ = ctx;
+    s_ = ctx->x->stream;
     n_ = bytes;
     ctx->in_use += (int64_t)bytes;
 }
@@ -87,7 +89,7 @@ void DevBuf::alloc(Ctx* ctx, size_t bytes)
 void DevBuf::release()
 {
     if (p_ != nullptr && ctx_ != nullptr) {
-        cudaFreeAsync(p_, ctx_->stream);
+        cudaFreeAsync(p_, s_);
         ctx_->in_use -= (int64_t)n_;
     }
     p_ = nullptr;
@@ -100,7 +102,7 @@ static void upload(Ctx* ctx, DevBuf& buf, const T* src, size_t count)
 {
     buf.alloc(ctx, count * sizeof(T));
     if (count > 0)
-        cuda_check(cudaMemcpyAsync(buf.as<void>(), src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream),
+        cuda_check(cudaMemcpyAsync(buf.as<void>(), src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->x->stream),
                    "cudaMemcpyAsync H2D");
 }
 
@@ -226,15 +228,15 @@ static void hash_device(Ctx* ctx, const int32_t* data, int64_t n, uint64_t salt,
 {
     if (ctx->hash_acc.empty())
         ctx->hash_acc.alloc(ctx, 2 * sizeof(unsigned long long));
-    cuda_check(cudaMemsetAsync(ctx->hash_acc.as<void>(), 0, 2 * sizeof(unsigned long long), ctx->stream), "memset");
+    cuda_check(cudaMemsetAsync(ctx->hash_acc.as<void>(), 0, 2 * sizeof(unsigned long long), ctx->x->stream), "memset");
     if (n > 0) {
         unsigned blocks = (unsigned)std::min<int64_t>(148 * 8, grid_for(n, 256));
-        k_hash_i32<<<blocks, 256, 0, ctx->stream>>>(data, n, salt, ctx->hash_acc.as<unsigned long long>());
+        k_hash_i32<<<blocks, 256, 0, ctx->x->stream>>>(data, n, salt, ctx->hash_acc.as<unsigned long long>());
         cuda_check(cudaGetLastError(), "k_hash_i32");
     }
     unsigned long long h[2];
-    cuda_check(cudaMemcpyAsync(h, ctx->hash_acc.as<void>(), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "D2H hash");
-    cuda_check(cudaStreamSynchronize(ctx->stream), "sync hash");
+    cuda_check(cudaMemcpyAsync(h, ctx->hash_acc.as<void>(), sizeof(h), cudaMemcpyDeviceToHost, ctx->x->stream), "D2H hash");
+    cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync hash");
     out[0] = h[0];
     out[1] = h[1];
 }
@@ -429,19 +431,19 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     for (int k = 0; k < g.ntables; k++)
         cuda_check(cudaMemcpyAsync(gd->tables.as<double>() + gd->tab_off[k], g.tables[k].vals,
                                    (size_t)g.norient * g.tables[k].rows * g.ngp * sizeof(double), cudaMemcpyHostToDevice,
-                                   ctx->stream),
+                                   ctx->x->stream),
                    "upload tables");
     upload(ctx, gd->consts, g.consts, (size_t)g.nconsts);
     upload(ctx, gd->prog_d, gd->prog);
     gd->elemdata.alloc(ctx, (size_t)g.nelemdata * g.nelem * sizeof(double));
     for (int k = 0; k < g.nelemdata; k++)
         cuda_check(cudaMemcpyAsync(gd->elemdata.as<double>() + gd->elemdata_off[k], g.elemdata[k],
-                                   (size_t)g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                                   (size_t)g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->x->stream),
                    "upload elemdata");
     gd->fielddata.alloc(ctx, (size_t)field_total * sizeof(double));
     for (int k = 0; k < g.nfielddata; k++)
         cuda_check(cudaMemcpyAsync(gd->fielddata.as<double>() + gd->field_off[k], g.fielddata[k],
-                                   (size_t)g.fieldrows[k] * g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+                                   (size_t)g.fieldrows[k] * g.nelem * sizeof(double), cudaMemcpyHostToDevice, ctx->x->stream),
                    "upload fielddata");
     upload(ctx, gd->field_off_d, gd->field_off);
     upload(ctx, gd->field_rows_d, gd->field_rows);
@@ -532,39 +534,39 @@ static std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>
 // event pair; kstat_collect sums them once the stream has been synchronised.
 static int kstat_start(Ctx* ctx, const char* family, double work)
 {
-    const size_t i = ctx->kev_tag.size();
-    while (ctx->kev.size() < 2 * (i + 1)) {
+    const size_t i = ctx->x->kev_tag.size();
+    while (ctx->x->kev.size() < 2 * (i + 1)) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        ctx->kev.push_back(e);
+        ctx->x->kev.push_back(e);
     }
-    cuda_check(cudaEventRecord(ctx->kev[2 * i], ctx->stream), "cudaEventRecord");
-    ctx->kev_tag.emplace_back(family, work);
+    cuda_check(cudaEventRecord(ctx->x->kev[2 * i], ctx->x->stream), "cudaEventRecord");
+    ctx->x->kev_tag.emplace_back(family, work);
     return (int)i;
 }
 
-static void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->kev[2 * i + 1], ctx->stream), "cudaEventRecord"); }
+static void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->kev[2 * i + 1], ctx->x->stream), "cudaEventRecord"); }
 
 static void kstat_collect(Ctx* ctx)
 {
-    ctx->kstats.clear();
-    for (size_t i = 0; i < ctx->kev_tag.size(); i++) {
+    ctx->x->kstats.clear();
+    for (size_t i = 0; i < ctx->x->kev_tag.size(); i++) {
         float ms = 0;
-        cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]);
-        Ctx::KernelStat& k = ctx->kstats[ctx->kev_tag[i].first];
+        cudaEventElapsedTime(&ms, ctx->x->kev[2 * i], ctx->x->kev[2 * i + 1]);
+        KernelStat& k = ctx->x->kstats[ctx->x->kev_tag[i].first];
         k.ms += ms;
-        k.work += ctx->kev_tag[i].second;
+        k.work += ctx->x->kev_tag[i].second;
         k.launches++;
     }
-    ctx->kev_tag.clear();
+    ctx->x->kev_tag.clear();
 }
 
-static void ev_record(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->ev[i], ctx->stream), "cudaEventRecord"); }
+static void ev_record(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->ev[i], ctx->x->stream), "cudaEventRecord"); }
 
 static float ev_ms(Ctx* ctx, int a, int b)
 {
     float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+    cudaEventElapsedTime(&ms, ctx->x->ev[a], ctx->x->ev[b]);
     return ms;
 }
 
@@ -611,7 +613,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     idx.alloc(ctx, std::max<int64_t>(ncoo, 1) * 4);
     idx_alt.alloc(ctx, std::max<int64_t>(ncoo, 1) * 4);
     counter.alloc(ctx, 16);
-    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->x->stream), "memset");
     int si = 0;
     for (auto& g : M.groups) {
         for (int d = 0; d < g->ndests; d++, si++) {
@@ -631,7 +633,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
             kp.idx = idx.as<uint32_t>();
             kp.nvalid = counter.as<unsigned long long>();
             if (kp.count > 0) {
-                k_group_keys<<<grid_for(kp.count, 256), 256, 0, ctx->stream>>>(kp);
+                k_group_keys<<<grid_for(kp.count, 256), 256, 0, ctx->x->stream>>>(kp);
                 cuda_check(cudaGetLastError(), "k_group_keys");
             }
         }
@@ -652,21 +654,21 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         fp.idx = idx.as<uint32_t>();
         fp.nvalid = counter.as<unsigned long long>();
         fp.ndofs = M.ndofs;
-        k_frag_keys<<<grid_for((int64_t)f->nr * f->nc, 256), 256, 0, ctx->stream>>>(fp);
+        k_frag_keys<<<grid_for((int64_t)f->nr * f->nc, 256), 256, 0, ctx->x->stream>>>(fp);
         cuda_check(cudaGetLastError(), "k_frag_keys");
         si++;
     }
     cub::DoubleBuffer<unsigned long long> dk(keys.as<unsigned long long>(), keys_alt.as<unsigned long long>());
     cub::DoubleBuffer<uint32_t> dv(idx.as<uint32_t>(), idx_alt.as<uint32_t>());
-    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
+    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->x->stream),
                "SortPairs size");
     tmp.alloc(ctx, temp);
-    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->stream),
+    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, dk, dv, (int64_t)ncoo, 0, rowbits + colbits, ctx->x->stream),
                "SortPairs");
     tmp.release();
     unsigned long long counts_h[2] = {0, 0};
-    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H nvalid");
-    cuda_check(cudaStreamSynchronize(ctx->stream), "sync nvalid");
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H nvalid");
+    cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync nvalid");
     if (counts_h[1] != 0)
         fail(SLGPU_E_ARG, std::to_string(counts_h[1]) + " COO addresses are >= the DOF count");
     const int64_t nvalid = (int64_t)counts_h[0];
@@ -679,28 +681,28 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     head.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
     runidx.alloc(ctx, std::max<int64_t>(nvalid, 1) * 4);
     if (nvalid > 0) {
-        k_run_heads<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(sk, nvalid, head.as<uint32_t>());
+        k_run_heads<<<grid_for(nvalid, 256), 256, 0, ctx->x->stream>>>(sk, nvalid, head.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_run_heads");
         temp = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid, ctx->x->stream),
                    "scan size");
         tmp.alloc(ctx, temp);
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, head.as<uint32_t>(), runidx.as<uint32_t>(), (int64_t)nvalid,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         tmp.release();
     }
     uint32_t last[2] = {0, 0};
     if (nvalid > 0) {
-        cuda_check(cudaMemcpyAsync(&last[0], runidx.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaMemcpyAsync(&last[1], head.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+        cuda_check(cudaMemcpyAsync(&last[0], runidx.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&last[1], head.as<uint32_t>() + nvalid - 1, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
     }
     const int64_t nruns = nvalid > 0 ? (int64_t)last[0] + last[1] : 0;
     DevBuf run_start;
     run_start.alloc(ctx, (nruns + 1) * 4);
     if (nvalid > 0) {
-        k_run_starts<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid,
+        k_run_starts<<<grid_for(nvalid, 256), 256, 0, ctx->x->stream>>>(head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid,
                                                                      run_start.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_run_starts");
     }
@@ -715,28 +717,28 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         flagsD.alloc(ctx, (M.ndofs + 1) * 4);
         scanA.alloc(ctx, (M.ndofs + 1) * 4);
         scanD.alloc(ctx, (M.ndofs + 1) * 4);
-        k_constraint_flags<<<grid_for(M.ndofs + 1, 256), 256, 0, ctx->stream>>>(dconstr, M.ndofs, flagsA.as<uint32_t>(),
+        k_constraint_flags<<<grid_for(M.ndofs + 1, 256), 256, 0, ctx->x->stream>>>(dconstr, M.ndofs, flagsA.as<uint32_t>(),
                                                                                  flagsD.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_constraint_flags");
         temp = 0;
         cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(), (int64_t)M.ndofs + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan size");
         tmp.alloc(ctx, temp);
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsA.as<uint32_t>(), scanA.as<uint32_t>(), (int64_t)M.ndofs + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, flagsD.as<uint32_t>(), scanD.as<uint32_t>(), (int64_t)M.ndofs + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         tmp.release();
         uint32_t tot[2];
-        cuda_check(cudaMemcpyAsync(&tot[0], scanA.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaMemcpyAsync(&tot[1], scanD.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        k_renumber<<<grid_for(M.ndofs, 256), 256, 0, ctx->stream>>>(dconstr, M.ndofs, scanA.as<uint32_t>(), scanD.as<uint32_t>(),
+        cuda_check(cudaMemcpyAsync(&tot[0], scanA.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&tot[1], scanD.as<uint32_t>() + M.ndofs, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        k_renumber<<<grid_for(M.ndofs, 256), 256, 0, ctx->x->stream>>>(dconstr, M.ndofs, scanA.as<uint32_t>(), scanD.as<uint32_t>(),
                                                                      renum.as<int32_t>());
         cuda_check(cudaGetLastError(), "k_renumber");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
         nA = tot[0];
         nD = tot[1];
     }
@@ -754,39 +756,39 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         slotD.alloc(ctx, (nruns + 1) * 4);
         rowcA.alloc(ctx, (nA + 1) * 4);
         rowcD.alloc(ctx, (nA + 1) * 4);
-        cuda_check(cudaMemsetAsync(rowcA.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
-        cuda_check(cudaMemsetAsync(rowcD.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
-        k_classify_runs<<<grid_for(nruns + 1, 256), 256, 0, ctx->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, dconstr,
+        cuda_check(cudaMemsetAsync(rowcA.as<void>(), 0, (nA + 1) * 4, ctx->x->stream), "memset");
+        cuda_check(cudaMemsetAsync(rowcD.as<void>(), 0, (nA + 1) * 4, ctx->x->stream), "memset");
+        k_classify_runs<<<grid_for(nruns + 1, 256), 256, 0, ctx->x->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, dconstr,
                                                                             renum.as<int32_t>(), isA.as<uint32_t>(), isD.as<uint32_t>(),
                                                                             rowcA.as<uint32_t>(), rowcD.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_classify_runs");
         temp = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1, ctx->x->stream),
                    "scan size");
         size_t temp2 = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp2, rowcA.as<uint32_t>(), rowcA.as<uint32_t>(), (int64_t)nA + 1, ctx->stream),
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp2, rowcA.as<uint32_t>(), rowcA.as<uint32_t>(), (int64_t)nA + 1, ctx->x->stream),
                    "scan size");
         temp = std::max(temp, temp2);
         tmp.alloc(ctx, temp);
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, isA.as<uint32_t>(), slotA.as<uint32_t>(), (int64_t)nruns + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, isD.as<uint32_t>(), slotD.as<uint32_t>(), (int64_t)nruns + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         P->Arows.alloc(ctx, (nA + 1) * 4);
         P->Drows.alloc(ctx, (nA + 1) * 4);
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcA.as<uint32_t>(), P->Arows.as<uint32_t>(), (int64_t)nA + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcD.as<uint32_t>(), P->Drows.as<uint32_t>(), (int64_t)nA + 1,
-                                                 ctx->stream),
+                                                 ctx->x->stream),
                    "scan");
         tmp.release();
         uint32_t tot[2];
-        cuda_check(cudaMemcpyAsync(&tot[0], slotA.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaMemcpyAsync(&tot[1], slotD.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+        cuda_check(cudaMemcpyAsync(&tot[0], slotA.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(&tot[1], slotD.as<uint32_t>() + nruns, 4, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
         P->nnzA = tot[0];
         P->nnzD = tot[1];
         if (P->nnzA >= (int64_t(1) << 31) || P->nnzD >= (int64_t(1) << 31))
@@ -794,7 +796,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         P->Acols.alloc(ctx, std::max<int64_t>(P->nnzA, 1) * 4);
         P->Dcols.alloc(ctx, std::max<int64_t>(P->nnzD, 1) * 4);
         if (nruns > 0) {
-            k_fill_runs<<<grid_for(nruns, 256), 256, 0, ctx->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, isA.as<uint32_t>(),
+            k_fill_runs<<<grid_for(nruns, 256), 256, 0, ctx->x->stream>>>(sk, run_start.as<uint32_t>(), nruns, colbits, isA.as<uint32_t>(),
                                                                         slotA.as<uint32_t>(), slotD.as<uint32_t>(), renum.as<int32_t>(),
                                                                         run_target.as<int32_t>(), P->Acols.as<int32_t>(),
                                                                         P->Dcols.as<int32_t>());
@@ -805,8 +807,8 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 
     // ---- slot map: position of each kept COO entry inside its row segment.
     P->slotmap.alloc(ctx, std::max<int64_t>(ncoo, 1) * 2);
-    cuda_check(cudaMemsetAsync(P->slotmap.as<void>(), 0xFF, std::max<int64_t>(ncoo, 1) * 2, ctx->stream), "memset slotmap");
-    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+    cuda_check(cudaMemsetAsync(P->slotmap.as<void>(), 0xFF, std::max<int64_t>(ncoo, 1) * 2, ctx->x->stream), "memset slotmap");
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->x->stream), "memset");
     std::vector<CooSeg> csegs;
     {
         size_t s = 0;
@@ -817,9 +819,9 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     DevBuf dcsegs, dup;
     upload(ctx, dcsegs, csegs);
     dup.alloc(ctx, std::max<int64_t>(ncoo, 1));
-    cuda_check(cudaMemsetAsync(dup.as<void>(), 0, std::max<int64_t>(ncoo, 1), ctx->stream), "memset dup");
+    cuda_check(cudaMemsetAsync(dup.as<void>(), 0, std::max<int64_t>(ncoo, 1), ctx->x->stream), "memset dup");
     if (nvalid > 0) {
-        k_slotmap<<<grid_for(nvalid, 256), 256, 0, ctx->stream>>>(sk, perm, head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid, colbits,
+        k_slotmap<<<grid_for(nvalid, 256), 256, 0, ctx->x->stream>>>(sk, perm, head.as<uint32_t>(), runidx.as<uint32_t>(), nvalid, colbits,
                                                                   run_target.as<int32_t>(), renum.as<int32_t>(), P->Arows.as<uint32_t>(),
                                                                   P->Drows.as<uint32_t>(), P->slotmap.as<int16_t>(),
                                                                   counter.as<unsigned long long>(), dcsegs.as<CooSeg>(), (int)csegs.size(),
@@ -886,7 +888,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     for (size_t s = 0; s < isegs.size(); s++) {
         if (isegs[s].count == 0)
             continue;
-        k_inc_keys<<<grid_for(isegs[s].count, 256), 256, 0, ctx->stream>>>(disegs.as<IncSeg>(), (int)s, dconstr, M.ndofs,
+        k_inc_keys<<<grid_for(isegs[s].count, 256), 256, 0, ctx->x->stream>>>(disegs.as<IncSeg>(), (int)s, dconstr, M.ndofs,
                                                                           ikeys.as<uint32_t>(), iids.as<uint32_t>(),
                                                                           counter.as<unsigned long long>() + 1);
         cuda_check(cudaGetLastError(), "k_inc_keys");
@@ -894,12 +896,12 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     cub::DoubleBuffer<uint32_t> ik(ikeys.as<uint32_t>(), ikeys_alt.as<uint32_t>());
     cub::DoubleBuffer<uint32_t> iv(iids.as<uint32_t>(), iids_alt.as<uint32_t>());
     temp = 0;
-    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->stream), "SortPairs size");
+    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->x->stream), "SortPairs size");
     tmp.alloc(ctx, temp);
-    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->stream), "SortPairs");
+    cuda_check(cub::DeviceRadixSort::SortPairs(tmp.as<void>(), temp, ik, iv, (int64_t)ninc_total, 0, 32, ctx->x->stream), "SortPairs");
     tmp.release();
-    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+    cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
     if (counts_h[0] != 0)
         fail(SLGPU_E_UNSUPPORTED, "a CSR row is longer than 32767 entries");
     const int64_t ninc = (int64_t)counts_h[1];
@@ -907,11 +909,11 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     P->inc.alloc(ctx, std::max<int64_t>(ninc, 1) * 8);
     DevBuf rowcount;
     rowcount.alloc(ctx, (nA + 1) * 4);
-    cuda_check(cudaMemsetAsync(rowcount.as<void>(), 0, (nA + 1) * 4, ctx->stream), "memset");
+    cuda_check(cudaMemsetAsync(rowcount.as<void>(), 0, (nA + 1) * 4, ctx->x->stream), "memset");
     if (isegs.size() >= (size_t(1) << 23))
         fail(SLGPU_E_UNSUPPORTED, "too many element groups and fragments in one matrix");
     if (ninc > 0) {
-        k_inc_finalize<<<grid_for(ninc, 256), 256, 0, ctx->stream>>>(ik.Current(), iv.Current(), ninc, disegs.as<IncSeg>(),
+        k_inc_finalize<<<grid_for(ninc, 256), 256, 0, ctx->x->stream>>>(ik.Current(), iv.Current(), ninc, disegs.as<IncSeg>(),
                                                                      (int)isegs.size(), renum.as<int32_t>(), dup.as<uint8_t>(),
                                                                      P->inc.as<unsigned long long>(), rowcount.as<uint32_t>());
         cuda_check(cudaGetLastError(), "k_inc_finalize");
@@ -919,22 +921,22 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     dup.release();
     P->inc_ptr.alloc(ctx, (nA + 1) * 4);
     temp = 0;
-    cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, rowcount.as<uint32_t>(), P->inc_ptr.as<uint32_t>(), (int64_t)nA + 1, ctx->stream),
+    cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp, rowcount.as<uint32_t>(), P->inc_ptr.as<uint32_t>(), (int64_t)nA + 1, ctx->x->stream),
                "scan size");
     tmp.alloc(ctx, temp);
     cuda_check(cub::DeviceScan::ExclusiveSum(tmp.as<void>(), temp, rowcount.as<uint32_t>(), P->inc_ptr.as<uint32_t>(), (int64_t)nA + 1,
-                                             ctx->stream),
+                                             ctx->x->stream),
                "scan");
     tmp.release();
     // Longest row.
-    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->stream), "memset");
+    cuda_check(cudaMemsetAsync(counter.as<void>(), 0, 16, ctx->x->stream), "memset");
     if (nA > 0) {
-        k_max_rowlen<<<grid_for(nA, 256), 256, 0, ctx->stream>>>(P->Arows.as<uint32_t>(), P->Drows.as<uint32_t>(), nA,
+        k_max_rowlen<<<grid_for(nA, 256), 256, 0, ctx->x->stream>>>(P->Arows.as<uint32_t>(), P->Drows.as<uint32_t>(), nA,
                                                                    counter.as<unsigned long long>());
         cuda_check(cudaGetLastError(), "k_max_rowlen");
     }
-    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    cuda_check(cudaMemcpyAsync(counts_h, counter.as<void>(), 16, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+    cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
     P->lmax = (int)counts_h[0];
 
     P->last_use = ++ctx->use_clock;
@@ -983,7 +985,7 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
     rp.rowexp = sp->rowexp.as<int32_t>();
     if (g.norient > 65535)
         fail(SLGPU_E_UNSUPPORTED, "too many orientation variants");
-    k_slice_rows<<<dim3((unsigned)sp->Ppad, (unsigned)g.norient), 256, 0, ctx->stream>>>(rp);
+    k_slice_rows<<<dim3((unsigned)sp->Ppad, (unsigned)g.norient), 256, 0, ctx->x->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_slice_rows");
     ctx->launches++;
     return *sp;
@@ -1009,7 +1011,7 @@ static void launch_split(Ctx* ctx, const SplitParams& p)
         attr = true;
     }
     const int64_t grid = std::min<int64_t>(p.nwork, std::max(ctx->nsm, 1));
-    k_contract_split<S, L, NE><<<(unsigned)grid, kSplitThreads, smem, ctx->stream>>>(p);
+    k_contract_split<S, L, NE><<<(unsigned)grid, kSplitThreads, smem, ctx->x->stream>>>(p);
 }
 
 // Element-tile width of the split kernel: SLGPU_SPLIT_TILE=32 or 64 (default 64).
@@ -1031,10 +1033,10 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     const int NE = split_tile_width();
     const int64_t ntiles = (int64_t)g.tiles.size();
     const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
-    if (ctx->split_cols.bytes() < colbytes)
-        ctx->split_cols.alloc(ctx, colbytes);
-    if (ctx->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
-        ctx->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
+    if (ctx->x->split_cols.bytes() < colbytes)
+        ctx->x->split_cols.alloc(ctx, colbytes);
+    if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
+        ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
     ColSliceParams cs{};
     cs.C = C;
     cs.elemexp = elemexp;
@@ -1043,18 +1045,18 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     cs.Qpad = sp.Qpad;
     cs.nelem = g.nelem;
     cs.ntiles = ntiles;
-    cs.slices = ctx->split_cols.as<int8_t>();
-    cs.colexp = ctx->split_colexp.as<int32_t>();
+    cs.slices = ctx->x->split_cols.as<int8_t>();
+    cs.colexp = ctx->x->split_colexp.as<int32_t>();
     const dim3 cgrid = grid_for(ntiles * 64, 128);
     const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + 4.0 * g.nelem + (double)colbytes + 4.0 * ntiles * 64);
     if (sp.S == 7 && NE == 64)
-        k_slice_cols<7, 64><<<cgrid, 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<7, 64><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
     else if (sp.S == 7)
-        k_slice_cols<7, 32><<<cgrid, 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<7, 32><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
     else if (sp.S == 5 && NE == 64)
-        k_slice_cols<5, 64><<<cgrid, 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<5, 64><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
     else if (sp.S == 5)
-        k_slice_cols<5, 32><<<cgrid, 128, 0, ctx->stream>>>(cs);
+        k_slice_cols<5, 32><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
     else
         fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
     kstat_stop(ctx, kt);
@@ -1068,11 +1070,11 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     p.nwork = (int64_t)p.ntp * ntiles * (64 / NE);
     p.tiles = g.tiles_d.as<Tile>();
     p.A = sp.slices.as<int8_t>();
-    p.B = ctx->split_cols.as<int8_t>();
+    p.B = ctx->x->split_cols.as<int8_t>();
     p.rowexp = sp.rowexp.as<int32_t>();
-    p.colexp = ctx->split_colexp.as<int32_t>();
+    p.colexp = ctx->x->split_colexp.as<int32_t>();
     p.out = out;
-    p.error = ctx->split_error.as<unsigned int>();
+    p.error = ctx->x->split_error.as<unsigned int>();
     // Algorithmic INT8 operations: 2 per product, pairs (a, b) with a + b <= L.
     int pairs = 0;
     for (int a = 1; a <= sp.S; a++)
@@ -1162,7 +1164,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 double cbytes = 0;
                 for (size_t j = k; j < k1; j++) cbytes += 8.0 * M.groups[j]->nterms * M.groups[j]->ngp * M.groups[j]->nelem;
                 const int kt = kstat_start(ctx, "coefficients", cbytes);
-                cuda_check(cudaLaunchKernel((const void*)kern, dim3(grid_for(n, 128)), dim3(128), args, 0, ctx->stream),
+                cuda_check(cudaLaunchKernel((const void*)kern, dim3(grid_for(n, 128)), dim3(128), args, 0, ctx->x->stream),
                            "coefficient kernel launch");
                 kstat_stop(ctx, kt);
                 ctx->launches++;
@@ -1181,7 +1183,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 cp.elemexp = eoff[j] >= 0 ? elemexp + eoff[j] : nullptr;
                 const int64_t n = G.nelem * (int64_t)G.ngp;
                 const int kt = kstat_start(ctx, "coefficients", 8.0 * G.nterms * G.ngp * G.nelem);
-                k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->stream>>>(cp);
+                k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->x->stream>>>(cp);
                 kstat_stop(ctx, kt);
                 cuda_check(cudaGetLastError(), "k_geometry_coef");
                 ctx->launches++;
@@ -1193,7 +1195,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
 
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
 {
-    ctx->kev_tag.clear();
+    ctx->x->kev_tag.clear();
     if (ctx->record_only) {
         if (isconstrained != nullptr)
             M.rec_constrained.assign(isconstrained, isconstrained + M.ndofs);
@@ -1222,7 +1224,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     if (!same) {
         ctx->constr_host.assign(hconstr, hconstr + M.ndofs);
         ctx->constr_dev.alloc(ctx, (size_t)M.ndofs + 1);
-        cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), hconstr, M.ndofs, cudaMemcpyHostToDevice, ctx->stream), "H2D constr");
+        cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), hconstr, M.ndofs, cudaMemcpyHostToDevice, ctx->x->stream), "H2D constr");
         std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
         std::memcpy(packed.data(), hconstr, M.ndofs);
         uint64_t a = 0x12345, b = 0x6789;
@@ -1259,14 +1261,14 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     DevBuf C;
     C.alloc(ctx, std::max<int64_t>(ctot, 1) * 8);
     if (precision != SLGPU_PREC_FP64) {
-        if (ctx->split_error.empty())
-            ctx->split_error.alloc(ctx, 16);
-        cuda_check(cudaMemsetAsync(ctx->split_error.as<void>(), 0, 16, ctx->stream), "memset");
+        if (ctx->x->split_error.empty())
+            ctx->x->split_error.alloc(ctx, 16);
+        cuda_check(cudaMemsetAsync(ctx->x->split_error.as<void>(), 0, 16, ctx->x->stream), "memset");
     }
-    while (ctx->evpool.size() < 3) {
+    while (ctx->x->evpool.size() < 3) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        ctx->evpool.push_back(e);
+        ctx->x->evpool.push_back(e);
     }
     // Split-precision groups: per-element exponents of the coefficients,
     // gathered by the coefficient kernels (atomicMax from a very negative start).
@@ -1280,11 +1282,11 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     DevBuf E;
     if (etot > 0) {
         E.alloc(ctx, (size_t)etot * 4);
-        cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->stream), "memset");
+        cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
     }
-    cuda_check(cudaEventRecord(ctx->evpool[0], ctx->stream), "cudaEventRecord");
+    cuda_check(cudaEventRecord(ctx->x->evpool[0], ctx->x->stream), "cudaEventRecord");
     launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff);
-    cuda_check(cudaEventRecord(ctx->evpool[1], ctx->stream), "cudaEventRecord");
+    cuda_check(cudaEventRecord(ctx->x->evpool[1], ctx->x->stream), "cudaEventRecord");
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
@@ -1314,14 +1316,14 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             if (grid.y > 65535)
                 fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
             const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
-            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->stream>>>(kp);
+            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
             kstat_stop(ctx, kt);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
             ctx->launches++;
         }
         gi++;
     }
-    cuda_check(cudaEventRecord(ctx->evpool[2], ctx->stream), "cudaEventRecord");
+    cuda_check(cudaEventRecord(ctx->x->evpool[2], ctx->x->stream), "cudaEventRecord");
     C.release();
     {
         int64_t vb = 0;
@@ -1329,7 +1331,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         for (auto& f : M.frags) {
             int64_t n = (int64_t)f->nr * f->nc;
             if (n > 0)
-                cuda_check(cudaMemcpyAsync(M.vals.as<double>() + vb, f->vals.as<double>(), n * 8, cudaMemcpyDeviceToDevice, ctx->stream),
+                cuda_check(cudaMemcpyAsync(M.vals.as<double>() + vb, f->vals.as<double>(), n * 8, cudaMemcpyDeviceToDevice, ctx->x->stream),
                            "D2D fragment values");
             vb += n;
         }
@@ -1384,28 +1386,28 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         // pointers read; A and D values written.
         const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
         const int kt = kstat_start(ctx, "row_values", rbytes);
-        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->stream>>>(rp);
+        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
         kstat_stop(ctx, kt);
         cuda_check(cudaGetLastError(), "k_row_values");
         ctx->launches++;
     }
     ev_record(ctx, 3);
-    cuda_check(cudaEventSynchronize(ctx->ev[3]), "sync");
+    cuda_check(cudaEventSynchronize(ctx->x->ev[3]), "sync");
     kstat_collect(ctx);
     if (precision != SLGPU_PREC_FP64) {
         unsigned int err = 0;
-        cuda_check(cudaMemcpy(&err, ctx->split_error.as<void>(), 4, cudaMemcpyDeviceToHost), "D2H split error");
+        cuda_check(cudaMemcpy(&err, ctx->x->split_error.as<void>(), 4, cudaMemcpyDeviceToHost), "D2H split error");
         if (err != 0)
             fail(SLGPU_E_TIMEOUT, "a split-precision contraction tile timed out waiting for its data");
     }
     float coef_ms = 0, contract_ms = 0;
-    cudaEventElapsedTime(&coef_ms, ctx->evpool[0], ctx->evpool[1]);
-    cudaEventElapsedTime(&contract_ms, ctx->evpool[1], ctx->evpool[2]);
-    ctx->timings[0] = coef_ms;
-    ctx->timings[1] = contract_ms;
-    ctx->timings[2] = ev_ms(ctx, 1, 2);
-    ctx->timings[3] = ev_ms(ctx, 2, 3);
-    ctx->timings[4] = ev_ms(ctx, 0, 3);
+    cudaEventElapsedTime(&coef_ms, ctx->x->evpool[0], ctx->x->evpool[1]);
+    cudaEventElapsedTime(&contract_ms, ctx->x->evpool[1], ctx->x->evpool[2]);
+    ctx->x->timings[0] = coef_ms;
+    ctx->x->timings[1] = contract_ms;
+    ctx->x->timings[2] = ev_ms(ctx, 1, 2);
+    ctx->x->timings[3] = ev_ms(ctx, 2, 3);
+    ctx->x->timings[4] = ev_ms(ctx, 0, 3);
     if (info != nullptr) {
         info->nA = P.nA;
         info->nD = P.nD;
@@ -1476,12 +1478,12 @@ int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** 
             return SLGPU_E_NODEVICE;
         }
         ctx->device = device;
-        if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->x->stream, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
             delete ctx;
             return SLGPU_E_CUDA;
         }
-        for (auto& e : ctx->ev) cudaEventCreate(&e);
+        for (auto& e : ctx->x->ev) cudaEventCreate(&e);
         cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
         // Keep freed blocks in the stream-ordered pool between assemblies.
         cudaMemPool_t pool;
@@ -1508,19 +1510,19 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
     ctx->constr_dev.release();
     // Every device buffer the context owns is freed on its stream, so all of
     // them must go before the stream does.
-    ctx->split_cols.release();
-    ctx->split_colexp.release();
-    ctx->split_error.release();
+    ctx->x->split_cols.release();
+    ctx->x->split_colexp.release();
+    ctx->x->split_error.release();
     ctx->rhs_record.clear();
     for (cudaLibrary_t lib : ctx->jit_libs) cudaLibraryUnload(lib);
     ctx->jit_libs.clear();
     ctx->jit_kernels.clear();
     if (!ctx->record_only) {
-        cudaStreamSynchronize(ctx->stream);
-        for (auto& e : ctx->ev) cudaEventDestroy(e);
-        for (auto& e : ctx->evpool) cudaEventDestroy(e);
-        for (auto& e : ctx->kev) cudaEventDestroy(e);
-        cudaStreamDestroy(ctx->stream);
+        cudaStreamSynchronize(ctx->x->stream);
+        for (auto& e : ctx->x->ev) cudaEventDestroy(e);
+        for (auto& e : ctx->x->evpool) cudaEventDestroy(e);
+        for (auto& e : ctx->x->kev) cudaEventDestroy(e);
+        cudaStreamDestroy(ctx->x->stream);
     }
     delete ctx;
 }
@@ -1668,7 +1670,7 @@ int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const d
             return;
         }
         cuda_check(cudaMemcpyAsync(g.elemdata.as<double>() + g.elemdata_off[k], values, (size_t)g.nelem * 8, cudaMemcpyHostToDevice,
-                                   ctx->stream),
+                                   ctx->x->stream),
                    "upload elemdata");
     });
 }
@@ -1687,7 +1689,7 @@ int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const 
             std::copy(values, values + n, g.rec->fielddata[k].begin());
             return;
         }
-        cuda_check(cudaMemcpyAsync(g.fielddata.as<double>() + g.field_off[k], values, n * 8, cudaMemcpyHostToDevice, ctx->stream),
+        cuda_check(cudaMemcpyAsync(g.fielddata.as<double>() + g.field_off[k], values, n * 8, cudaMemcpyHostToDevice, ctx->x->stream),
                    "upload fielddata");
     });
 }
@@ -1750,7 +1752,7 @@ int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* te
             g.term_scale.assign(term_scales, term_scales + g.nterms);
             if (!ctx->record_only)
                 cuda_check(cudaMemcpyAsync(g.term_scale_d.as<void>(), term_scales, (size_t)g.nterms * 8, cudaMemcpyHostToDevice,
-                                           ctx->stream),
+                                           ctx->x->stream),
                            "upload scales");
         }
         if (dest_multipliers != nullptr)
@@ -1778,7 +1780,7 @@ int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* A
         Pattern& P = *M.pattern;
         auto d2h = [&](void* dst, const void* src, size_t n) {
             if (n > 0)
-                cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->stream), "D2H csr");
+                cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H csr");
         };
         d2h(Arows, P.Arows.as<void>(), (P.nA + 1) * 4);
         d2h(Acols, P.Acols.as<void>(), P.nnzA * 4);
@@ -1786,7 +1788,7 @@ int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* A
         d2h(Drows, P.Drows.as<void>(), (P.nA + 1) * 4);
         d2h(Dcols, P.Dcols.as<void>(), P.nnzD * 4);
         d2h(Dvals, M.Dvals.as<void>(), P.nnzD * 8);
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync download");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync download");
     });
 }
 
@@ -1798,10 +1800,10 @@ int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, doub
             fail(SLGPU_E_STATE, "matrix not processed");
         Pattern& P = *M.pattern;
         if (P.nnzA > 0)
-            cuda_check(cudaMemcpyAsync(Avals, M.Avals.as<void>(), P.nnzA * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            cuda_check(cudaMemcpyAsync(Avals, M.Avals.as<void>(), P.nnzA * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
         if (P.nnzD > 0)
-            cuda_check(cudaMemcpyAsync(Dvals, M.Dvals.as<void>(), P.nnzD * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync download");
+            cuda_check(cudaMemcpyAsync(Dvals, M.Dvals.as<void>(), P.nnzD * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync download");
     });
 }
 
@@ -1839,8 +1841,8 @@ int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int 
         process_matrix(ctx, M, nullptr, precision, true, nullptr);
         std::vector<double> dense((size_t)ndofs);
         if (ndofs > 0)
-            cuda_check(cudaMemcpyAsync(dense.data(), M.Avals.as<void>(), (size_t)ndofs * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "sync rhs");
+            cuda_check(cudaMemcpyAsync(dense.data(), M.Avals.as<void>(), (size_t)ndofs * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync rhs");
         for (int64_t i = 0; i < ndofs; i++) b_accum[i] += dense[i];
     });
 }
@@ -1849,7 +1851,7 @@ int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5)
 {
     if (ctx == nullptr || ms5 == nullptr)
         return SLGPU_E_ARG;
-    for (int i = 0; i < 5; i++) ms5[i] = ctx->timings[i];
+    for (int i = 0; i < 5; i++) ms5[i] = ctx->x->timings[i];
     return SLGPU_OK;
 }
 
@@ -1857,9 +1859,9 @@ int slgpu_kernel_stats(const slgpu_ctx* ctx, const char* family, double* total_m
 {
     if (ctx == nullptr || family == nullptr)
         return SLGPU_E_ARG;
-    auto it = ctx->kstats.find(family);
-    const Ctx::KernelStat none{};
-    const Ctx::KernelStat& k = it == ctx->kstats.end() ? none : it->second;
+    auto it = ctx->x->kstats.find(family);
+    const KernelStat none{};
+    const KernelStat& k = it == ctx->x->kstats.end() ? none : it->second;
     if (total_ms != nullptr)
         *total_ms = k.ms;
     if (launches != nullptr)

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -32,6 +33,7 @@ public:
 
 private:
     Ctx* ctx_ = nullptr;
+    cudaStream_t s_ = nullptr;  // allocated (and freed) in this stream's order
     void* p_ = nullptr;
     size_t n_ = 0;
 };
@@ -147,15 +149,37 @@ struct Matrix {
     slgpu_csr_info info{};
 };
 
+// Per kernel family: device time (CUDA events around each launch on the
+// stream), launches and algorithmic work of the last process().
+struct KernelStat {
+    double ms = 0, work = 0;
+    int64_t launches = 0;
+};
+
+// Everything a sequence of launches needs for itself: its stream, timing
+// events and per-call scratch.  A context has one (main); a server adds one
+// per slot, so that requests run on their own streams.
+struct Exec {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    double timings[5] = {0, 0, 0, 0, 0};
+    std::vector<cudaEvent_t> evpool;                       // per-phase events
+    std::vector<cudaEvent_t> kev;                          // start/stop pairs
+    std::vector<std::pair<std::string, double>> kev_tag;   // family, work of each pair
+    std::map<std::string, KernelStat> kstats;
+    DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
+    DevBuf split_error;                // device flag set by a timed-out wait
+};
+
 struct Ctx {
     int device = -1;
     int nsm = 0;  // multiprocessors of the device
     bool record_only = false;
     size_t budget = 0;
     int64_t in_use = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[6] = {};
-    double timings[5] = {0, 0, 0, 0, 0};
+    Exec main;
+    Exec* x = &main;        // the execution state launches are issued on
+    std::recursive_mutex mu;  // one thread at a time inside the context
     std::string last_error;
     std::map<int, MeshDev> meshes;
     std::map<int, std::unique_ptr<Matrix>> matrices;
@@ -167,19 +191,7 @@ struct Ctx {
     std::vector<uint8_t> constr_host;  // last constraint array seen by process()
     DevBuf constr_dev;
     uint64_t constr_key[2] = {0, 0};
-    std::vector<cudaEvent_t> evpool;   // per-group phase events
     int64_t launches = 0;              // kernels launched by this context
-    // Per kernel family: device time (CUDA events around each launch on the
-    // stream), launches and algorithmic work of the last process().
-    struct KernelStat {
-        double ms = 0, work = 0;
-        int64_t launches = 0;
-    };
-    std::map<std::string, KernelStat> kstats;
-    std::vector<cudaEvent_t> kev;                          // start/stop pairs
-    std::vector<std::pair<std::string, double>> kev_tag;   // family, work of each pair
-    DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
-    DevBuf split_error;                // device flag set by a timed-out wait
     std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source
     std::vector<cudaLibrary_t> jit_libs;
     bool jit_broken = false;  // a coefficient kernel failed to compile: interpreter from then on

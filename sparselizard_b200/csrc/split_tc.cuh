@@ -35,7 +35,7 @@ namespace slgpu {
 constexpr int kSplitM = 128;     // element-matrix entries per tile (TMEM lanes)
 constexpr int kSplitKStep = 32;  // bytes of K per pipeline stage (one MMA K)
 constexpr int kSplitMaxS = 7;    // slices per operand (levels 2..8)
-constexpr int kSplitEpiWarps = 8;
+constexpr int kSplitEpiWarps = 16;  // 4 per TMEM lane quarter, 16 columns each
 constexpr int kSplitThreads = 64 + 32 * kSplitEpiWarps;
 constexpr int kSplitABytes = 2 * kSplitM * 16;  // one slice of one K step of A
 
@@ -339,8 +339,8 @@ constexpr size_t split_smem_bytes() { return sizeof(SplitSmem<NE>) + 1024; }
 // role alike.
 //   warp 0 (one thread): bulk copies of each K step into the stage ring;
 //   warp 1 (one thread): MMAs; owns the TMEM allocation;
-//   warps 2-9: epilogue; warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31 and
-//              half of the NE columns.
+//   warps 2-17: epilogue; warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31 and
+//              16 of the NE columns.
 // Barriers: full/empty per stage (copies -> MMA -> copies), tmem_full[b] (MMAs
 // of a tile done -> epilogue) and tmem_empty[b] (epilogue has read
 // accumulator b -> MMAs of the next tile using it).  Every wait is bounded: on
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&sm.tmem_full[b], 1);
-            mbar_init(&sm.tmem_empty[b], kSplitEpiWarps);
+            mbar_init(&sm.tmem_empty[b], NE / 4);  // epilogue warps with columns
         }
         mbar_init(&sm.drain, 1);
         sm.failed = 0;
@@ -481,11 +481,15 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
             atomicOr(p.error, 2u);
     } else if (warp >= 2) {
         // ------------------------------------------------ epilogue
+        // Warp w reads TMEM lane quarter w % 4 and columns c0 .. c0+15 of
+        // each level.  Only levels 2..5 (combined into H) and then 6..L are
+        // held in registers before the accumulator is released; the rest of
+        // the recombination and the stores overlap the next tile's MMAs.
         const int quarter = warp & 3;
-        const int cbeg = ((warp - 2) / 4) * (NE / 2);  // this warp's half of the columns
+        const int c0 = ((warp - 2) >> 2) * 16;
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         int64_t i = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork; w += gridDim.x) {
+        for (int64_t w = blockIdx.x; w < p.nwork && c0 < NE; w += gridDim.x) {
             const int pt = (int)(w % p.ntp);
             const int64_t u = w / p.ntp;
             const Tile unit = split_unit<NE>(p.tiles, u);
@@ -498,46 +502,47 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int pe = pt * kSplitM + quarter * 32 + lane;
-            const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
-            const int32_t* ce = p.colexp + u * NE;
-            double* outp = p.out + (int64_t)unit.e0 * p.P + pe;
-#pragma unroll 1
-            for (int c0 = cbeg; c0 < cbeg + NE / 2; c0 += 16) {
-                int32_t r[L - 1][16];
+            const uint32_t col = lane_base + (uint32_t)(buf * 256 + c0);
+            // V = 2^-35 (H + 2^-21 Lo): H = sum_{l<=5} r_l 2^(7(5-l)),
+            // Lo = sum_{l>=6} r_l 2^(7(8-l)); both exact in int64.
+            long long H[16];
+            {
+                int32_t r[4][16];
 #pragma unroll
-                for (int l = 0; l < L - 1; l++) tmem_ld16_nowait(lane_base + (uint32_t)(buf * 256 + l * NE + c0), r[l]);
+                for (int l = 0; l < 4; l++) tmem_ld16_nowait(col + (uint32_t)(l * NE), r[l]);
                 tmem_ld_wait();
-                if (c0 + 16 == cbeg + NE / 2) {
-                    // All of this warp's accumulators are in registers: release.
-                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0)
-                        mbar_arrive(&sm.tmem_empty[buf]);
-                }
-                int cx[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    H[j] = (((long long)r[0][j] * 128 + r[1][j]) * 128 + r[2][j]) * 128 + r[3][j];
+            }
+            int32_t r[L - 5][16];
+#pragma unroll
+            for (int l = 0; l < L - 5; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), r[l]);
+            tmem_ld_wait();
+            // This warp's accumulators are in registers: release them.
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(&sm.tmem_empty[buf]);
+            const int pe = pt * kSplitM + quarter * 32 + lane;
+            if (pe < p.P) {
+                const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
+                const int32_t* ce = p.colexp + u * NE + c0;
+                double* outp = p.out + (int64_t)(unit.e0 + c0) * p.P + pe;
+                const int nj = min(16, unit.ne - c0);
 #pragma unroll
                 for (int j = 0; j < 16; j += 4) {
-                    const int4 c4 = *reinterpret_cast<const int4*>(ce + c0 + j);
-                    cx[j] = c4.x;
-                    cx[j + 1] = c4.y;
-                    cx[j + 2] = c4.z;
-                    cx[j + 3] = c4.w;
-                }
-                if (pe < p.P) {
+                    const int4 c4 = *reinterpret_cast<const int4*>(ce + j);
+                    const int cx[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        // V = 2^-35 (H + 2^-21 Lo): H = sum_{l<=5} r_l 2^(7(5-l)),
-                        // Lo = sum_{l>=6} r_l 2^(7(8-l)); both exact in int64.
-                        long long H = 0, Lo = 0;
+                    for (int jj = 0; jj < 4; jj++) {
+                        long long Lo = 0;
 #pragma unroll
-                        for (int l = 2; l <= 5; l++) H = H * 128 + r[l - 2][j];
-#pragma unroll
-                        for (int l = 6; l <= L; l++) Lo = Lo * 128 + r[l - 2][j];
+                        for (int l = 0; l < L - 5; l++) Lo = Lo * 128 + r[l][j + jj];
                         Lo <<= 7 * (8 - L);
-                        const double d = fma((double)Lo, 0x1p-21, (double)H);
-                        if (c0 + j < unit.ne)
-                            outp[(int64_t)(c0 + j) * p.P] = scale2(d, rex + cx[j]);
+                        const double d = fma((double)Lo, 0x1p-21, (double)H[j + jj]);
+                        if (j + jj < nj)
+                            outp[(int64_t)(j + jj) * p.P] = scale2(d, rex + cx[jj]);
                     }
                 }
             }
