@@ -268,6 +268,83 @@ int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nno
                       int64_t* nelem, const int32_t** conn);
 
 /*
+ * Serving: assembly requests on resident problems, run concurrently.
+ * No counterpart in the reference, whose generate()/A() is one synchronous
+ * assembly; this is the request loop around the same path.
+ *
+ * A template is a matrix handle that has been processed once (its pattern,
+ * meshes, tables and addresses are resident).  A request recomputes its
+ * values with new per-element coefficient data and downloads them:
+ *   - updates replace per-element data arrays of the template's groups
+ *     (SLGPU_UPDATE_ELEMDATA: elemdata array `index`, 1 row;
+ *     SLGPU_UPDATE_FIELDDATA: fielddata array `index`, `rows` rows), given in
+ *     mesh element order of the group's element type ([rows][count], count =
+ *     elements of that type in the mesh) and gathered into each group's own
+ *     element order on the device;
+ *   - Avals / Dvals receive nnzA / nnzD values (the template's pattern);
+ *     page-locked buffers (slgpu_host_alloc) are written by the copy engine
+ *     directly, others through a staging copy.
+ * A server thread admits queued requests in arrival order as soon as one of
+ * `nslots` execution slots is free and the request's device memory fits the
+ * context's HBM budget; each slot has its own stream, so admitted requests
+ * overlap on the device.  Results are bit-identical to the same request run
+ * alone (fixed summation order, no atomics in the values).
+ * While a server exists, every other call on its context is serialised with
+ * it (context lock); destroying the server waits for its requests.  A
+ * template must not be changed (set_elemdata/fielddata/scales, destroy is
+ * safe) while requests on it are queued or running.
+ */
+typedef struct slgpu_server slgpu_server;
+
+enum { SLGPU_UPDATE_ELEMDATA = 0, SLGPU_UPDATE_FIELDDATA = 1 };
+
+typedef struct {
+    int32_t group; /* group index in the template */
+    int32_t kind;  /* SLGPU_UPDATE_* */
+    int32_t index; /* elemdata / fielddata array index in the group */
+    int32_t rows;  /* rows of the array (1 for elemdata) */
+    const double* values; /* [rows][count], mesh element order; copied at submit */
+    int64_t count;
+} slgpu_update;
+
+typedef struct {
+    int32_t handle;    /* template matrix */
+    int32_t precision; /* SLGPU_PREC_* */
+    int32_t nupdates;
+    int32_t pad;
+    const slgpu_update* updates;
+    double* Avals; /* host, nnzA values */
+    double* Dvals; /* host, nnzD values (may be NULL when nnzD = 0) */
+} slgpu_request;
+
+typedef struct {
+    double submit_s; /* host times (seconds since the server was created) */
+    double start_s;  /* launched on a slot */
+    double done_s;   /* results in host memory */
+    double device_ms; /* event time from the first to the last operation on the slot */
+    int32_t slot;
+    int32_t status;  /* SLGPU_OK, or the request's error code */
+} slgpu_request_stats;
+
+int slgpu_server_create(slgpu_ctx* ctx, int nslots, slgpu_server** out);
+/* Queues a request; returns its ticket.  The update values are copied. */
+int slgpu_server_submit(slgpu_server* s, const slgpu_request* r, int64_t* ticket);
+/* Waits up to timeout_s (< 0: no limit) for a request.  Returns SLGPU_OK when
+ * it completed, SLGPU_E_TIMEOUT when still running, or the request's own
+ * error code (message via slgpu_server_error).  stats may be NULL. */
+int slgpu_server_wait(slgpu_server* s, int64_t ticket, double timeout_s, slgpu_request_stats* stats);
+int slgpu_server_error(slgpu_server* s, int64_t ticket, char* buf, size_t len);
+/* Forgets a completed request. */
+int slgpu_server_release(slgpu_server* s, int64_t ticket);
+/* Requests queued or running. */
+int64_t slgpu_server_pending(slgpu_server* s);
+/* Waits for every request, stops the server thread and frees its slots. */
+void slgpu_server_destroy(slgpu_server* s);
+/* Page-locked host memory for request outputs (and inputs). */
+int slgpu_host_alloc(slgpu_ctx* ctx, size_t bytes, void** out);
+void slgpu_host_free(void* p);
+
+/*
  * Element matrices of one group without allocating device memory.
  * This entry point has no counterpart in the reference: it exists for
  * callers that cannot allocate GPU memory themselves -- a host application

@@ -68,6 +68,24 @@ class Work(ctypes.Structure):
                 ("nnz", c_int64), ("nA", c_int64), ("ngroups", c_int32), ("pad", c_int32)]
 
 
+UPDATE_ELEMDATA, UPDATE_FIELDDATA = 0, 1
+
+
+class Update(ctypes.Structure):
+    _fields_ = [("group", c_int32), ("kind", c_int32), ("index", c_int32), ("rows", c_int32),
+                ("values", POINTER(c_double)), ("count", c_int64)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("handle", c_int32), ("precision", c_int32), ("nupdates", c_int32), ("pad", c_int32),
+                ("updates", POINTER(Update)), ("Avals", POINTER(c_double)), ("Dvals", POINTER(c_double))]
+
+
+class RequestStats(ctypes.Structure):
+    _fields_ = [("submit_s", c_double), ("start_s", c_double), ("done_s", c_double), ("device_ms", c_double),
+                ("slot", c_int32), ("status", c_int32)]
+
+
 # Every exported symbol with (restype, argtypes); the tests check that the
 # library exports each of them.
 SIGNATURES = {
@@ -109,6 +127,15 @@ SIGNATURES = {
     "slgpu_record_rhs_group": (c_int, [c_void_p, c_int, POINTER(Group), POINTER(c_int64)]),
     "slgpu_record_mesh": (c_int, [c_void_p, c_int, c_int, POINTER(c_int64), POINTER(POINTER(c_double)), POINTER(c_int),
                                   POINTER(c_int64), POINTER(POINTER(c_int32))]),
+    "slgpu_server_create": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    "slgpu_server_submit": (c_int, [c_void_p, POINTER(Request), POINTER(c_int64)]),
+    "slgpu_server_wait": (c_int, [c_void_p, c_int64, c_double, POINTER(RequestStats)]),
+    "slgpu_server_error": (c_int, [c_void_p, c_int64, c_char_p, c_size_t]),
+    "slgpu_server_release": (c_int, [c_void_p, c_int64]),
+    "slgpu_server_pending": (c_int64, [c_void_p]),
+    "slgpu_server_destroy": (None, [c_void_p]),
+    "slgpu_host_alloc": (c_int, [c_void_p, c_size_t, POINTER(c_void_p)]),
+    "slgpu_host_free": (None, [c_void_p]),
 }
 
 

@@ -448,7 +448,7 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
                 units.push_back(Unit{norm, {{b.first, f[lead]}}});
         }
 
-        slgpu_adapter::ensure_mesh(elemtype);
+        const int mesh_id = slgpu_adapter::ensure_mesh(elemtype);
         element curved(elemtype, universe::getrawmesh()->getelements()->getcurvatureorder());
         const int ncn = curved.countcurvednodes();
         lagrangeformfunction lag(elemtype, universe::getrawmesh()->getelements()->getcurvatureorder(), gpcoords);
@@ -485,7 +485,7 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
                 dests.push_back(slgpu_dest{tfa.getvalues(), dofp, d.second});
             }
             slgpu_group g{};
-            g.mesh = 0;
+            g.mesh = mesh_id;
             g.elemtype = elemtype;
             g.elemdim = elemdim;
             g.problemdim = meshdim;

@@ -35,13 +35,16 @@ std::map<rawmat*, std::shared_ptr<MatEntry>> g_mats;
 std::shared_ptr<MatEntry> g_last_entry;
 std::map<rawmat*, std::shared_ptr<MatEntry>> g_processed;
 
+// One engine mesh per sparselizard mesh (rawmesh number), so that matrices
+// assembled on earlier meshes stay valid as templates after another mesh is
+// loaded.  A mesh whose nodes move in place is updated in place.
 struct MeshState {
-    int rawmeshnumber = -1;
+    int id = 0;  // engine mesh id
     long long nnodes = -1;
     unsigned long long coordhash = 0;
     std::map<int, long long> typecounts;  // element type -> uploaded count
 };
-MeshState g_mesh;
+std::map<int, MeshState> g_meshes;  // by rawmesh number
 
 struct CtxGuard {
     ~CtxGuard()
@@ -123,9 +126,15 @@ int ensure_mesh(int elemtype)
     unsigned long long h = 1469598103934665603ull;
     const unsigned long long* words = reinterpret_cast<const unsigned long long*>(xyz->data());
     for (size_t i = 0; i < xyz->size(); i++) h = (h ^ words[i]) * 1099511628211ull;
-    if (g_mesh.rawmeshnumber != rm->getmeshnumber() || g_mesh.nnodes != nn || g_mesh.coordhash != h) {
-        check(slgpu_mesh_set_nodes(ctx, 0, nn, xyz->data()), "slgpu_mesh_set_nodes");
-        g_mesh.rawmeshnumber = rm->getmeshnumber();
+    auto mit = g_meshes.find(rm->getmeshnumber());
+    if (mit == g_meshes.end()) {
+        MeshState st;
+        st.id = (int)g_meshes.size();
+        mit = g_meshes.emplace(rm->getmeshnumber(), st).first;
+    }
+    MeshState& g_mesh = mit->second;
+    if (g_mesh.nnodes != nn || g_mesh.coordhash != h) {
+        check(slgpu_mesh_set_nodes(ctx, g_mesh.id, nn, xyz->data()), "slgpu_mesh_set_nodes");
         g_mesh.nnodes = nn;
         g_mesh.coordhash = h;
         g_mesh.typecounts.clear();
@@ -139,10 +148,10 @@ int ensure_mesh(int elemtype)
         std::vector<int32_t> conn((size_t)ne * ncn);
         for (long long e = 0; e < ne; e++)
             for (int k = 0; k < ncn; k++) conn[(size_t)e * ncn + k] = els->getsubelement(0, elemtype, (int)e, k);
-        check(slgpu_mesh_set_elements(ctx, 0, elemtype, ncn, ne, conn.data()), "slgpu_mesh_set_elements");
+        check(slgpu_mesh_set_elements(ctx, g_mesh.id, elemtype, ncn, ne, conn.data()), "slgpu_mesh_set_elements");
         g_mesh.typecounts[elemtype] = ne;
     }
-    return 0;
+    return g_mesh.id;
 }
 
 int find_matrix_handle(rawmat* m)

@@ -37,11 +37,6 @@ namespace slgpu {
 
 static const char* kNoDevice = "record-only context: nothing is executed";
 
-struct SlgpuException : std::exception {
-    Error e;
-    SlgpuException(int code, std::string msg) : e{code, std::move(msg)} {}
-    const char* what() const noexcept override { return e.msg.c_str(); }
-};
 
 [[noreturn]] static void fail(int code, const std::string& msg) { throw SlgpuException(code, msg); }
 
@@ -320,7 +315,7 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
         // Gauss points and Lagrange tables, so one kernel evaluates them all.
         uint64_t h = mix64((uint64_t)g.mesh ^ (uint64_t)g.elemtype << 8 ^ (uint64_t)g.ngp << 16 ^ (uint64_t)g.ncurvednodes << 32 ^
                            (uint64_t)g.problemdim << 48);
-        h = mix64(h ^ (uint64_t)g.nelem);
+        h = mix64(h ^ (uint64_t)g.nelem ^ (uint64_t)(uint32_t)g.mesh << 40 ^ (uint64_t)(uint32_t)g.elemtype << 56);
         for (int64_t e = 0; e < g.nelem; e++) h = mix64(h ^ ((uint64_t)(uint32_t)g.elems[e] << 8 | (uint64_t)(uint32_t)g.orient[e] << 40));
         const size_t nl = (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp;
         for (size_t k = 0; k < nl; k++) {
@@ -506,7 +501,7 @@ static CoefParams coef_params(Ctx* ctx, const GroupDev& g, double* C)
 }
 
 // Segments of the COO space: (group, destination) blocks then raw fragments.
-static std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals)
+std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals)
 {
     std::vector<Segment> segs;
     int64_t coo = 0, vb = 0;
@@ -532,7 +527,7 @@ static std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>
 
 // Kernel-family timers: kstat_start/kstat_stop bracket launches with an
 // event pair; kstat_collect sums them once the stream has been synchronised.
-static int kstat_start(Ctx* ctx, const char* family, double work)
+int kstat_start(Ctx* ctx, const char* family, double work)
 {
     const size_t i = ctx->x->kev_tag.size();
     while (ctx->x->kev.size() < 2 * (i + 1)) {
@@ -545,9 +540,9 @@ static int kstat_start(Ctx* ctx, const char* family, double work)
     return (int)i;
 }
 
-static void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->kev[2 * i + 1], ctx->x->stream), "cudaEventRecord"); }
+void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->kev[2 * i + 1], ctx->x->stream), "cudaEventRecord"); }
 
-static void kstat_collect(Ctx* ctx)
+void kstat_collect(Ctx* ctx)
 {
     ctx->x->kstats.clear();
     for (size_t i = 0; i < ctx->x->kev_tag.size(); i++) {
@@ -955,7 +950,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 // Tier 0: 7 slices, levels <= 8 (28 INT8 products; about 1e-12 relative per
 // element matrix, well inside 1e-10); tier 1: 5 slices, levels <= 6 (15
 // products; about 1e-8, inside the FP32-level 1e-6).
-static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
+static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int tier)
 {
     std::unique_ptr<GroupDev::Split>& sp = g.split[tier];
     if (sp)
@@ -989,6 +984,31 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
     cuda_check(cudaGetLastError(), "k_slice_rows");
     ctx->launches++;
     return *sp;
+}
+
+// The row slices are resident with the group, so they are built in the main
+// execution state's stream order; a request stream waits for them.
+static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
+{
+    if (g.split[tier])
+        return *g.split[tier];
+    Exec* cur = ctx->x;
+    ctx->x = &ctx->main;
+    try {
+        build_split(ctx, g, tier);
+    } catch (...) {
+        ctx->x = cur;
+        throw;
+    }
+    ctx->x = cur;
+    if (cur != &ctx->main) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_check(cudaEventRecord(e, ctx->main.stream), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(cur->stream, e, 0), "cudaStreamWaitEvent");
+        cudaEventDestroy(e);
+    }
+    return *g.split[tier];
 }
 
 // Whether a group's contraction can take the split path: level sums stay
@@ -1124,8 +1144,8 @@ struct JitGroup {
 // groups with the same geometry key run as one runtime-compiled kernel; the
 // interpreter kernel is used when SLGPU_COEF_INTERPRETER=1 or when a kernel
 // cannot be compiled.
-static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vector<int64_t>& coff, int32_t* elemexp,
-                                const std::vector<int64_t>& eoff)
+static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std::vector<int64_t>& coff, int32_t* elemexp,
+                                const std::vector<int64_t>& eoff, const std::vector<GroupData>* ov)
 {
     static const bool interp_only = [] {
         const char* v = std::getenv("SLGPU_COEF_INTERPRETER");
@@ -1134,7 +1154,7 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
     const size_t ng = M.groups.size();
     size_t k = 0;
     while (k < ng) {
-        GroupDev& g0 = *M.groups[k];
+        const GroupDev& g0 = *M.groups[k];
         size_t k1 = k + 1;
         while (k1 < ng && M.groups[k1]->geom_hash == g0.geom_hash) k1++;
         if (g0.nelem == 0) {
@@ -1150,8 +1170,10 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 std::vector<JitGroup> jg;
                 for (size_t j = k; j < k1; j++) {
                     GroupDev& G = *M.groups[j];
-                    jg.push_back(JitGroup{G.tables.as<double>(), G.elemdata.as<double>(), G.fielddata.as<double>(),
-                                          G.term_scale_d.as<double>(), C + coff[j], eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
+                    const double* ed = ov != nullptr && (*ov)[j].elemdata != nullptr ? (*ov)[j].elemdata : G.elemdata.as<double>();
+                    const double* fd = ov != nullptr && (*ov)[j].fielddata != nullptr ? (*ov)[j].fielddata : G.fielddata.as<double>();
+                    jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, G.term_scale_d.as<double>(), C + coff[j],
+                                          eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
                 }
                 DevBuf djg;
                 upload(ctx, djg, jg);
@@ -1181,6 +1203,10 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
                 GroupDev& G = *M.groups[j];
                 CoefParams cp = coef_params(ctx, G, C + coff[j]);
                 cp.elemexp = eoff[j] >= 0 ? elemexp + eoff[j] : nullptr;
+                if (ov != nullptr && (*ov)[j].elemdata != nullptr)
+                    cp.elemdata = (*ov)[j].elemdata;
+                if (ov != nullptr && (*ov)[j].fielddata != nullptr)
+                    cp.fielddata = (*ov)[j].fielddata;
                 const int64_t n = G.nelem * (int64_t)G.ngp;
                 const int kt = kstat_start(ctx, "coefficients", 8.0 * G.nterms * G.ngp * G.nelem);
                 k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->x->stream>>>(cp);
@@ -1190,6 +1216,147 @@ static void launch_coefficients(Ctx* ctx, Matrix& M, double* C, const std::vecto
             }
         }
         k = k1;
+    }
+}
+
+// Steps 1 and 2 on the current execution state's stream: coefficients of
+// every group (with per-group data overrides, if given), contraction of each
+// group into `vals` at the group's value base, fragment values after them.
+void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::vector<int64_t>& gvb, double* vals,
+                         const std::vector<GroupData>* ov)
+{
+    // Coefficients of every group coexist ([term][gp][element] per group) so
+    // that groups sharing geometry are evaluated by one kernel.
+    std::vector<int64_t> coff(M.groups.size());
+    int64_t ctot = 0;
+    for (size_t k = 0; k < M.groups.size(); k++) {
+        coff[k] = ctot;
+        ctot += (int64_t)M.groups[k]->nterms * M.groups[k]->ngp * M.groups[k]->nelem;
+    }
+    DevBuf C;
+    C.alloc(ctx, std::max<int64_t>(ctot, 1) * 8);
+    if (precision != SLGPU_PREC_FP64) {
+        if (ctx->x->split_error.empty())
+            ctx->x->split_error.alloc(ctx, 16);
+        cuda_check(cudaMemsetAsync(ctx->x->split_error.as<void>(), 0, 16, ctx->x->stream), "memset");
+    }
+    while (ctx->x->evpool.size() < 3) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        ctx->x->evpool.push_back(e);
+    }
+    // Split-precision groups: per-element exponents of the coefficients,
+    // gathered by the coefficient kernels (atomicMax from a very negative start).
+    std::vector<int64_t> eoff(M.groups.size(), -1);
+    int64_t etot = 0;
+    for (size_t k = 0; k < M.groups.size(); k++)
+        if (uses_split(*M.groups[k], precision)) {
+            eoff[k] = etot;
+            etot += M.groups[k]->nelem;
+        }
+    DevBuf E;
+    if (etot > 0) {
+        E.alloc(ctx, (size_t)etot * 4);
+        cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
+    }
+    cuda_check(cudaEventRecord(ctx->x->evpool[0], ctx->x->stream), "cudaEventRecord");
+    launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov);
+    cuda_check(cudaEventRecord(ctx->x->evpool[1], ctx->x->stream), "cudaEventRecord");
+    size_t gi = 0;
+    for (auto& g : M.groups) {
+        if (g->nelem > 0) {
+            double* Cg = C.as<double>() + coff[gi];
+            // Split precision for the larger element matrices (order >= 2);
+            // right-hand sides and small matrices stay in FP64.
+            if (uses_split(*g, precision)) {
+                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], vals + gvb[gi]);
+                gi++;
+                continue;
+            }
+            ContractParams kp{};
+            kp.tables = g->tables.as<double>();
+            kp.tab_off = g->tab_off_d.as<int64_t>();
+            kp.term_tf = g->term_tf_d.as<int32_t>();
+            kp.term_dof = g->term_dof_d.as<int32_t>();
+            kp.nterms = g->nterms;
+            kp.ngp = g->ngp;
+            kp.ntf = g->ntf;
+            kp.ndof = g->ndof;
+            kp.nelem = g->nelem;
+            kp.C = Cg;
+            kp.tiles = g->tiles_d.as<Tile>();
+            kp.out = vals + gvb[gi];
+            const int64_t P = (int64_t)g->ntf * g->ndof;
+            dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
+            if (grid.y > 65535)
+                fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
+            const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
+            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
+            kstat_stop(ctx, kt);
+            cuda_check(cudaGetLastError(), "k_contract_fp64");
+            ctx->launches++;
+        }
+        gi++;
+    }
+    cuda_check(cudaEventRecord(ctx->x->evpool[2], ctx->x->stream), "cudaEventRecord");
+    C.release();
+    {
+        int64_t vb = 0;
+        for (auto& g : M.groups) vb += (int64_t)g->ntf * g->ndof * g->nelem;
+        for (auto& f : M.frags) {
+            int64_t n = (int64_t)f->nr * f->nc;
+            if (n > 0)
+                cuda_check(cudaMemcpyAsync(vals + vb, f->vals.as<double>(), n * 8, cudaMemcpyDeviceToDevice, ctx->x->stream),
+                           "D2D fragment values");
+            vb += n;
+        }
+    }
+}
+
+// Step 4 on the current execution state's stream: A/D values (or the dense
+// right-hand side) from the element values through the resident pattern.
+void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::vector<Segment>& segs, bool rhs, const double* vals,
+                       double* Avals, double* Dvals)
+{
+    std::vector<RowSeg> rsegs(segs.size());
+    {
+        size_t s = 0;
+        for (auto& g : M.groups)
+            for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
+        for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
+    }
+    DevBuf drsegs;
+    upload(ctx, drsegs, rsegs);
+    if (P.nA > 0) {
+        RowParams rp{};
+        rp.inc_ptr = P.inc_ptr.as<uint32_t>();
+        rp.inc = P.inc.as<unsigned long long>();
+        rp.segs = drsegs.as<RowSeg>();
+        rp.slotmap = P.slotmap.as<int16_t>();
+        rp.vals = vals;
+        rp.Arows = P.Arows.as<uint32_t>();
+        rp.Drows = P.Drows.as<uint32_t>();
+        rp.nrows = P.nA;
+        rp.lmax = std::max(1, P.lmax);
+        rp.Avals = Avals;
+        rp.Dvals = rhs ? nullptr : Dvals;
+        rp.dense = rhs ? Avals : nullptr;
+        const size_t per_warp = (size_t)rp.lmax * 8;
+        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
+        size_t smem = per_warp * wpb;
+        if (smem > 48 * 1024) {
+            if (smem > 227 * 1024)
+                fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
+            cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        }
+        // Bytes: kept element values and their slots, incidences, row
+        // pointers read; A and D values written.
+        const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
+        const int kt = kstat_start(ctx, "row_values", rbytes);
+        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
+        kstat_stop(ctx, kt);
+        cuda_check(cudaGetLastError(), "k_row_values");
+        ctx->launches++;
     }
 }
 
@@ -1250,92 +1417,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     // 1+2: geometry, coefficients and contraction into the value buffer.
     if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
         M.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
-    // Coefficients of every group coexist ([term][gp][element] per group) so
-    // that groups sharing geometry are evaluated by one kernel.
-    std::vector<int64_t> coff(M.groups.size());
-    int64_t ctot = 0;
-    for (size_t k = 0; k < M.groups.size(); k++) {
-        coff[k] = ctot;
-        ctot += (int64_t)M.groups[k]->nterms * M.groups[k]->ngp * M.groups[k]->nelem;
-    }
-    DevBuf C;
-    C.alloc(ctx, std::max<int64_t>(ctot, 1) * 8);
-    if (precision != SLGPU_PREC_FP64) {
-        if (ctx->x->split_error.empty())
-            ctx->x->split_error.alloc(ctx, 16);
-        cuda_check(cudaMemsetAsync(ctx->x->split_error.as<void>(), 0, 16, ctx->x->stream), "memset");
-    }
-    while (ctx->x->evpool.size() < 3) {
-        cudaEvent_t e;
-        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        ctx->x->evpool.push_back(e);
-    }
-    // Split-precision groups: per-element exponents of the coefficients,
-    // gathered by the coefficient kernels (atomicMax from a very negative start).
-    std::vector<int64_t> eoff(M.groups.size(), -1);
-    int64_t etot = 0;
-    for (size_t k = 0; k < M.groups.size(); k++)
-        if (uses_split(*M.groups[k], precision)) {
-            eoff[k] = etot;
-            etot += M.groups[k]->nelem;
-        }
-    DevBuf E;
-    if (etot > 0) {
-        E.alloc(ctx, (size_t)etot * 4);
-        cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
-    }
-    cuda_check(cudaEventRecord(ctx->x->evpool[0], ctx->x->stream), "cudaEventRecord");
-    launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff);
-    cuda_check(cudaEventRecord(ctx->x->evpool[1], ctx->x->stream), "cudaEventRecord");
-    size_t gi = 0;
-    for (auto& g : M.groups) {
-        if (g->nelem > 0) {
-            double* Cg = C.as<double>() + coff[gi];
-            // Split precision for the larger element matrices (order >= 2);
-            // right-hand sides and small matrices stay in FP64.
-            if (uses_split(*g, precision)) {
-                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], M.vals.as<double>() + gvb[gi]);
-                gi++;
-                continue;
-            }
-            ContractParams kp{};
-            kp.tables = g->tables.as<double>();
-            kp.tab_off = g->tab_off_d.as<int64_t>();
-            kp.term_tf = g->term_tf_d.as<int32_t>();
-            kp.term_dof = g->term_dof_d.as<int32_t>();
-            kp.nterms = g->nterms;
-            kp.ngp = g->ngp;
-            kp.ntf = g->ntf;
-            kp.ndof = g->ndof;
-            kp.nelem = g->nelem;
-            kp.C = Cg;
-            kp.tiles = g->tiles_d.as<Tile>();
-            kp.out = M.vals.as<double>() + gvb[gi];
-            const int64_t P = (int64_t)g->ntf * g->ndof;
-            dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
-            if (grid.y > 65535)
-                fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
-            const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
-            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
-            kstat_stop(ctx, kt);
-            cuda_check(cudaGetLastError(), "k_contract_fp64");
-            ctx->launches++;
-        }
-        gi++;
-    }
-    cuda_check(cudaEventRecord(ctx->x->evpool[2], ctx->x->stream), "cudaEventRecord");
-    C.release();
-    {
-        int64_t vb = 0;
-        for (auto& g : M.groups) vb += (int64_t)g->ntf * g->ndof * g->nelem;
-        for (auto& f : M.frags) {
-            int64_t n = (int64_t)f->nr * f->nc;
-            if (n > 0)
-                cuda_check(cudaMemcpyAsync(M.vals.as<double>() + vb, f->vals.as<double>(), n * 8, cudaMemcpyDeviceToDevice, ctx->x->stream),
-                           "D2D fragment values");
-            vb += n;
-        }
-    }
+    launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
     ev_record(ctx, 1);
 
     // 3: pattern.
@@ -1345,52 +1427,13 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     ev_record(ctx, 2);
 
     // 4: values, one warp per row.
-    std::vector<RowSeg> rsegs(segs.size());
-    {
-        size_t s = 0;
-        for (auto& g : M.groups)
-            for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
-        for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
-    }
-    DevBuf drsegs;
-    upload(ctx, drsegs, rsegs);
     if (rhs) {
         M.Avals.alloc(ctx, (size_t)std::max<int64_t>(M.ndofs, 1) * 8);
     } else {
         M.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
         M.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
     }
-    if (P.nA > 0) {
-        RowParams rp{};
-        rp.inc_ptr = P.inc_ptr.as<uint32_t>();
-        rp.inc = P.inc.as<unsigned long long>();
-        rp.segs = drsegs.as<RowSeg>();
-        rp.slotmap = P.slotmap.as<int16_t>();
-        rp.vals = M.vals.as<double>();
-        rp.Arows = P.Arows.as<uint32_t>();
-        rp.Drows = P.Drows.as<uint32_t>();
-        rp.nrows = P.nA;
-        rp.lmax = std::max(1, P.lmax);
-        rp.Avals = M.Avals.as<double>();
-        rp.Dvals = rhs ? nullptr : M.Dvals.as<double>();
-        rp.dense = rhs ? M.Avals.as<double>() : nullptr;
-        const size_t per_warp = (size_t)rp.lmax * 8;
-        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
-        size_t smem = per_warp * wpb;
-        if (smem > 48 * 1024) {
-            if (smem > 227 * 1024)
-                fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
-            cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-        }
-        // Bytes: kept element values and their slots, incidences, row
-        // pointers read; A and D values written.
-        const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
-        const int kt = kstat_start(ctx, "row_values", rbytes);
-        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
-        kstat_stop(ctx, kt);
-        cuda_check(cudaGetLastError(), "k_row_values");
-        ctx->launches++;
-    }
+    launch_row_values(ctx, M, P, segs, rhs, M.vals.as<double>(), M.Avals.as<double>(), rhs ? nullptr : M.Dvals.as<double>());
     ev_record(ctx, 3);
     cuda_check(cudaEventSynchronize(ctx->x->ev[3]), "sync");
     kstat_collect(ctx);
@@ -1435,6 +1478,7 @@ static int guarded(slgpu_ctx* ctx, F&& f)
 {
     if (ctx == nullptr)
         return SLGPU_E_ARG;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     try {
         if (!ctx->record_only && ctx->device >= 0)
             cudaSetDevice(ctx->device);

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -41,6 +42,12 @@ private:
 struct Error {
     int code;
     std::string msg;
+};
+
+struct SlgpuException : std::exception {
+    Error e;
+    SlgpuException(int code, std::string msg) : e{code, std::move(msg)} {}
+    const char* what() const noexcept override { return e.msg.c_str(); }
 };
 
 // One instruction of a compiled coefficient program (register-allocated DAG).
@@ -200,6 +207,23 @@ struct Ctx {
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;
 };
+
+// Per-group replacements of the coefficient data for one request (nullptr:
+// the group's resident array).
+struct GroupData {
+    const double* elemdata = nullptr;
+    const double* fielddata = nullptr;
+};
+
+// Launch pieces of one assembly (engine.cu), issued on ctx->x's stream.
+std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals);
+void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::vector<int64_t>& gvb, double* vals,
+                         const std::vector<GroupData>* ov);
+void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::vector<Segment>& segs, bool rhs, const double* vals,
+                       double* Avals, double* Dvals);
+int kstat_start(Ctx* ctx, const char* family, double work);
+void kstat_stop(Ctx* ctx, int i);
+void kstat_collect(Ctx* ctx);
 
 // Runtime-compiled coefficient kernels (coef_jit.cu).
 std::string jit_coef_source(const std::vector<const GroupDev*>& batch);

@@ -1,0 +1,597 @@
+// Serving loop: assembly requests on resident templates, admitted against
+// the HBM budget onto execution slots (one stream each) by a server thread,
+// so that requests that arrive while others run overlap on the device.
+//
+// A request runs the value path of slgpu_matrix_process on the template's
+// resident groups and pattern -- coefficients (with the request's
+// per-element data gathered into each group's element order), contraction,
+// CSR values -- on its slot's stream, then copies the values to the host.
+// The pattern, meshes, tables and addresses are never rebuilt.
+#include "engine_internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+
+namespace slgpu {
+
+static void cuda_check_srv(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+        throw SlgpuException(SLGPU_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// dst[r][e] = src[r][elems[e]]: per-element data from mesh order into the
+// group's element order.
+__global__ void k_gather_elements(const double* __restrict__ src, const int32_t* __restrict__ elems, int64_t nelem, int rows,
+                                  int64_t count, double* __restrict__ dst)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nelem * rows)
+        return;
+    const int64_t r = i / nelem, e = i - r * nelem;
+    dst[i] = src[r * count + elems[e]];
+}
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    int64_t ticket = 0;
+    int handle = 0, precision = 0;
+    struct Update {
+        int group, kind, index, rows;
+        int64_t count;
+        std::vector<double> values;
+    };
+    std::vector<Update> updates;
+    double* Aout = nullptr;
+    double* Dout = nullptr;
+    bool pinned_out = false;
+    // Template state kept alive while the request runs.
+    std::shared_ptr<Matrix> tmpl;
+    int64_t est_bytes = 0;
+    // Device and host resources while running.
+    DevBuf vals, Avals, Dvals, upd;
+    std::vector<DevBuf> ed, fd;
+    std::vector<double> stageA, stageD;  // pageable outputs: filled from the slot's pinned staging
+    int64_t nnzA = 0, nnzD = 0;
+    int status = -1;  // -1 queued, -2 running, else the final status
+    std::string error;
+    double t_submit = 0, t_start = 0, t_done = 0, dev_ms = 0;
+    int slot = -1;
+};
+
+struct Slot {
+    Exec ex;
+    cudaEvent_t start = nullptr, done = nullptr;
+    std::shared_ptr<Request> req;
+    void* pinned = nullptr;  // staging for inputs and pageable outputs
+    size_t pinned_bytes = 0;
+};
+
+}  // namespace
+
+struct Server {
+    Ctx* ctx = nullptr;
+    std::vector<Slot> slots;
+    std::thread th;
+    std::mutex mu;  // queue, request table, stop flag
+    std::condition_variable wake, done_cv;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::map<int64_t, std::shared_ptr<Request>> reqs;
+    int64_t next_ticket = 1;
+    int64_t running = 0;
+    bool stop = false;
+    Clock::time_point t0 = Clock::now();
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+// Device bytes a request allocates while it runs.
+int64_t estimate_bytes(const Matrix& M, int precision, const Request& r)
+{
+    int64_t vals = 0, coef = 0, exps = 0, split = 0;
+    for (auto& g : M.groups) {
+        vals += (int64_t)g->ntf * g->ndof * g->nelem;
+        coef += (int64_t)g->nterms * g->ngp * g->nelem;
+        exps += g->nelem;
+        const int64_t Qpad = ((int64_t)g->nterms * g->ngp + 31) / 32 * 32;
+        split = std::max<int64_t>(split, 7 * Qpad * (int64_t)g->tiles.size() * 64 + (int64_t)g->tiles.size() * 256);
+    }
+    for (auto& f : M.frags) vals += (int64_t)f->nr * f->nc;
+    int64_t upd = 0, over = 0;
+    for (auto& u : r.updates) {
+        upd += (int64_t)u.values.size();
+        const GroupDev& g = *M.groups[u.group];
+        over += (u.kind == SLGPU_UPDATE_ELEMDATA ? (int64_t)g.elemdata.bytes() : (int64_t)g.fielddata.bytes()) / 8;
+    }
+    const int64_t csr = M.pattern ? M.pattern->nnzA + M.pattern->nnzD : 0;
+    int64_t b = 8 * (vals + coef + csr + upd + over) + 4 * exps;
+    if (precision != SLGPU_PREC_FP64)
+        b += split;
+    return b + (int64_t(1) << 20);
+}
+
+void ensure_pinned(Slot& s, size_t bytes)
+{
+    if (s.pinned_bytes >= bytes)
+        return;
+    if (s.pinned != nullptr)
+        cudaFreeHost(s.pinned);
+    s.pinned = nullptr;
+    s.pinned_bytes = 0;
+    cuda_check_srv(cudaHostAlloc(&s.pinned, bytes, cudaHostAllocDefault), "cudaHostAlloc");
+    s.pinned_bytes = bytes;
+}
+
+// Issues a request on its slot (server thread, context lock held).
+void launch(Server& S, Slot& s, Request& r)
+{
+    Ctx* ctx = S.ctx;
+    const Matrix& M = *r.tmpl;
+    const Pattern& P = *M.pattern;
+    ctx->x = &s.ex;
+    cudaStream_t st = s.ex.stream;
+    cuda_check_srv(cudaEventRecord(s.start, st), "cudaEventRecord");
+    // Inputs: all update arrays in one pinned block, one copy to the device,
+    // then per update a copy of the group's resident array with the slice
+    // replaced by the gathered values.
+    int64_t nin = 0;
+    for (auto& u : r.updates) nin += (int64_t)u.values.size();
+    r.nnzA = P.nnzA;
+    r.nnzD = P.nnzD;
+    const size_t outbytes = r.pinned_out ? 0 : (size_t)(r.nnzA + r.nnzD) * 8;
+    ensure_pinned(s, std::max<size_t>((size_t)nin * 8, outbytes) + 64);
+    std::vector<GroupData> ov(M.groups.size());
+    r.ed.clear();
+    r.fd.clear();
+    r.ed.resize(M.groups.size());
+    r.fd.resize(M.groups.size());
+    if (nin > 0) {
+        double* hp = static_cast<double*>(s.pinned);
+        int64_t o = 0;
+        for (auto& u : r.updates) {
+            std::memcpy(hp + o, u.values.data(), u.values.size() * 8);
+            o += (int64_t)u.values.size();
+        }
+        r.upd.alloc(ctx, (size_t)nin * 8);
+        cuda_check_srv(cudaMemcpyAsync(r.upd.as<void>(), hp, (size_t)nin * 8, cudaMemcpyHostToDevice, st), "H2D request inputs");
+        o = 0;
+        for (auto& u : r.updates) {
+            GroupDev& g = *M.groups[u.group];
+            const bool elem = u.kind == SLGPU_UPDATE_ELEMDATA;
+            DevBuf& dst = elem ? r.ed[u.group] : r.fd[u.group];
+            const DevBuf& res = elem ? g.elemdata : g.fielddata;
+            if (dst.empty()) {
+                dst.alloc(ctx, res.bytes());
+                cuda_check_srv(cudaMemcpyAsync(dst.as<void>(), res.as<void>(), res.bytes(), cudaMemcpyDeviceToDevice, st), "D2D group data");
+            }
+            const int64_t base = elem ? g.elemdata_off[u.index] : g.field_off[u.index];
+            const int64_t n = g.nelem * u.rows;
+            if (n > 0) {
+                k_gather_elements<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(r.upd.as<double>() + o, g.elems.as<int32_t>(), g.nelem,
+                                                                            u.rows, u.count, dst.as<double>() + base);
+                cuda_check_srv(cudaGetLastError(), "k_gather_elements");
+                ctx->launches++;
+            }
+            o += (int64_t)u.values.size();
+            (elem ? ov[u.group].elemdata : ov[u.group].fielddata) = dst.as<double>();
+        }
+    }
+    std::vector<int64_t> gvb;
+    int64_t total_vals = 0;
+    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
+    r.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
+    ctx->x->kev_tag.clear();
+    launch_contractions(ctx, M, r.precision, gvb, r.vals.as<double>(), &ov);
+    r.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
+    r.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
+    launch_row_values(ctx, M, P, segs, false, r.vals.as<double>(), r.Avals.as<double>(), r.Dvals.as<double>());
+    r.vals.release();  // stream-ordered: after the value kernel
+    double* hA = r.pinned_out ? r.Aout : static_cast<double*>(s.pinned);
+    double* hD = r.pinned_out ? r.Dout : static_cast<double*>(s.pinned) + r.nnzA;
+    if (r.nnzA > 0)
+        cuda_check_srv(cudaMemcpyAsync(hA, r.Avals.as<void>(), (size_t)r.nnzA * 8, cudaMemcpyDeviceToHost, st), "D2H Avals");
+    if (r.nnzD > 0 && hD != nullptr)
+        cuda_check_srv(cudaMemcpyAsync(hD, r.Dvals.as<void>(), (size_t)r.nnzD * 8, cudaMemcpyDeviceToHost, st), "D2H Dvals");
+    cuda_check_srv(cudaEventRecord(s.done, st), "cudaEventRecord");
+    ctx->x = &ctx->main;
+}
+
+// Completion of the request on slot s (server thread, context lock held).
+void finish(Server& S, Slot& s)
+{
+    Request& r = *s.req;
+    Ctx* ctx = S.ctx;
+    int status = SLGPU_OK;
+    std::string msg;
+    cudaError_t e = cudaEventQuery(s.done);
+    if (e != cudaSuccess) {
+        status = SLGPU_E_CUDA;
+        msg = std::string("request failed on the device: ") + cudaGetErrorString(e);
+    } else {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s.start, s.done);
+        r.dev_ms = ms;
+        if (r.precision != SLGPU_PREC_FP64 && !s.ex.split_error.empty()) {
+            unsigned int err = 0;
+            if (cudaMemcpy(&err, s.ex.split_error.as<void>(), 4, cudaMemcpyDeviceToHost) == cudaSuccess && err != 0) {
+                status = SLGPU_E_TIMEOUT;
+                msg = "a split-precision contraction tile timed out waiting for its data";
+            }
+        }
+        if (!r.pinned_out) {
+            const double* hp = static_cast<const double*>(s.pinned);
+            if (r.nnzA > 0)
+                std::memcpy(r.Aout, hp, (size_t)r.nnzA * 8);
+            if (r.nnzD > 0 && r.Dout != nullptr)
+                std::memcpy(r.Dout, hp + r.nnzA, (size_t)r.nnzD * 8);
+        }
+    }
+    // Device buffers: freed in the slot stream's order (its work is done).
+    ctx->x = &s.ex;
+    r.Avals.release();
+    r.Dvals.release();
+    r.upd.release();
+    r.ed.clear();
+    r.fd.clear();
+    r.tmpl.reset();
+    ctx->x = &ctx->main;
+    std::lock_guard<std::mutex> lk(S.mu);
+    r.t_done = S.now();
+    r.status = status;
+    r.error = msg;
+    S.running--;
+    s.req.reset();
+    S.done_cv.notify_all();
+}
+
+void server_loop(Server& S)
+{
+    Ctx* ctx = S.ctx;
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        bool progress = false;
+        // Completions.
+        for (Slot& s : S.slots) {
+            if (!s.req)
+                continue;
+            if (cudaEventQuery(s.done) == cudaErrorNotReady)
+                continue;
+            std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+            finish(S, s);
+            progress = true;
+        }
+        // Admissions, in arrival order.
+        for (;;) {
+            Slot* free_slot = nullptr;
+            for (Slot& s : S.slots)
+                if (!s.req) {
+                    free_slot = &s;
+                    break;
+                }
+            std::shared_ptr<Request> r;
+            {
+                std::lock_guard<std::mutex> lk(S.mu);
+                if (free_slot == nullptr || S.queue.empty())
+                    break;
+                r = S.queue.front();
+            }
+            std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+            if (ctx->in_use + r->est_bytes > (int64_t)ctx->budget) {
+                bool busy = false;
+                for (Slot& s : S.slots) busy = busy || (bool)s.req;
+                if (busy)
+                    break;  // wait for memory to free up
+            }
+            {
+                std::lock_guard<std::mutex> lk(S.mu);
+                S.queue.pop_front();
+                r->t_start = S.now();
+                r->status = -2;
+                r->slot = (int)(free_slot - S.slots.data());
+            }
+            free_slot->req = r;
+            int code = SLGPU_OK;
+            std::string msg;
+            try {
+                launch(S, *free_slot, *r);
+            } catch (const SlgpuException& e) {
+                code = e.e.code;
+                msg = e.e.msg;
+            } catch (const std::exception& e) {
+                code = SLGPU_E_ARG;
+                msg = e.what();
+            }
+            if (code != SLGPU_OK) {
+                ctx->x = &ctx->main;
+                cudaStreamSynchronize(free_slot->ex.stream);
+                std::lock_guard<std::mutex> lk(S.mu);
+                r->status = code;
+                r->error = msg;
+                r->t_done = S.now();
+                r->Avals.release();
+                r->Dvals.release();
+                r->vals.release();
+                r->upd.release();
+                r->ed.clear();
+                r->fd.clear();
+                r->tmpl.reset();
+                S.running--;
+                free_slot->req.reset();
+                S.done_cv.notify_all();
+            }
+            progress = true;
+        }
+        std::unique_lock<std::mutex> lk(S.mu);
+        bool busy = false;
+        for (Slot& s : S.slots) busy = busy || (bool)s.req;
+        if (S.stop && S.queue.empty() && !busy)
+            break;
+        if (!progress) {
+            if (busy)
+                S.wake.wait_for(lk, std::chrono::microseconds(20));
+            else
+                S.wake.wait_for(lk, std::chrono::milliseconds(5));
+        }
+    }
+}
+
+}  // namespace
+}  // namespace slgpu
+
+using namespace slgpu;
+
+struct slgpu_server : public slgpu::Server {};
+struct slgpu_ctx : public slgpu::Ctx {};
+
+extern "C" {
+
+int slgpu_server_create(slgpu_ctx* ctx, int nslots, slgpu_server** out)
+{
+    if (ctx == nullptr || out == nullptr || nslots < 1 || nslots > 64)
+        return SLGPU_E_ARG;
+    *out = nullptr;
+    if (ctx->record_only) {
+        ctx->last_error = "no CUDA device: a record-only context cannot serve requests";
+        return SLGPU_E_NODEVICE;
+    }
+    std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+    cudaSetDevice(ctx->device);
+    auto* S = new slgpu_server();
+    S->ctx = ctx;
+    S->slots.resize(nslots);
+    for (Slot& s : S->slots) {
+        if (cudaStreamCreateWithFlags(&s.ex.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&s.start) != cudaSuccess || cudaEventCreate(&s.done) != cudaSuccess) {
+            ctx->last_error = "cannot create the server's streams";
+            slgpu_server_destroy(S);
+            return SLGPU_E_CUDA;
+        }
+        for (auto& e : s.ex.ev) cudaEventCreate(&e);
+    }
+    S->th = std::thread([S] { server_loop(*S); });
+    *out = S;
+    return SLGPU_OK;
+}
+
+int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticket)
+{
+    if (S == nullptr || rq == nullptr || ticket == nullptr)
+        return SLGPU_E_ARG;
+    Ctx* ctx = S->ctx;
+    auto r = std::make_shared<Request>();
+    {
+        std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+        auto it = ctx->matrices.find(rq->handle);
+        if (it == ctx->matrices.end()) {
+            ctx->last_error = "unknown matrix handle " + std::to_string(rq->handle);
+            return SLGPU_E_ARG;
+        }
+        Matrix& M = *it->second;
+        if (!M.pattern) {
+            ctx->last_error = "a template must be processed once before it serves requests";
+            return SLGPU_E_ARG;
+        }
+        if (rq->precision != SLGPU_PREC_FP64 && rq->precision != SLGPU_PREC_SPLIT && rq->precision != SLGPU_PREC_FP32) {
+            ctx->last_error = "unknown precision mode";
+            return SLGPU_E_ARG;
+        }
+        if (rq->Avals == nullptr || (M.pattern->nnzD > 0 && rq->Dvals == nullptr)) {
+            ctx->last_error = "request output buffers missing";
+            return SLGPU_E_ARG;
+        }
+        // The request keeps the template's resident parts alive, not its
+        // value buffers (a shallow copy of the matrix description).
+        auto t = std::make_shared<Matrix>();
+        t->ndofs = M.ndofs;
+        t->groups = M.groups;
+        t->frags = M.frags;
+        t->pattern = M.pattern;
+        r->tmpl = t;
+        for (int i = 0; i < rq->nupdates; i++) {
+            const slgpu_update& u = rq->updates[i];
+            if (u.group < 0 || u.group >= (int)M.groups.size()) {
+                ctx->last_error = "update: group index out of range";
+                return SLGPU_E_ARG;
+            }
+            const GroupDev& g = *M.groups[u.group];
+            const bool elem = u.kind == SLGPU_UPDATE_ELEMDATA;
+            if (!elem && u.kind != SLGPU_UPDATE_FIELDDATA) {
+                ctx->last_error = "update: unknown kind";
+                return SLGPU_E_ARG;
+            }
+            const int narr = elem ? (int)g.elemdata_off.size() : (int)g.field_off.size();
+            if (u.index < 0 || u.index >= narr) {
+                ctx->last_error = "update: array index out of range";
+                return SLGPU_E_ARG;
+            }
+            const int rows = elem ? 1 : g.field_rows[u.index];
+            if (u.rows != rows) {
+                ctx->last_error = "update: row count does not match the array";
+                return SLGPU_E_ARG;
+            }
+            const auto& types = ctx->meshes.at(g.mesh).types;
+            const int64_t mesh_n = types.count(g.elemtype) ? types.at(g.elemtype).nelem : 0;
+            if (u.count != mesh_n || u.values == nullptr) {
+                ctx->last_error = "update: count must be the number of mesh elements of the group's type";
+                return SLGPU_E_ARG;
+            }
+            r->updates.push_back(Request::Update{u.group, u.kind, u.index, rows, u.count,
+                                                 std::vector<double>(u.values, u.values + (size_t)rows * u.count)});
+        }
+        r->handle = rq->handle;
+        r->precision = rq->precision;
+        r->Aout = rq->Avals;
+        r->Dout = rq->Dvals;
+        cudaPointerAttributes pa{}, pd{};
+        const bool pA = cudaPointerGetAttributes(&pa, rq->Avals) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        const bool pD = rq->Dvals == nullptr ||
+                        (cudaPointerGetAttributes(&pd, rq->Dvals) == cudaSuccess && pd.type == cudaMemoryTypeHost);
+        cudaGetLastError();
+        r->pinned_out = pA && pD;
+        r->est_bytes = estimate_bytes(M, rq->precision, *r);
+        if (r->est_bytes > (int64_t)ctx->budget) {
+            ctx->last_error = "a request needs more device memory than the whole HBM budget";
+            return SLGPU_E_BUDGET;
+        }
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->ticket = S->next_ticket++;
+    r->t_submit = S->now();
+    S->reqs[r->ticket] = r;
+    S->queue.push_back(r);
+    S->running++;
+    *ticket = r->ticket;
+    S->wake.notify_one();
+    return SLGPU_OK;
+}
+
+int slgpu_server_wait(slgpu_server* S, int64_t ticket, double timeout_s, slgpu_request_stats* stats)
+{
+    if (S == nullptr)
+        return SLGPU_E_ARG;
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end())
+        return SLGPU_E_ARG;
+    std::shared_ptr<Request> r = it->second;
+    auto done = [&] { return r->status >= 0; };
+    if (timeout_s < 0)
+        S->done_cv.wait(lk, done);
+    else
+        S->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
+    if (stats != nullptr) {
+        stats->submit_s = r->t_submit;
+        stats->start_s = r->t_start;
+        stats->done_s = r->t_done;
+        stats->device_ms = r->dev_ms;
+        stats->slot = r->slot;
+        stats->status = r->status;
+    }
+    if (!done())
+        return SLGPU_E_TIMEOUT;
+    return r->status;
+}
+
+int slgpu_server_error(slgpu_server* S, int64_t ticket, char* buf, size_t len)
+{
+    if (S == nullptr || buf == nullptr || len == 0)
+        return SLGPU_E_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end())
+        return SLGPU_E_ARG;
+    std::snprintf(buf, len, "%s", it->second->error.c_str());
+    return SLGPU_OK;
+}
+
+int slgpu_server_release(slgpu_server* S, int64_t ticket)
+{
+    if (S == nullptr)
+        return SLGPU_E_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end() || it->second->status < 0)
+        return SLGPU_E_ARG;
+    S->reqs.erase(it);
+    return SLGPU_OK;
+}
+
+int64_t slgpu_server_pending(slgpu_server* S)
+{
+    if (S == nullptr)
+        return 0;
+    std::lock_guard<std::mutex> lk(S->mu);
+    return S->running;
+}
+
+void slgpu_server_destroy(slgpu_server* S)
+{
+    if (S == nullptr)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->wake.notify_all();
+    }
+    if (S->th.joinable())
+        S->th.join();
+    Ctx* ctx = S->ctx;
+    std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+    cudaSetDevice(ctx->device);
+    for (Slot& s : S->slots) {
+        if (s.ex.stream != nullptr)
+            cudaStreamSynchronize(s.ex.stream);
+        // Slot buffers go before their stream.
+        s.ex.split_cols.release();
+        s.ex.split_colexp.release();
+        s.ex.split_error.release();
+        if (s.ex.stream != nullptr)
+            cudaStreamSynchronize(s.ex.stream);
+        for (auto& e : s.ex.ev)
+            if (e != nullptr)
+                cudaEventDestroy(e);
+        for (auto& e : s.ex.evpool) cudaEventDestroy(e);
+        for (auto& e : s.ex.kev) cudaEventDestroy(e);
+        if (s.start != nullptr)
+            cudaEventDestroy(s.start);
+        if (s.done != nullptr)
+            cudaEventDestroy(s.done);
+        if (s.pinned != nullptr)
+            cudaFreeHost(s.pinned);
+        if (s.ex.stream != nullptr)
+            cudaStreamDestroy(s.ex.stream);
+    }
+    delete S;
+}
+
+int slgpu_host_alloc(slgpu_ctx* ctx, size_t bytes, void** out)
+{
+    if (ctx == nullptr || out == nullptr)
+        return SLGPU_E_ARG;
+    *out = nullptr;
+    if (ctx->record_only)
+        return SLGPU_E_NODEVICE;
+    cudaSetDevice(ctx->device);
+    if (cudaHostAlloc(out, std::max<size_t>(bytes, 16), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return SLGPU_E_BUDGET;
+    }
+    return SLGPU_OK;
+}
+
+void slgpu_host_free(void* p)
+{
+    if (p != nullptr)
+        cudaFreeHost(p);
+}
+
+}  // extern "C"

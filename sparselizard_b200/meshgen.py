@@ -79,6 +79,30 @@ def quad_mesh(path, n, jitter=0.2, seed=1):
     return {"nelem": quads.shape[0], "nnodes": nodes.shape[0]}
 
 
+def tri_mesh(path, n, jitter=0.2, seed=1):
+    """n x n squares split into 2 triangles each (diagonal (i,j)-(i+1,j+1));
+    VOL = all triangles, BOUNDARY = boundary lines."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nodes = _grid_nodes((n, n), jitter, rng)
+    nid = lambda i, j: i + (n + 1) * j
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    i, j = i.ravel(order="F"), j.ravel(order="F")
+    a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+    tris = np.concatenate([np.stack([a, b, c], axis=1), np.stack([a, c, d], axis=1)])
+    k = np.arange(n)
+    lines = np.concatenate([
+        np.stack([nid(k, 0), nid(k + 1, 0)], axis=1),
+        np.stack([nid(n, k), nid(n, k + 1)], axis=1),
+        np.stack([nid(k + 1, n), nid(k, n)], axis=1),
+        np.stack([nid(0, k + 1), nid(0, k)], axis=1),
+    ])
+    _write(path, nodes, [
+        (2, np.full(tris.shape[0], VOL), tris),
+        (1, np.full(lines.shape[0], BOUNDARY), lines),
+    ])
+    return {"nelem": tris.shape[0], "nnodes": nodes.shape[0]}
+
+
 def _hex_conn(n):
     nid = lambda i, j, k: i + (n + 1) * (j + (n + 1) * k)
     i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")

@@ -1,0 +1,148 @@
+"""Serving loop: requests on resident templates, several in flight at once.
+
+Each request carries new per-element coefficients (mesh element order) for a
+processed template.  The test submits a mix of requests on several
+templates, precisions and sizes to a 4-slot server at once, then runs every
+request again alone -- through a 1-slot server and through the plain
+set_elemdata + process path -- and requires the same values bit for bit
+(the value path has a fixed summation order and no atomics).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import _synthetic as S
+from sparselizard_b200 import abi, serving
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = abi.Context(0)
+    yield c
+    c.close()
+
+
+def _template(ctx, rng, mesh_id, grid, ntf, ndof, nterms, ngp1, ndofs):
+    gb, xyz, conn = S.group(rng, nelem_grid=grid, ntf=ntf, ndof=ndof, nterms=nterms, ngp1=ngp1, norient=2, ndests=2,
+                            ndofs=ndofs)
+    g = gb.g
+    g.mesh = mesh_id
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, mesh_id, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, mesh_id, 3, 4, conn.size // 4, abi.i32p(conn)))
+    h = ctypes.c_int()
+    ctx.check(L.slgpu_matrix_create(ctx.h, ndofs, ctypes.byref(h)))
+    ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g), None))
+    con = (rng.random(ndofs) < 0.1).astype(np.uint8)
+    info = abi.CsrInfo()
+    ctx.check(L.slgpu_matrix_process(ctx.h, h, con.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), abi.PREC_FP64,
+                                     ctypes.byref(info)))
+    elems = np.ctypeslib.as_array(g.elems, (g.nelem,)).copy()
+    return dict(gb=gb, handle=h.value, con=con, nnzA=info.nnzA, nnzD=info.nnzD, elems=elems, nmesh=conn.size // 4,
+                split=ntf * ndof >= 64)
+
+
+def _plain(ctx, t, values_mesh, precision):
+    """The same values through set_elemdata + process (group element order)."""
+    L = ctx.lib
+    vg = np.ascontiguousarray(values_mesh[t["elems"]])
+    ctx.check(L.slgpu_matrix_set_elemdata(ctx.h, t["handle"], 0, 0, abi.f64p(vg)))
+    info = abi.CsrInfo()
+    ctx.check(L.slgpu_matrix_process(ctx.h, t["handle"], t["con"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                     precision, ctypes.byref(info)))
+    A, D = np.zeros(max(1, t["nnzA"])), np.zeros(max(1, t["nnzD"]))
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, t["handle"], abi.f64p(A), abi.f64p(D)))
+    return A[: t["nnzA"]], D[: t["nnzD"]]
+
+
+def test_served_results_same_alone_and_in_the_mix(ctx):
+    rng = np.random.Generator(np.random.PCG64(7))
+    temps = [
+        _template(ctx, rng, 1, 40, 4, 4, 3, 2, 900),      # small, FP64 only
+        _template(ctx, rng, 2, 60, 9, 9, 4, 3, 2000),     # split-eligible
+        _template(ctx, rng, 3, 90, 10, 8, 5, 3, 6000),    # split-eligible, more elements
+    ]
+    reqs = []
+    for k in range(18):
+        t = temps[k % 3]
+        prec = [abi.PREC_FP64, abi.PREC_SPLIT, abi.PREC_FP32][k % 3] if t["split"] else abi.PREC_FP64
+        vals = rng.lognormal(0.0, 0.4, t["nmesh"])
+        reqs.append((t, prec, vals))
+
+    def run(nslots, which):
+        srv = serving.Server(ctx.lib, ctx.h, nslots)
+        outs = {}
+        tickets = {}
+        try:
+            for i in which:
+                t, prec, vals = reqs[i]
+                A = np.full(t["nnzA"], np.nan)
+                D = np.full(max(1, t["nnzD"]), np.nan)[: t["nnzD"]]
+                up = serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vals)
+                tickets[i] = srv.submit(t["handle"], prec, [up], A, D)
+                outs[i] = (A, D)
+                if nslots == 1:
+                    srv.wait(tickets.pop(i))
+            for i, tk in tickets.items():
+                st = srv.wait(tk)
+                assert st.status == abi.OK
+        finally:
+            srv.close()
+        return outs
+
+    mixed = run(4, range(len(reqs)))
+    alone = run(1, range(len(reqs)))
+    for i, (t, prec, vals) in enumerate(reqs):
+        A, D = mixed[i]
+        assert np.all(np.isfinite(A)) and np.all(np.isfinite(D))
+        assert np.array_equal(A, alone[i][0]) and np.array_equal(D, alone[i][1]), f"request {i}: mixed != alone"
+        pA, pD = _plain(ctx, t, vals, prec)
+        assert np.array_equal(A, pA) and np.array_equal(D, pD), f"request {i}: served != process()"
+
+
+def test_server_rejects_bad_requests(ctx):
+    rng = np.random.Generator(np.random.PCG64(8))
+    t = _template(ctx, rng, 4, 20, 4, 4, 2, 2, 300)
+    srv = serving.Server(ctx.lib, ctx.h, 2)
+    try:
+        A, D = np.zeros(t["nnzA"]), np.zeros(max(1, t["nnzD"]))
+        with pytest.raises(abi.SlgpuError):  # wrong element count
+            srv.submit(t["handle"], abi.PREC_FP64, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, np.ones(3))], A, D)
+        with pytest.raises(abi.SlgpuError):  # unknown template
+            srv.submit(9999, abi.PREC_FP64, [], A, D)
+        with pytest.raises(abi.SlgpuError):  # array index out of range
+            srv.submit(t["handle"], abi.PREC_FP64, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 5, np.ones(t["nmesh"]))], A, D)
+        # A valid request still runs after the rejected ones.
+        tk = srv.submit(t["handle"], abi.PREC_FP64, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, np.ones(t["nmesh"]))], A, D)
+        assert srv.wait(tk).status == abi.OK
+    finally:
+        srv.close()
+
+
+def test_pinned_outputs_and_pending_count(ctx):
+    rng = np.random.Generator(np.random.PCG64(9))
+    t = _template(ctx, rng, 5, 50, 9, 9, 3, 3, 1500)
+    srv = serving.Server(ctx.lib, ctx.h, 3)
+    pins = []
+    try:
+        tickets = []
+        for k in range(6):
+            A = serving.PinnedArray(ctx.lib, ctx.h, t["nnzA"])
+            D = serving.PinnedArray(ctx.lib, ctx.h, max(1, t["nnzD"]))
+            pins += [A, D]
+            vals = rng.lognormal(0.0, 0.3, t["nmesh"])
+            tickets.append((srv.submit(t["handle"], abi.PREC_SPLIT, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vals)],
+                                       A.array, D.array[: t["nnzD"]]), A, D, vals))
+        for tk, A, D, vals in tickets:
+            st = srv.wait(tk)
+            assert st.status == abi.OK and st.done_s >= st.start_s >= st.submit_s
+            pA, pD = _plain(ctx, t, vals, abi.PREC_SPLIT)
+            assert np.array_equal(A.array, pA) and np.array_equal(D.array[: t["nnzD"]], pD)
+        assert srv.pending() == 0
+    finally:
+        srv.close()
+        for p in pins:
+            p.close()
