@@ -52,9 +52,23 @@ WORKLOADS = {
                name="elasticity_hex_64^3_h1xyz_order2"),
     "c3": dict(kind=W.HELMHOLTZ_TET, mesh="tet_orders", n=32, params=[], ref_n=8,
                name="helmholtz_tet_32^3x6_orders1to5"),
-    "c4": dict(kind=W.EDDY_TET, mesh="tet_sigma", n=24, params=[2, 1.0e3] + SIGMAS, ref_n=8,
-               name="eddy_hcurl_tet_24^3x6_order2_harmonics23"),
+    "c4": dict(kind=W.EDDY_TET, mesh="tet_sigma", n=24, params=[2, 1.0e3] + SIGMAS, ref_n=8, sweep=64,
+               name="eddy_hcurl_tet_24^3x6_order2_harmonics23_sweep64_1Hz_1MHz"),
+    "c5": dict(kind="serve", name="serving_stream_2000req_poisson200rps_16meshes", requests=2000, rate=200.0),
 }
+
+# Serving pool: (physics 1 Poisson / 2 elasticity, mesh, n, dim, order); 1e3..1e6
+# elements of quads, triangles, hexahedra and tetrahedra, orders 1..4.
+SERVE_POOL = [
+    (1, "quad", 1000, 2, 1), (1, "quad", 300, 2, 2), (1, "quad", 100, 2, 3), (1, "quad", 32, 2, 4),
+    (1, "tri", 700, 2, 1), (1, "tri", 200, 2, 2), (1, "tri", 60, 2, 3), (1, "tri", 25, 2, 4),
+    (1, "hex", 80, 3, 1), (2, "hex", 40, 3, 1), (2, "hex", 16, 3, 2), (1, "hex", 12, 3, 3),
+    (1, "tet", 50, 3, 1), (2, "tet", 20, 3, 1), (1, "tet", 30, 3, 2), (1, "tet", 8, 3, 4),
+]
+
+
+def write_pool_mesh(kind, n, path):
+    {"quad": meshgen.quad_mesh, "tri": meshgen.tri_mesh, "hex": meshgen.hex_mesh, "tet": meshgen.tet_mesh}[kind](path, n)
 
 
 def write_mesh(spec, n, path):
@@ -130,7 +144,14 @@ def peaks():
 # captures of a smaller case of the same workload, per element of the
 # launch's group (traffic grows in proportion to the elements).  Summaries
 # and the commands that made them are under profiles/.
-TRAFFIC_PER_ELEMENT = {}
+TRAFFIC_PER_ELEMENT = {
+    # profiles/k_contract_split_elasticity_hex32.md: 60.29 MB read + 135.83 MB
+    # written by one group launch over 32768 elements.
+    ("c2", "contract_split"): (60.287488e6 + 135.8272e6) / 32768,
+    # profiles/k_row_values_elasticity_hex32.md: 2.487 GB read + 1.182 GB
+    # written by the launch over all 9 groups of 32768 elements.
+    ("c2", "row_values"): (2.487337e9 + 1.182009e9) / 32768,
+}
 
 
 def traffic_per_launch(workload, family, n, launches):
@@ -158,6 +179,9 @@ def kernel_stats(lib, ctx, acc):
 
 
 def dist_setup(n_gpus):
+    """One process per GPU (torchrun sets RANK/WORLD_SIZE/LOCAL_RANK).  The
+    process group only carries the barrier and the max/sum over replicas:
+    NCCL on GPUs, gloo where there is no CUDA device (tests)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -167,20 +191,37 @@ def dist_setup(n_gpus):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return rank, world, local
 
 
 def allreduce(vals, op):
+    """Element-wise reduction of a list of floats over the replicas."""
     import torch
     import torch.distributed as dist
 
     if not dist.is_initialized():
         return vals
-    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=op)
     return t.tolist()
+
+
+def replica_value(total_units_local, seconds_local):
+    """Whole-job throughput of N replicas: units of all ranks / the slowest
+    rank's time (max over ranks), as the timing rules ask."""
+    import torch.distributed as dist
+
+    if dist.is_initialized():
+        secs, = allreduce([seconds_local], dist.ReduceOp.MAX)
+        units, = allreduce([float(total_units_local)], dist.ReduceOp.SUM)
+    else:
+        secs, units = seconds_local, float(total_units_local)
+    return units / secs, secs, units
 
 
 def cpu_reference_run(spec, n, reps, warmup, threads):
@@ -403,6 +444,147 @@ def run_ours(args, spec):
         torch.distributed.destroy_process_group()
 
 
+def run_sweep(args, spec):
+    """C4: the harmonic problem re-assembled at 64 log-spaced frequencies on its
+    resident pattern (scales set per frequency, no generate())."""
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    os.environ["SLGPU_DEVICE"] = str(local)
+    os.environ["SLGPU_PRECISION"] = args.precision
+    prec = {"fp64": abi.PREC_FP64, "split": abi.PREC_SPLIT, "fp32": abi.PREC_FP32}[args.precision]
+    tmpd = tempfile.mkdtemp(prefix=f"slsweep{rank}_")
+    msh = os.path.join(tmpd, "m.msh")
+    n = args.n or spec["n"]
+    write_mesh(spec, n, msh)
+    lib = W.load(GPU_LIB)
+    abi.bind(lib)
+    lib.slz_sweep_prepare.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                      ctypes.c_double, ctypes.POINTER(ctypes.c_longlong)]
+    lib.slz_sweep_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double)]
+    lib.slz_sweep_values.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.slz_sweep_values.restype = ctypes.c_longlong
+    sig = (ctypes.c_double * 4)(*SIGMAS)
+    info = (ctypes.c_longlong * 4)()
+    t0 = time.perf_counter()
+    if lib.slz_sweep_prepare(msh.encode(), 2, sig, 1.0e3, 1.0e5, info) != 0:
+        raise RuntimeError("sweep prepare failed: " + lib.slz_last_error().decode(errors="replace"))
+    prep_s = time.perf_counter() - t0
+    nnz = int(info[2])
+    nf = spec["sweep"]
+    freqs = np.logspace(0.0, 6.0, nf)
+    dev, host = np.zeros(nf), np.zeros(nf)
+    for _ in range(args.warmup):
+        lib.slz_sweep_run(min(nf, 3), abi.f64p(freqs), prec, abi.f64p(dev), abi.f64p(host))
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if lib.slz_sweep_run(nf, abi.f64p(freqs), prec, abi.f64p(dev), abi.f64p(host)) != 0:
+            raise RuntimeError("sweep failed: " + lib.slz_last_error().decode(errors="replace"))
+        torch.cuda.synchronize()
+    dev_s = dev.sum() * 1e-3
+    dev_s_max, = allreduce([dev_s], torch.distributed.ReduceOp.MAX) if world > 1 else [dev_s]
+    total, = allreduce([float(nnz) * nf], torch.distributed.ReduceOp.SUM) if world > 1 else [float(nnz) * nf]
+    # End to end: scale update, process and download of the values per frequency.
+    nnzA = int(lib.slz_sweep_values(None, None))
+    A = np.zeros(max(1, nnzA))
+    D = np.zeros(max(1, nnz - nnzA))
+    d1, h1 = np.zeros(1), np.zeros(1)
+    t0 = time.perf_counter()
+    for f in freqs:
+        lib.slz_sweep_run(1, abi.f64p(np.array([f])), prec, abi.f64p(d1), abi.f64p(h1))
+        lib.slz_sweep_values(abi.f64p(A), abi.f64p(D))
+    e2e_s = time.perf_counter() - t0
+    lib.slz_sweep_release()
+    if rank == 0:
+        line = {
+            "metric": "assembled_nnz_per_s", "value": total / dev_s_max, "unit": "nnz/s", "n_gpus": world, "steps": nf,
+            "warmup": args.warmup, "ms_per_step": dev_s_max * 1e3 / nf, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered tet mesh, random material regions)",
+            "config": {"workload": spec["name"], "n": n, "precision": args.precision, "nnz": nnz, "frequencies": nf,
+                       "prepare_s": prep_s, "parallelism": f"replicas{world}", "l2": "inputs larger than L2"},
+            "e2e": {"value": total / e2e_s, "unit": "nnz/s", "ms_per_step": e2e_s * 1e3 / nf, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * nnz},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_serving(args, spec):
+    """C5: a pool of resident problems and a Poisson stream of requests with new
+    per-element coefficient fields, served by the engine's request server."""
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    os.environ["SLGPU_DEVICE"] = str(local)
+    lib = W.load(GPU_LIB)
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    lib.slz_serve_add.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    lib.slz_serve_run_warm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    tmpd = tempfile.mkdtemp(prefix=f"slserve{rank}_")
+    pool = []
+    t0 = time.perf_counter()
+    for i, (phys, mk, n, dim, order) in enumerate(SERVE_POOL):
+        msh = os.path.join(tmpd, f"p{i}.msh")
+        write_pool_mesh(mk, n, msh)
+        info = (ctypes.c_longlong * 6)()
+        idx = lib.slz_serve_add(phys, msh.encode(), dim, order, info)
+        if idx < 0:
+            raise RuntimeError("serve_add failed: " + lib.slz_last_error().decode(errors="replace"))
+        pool.append(dict(physics=["poisson", "elasticity"][phys - 1], mesh=mk, n=n, order=order, nnz=int(info[1] + info[2]),
+                         elements=int(info[3]), ndofs=int(info[5])))
+        os.remove(msh)
+    setup_s = time.perf_counter() - t0
+    nreq = args.requests or spec["requests"]
+    nwarm = max(args.warmup, 0) * 50  # warm-up requests on the same server before the measured stream
+    rate = spec["rate"]
+    res = {}
+    for name, prec in (("split", abi.PREC_SPLIT), ("fp64", abi.PREC_FP64)):
+        lat = np.zeros(nreq)
+        done = np.zeros(nreq)
+        dev = np.zeros(nreq)
+        prob = np.zeros(nreq, np.int32)
+        summ = np.zeros(9)
+        with ClockSampler(local) as clk:
+            rc = lib.slz_serve_run_warm(nwarm, nreq, rate, args.slots, prec, 12345, min(8, os.cpu_count() or 4), abi.f64p(lat),
+                                        abi.f64p(done), abi.f64p(dev), prob.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        abi.f64p(summ))
+        if rc != 0:
+            raise RuntimeError("serve_run failed: " + lib.slz_last_error().decode(errors="replace"))
+        res[name] = dict(p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                         p90_ms=float(np.percentile(lat, 90) * 1e3), max_ms=float(lat.max() * 1e3), warmup_requests=nwarm,
+                         mean_ms=float(lat.mean() * 1e3), matrices_per_s=nreq / summ[0], nnz_per_s=summ[1] / summ[0],
+                         wall_s=float(summ[0]), device_busy=float(summ[2] * 1e-3 / summ[0]), late_submissions=int(summ[3]),
+                         launch_ms=float(summ[4]), launch_parts_ms=[float(x) for x in summ[6:9]], queue_ms=float(summ[5]),
+                         clocks=clk.summary())
+    lib.slz_serve_release()
+    if rank == 0:
+        mixed, plain = res["split"], res["fp64"]
+        line = {
+            "metric": "assembled_nnz_per_s", "value": mixed["nnz_per_s"], "unit": "nnz/s", "n_gpus": world,
+            "steps": nreq, "warmup": nwarm, "ms_per_step": mixed["mean_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded meshes, lognormal per-element coefficients)",
+            "config": {"workload": spec["name"], "requests": nreq, "rate_per_s": rate, "slots": args.slots,
+                       "pool": pool, "setup_s": setup_s, "parallelism": f"replicas{world}",
+                       "l2": "per-request inputs and outputs cross PCIe; no L2 flush"},
+            "serving": {"mixed_precision": mixed, "fp64": plain},
+            "e2e": {"value": mixed["nnz_per_s"], "unit": "nnz/s", "note": "the served stream is end to end (host inputs to host outputs)",
+                    "h2d_bytes_per_step": int(np.mean([p["elements"] for p in pool]) * 8),
+                    "d2h_bytes_per_step": int(np.mean([p["nnz"] for p in pool]) * 8)},
+            "clocks": mixed["clocks"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,10 +595,19 @@ def main():
     ap.add_argument("--precision", default="split", choices=["fp64", "split", "fp32"])
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (elements per side)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=0, help="serving: number of requests (default 2000)")
+    ap.add_argument("--slots", type=int, default=4, help="serving: concurrent request slots")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
-    if args.impl == "reference":
+    if spec["kind"] == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "serving has no counterpart in the reference"}), flush=True)
+        else:
+            run_serving(args, spec)
+    elif args.impl == "reference":
         run_reference(args, spec)
+    elif spec.get("sweep"):
+        run_sweep(args, spec)
     else:
         run_ours(args, spec)
 

@@ -192,8 +192,20 @@ int slgpu_matrix_add_fragment(slgpu_ctx* ctx, int handle, int32_t ntr, int32_t n
 int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values);
 /* Replaces field coefficient array `k` ([rows][nelem]) of group `gi`. */
 int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values);
+/* Shape of group `gi` of a matrix (what requests may update). */
+typedef struct {
+    int32_t mesh, elemtype, ntf, ndof, nterms, ngp, norient, ndests;
+    int32_t nelemdata, nfielddata;
+    int32_t fieldrows[8]; /* rows of the first 8 fielddata arrays */
+    int64_t nelem;        /* elements of the group */
+    int64_t mesh_nelem;   /* elements of the group's type in its mesh */
+} slgpu_group_desc;
+int slgpu_matrix_group_count(slgpu_ctx* ctx, int handle, int* ngroups);
+int slgpu_matrix_group_desc(slgpu_ctx* ctx, int handle, int gi, slgpu_group_desc* out);
 /* Replaces term scales and destination multipliers of group `gi` (e.g. a new frequency). */
 int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* term_scales, const double* dest_multipliers);
+/* Current term scales (nterms) and destination multipliers (ndests) of group `gi`. */
+int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_scales, double* dest_multipliers);
 /* isconstrained [ndofs] (dofmanager::isconstrained, src/formulation/dofmanager.cpp:366-382). */
 int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstrained, int precision, slgpu_csr_info* info);
 /* Copies the processed CSR blocks to host memory: Arows/Drows [nA+1], Acols/Avals [nnzA], Dcols/Dvals [nnzD]. */
@@ -324,6 +336,8 @@ typedef struct {
     double device_ms; /* event time from the first to the last operation on the slot */
     int32_t slot;
     int32_t status;  /* SLGPU_OK, or the request's error code */
+    double launch_ms; /* host time the server thread spent issuing the request */
+    double launch_parts_ms[3]; /* of which: inputs and gathers, contractions, values and copies */
 } slgpu_request_stats;
 
 int slgpu_server_create(slgpu_ctx* ctx, int nslots, slgpu_server** out);
@@ -338,6 +352,9 @@ int slgpu_server_error(slgpu_server* s, int64_t ticket, char* buf, size_t len);
 int slgpu_server_release(slgpu_server* s, int64_t ticket);
 /* Requests queued or running. */
 int64_t slgpu_server_pending(slgpu_server* s);
+/* The server's clock: seconds since it was created (the time base of
+ * slgpu_request_stats). */
+double slgpu_server_clock(slgpu_server* s);
 /* Waits for every request, stops the server thread and frees its slots. */
 void slgpu_server_destroy(slgpu_server* s);
 /* Page-locked host memory for request outputs (and inputs). */

@@ -71,6 +71,12 @@ class Work(ctypes.Structure):
 UPDATE_ELEMDATA, UPDATE_FIELDDATA = 0, 1
 
 
+class GroupDesc(ctypes.Structure):
+    _fields_ = [("mesh", c_int32), ("elemtype", c_int32), ("ntf", c_int32), ("ndof", c_int32), ("nterms", c_int32),
+                ("ngp", c_int32), ("norient", c_int32), ("ndests", c_int32), ("nelemdata", c_int32),
+                ("nfielddata", c_int32), ("fieldrows", c_int32 * 8), ("nelem", c_int64), ("mesh_nelem", c_int64)]
+
+
 class Update(ctypes.Structure):
     _fields_ = [("group", c_int32), ("kind", c_int32), ("index", c_int32), ("rows", c_int32),
                 ("values", POINTER(c_double)), ("count", c_int64)]
@@ -83,7 +89,7 @@ class Request(ctypes.Structure):
 
 class RequestStats(ctypes.Structure):
     _fields_ = [("submit_s", c_double), ("start_s", c_double), ("done_s", c_double), ("device_ms", c_double),
-                ("slot", c_int32), ("status", c_int32)]
+                ("slot", c_int32), ("status", c_int32), ("launch_ms", c_double), ("launch_parts_ms", c_double * 3)]
 
 
 # Every exported symbol with (restype, argtypes); the tests check that the
@@ -104,6 +110,7 @@ SIGNATURES = {
     "slgpu_matrix_set_elemdata": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double)]),
     "slgpu_matrix_set_fielddata": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double)]),
     "slgpu_matrix_set_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
+    "slgpu_matrix_get_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
     "slgpu_kernel_stats": (c_int, [c_void_p, c_char_p, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]),
     "slgpu_check_coefficient_kernels": (c_int, [c_void_p, c_int, c_char_p, c_size_t]),
@@ -127,12 +134,15 @@ SIGNATURES = {
     "slgpu_record_rhs_group": (c_int, [c_void_p, c_int, POINTER(Group), POINTER(c_int64)]),
     "slgpu_record_mesh": (c_int, [c_void_p, c_int, c_int, POINTER(c_int64), POINTER(POINTER(c_double)), POINTER(c_int),
                                   POINTER(c_int64), POINTER(POINTER(c_int32))]),
+    "slgpu_matrix_group_count": (c_int, [c_void_p, c_int, POINTER(c_int)]),
+    "slgpu_matrix_group_desc": (c_int, [c_void_p, c_int, c_int, POINTER(GroupDesc)]),
     "slgpu_server_create": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     "slgpu_server_submit": (c_int, [c_void_p, POINTER(Request), POINTER(c_int64)]),
     "slgpu_server_wait": (c_int, [c_void_p, c_int64, c_double, POINTER(RequestStats)]),
     "slgpu_server_error": (c_int, [c_void_p, c_int64, c_char_p, c_size_t]),
     "slgpu_server_release": (c_int, [c_void_p, c_int64]),
     "slgpu_server_pending": (c_int64, [c_void_p]),
+    "slgpu_server_clock": (c_double, [c_void_p]),
     "slgpu_server_destroy": (None, [c_void_p]),
     "slgpu_host_alloc": (c_int, [c_void_p, c_size_t, POINTER(c_void_p)]),
     "slgpu_host_free": (None, [c_void_p]),

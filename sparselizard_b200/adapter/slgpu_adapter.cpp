@@ -35,16 +35,17 @@ std::map<rawmat*, std::shared_ptr<MatEntry>> g_mats;
 std::shared_ptr<MatEntry> g_last_entry;
 std::map<rawmat*, std::shared_ptr<MatEntry>> g_processed;
 
-// One engine mesh per sparselizard mesh (rawmesh number), so that matrices
-// assembled on earlier meshes stay valid as templates after another mesh is
-// loaded.  A mesh whose nodes move in place is updated in place.
+// One engine mesh per sparselizard mesh -- the rawmesh object together with
+// its number, which only counts adaptations of one loaded mesh -- so that
+// matrices assembled on earlier meshes stay valid as templates after another
+// mesh is loaded.  A mesh whose nodes move in place is updated in place.
 struct MeshState {
     int id = 0;  // engine mesh id
     long long nnodes = -1;
     unsigned long long coordhash = 0;
     std::map<int, long long> typecounts;  // element type -> uploaded count
 };
-std::map<int, MeshState> g_meshes;  // by rawmesh number
+std::map<std::pair<const void*, int>, MeshState> g_meshes;  // by (rawmesh, number)
 
 struct CtxGuard {
     ~CtxGuard()
@@ -126,11 +127,12 @@ int ensure_mesh(int elemtype)
     unsigned long long h = 1469598103934665603ull;
     const unsigned long long* words = reinterpret_cast<const unsigned long long*>(xyz->data());
     for (size_t i = 0; i < xyz->size(); i++) h = (h ^ words[i]) * 1099511628211ull;
-    auto mit = g_meshes.find(rm->getmeshnumber());
+    const std::pair<const void*, int> key(rm.get(), rm->getmeshnumber());
+    auto mit = g_meshes.find(key);
     if (mit == g_meshes.end()) {
         MeshState st;
         st.id = (int)g_meshes.size();
-        mit = g_meshes.emplace(rm->getmeshnumber(), st).first;
+        mit = g_meshes.emplace(key, st).first;
     }
     MeshState& g_mesh = mit->second;
     if (g_mesh.nnodes != nn || g_mesh.coordhash != h) {

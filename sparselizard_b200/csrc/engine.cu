@@ -293,6 +293,7 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
 {
     validate_group(g);
     auto gd = std::make_shared<GroupDev>();
+    gd->serial = ctx->next_serial++;
     gd->mesh = g.mesh;
     gd->elemtype = g.elemtype;
     gd->elemdim = g.elemdim;
@@ -523,6 +524,42 @@ std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group
     }
     *total_vals = vb;
     return segs;
+}
+
+void stage_reset(Exec& x) { x.stage_used = 0; }
+
+void stage_free(Exec& x)
+{
+    if (x.stage != nullptr)
+        cudaFreeHost(x.stage);
+    for (char* p : x.stage_old) cudaFreeHost(p);
+    x.stage = nullptr;
+    x.stage_old.clear();
+    x.stage_bytes = x.stage_used = 0;
+}
+
+void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes)
+{
+    Exec& x = *ctx->x;
+    buf.alloc(ctx, bytes);
+    if (bytes == 0)
+        return;
+    const size_t need = (bytes + 255) & ~size_t(255);
+    if (x.stage_used + need > x.stage_bytes) {
+        // Grow; the old block may still be read by queued copies of this
+        // call, so it is kept until the state is freed.
+        if (x.stage != nullptr)
+            x.stage_old.push_back(x.stage);
+        x.stage = nullptr;
+        const size_t nb = std::max<size_t>(need, std::max<size_t>(2 * x.stage_bytes, 1 << 16));
+        cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&x.stage), nb, cudaHostAllocDefault), "cudaHostAlloc staging");
+        x.stage_bytes = nb;
+        x.stage_used = 0;
+    }
+    char* p = x.stage + x.stage_used;
+    x.stage_used += need;
+    std::memcpy(p, src, bytes);
+    cuda_check(cudaMemcpyAsync(buf.as<void>(), p, bytes, cudaMemcpyHostToDevice, x.stream), "cudaMemcpyAsync H2D staged");
 }
 
 // Kernel-family timers: kstat_start/kstat_stop bracket launches with an
@@ -1166,7 +1203,18 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
             try {
                 std::vector<const GroupDev*> batch;
                 for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
-                cudaKernel_t kern = jit_coef_kernel(ctx, jit_coef_source(batch));
+                // The kernel of a batch is remembered by its first group (the
+                // source depends only on the batch's groups).
+                std::vector<uint64_t> ids;
+                for (const GroupDev* b : batch) ids.push_back(b->serial);
+                cudaKernel_t kern = nullptr;
+                if (g0.jit_members == ids)
+                    kern = g0.jit_kernel;
+                else {
+                    kern = jit_coef_kernel(ctx, jit_coef_source(batch));
+                    g0.jit_members = ids;
+                    g0.jit_kernel = kern;
+                }
                 std::vector<JitGroup> jg;
                 for (size_t j = k; j < k1; j++) {
                     GroupDev& G = *M.groups[j];
@@ -1176,7 +1224,7 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                                           eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
                 }
                 DevBuf djg;
-                upload(ctx, djg, jg);
+                upload_staged(ctx, djg, jg.data(), jg.size() * sizeof(JitGroup));
                 const MeshDev& m = ctx->meshes.at(g0.mesh);
                 JitGeom geom{m.xyz.as<double>(), m.types.at(g0.elemtype).conn.as<int32_t>(), g0.elems.as<int32_t>(), g0.orient.as<int32_t>(),
                              (long long)g0.nelem, g0.weights.as<double>(), g0.lagrange.as<double>()};
@@ -1326,7 +1374,7 @@ void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::v
         for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
     }
     DevBuf drsegs;
-    upload(ctx, drsegs, rsegs);
+    upload_staged(ctx, drsegs, rsegs.data(), rsegs.size() * sizeof(RowSeg));
     if (P.nA > 0) {
         RowParams rp{};
         rp.inc_ptr = P.inc_ptr.as<uint32_t>();
@@ -1363,6 +1411,7 @@ void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::v
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
 {
     ctx->x->kev_tag.clear();
+    stage_reset(*ctx->x);
     if (ctx->record_only) {
         if (isconstrained != nullptr)
             M.rec_constrained.assign(isconstrained, isconstrained + M.ndofs);
@@ -1566,6 +1615,7 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
         for (auto& e : ctx->x->ev) cudaEventDestroy(e);
         for (auto& e : ctx->x->evpool) cudaEventDestroy(e);
         for (auto& e : ctx->x->kev) cudaEventDestroy(e);
+        stage_free(ctx->main);
         cudaStreamDestroy(ctx->x->stream);
     }
     delete ctx;
@@ -1700,6 +1750,42 @@ int slgpu_matrix_add_fragment(slgpu_ctx* ctx, int handle, int32_t ntr, int32_t n
     });
 }
 
+int slgpu_matrix_group_count(slgpu_ctx* ctx, int handle, int* ngroups)
+{
+    return guarded(ctx, [&] {
+        if (ngroups == nullptr)
+            fail(SLGPU_E_ARG, "null output");
+        *ngroups = (int)get_matrix(ctx, handle).groups.size();
+    });
+}
+
+int slgpu_matrix_group_desc(slgpu_ctx* ctx, int handle, int gi, slgpu_group_desc* out)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (out == nullptr || gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        const GroupDev& g = *M.groups[gi];
+        slgpu_group_desc d{};
+        d.mesh = g.mesh;
+        d.elemtype = g.elemtype;
+        d.ntf = g.ntf;
+        d.ndof = g.ndof;
+        d.nterms = g.nterms;
+        d.ngp = g.ngp;
+        d.norient = g.norient;
+        d.ndests = g.ndests;
+        d.nelemdata = (int)g.elemdata_off.size();
+        d.nfielddata = (int)g.field_off.size();
+        for (int k = 0; k < 8 && k < d.nfielddata; k++) d.fieldrows[k] = g.field_rows[k];
+        d.nelem = g.nelem;
+        auto mit = ctx->meshes.find(g.mesh);
+        if (mit != ctx->meshes.end() && mit->second.types.count(g.elemtype))
+            d.mesh_nelem = mit->second.types.at(g.elemtype).nelem;
+        *out = d;
+    });
+}
+
 int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const double* values)
 {
     return guarded(ctx, [&] {
@@ -1801,6 +1887,20 @@ int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* te
         }
         if (dest_multipliers != nullptr)
             g.dest_mult.assign(dest_multipliers, dest_multipliers + g.ndests);
+    });
+}
+
+int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_scales, double* dest_multipliers)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        const GroupDev& g = *M.groups[gi];
+        if (term_scales != nullptr)
+            std::copy(g.term_scale.begin(), g.term_scale.end(), term_scales);
+        if (dest_multipliers != nullptr)
+            std::copy(g.dest_mult.begin(), g.dest_mult.end(), dest_multipliers);
     });
 }
 

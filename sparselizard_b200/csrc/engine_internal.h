@@ -98,6 +98,11 @@ struct GroupDev {
     std::vector<int> term_node;
     std::vector<double> hconsts;
     uint64_t geom_hash = 0;
+    uint64_t serial = 0;  // unique per group created by the context
+    // Runtime-compiled coefficient kernel of the batch this group leads
+    // (batch members by serial).
+    mutable std::vector<uint64_t> jit_members;
+    mutable cudaKernel_t jit_kernel = nullptr;
 
     DevBuf elems, orient, weights, lagrange, tables, consts, prog_d, elemdata, fielddata, field_off_d, field_rows_d,
         tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
@@ -176,6 +181,12 @@ struct Exec {
     std::map<std::string, KernelStat> kstats;
     DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
     DevBuf split_error;                // device flag set by a timed-out wait
+    // Page-locked staging for the small uploads of one call (kernel argument
+    // arrays), so that they never wait for the stream: reset at the start of
+    // each call on this execution state (the previous call has completed).
+    char* stage = nullptr;
+    size_t stage_bytes = 0, stage_used = 0;
+    std::vector<char*> stage_old;  // outgrown blocks, freed when the state is
 };
 
 struct Ctx {
@@ -199,6 +210,7 @@ struct Ctx {
     DevBuf constr_dev;
     uint64_t constr_key[2] = {0, 0};
     int64_t launches = 0;              // kernels launched by this context
+    uint64_t next_serial = 1;          // group serial numbers
     std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source
     std::vector<cudaLibrary_t> jit_libs;
     bool jit_broken = false;  // a coefficient kernel failed to compile: interpreter from then on
@@ -221,6 +233,11 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
                          const std::vector<GroupData>* ov);
 void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::vector<Segment>& segs, bool rhs, const double* vals,
                        double* Avals, double* Dvals);
+// Copies `bytes` from host memory to a new device buffer through the current
+// execution state's page-locked staging (asynchronous, stream-ordered).
+void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes);
+void stage_reset(Exec& x);
+void stage_free(Exec& x);
 int kstat_start(Ctx* ctx, const char* family, double work);
 void kstat_stop(Ctx* ctx, int i);
 void kstat_collect(Ctx* ctx);

@@ -46,9 +46,12 @@ struct Request {
     struct Update {
         int group, kind, index, rows;
         int64_t count;
-        std::vector<double> values;
+        int64_t offset;  // in doubles, within the request's input block
     };
     std::vector<Update> updates;
+    double* in = nullptr;  // page-locked block with every update's values
+    size_t in_cap = 0;
+    int64_t nin = 0;
     double* Aout = nullptr;
     double* Dout = nullptr;
     bool pinned_out = false;
@@ -58,11 +61,11 @@ struct Request {
     // Device and host resources while running.
     DevBuf vals, Avals, Dvals, upd;
     std::vector<DevBuf> ed, fd;
-    std::vector<double> stageA, stageD;  // pageable outputs: filled from the slot's pinned staging
     int64_t nnzA = 0, nnzD = 0;
     int status = -1;  // -1 queued, -2 running, else the final status
     std::string error;
-    double t_submit = 0, t_start = 0, t_done = 0, dev_ms = 0;
+    double t_submit = 0, t_start = 0, t_done = 0, dev_ms = 0, launch_ms = 0;
+    double parts_ms[3] = {0, 0, 0};
     int slot = -1;
 };
 
@@ -72,6 +75,7 @@ struct Slot {
     std::shared_ptr<Request> req;
     void* pinned = nullptr;  // staging for inputs and pageable outputs
     size_t pinned_bytes = 0;
+    unsigned int* err_host = nullptr;  // page-locked copy of the split-precision error flag
 };
 
 }  // namespace
@@ -89,6 +93,9 @@ struct Server {
     bool stop = false;
     Clock::time_point t0 = Clock::now();
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+    // Page-locked blocks for request inputs, reused by size class (under mu).
+    std::multimap<size_t, void*> pin_free;
+    std::vector<void*> pin_all;
 };
 
 namespace {
@@ -105,9 +112,8 @@ int64_t estimate_bytes(const Matrix& M, int precision, const Request& r)
         split = std::max<int64_t>(split, 7 * Qpad * (int64_t)g->tiles.size() * 64 + (int64_t)g->tiles.size() * 256);
     }
     for (auto& f : M.frags) vals += (int64_t)f->nr * f->nc;
-    int64_t upd = 0, over = 0;
+    int64_t upd = r.nin, over = 0;
     for (auto& u : r.updates) {
-        upd += (int64_t)u.values.size();
         const GroupDev& g = *M.groups[u.group];
         over += (u.kind == SLGPU_UPDATE_ELEMDATA ? (int64_t)g.elemdata.bytes() : (int64_t)g.fielddata.bytes()) / 8;
     }
@@ -136,60 +142,59 @@ void launch(Server& S, Slot& s, Request& r)
     Ctx* ctx = S.ctx;
     const Matrix& M = *r.tmpl;
     const Pattern& P = *M.pattern;
+    const double t0 = S.now();
     ctx->x = &s.ex;
+    stage_reset(s.ex);
     cudaStream_t st = s.ex.stream;
     cuda_check_srv(cudaEventRecord(s.start, st), "cudaEventRecord");
-    // Inputs: all update arrays in one pinned block, one copy to the device,
-    // then per update a copy of the group's resident array with the slice
-    // replaced by the gathered values.
-    int64_t nin = 0;
-    for (auto& u : r.updates) nin += (int64_t)u.values.size();
+    // Inputs: every update's values are in the request's page-locked block
+    // (filled at submit): one copy to the device, then per updated group a
+    // copy of its resident array (unless the update replaces all of it) with
+    // the slice replaced by the gathered values.
     r.nnzA = P.nnzA;
     r.nnzD = P.nnzD;
     const size_t outbytes = r.pinned_out ? 0 : (size_t)(r.nnzA + r.nnzD) * 8;
-    ensure_pinned(s, std::max<size_t>((size_t)nin * 8, outbytes) + 64);
+    if (outbytes > 0)
+        ensure_pinned(s, outbytes + 64);
     std::vector<GroupData> ov(M.groups.size());
     r.ed.clear();
     r.fd.clear();
     r.ed.resize(M.groups.size());
     r.fd.resize(M.groups.size());
-    if (nin > 0) {
-        double* hp = static_cast<double*>(s.pinned);
-        int64_t o = 0;
-        for (auto& u : r.updates) {
-            std::memcpy(hp + o, u.values.data(), u.values.size() * 8);
-            o += (int64_t)u.values.size();
-        }
-        r.upd.alloc(ctx, (size_t)nin * 8);
-        cuda_check_srv(cudaMemcpyAsync(r.upd.as<void>(), hp, (size_t)nin * 8, cudaMemcpyHostToDevice, st), "H2D request inputs");
-        o = 0;
+    if (r.nin > 0) {
+        r.upd.alloc(ctx, (size_t)r.nin * 8);
+        cuda_check_srv(cudaMemcpyAsync(r.upd.as<void>(), r.in, (size_t)r.nin * 8, cudaMemcpyHostToDevice, st), "H2D request inputs");
         for (auto& u : r.updates) {
             GroupDev& g = *M.groups[u.group];
             const bool elem = u.kind == SLGPU_UPDATE_ELEMDATA;
             DevBuf& dst = elem ? r.ed[u.group] : r.fd[u.group];
             const DevBuf& res = elem ? g.elemdata : g.fielddata;
+            const bool whole = elem ? g.elemdata_off.size() == 1 : g.field_off.size() == 1;
             if (dst.empty()) {
                 dst.alloc(ctx, res.bytes());
-                cuda_check_srv(cudaMemcpyAsync(dst.as<void>(), res.as<void>(), res.bytes(), cudaMemcpyDeviceToDevice, st), "D2D group data");
+                if (!whole)
+                    cuda_check_srv(cudaMemcpyAsync(dst.as<void>(), res.as<void>(), res.bytes(), cudaMemcpyDeviceToDevice, st),
+                                   "D2D group data");
             }
             const int64_t base = elem ? g.elemdata_off[u.index] : g.field_off[u.index];
             const int64_t n = g.nelem * u.rows;
             if (n > 0) {
-                k_gather_elements<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(r.upd.as<double>() + o, g.elems.as<int32_t>(), g.nelem,
-                                                                            u.rows, u.count, dst.as<double>() + base);
+                k_gather_elements<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(r.upd.as<double>() + u.offset, g.elems.as<int32_t>(),
+                                                                            g.nelem, u.rows, u.count, dst.as<double>() + base);
                 cuda_check_srv(cudaGetLastError(), "k_gather_elements");
                 ctx->launches++;
             }
-            o += (int64_t)u.values.size();
             (elem ? ov[u.group].elemdata : ov[u.group].fielddata) = dst.as<double>();
         }
     }
+    const double t1 = S.now();
     std::vector<int64_t> gvb;
     int64_t total_vals = 0;
     std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
     r.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
     ctx->x->kev_tag.clear();
     launch_contractions(ctx, M, r.precision, gvb, r.vals.as<double>(), &ov);
+    const double t2 = S.now();
     r.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
     r.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
     launch_row_values(ctx, M, P, segs, false, r.vals.as<double>(), r.Avals.as<double>(), r.Dvals.as<double>());
@@ -200,8 +205,15 @@ void launch(Server& S, Slot& s, Request& r)
         cuda_check_srv(cudaMemcpyAsync(hA, r.Avals.as<void>(), (size_t)r.nnzA * 8, cudaMemcpyDeviceToHost, st), "D2H Avals");
     if (r.nnzD > 0 && hD != nullptr)
         cuda_check_srv(cudaMemcpyAsync(hD, r.Dvals.as<void>(), (size_t)r.nnzD * 8, cudaMemcpyDeviceToHost, st), "D2H Dvals");
+    *s.err_host = 0;
+    if (r.precision != SLGPU_PREC_FP64 && !s.ex.split_error.empty())
+        cuda_check_srv(cudaMemcpyAsync(s.err_host, s.ex.split_error.as<void>(), 4, cudaMemcpyDeviceToHost, st), "D2H split error");
     cuda_check_srv(cudaEventRecord(s.done, st), "cudaEventRecord");
     ctx->x = &ctx->main;
+    const double t3 = S.now();
+    r.parts_ms[0] = (t1 - t0) * 1e3;
+    r.parts_ms[1] = (t2 - t1) * 1e3;
+    r.parts_ms[2] = (t3 - t2) * 1e3;
 }
 
 // Completion of the request on slot s (server thread, context lock held).
@@ -219,12 +231,9 @@ void finish(Server& S, Slot& s)
         float ms = 0;
         cudaEventElapsedTime(&ms, s.start, s.done);
         r.dev_ms = ms;
-        if (r.precision != SLGPU_PREC_FP64 && !s.ex.split_error.empty()) {
-            unsigned int err = 0;
-            if (cudaMemcpy(&err, s.ex.split_error.as<void>(), 4, cudaMemcpyDeviceToHost) == cudaSuccess && err != 0) {
-                status = SLGPU_E_TIMEOUT;
-                msg = "a split-precision contraction tile timed out waiting for its data";
-            }
+        if (*s.err_host != 0) {
+            status = SLGPU_E_TIMEOUT;
+            msg = "a split-precision contraction tile timed out waiting for its data";
         }
         if (!r.pinned_out) {
             const double* hp = static_cast<const double*>(s.pinned);
@@ -244,6 +253,10 @@ void finish(Server& S, Slot& s)
     r.tmpl.reset();
     ctx->x = &ctx->main;
     std::lock_guard<std::mutex> lk(S.mu);
+    if (r.in != nullptr) {
+        S.pin_free.emplace(r.in_cap, r.in);
+        r.in = nullptr;
+    }
     r.t_done = S.now();
     r.status = status;
     r.error = msg;
@@ -301,7 +314,9 @@ void server_loop(Server& S)
             int code = SLGPU_OK;
             std::string msg;
             try {
+                const double tl = S.now();
                 launch(S, *free_slot, *r);
+                r->launch_ms = (S.now() - tl) * 1e3;
             } catch (const SlgpuException& e) {
                 code = e.e.code;
                 msg = e.e.msg;
@@ -315,6 +330,10 @@ void server_loop(Server& S)
                 std::lock_guard<std::mutex> lk(S.mu);
                 r->status = code;
                 r->error = msg;
+                if (r->in != nullptr) {
+                    S.pin_free.emplace(r->in_cap, r->in);
+                    r->in = nullptr;
+                }
                 r->t_done = S.now();
                 r->Avals.release();
                 r->Dvals.release();
@@ -375,6 +394,12 @@ int slgpu_server_create(slgpu_ctx* ctx, int nslots, slgpu_server** out)
             return SLGPU_E_CUDA;
         }
         for (auto& e : s.ex.ev) cudaEventCreate(&e);
+        if (cudaHostAlloc(reinterpret_cast<void**>(&s.err_host), 16, cudaHostAllocDefault) != cudaSuccess) {
+            ctx->last_error = "cannot allocate page-locked memory";
+            slgpu_server_destroy(S);
+            return SLGPU_E_CUDA;
+        }
+        *s.err_host = 0;
     }
     S->th = std::thread([S] { server_loop(*S); });
     *out = S;
@@ -415,6 +440,7 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
         t->frags = M.frags;
         t->pattern = M.pattern;
         r->tmpl = t;
+        std::map<std::pair<const double*, int64_t>, int64_t> seen;  // identical arrays are sent once
         for (int i = 0; i < rq->nupdates; i++) {
             const slgpu_update& u = rq->updates[i];
             if (u.group < 0 || u.group >= (int)M.groups.size()) {
@@ -443,8 +469,15 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
                 ctx->last_error = "update: count must be the number of mesh elements of the group's type";
                 return SLGPU_E_ARG;
             }
-            r->updates.push_back(Request::Update{u.group, u.kind, u.index, rows, u.count,
-                                                 std::vector<double>(u.values, u.values + (size_t)rows * u.count)});
+            const int64_t n = (int64_t)rows * u.count;
+            auto it = seen.find({u.values, n});
+            int64_t off = r->nin;
+            if (it == seen.end()) {
+                seen[{u.values, n}] = off;
+                r->nin += n;
+            } else
+                off = it->second;
+            r->updates.push_back(Request::Update{u.group, u.kind, u.index, rows, u.count, off});
         }
         r->handle = rq->handle;
         r->precision = rq->precision;
@@ -460,6 +493,43 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
         if (r->est_bytes > (int64_t)ctx->budget) {
             ctx->last_error = "a request needs more device memory than the whole HBM budget";
             return SLGPU_E_BUDGET;
+        }
+    }
+    // Inputs into a page-locked block (outside the context lock).
+    if (r->nin > 0) {
+        const size_t need = (size_t)r->nin * 8;
+        size_t cap = size_t(1) << 16;
+        while (cap < need) cap <<= 1;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            auto it = S->pin_free.lower_bound(cap);
+            if (it != S->pin_free.end() && it->first == cap) {
+                r->in = static_cast<double*>(it->second);
+                S->pin_free.erase(it);
+            }
+        }
+        if (r->in == nullptr) {
+            void* p = nullptr;
+            if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                ctx->last_error = "cannot allocate page-locked memory for the request inputs";
+                return SLGPU_E_BUDGET;
+            }
+            r->in = static_cast<double*>(p);
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->pin_all.push_back(p);
+        }
+        r->in_cap = cap;
+        std::map<int64_t, const double*> src;
+        for (int i = 0; i < rq->nupdates; i++) src[r->updates[i].offset] = rq->updates[i].values;
+        for (auto& kv : src) {
+            const Request::Update* u = nullptr;
+            for (auto& x : r->updates)
+                if (x.offset == kv.first) {
+                    u = &x;
+                    break;
+                }
+            std::memcpy(r->in + kv.first, kv.second, (size_t)u->rows * u->count * 8);
         }
     }
     std::lock_guard<std::mutex> lk(S->mu);
@@ -494,6 +564,8 @@ int slgpu_server_wait(slgpu_server* S, int64_t ticket, double timeout_s, slgpu_r
         stats->device_ms = r->dev_ms;
         stats->slot = r->slot;
         stats->status = r->status;
+        stats->launch_ms = r->launch_ms;
+        for (int i = 0; i < 3; i++) stats->launch_parts_ms[i] = r->parts_ms[i];
     }
     if (!done())
         return SLGPU_E_TIMEOUT;
@@ -532,6 +604,8 @@ int64_t slgpu_server_pending(slgpu_server* S)
     return S->running;
 }
 
+double slgpu_server_clock(slgpu_server* S) { return S == nullptr ? 0.0 : S->now(); }
+
 void slgpu_server_destroy(slgpu_server* S)
 {
     if (S == nullptr)
@@ -566,9 +640,13 @@ void slgpu_server_destroy(slgpu_server* S)
             cudaEventDestroy(s.done);
         if (s.pinned != nullptr)
             cudaFreeHost(s.pinned);
+        if (s.err_host != nullptr)
+            cudaFreeHost(s.err_host);
+        stage_free(s.ex);
         if (s.ex.stream != nullptr)
             cudaStreamDestroy(s.ex.stream);
     }
+    for (void* p : S->pin_all) cudaFreeHost(p);
     delete S;
 }
 

@@ -59,6 +59,13 @@ struct Normal {
         double u1 = uniform(), u2 = uniform();
         return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
     }
+    // Both normals of one Box-Muller step.
+    void draw2(double& a, double& b)
+    {
+        const double r = std::sqrt(-2.0 * std::log(uniform())), t = 6.283185307179586 * uniform();
+        a = r * std::cos(t);
+        b = r * std::sin(t);
+    }
 };
 
 void capture(mat& A, vec& b)
@@ -332,5 +339,442 @@ long long slz_bench_nodes(const double** xyz)
 }
 
 void slz_bench_release(void) { g_bench.reset(); }
+}
+
+// ---------------------------------------------------------------- serving
+// A pool of resident problems (each assembled once through generate()/A(),
+// which leaves its mesh, tables, addresses and pattern on the device) and a
+// stream of requests that re-assemble them with new per-element coefficient
+// fields through the engine's request server.
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+
+namespace {
+struct ServeProblem {
+    std::unique_ptr<Problem> P;
+    mat A;
+    int handle = 0;
+    long long nnzA = 0, nnzD = 0, nmesh = 0, ndofs = 0;
+    double median = 1.0;
+    std::vector<int> groups;  // groups whose fielddata array 0 is the coefficient field
+};
+std::vector<std::unique_ptr<ServeProblem>> g_serve;
+
+// exp(0.3 z) at the 65536 quantiles z_i = Phi^-1((i + 0.5) / 65536) of the
+// standard normal: a request's per-element lognormal field (sigma 0.3) is one
+// uniform 16-bit draw per element into this table (Phi^-1 by bisection on
+// erfc, exact to double rounding).
+const std::vector<double>& lognormal_table(void)
+{
+    static const std::vector<double> T = [] {
+        std::vector<double> t(65536);
+        for (int i = 0; i < 65536; i++) {
+            const double p = (i + 0.5) / 65536.0;
+            double lo = -10, hi = 10;
+            for (int it = 0; it < 80; it++) {
+                const double mid = 0.5 * (lo + hi);
+                (0.5 * std::erfc(-mid / std::sqrt(2.0)) < p ? lo : hi) = mid;
+            }
+            t[i] = std::exp(0.3 * 0.5 * (lo + hi));
+        }
+        return t;
+    }();
+    return T;
+}
+}  // namespace
+
+extern "C" {
+
+// kind 1: Poisson, integral(VOL, -k*grad(dof(v))*grad(tf(v))), v = 0 on
+// BOUNDARY (2D) or CLAMP (3D); kind 2: elasticity,
+// integral(VOL, predefinedelasticity(dof(u), tf(u), E, 0.3)) (plane strain in
+// 2D), u = 0 on the same region.  k / E is a "one" field with one value per
+// element.  info6: handle, nnzA, nnzD, mesh elements, groups, ndofs.
+int slz_serve_add(int kind, const char* msh, int dim, int order, long long* info6)
+{
+    g_error.clear();
+    try {
+        auto S = std::make_unique<ServeProblem>();
+        S->P = std::make_unique<Problem>();
+        Problem& P = *S->P;
+        P.m = mesh(msh, 0);
+        field c("one");
+        const int fixreg = dim == 2 ? BOUNDARY : CLAMP;
+        S->median = kind == 1 ? 1.0 : 150e9;
+        set_per_element(c, VOL, {S->median});
+        if (kind == 1) {
+            field v("h1");
+            v.setorder(VOL, order);
+            v.setconstraint(fixreg);
+            P.f += integral(VOL, -c * grad(dof(v)) * grad(tf(v)));
+            P.fields = {v, c};
+        } else {
+            field u(dim == 2 ? "h1xy" : "h1xyz");
+            u.setorder(VOL, order);
+            u.setconstraint(fixreg);
+            P.f += integral(VOL, predefinedelasticity(dof(u), tf(u), c, 0.3, dim == 2 ? "planestrain" : ""));
+            P.fields = {u, c};
+        }
+        P.f.generate();
+        S->A = P.f.A();
+        std::shared_ptr<rawmat> raw = S->A.getpointer();
+        S->handle = slgpu_adapter::find_matrix_handle(raw.get());
+        S->ndofs = raw->countrows();
+        slgpu_ctx* ctx = slgpu_adapter_ctx();
+        int ng = 0;
+        if (slgpu_matrix_group_count(ctx, S->handle, &ng) != SLGPU_OK)
+            throw std::runtime_error("template has no engine matrix");
+        for (int gi = 0; gi < ng; gi++) {
+            slgpu_group_desc d;
+            slgpu_matrix_group_desc(ctx, S->handle, gi, &d);
+            if (d.nfielddata != 1 || d.fieldrows[0] != 1)
+                throw std::runtime_error("a served group must hold exactly the per-element coefficient field");
+            if (S->nmesh != 0 && S->nmesh != d.mesh_nelem)
+                throw std::runtime_error("groups of one template on different element types");
+            S->nmesh = d.mesh_nelem;
+            S->groups.push_back(gi);
+        }
+        // nnzA and nnzD of the resident pattern (the engine's last process).
+        slgpu_work w;
+        if (slgpu_matrix_work(ctx, S->handle, &w) != SLGPU_OK)
+            throw std::runtime_error("slgpu_matrix_work failed");
+        S->nnzA = raw->countnnz();
+        S->nnzD = w.nnz - S->nnzA;
+        info6[0] = S->handle;
+        info6[1] = S->nnzA;
+        info6[2] = S->nnzD;
+        info6[3] = S->nmesh;
+        info6[4] = (long long)S->groups.size();
+        info6[5] = S->ndofs;
+        g_serve.push_back(std::move(S));
+        return (int)g_serve.size() - 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -2;
+    }
+}
+
+// Runs `nreq` requests arriving as a Poisson process of `rate` per second
+// (seeded), each on a problem drawn uniformly from the pool with a new
+// lognormal coefficient field (median of the problem, sigma 0.3, one seeded
+// draw per element from 65536 quantile levels), through a
+// server with `nslots` slots.  ngen threads prepare the coefficient fields
+// ahead of their arrival times.  Per request: latency (scheduled arrival to
+// results in host memory), completion time and device time (seconds, ms);
+// summary: [0] wall seconds from the first arrival to the last completion,
+// [1] sum of nnz, [2] sum of device ms, [3] requests whose submission was late
+// by more than 1 ms, [4] mean host ms the server spent issuing a request,
+// [5] mean ms a request waited in the queue, [6..8] mean host ms of the
+// launch parts (inputs, contractions, values and copies).
+int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency_out,
+                       double* done_out, double* device_out, int* problem_out, double* summary);
+
+int slz_serve_run(int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency, double* done_s,
+                  double* device_ms, int* problem, double* summary)
+{
+    return slz_serve_run_warm(0, nreq, rate, nslots, precision, seed, ngen, latency, done_s, device_ms, problem, summary);
+}
+
+// As slz_serve_run, with `nwarm` requests of the same stream before the
+// measured ones (same server, so page-locked pools and split-precision
+// tables are warm); the outputs and summary cover the last `nreq` requests.
+int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency_out,
+                       double* done_out, double* device_out, int* problem_out, double* summary)
+{
+    const int ntot = nwarm + nreq;
+    std::vector<double> latency(ntot), done_s(ntot), device_ms(ntot);
+    std::vector<int> problem(ntot);
+    g_error.clear();
+    const int np = (int)g_serve.size();
+    if (np == 0 || ntot <= 0) {
+        g_error = "no served problems";
+        return -1;
+    }
+    slgpu_ctx* ctx = slgpu_adapter_ctx();
+    slgpu_server* srv = nullptr;
+    if (slgpu_server_create(ctx, nslots, &srv) != SLGPU_OK) {
+        g_error = "slgpu_server_create failed";
+        return -1;
+    }
+    // Schedule.
+    Normal rs(seed);
+    std::vector<double> arrival(ntot);
+    double t = 0.05;
+    for (int k = 0; k < ntot; k++) {
+        t += -std::log(rs.uniform()) / rate;
+        arrival[k] = t;
+        problem[k] = (int)(rs.next() % (uint64_t)np);
+    }
+    // Output buffers: a few page-locked pairs per problem.
+    const int B = 4;
+    std::vector<std::vector<std::pair<double*, double*>>> free_out(np);
+    std::vector<void*> pinned;
+    for (int p = 0; p < np; p++)
+        for (int b = 0; b < B; b++) {
+            void *a = nullptr, *d = nullptr;
+            slgpu_host_alloc(ctx, (size_t)std::max(1LL, g_serve[p]->nnzA) * 8, &a);
+            slgpu_host_alloc(ctx, (size_t)std::max(1LL, g_serve[p]->nnzD) * 8, &d);
+            pinned.push_back(a);
+            pinned.push_back(d);
+            free_out[p].push_back({(double*)a, (double*)d});
+        }
+    lognormal_table();
+    // Time origin of the arrivals: after the set-up above.
+    const auto t_create = std::chrono::steady_clock::now();
+    const double offset = slgpu_server_clock(srv);  // server time at t_create
+    std::mutex mu;
+    std::condition_variable cv;
+    // Prepared inputs (lookahead window of L requests).
+    const int L = 64;
+    std::vector<std::vector<double>> inputs(L);
+    std::vector<int> ready(ntot, 0);
+    std::atomic<int> consumed{0};
+    std::vector<std::thread> gens;
+    for (int gth = 0; gth < ngen; gth++)
+        gens.emplace_back([&, gth] {
+            for (int k = gth; k < ntot; k += ngen) {
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    cv.wait(lk, [&] { return k < consumed.load() + L; });
+                }
+                const ServeProblem& S = *g_serve[problem[k]];
+                std::vector<double> v((size_t)S.nmesh);
+                Normal r(seed * 1000003ull + (uint64_t)k * 7919ull + 17);
+                const double* T = lognormal_table().data();
+                for (double& x : v) x = S.median * T[r.next() >> 48];
+                std::lock_guard<std::mutex> lk(mu);
+                inputs[k % L] = std::move(v);
+                ready[k] = 1;
+                cv.notify_all();
+            }
+        });
+    std::vector<int64_t> tickets(ntot, 0);
+    std::vector<std::pair<double*, double*>> outs(ntot);
+    std::vector<int> submitted(ntot, 0);
+    double late = 0, late_measured = 0, launch_ms_sum = 0, queue_s_sum = 0, parts_sum[3] = {0, 0, 0};
+    // Waiter: completions in submission order; frees output buffers.
+    std::thread waiter([&] {
+        for (int k = 0; k < ntot; k++) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return submitted[k] != 0; });
+            }
+            slgpu_request_stats st{};
+            int rc = slgpu_server_wait(srv, tickets[k], -1.0, &st);
+            latency[k] = rc == SLGPU_OK ? st.done_s - (arrival[k] + offset) : -1.0;
+            done_s[k] = st.done_s;
+            device_ms[k] = st.device_ms;
+            launch_ms_sum += st.launch_ms;
+            for (int i = 0; i < 3; i++) parts_sum[i] += st.launch_parts_ms[i];
+            queue_s_sum += st.start_s - st.submit_s;
+            slgpu_server_release(srv, tickets[k]);
+            std::lock_guard<std::mutex> lk(mu);
+            free_out[problem[k]].push_back(outs[k]);
+            cv.notify_all();
+        }
+    });
+    // Submitter: on the server clock (t_create ~ the server's start).
+    for (int k = 0; k < ntot; k++) {
+        const ServeProblem& S = *g_serve[problem[k]];
+        std::vector<double> v;
+        std::pair<double*, double*> o;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return ready[k] != 0 && !free_out[problem[k]].empty(); });
+            v = std::move(inputs[k % L]);
+            o = free_out[problem[k]].back();
+            free_out[problem[k]].pop_back();
+        }
+        std::this_thread::sleep_until(t_create + std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                                                     std::chrono::duration<double>(arrival[k])));
+        const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_create).count();
+        if (now > arrival[k] + 1e-3) {
+            late += 1;
+            if (k >= nwarm)
+                late_measured += 1;
+        }
+        std::vector<slgpu_update> ups;
+        for (int gi : S.groups) ups.push_back(slgpu_update{gi, SLGPU_UPDATE_FIELDDATA, 0, 1, v.data(), S.nmesh});
+        slgpu_request rq{S.handle, precision, (int32_t)ups.size(), 0, ups.data(), o.first, o.second};
+        int64_t tk = 0;
+        if (slgpu_server_submit(srv, &rq, &tk) != SLGPU_OK) {
+            char buf[512];
+            slgpu_last_error(ctx, buf, sizeof(buf));
+            g_error = buf;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        tickets[k] = tk;
+        outs[k] = o;
+        submitted[k] = 1;
+        consumed.store(k + 1);
+        cv.notify_all();
+    }
+    waiter.join();
+    for (auto& g : gens) g.join();
+    double last = 0, nnz = 0, dev = 0;
+    for (int k = nwarm; k < ntot; k++) {
+        last = std::max(last, done_s[k]);
+        nnz += (double)(g_serve[problem[k]]->nnzA + g_serve[problem[k]]->nnzD);
+        dev += device_ms[k];
+        latency_out[k - nwarm] = latency[k];
+        done_out[k - nwarm] = done_s[k];
+        device_out[k - nwarm] = device_ms[k];
+        problem_out[k - nwarm] = problem[k];
+    }
+    summary[0] = last - (arrival[nwarm] + offset);
+    summary[1] = nnz;
+    summary[2] = dev;
+    summary[3] = late_measured;
+    summary[4] = launch_ms_sum / ntot;
+    summary[5] = queue_s_sum / ntot * 1e3;
+    for (int i = 0; i < 3; i++) summary[6 + i] = parts_sum[i] / ntot;
+    slgpu_server_destroy(srv);
+    for (void* p : pinned) slgpu_host_free(p);
+    return g_error.empty() ? 0 : -1;
+}
+
+void slz_serve_release(void) { g_serve.clear(); }
+}
+
+// ---------------------------------------------------------------- frequency sweep
+// The harmonic eddy-current problem assembled at two fundamental frequencies
+// through generate()/A(); every term scale and destination multiplier of its
+// resident groups is then known as a + b*omega (the harmonic derivation
+// factor of dt(), src/harmonic.cpp:110-135, is linear in omega), so a sweep
+// sets the scales for each frequency and re-processes on the resident
+// pattern instead of re-running generate().
+namespace {
+struct SweepState {
+    std::unique_ptr<Problem> P;
+    mat A1, A2;
+    int handle = 0;
+    std::vector<unsigned char> constrained;
+    std::vector<std::vector<double>> ta, tb, da, db;  // per group: a and b of term scales and multipliers
+    long long nnzA = 0, nnz = 0;
+};
+std::unique_ptr<SweepState> g_sweep;
+
+void read_scales(int handle, std::vector<std::vector<double>>& t, std::vector<std::vector<double>>& d)
+{
+    slgpu_ctx* ctx = slgpu_adapter_ctx();
+    int ng = 0;
+    slgpu_matrix_group_count(ctx, handle, &ng);
+    t.assign(ng, {});
+    d.assign(ng, {});
+    for (int gi = 0; gi < ng; gi++) {
+        slgpu_group_desc g;
+        slgpu_matrix_group_desc(ctx, handle, gi, &g);
+        t[gi].resize(g.nterms);
+        d[gi].resize(g.ndests);
+        slgpu_matrix_get_scales(ctx, handle, gi, t[gi].data(), d[gi].data());
+    }
+}
+}  // namespace
+
+extern "C" {
+
+// info4: template handle, ndofs, nnz, groups.
+int slz_sweep_prepare(const char* msh, int order, const double* sigmas, double f1, double f2, long long* info4)
+{
+    g_error.clear();
+    try {
+        g_sweep.reset();
+        auto W = std::make_unique<SweepState>();
+        W->P = std::make_unique<Problem>();
+        eddy_tet(*W->P, msh, order, sigmas, f1);
+        W->P->f.generate();
+        W->A1 = W->P->f.A();
+        const int h1 = slgpu_adapter::find_matrix_handle(W->A1.getpointer().get());
+        std::vector<std::vector<double>> t1, d1, t2, d2;
+        read_scales(h1, t1, d1);
+        setfundamentalfrequency(f2);
+        W->P->f.generate();
+        W->A2 = W->P->f.A();
+        std::shared_ptr<rawmat> raw = W->A2.getpointer();
+        W->handle = slgpu_adapter::find_matrix_handle(raw.get());
+        read_scales(W->handle, t2, d2);
+        if (t1.size() != t2.size())
+            throw std::runtime_error("the two assemblies have different groups");
+        const double w1 = 2 * 3.141592653589793 * f1, w2 = 2 * 3.141592653589793 * f2;
+        auto fit = [&](const std::vector<std::vector<double>>& s1, const std::vector<std::vector<double>>& s2,
+                       std::vector<std::vector<double>>& a, std::vector<std::vector<double>>& b) {
+            a = s1;
+            b = s1;
+            for (size_t g = 0; g < s1.size(); g++) {
+                if (s1[g].size() != s2[g].size())
+                    throw std::runtime_error("the two assemblies have different terms");
+                for (size_t k = 0; k < s1[g].size(); k++) {
+                    b[g][k] = (s2[g][k] - s1[g][k]) / (w2 - w1);
+                    a[g][k] = s1[g][k] - b[g][k] * w1;
+                }
+            }
+        };
+        fit(t1, t2, W->ta, W->tb);
+        fit(d1, d2, W->da, W->db);
+        std::vector<bool> c = raw->getdofmanager()->isconstrained();
+        W->constrained.assign(c.begin(), c.end());
+        slgpu_work w;
+        slgpu_matrix_work(slgpu_adapter_ctx(), W->handle, &w);
+        W->nnzA = raw->countnnz();
+        W->nnz = w.nnz;
+        info4[0] = W->handle;
+        info4[1] = raw->countrows();
+        info4[2] = W->nnz;
+        info4[3] = (long long)t1.size();
+        g_sweep = std::move(W);
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+    return 0;
+}
+
+// Re-assembles the template at each frequency; device_ms: engine device time
+// of the process, host_ms: wall time of the scale update and the process.
+int slz_sweep_run(int nfreq, const double* freqs, int precision, double* device_ms, double* host_ms)
+{
+    if (!g_sweep)
+        return 1;
+    SweepState& W = *g_sweep;
+    slgpu_ctx* ctx = slgpu_adapter_ctx();
+    for (int i = 0; i < nfreq; i++) {
+        const double t0 = now_s();
+        const double w = 2 * 3.141592653589793 * freqs[i];
+        for (size_t g = 0; g < W.ta.size(); g++) {
+            std::vector<double> ts(W.ta[g].size()), ds(W.da[g].size());
+            for (size_t k = 0; k < ts.size(); k++) ts[k] = W.ta[g][k] + W.tb[g][k] * w;
+            for (size_t k = 0; k < ds.size(); k++) ds[k] = W.da[g][k] + W.db[g][k] * w;
+            if (slgpu_matrix_set_scales(ctx, W.handle, (int)g, ts.data(), ds.data()) != SLGPU_OK)
+                return 2;
+        }
+        slgpu_csr_info info;
+        if (slgpu_matrix_process(ctx, W.handle, W.constrained.data(), precision, &info) != SLGPU_OK) {
+            char buf[512];
+            slgpu_last_error(ctx, buf, sizeof(buf));
+            g_error = buf;
+            return 3;
+        }
+        double ms[5];
+        slgpu_last_timings(ctx, ms);
+        device_ms[i] = ms[4];
+        host_ms[i] = (now_s() - t0) * 1e3;
+    }
+    return 0;
+}
+
+// A and D values of the template after the last sweep step (nnzA + nnzD).
+long long slz_sweep_values(double* Avals, double* Dvals)
+{
+    if (!g_sweep)
+        return -1;
+    if (Avals != nullptr)
+        slgpu_matrix_download_values(slgpu_adapter_ctx(), g_sweep->handle, Avals, Dvals);
+    return g_sweep->nnzA;
+}
+
+void slz_sweep_release(void) { g_sweep.reset(); }
 }
 #endif

@@ -47,9 +47,50 @@ def _child_main(mode, workload, msh, params, out, reps):
     elif mode == "record":
         np.savez(out, **record_oracle_inproc(workload, msh, params))
         return
+    elif mode.startswith("sweep"):
+        np.savez(out, **sweep_inproc(msh, params, mode.split(":")[1]))
+        return
     else:
         raise ValueError(mode)
     np.savez(out, ndofs=np.array(r.ndofs), times=r.times, **{k: getattr(r, k) for k in KEYS})
+
+
+def sweep_inproc(msh, params, precision):
+    """Frequency sweep through the drop-in: template assembled at params[1]
+    and params[2] (Hz), then re-assembled at each frequency of params[3:] by
+    setting fitted scales; returns the A/D values at the last frequency."""
+    from sparselizard_b200 import abi, workloads as W
+
+    os.environ["SLGPU_PRECISION"] = precision
+    lib = W.load(GPU_LIB)
+    abi.bind(lib)
+    lib.slz_sweep_prepare.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                      ctypes.c_double, ctypes.POINTER(ctypes.c_longlong)]
+    lib.slz_sweep_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double)]
+    lib.slz_sweep_values.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.slz_sweep_values.restype = ctypes.c_longlong
+    order, f1, f2, sig = int(params[0]), params[1], params[2], params[3:7]
+    freqs = np.array(params[7:], dtype=np.float64)
+    sigmas = (ctypes.c_double * 4)(*sig)
+    info = (ctypes.c_longlong * 4)()
+    if lib.slz_sweep_prepare(msh.encode(), order, sigmas, f1, f2, info) != 0:
+        raise RuntimeError(lib.slz_last_error().decode(errors="replace"))
+    dev, host = np.zeros(freqs.size), np.zeros(freqs.size)
+    prec = {"fp64": abi.PREC_FP64, "split": abi.PREC_SPLIT, "fp32": abi.PREC_FP32}[precision]
+    rc = lib.slz_sweep_run(freqs.size, abi.f64p(freqs), prec, abi.f64p(dev), abi.f64p(host))
+    if rc != 0:
+        raise RuntimeError("sweep failed: " + lib.slz_last_error().decode(errors="replace"))
+    nnz = int(info[2])
+    nnzA = int(lib.slz_sweep_values(None, None))
+    A, D = np.zeros(max(1, nnzA)), np.zeros(max(1, nnz - nnzA))
+    lib.slz_sweep_values(abi.f64p(A), abi.f64p(D))
+    return dict(Avals=A[:nnzA], Dvals=D[: nnz - nnzA], device_ms=dev, host_ms=host)
+
+
+def sweep(msh, order, f1, f2, sigmas, freqs, precision="fp64"):
+    with tempfile.TemporaryDirectory() as d:
+        return _child("sweep:" + precision, 0, msh, [order, f1, f2] + list(sigmas) + list(freqs), os.path.join(d, "o.npz"))
 
 
 def reference(workload, msh, params, reps=1):

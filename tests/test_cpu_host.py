@@ -14,7 +14,7 @@ HEADER = os.path.join(P.ROOT, "include", "slgpu.h")
 
 def declared_symbols():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|int64_t)\s+\**(slgpu_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|int64_t|double)\s+\**(slgpu_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
