@@ -67,6 +67,25 @@ SERVE_POOL = [
 ]
 
 
+def serving_per_problem(pool, prob, lat, dev, detail):
+    """Per pool problem: requests, latency p50/p99, mean device time, mean
+    server-thread launch time (and its input / contraction / value parts),
+    mean queueing and submission delay (ms)."""
+    out = []
+    for i, p in enumerate(pool):
+        m = prob == i
+        if not m.any():
+            continue
+        d = detail[m]
+        out.append(dict(problem=f'{p["physics"]} {p["mesh"]} n={p["n"]} order {p["order"]}', requests=int(m.sum()),
+                        p50_ms=round(float(np.percentile(lat[m], 50) * 1e3), 3),
+                        p99_ms=round(float(np.percentile(lat[m], 99) * 1e3), 3),
+                        device_ms=round(float(dev[m].mean()), 3), launch_ms=round(float(d[:, 0].mean()), 3),
+                        launch_parts_ms=[round(float(x), 3) for x in d[:, 1:4].mean(axis=0)],
+                        queue_ms=round(float(d[:, 4].mean()), 3), submit_delay_ms=round(float(d[:, 5].mean()), 3)))
+    return out
+
+
 def write_pool_mesh(kind, n, path):
     {"quad": meshgen.quad_mesh, "tri": meshgen.tri_mesh, "hex": meshgen.hex_mesh, "tet": meshgen.tet_mesh}[kind](path, n)
 
@@ -527,7 +546,8 @@ def run_serving(args, spec):
     lib.slz_serve_add.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
     lib.slz_serve_run_warm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
-                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double)]
     tmpd = tempfile.mkdtemp(prefix=f"slserve{rank}_")
     pool = []
     t0 = time.perf_counter()
@@ -551,11 +571,12 @@ def run_serving(args, spec):
         done = np.zeros(nreq)
         dev = np.zeros(nreq)
         prob = np.zeros(nreq, np.int32)
+        detail = np.zeros((nreq, 6))
         summ = np.zeros(9)
         with ClockSampler(local) as clk:
             rc = lib.slz_serve_run_warm(nwarm, nreq, rate, args.slots, prec, 12345, min(8, os.cpu_count() or 4), abi.f64p(lat),
                                         abi.f64p(done), abi.f64p(dev), prob.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                        abi.f64p(summ))
+                                        abi.f64p(detail), abi.f64p(summ))
         if rc != 0:
             raise RuntimeError("serve_run failed: " + lib.slz_last_error().decode(errors="replace"))
         res[name] = dict(p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
@@ -563,7 +584,7 @@ def run_serving(args, spec):
                          mean_ms=float(lat.mean() * 1e3), matrices_per_s=nreq / summ[0], nnz_per_s=summ[1] / summ[0],
                          wall_s=float(summ[0]), device_busy=float(summ[2] * 1e-3 / summ[0]), late_submissions=int(summ[3]),
                          launch_ms=float(summ[4]), launch_parts_ms=[float(x) for x in summ[6:9]], queue_ms=float(summ[5]),
-                         clocks=clk.summary())
+                         per_problem=serving_per_problem(pool, prob, lat, dev, detail), clocks=clk.summary())
     lib.slz_serve_release()
     if rank == 0:
         mixed, plain = res["split"], res["fp64"]

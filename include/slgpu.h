@@ -315,7 +315,9 @@ typedef struct {
     int32_t kind;  /* SLGPU_UPDATE_* */
     int32_t index; /* elemdata / fielddata array index in the group */
     int32_t rows;  /* rows of the array (1 for elemdata) */
-    const double* values; /* [rows][count], mesh element order; copied at submit */
+    const double* values; /* [rows][count], mesh element order; copied at submit, unless
+                             every array of the request is page-locked (slgpu_host_alloc):
+                             then read in place and kept unchanged until the request is done */
     int64_t count;
 } slgpu_update;
 
@@ -341,7 +343,8 @@ typedef struct {
 } slgpu_request_stats;
 
 int slgpu_server_create(slgpu_ctx* ctx, int nslots, slgpu_server** out);
-/* Queues a request; returns its ticket.  The update values are copied. */
+/* Queues a request; returns its ticket.  Update values in pageable memory
+ * are copied; page-locked ones are read in place (see slgpu_update). */
 int slgpu_server_submit(slgpu_server* s, const slgpu_request* r, int64_t* ticket);
 /* Waits up to timeout_s (< 0: no limit) for a request.  Returns SLGPU_OK when
  * it completed, SLGPU_E_TIMEOUT when still running, or the request's own
@@ -355,6 +358,13 @@ int64_t slgpu_server_pending(slgpu_server* s);
 /* The server's clock: seconds since it was created (the time base of
  * slgpu_request_stats). */
 double slgpu_server_clock(slgpu_server* s);
+/* Readies every slot for requests of `precision` on a template: the slot's
+ * request arena and split-precision scratch are grown to fit one request that
+ * updates every per-element array, and the template's split operands are
+ * built, so that the first requests allocate no device memory.  Only while
+ * the server has no queued or running requests (else SLGPU_E_ARG).  No
+ * counterpart in the reference. */
+int slgpu_server_prepare(slgpu_server* s, int handle, int precision);
 /* Waits for every request, stops the server thread and frees its slots. */
 void slgpu_server_destroy(slgpu_server* s);
 /* Page-locked host memory for request outputs (and inputs). */

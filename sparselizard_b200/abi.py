@@ -137,6 +137,7 @@ SIGNATURES = {
     "slgpu_matrix_group_count": (c_int, [c_void_p, c_int, POINTER(c_int)]),
     "slgpu_matrix_group_desc": (c_int, [c_void_p, c_int, c_int, POINTER(GroupDesc)]),
     "slgpu_server_create": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    "slgpu_server_prepare": (c_int, [c_void_p, c_int, c_int]),
     "slgpu_server_submit": (c_int, [c_void_p, POINTER(Request), POINTER(c_int64)]),
     "slgpu_server_wait": (c_int, [c_void_p, c_int64, c_double, POINTER(RequestStats)]),
     "slgpu_server_error": (c_int, [c_void_p, c_int64, c_char_p, c_size_t]),

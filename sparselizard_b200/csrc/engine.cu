@@ -26,6 +26,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -54,9 +55,11 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept
         s_ = o.s_;
         p_ = o.p_;
         n_ = o.n_;
+        arena_ = o.arena_;
         o.ctx_ = nullptr;
         o.p_ = nullptr;
         o.n_ = 0;
+        o.arena_ = false;
     }
     return *this;
 }
@@ -67,6 +70,19 @@ void DevBuf::alloc(Ctx* ctx, size_t bytes)
     if (bytes == 0)
         bytes = 16;
     bytes = (bytes + 255) & ~size_t(255);
+    Exec& x = *ctx->x;
+    if (x.arena_on) {
+        if (x.arena_off + bytes <= x.arena.bytes()) {
+            p_ = x.arena.as<char>() + x.arena_off;
+            x.arena_off += bytes;
+            ctx_ = ctx;
+            s_ = x.stream;
+            n_ = bytes;
+            arena_ = true;
+            return;
+        }
+        x.arena_miss += bytes;
+    }
     if ((size_t)ctx->in_use + bytes > ctx->budget)
         fail(SLGPU_E_BUDGET, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget (" +
                                  std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget) + " in use)");
@@ -83,13 +99,14 @@ void DevBuf::alloc(Ctx* ctx, size_t bytes)
 
 void DevBuf::release()
 {
-    if (p_ != nullptr && ctx_ != nullptr) {
+    if (p_ != nullptr && ctx_ != nullptr && !arena_) {
         cudaFreeAsync(p_, s_);
         ctx_->in_use -= (int64_t)n_;
     }
     p_ = nullptr;
     n_ = 0;
     ctx_ = nullptr;
+    arena_ = false;
 }
 
 template <class T>
@@ -560,6 +577,55 @@ void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes)
     x.stage_used += need;
     std::memcpy(p, src, bytes);
     cuda_check(cudaMemcpyAsync(buf.as<void>(), p, bytes, cudaMemcpyHostToDevice, x.stream), "cudaMemcpyAsync H2D staged");
+}
+
+namespace {
+struct HostTrace {
+    bool on = false;
+    std::mutex mu;
+    struct Acc {
+        double total = 0, max = 0;
+        int64_t n = 0;
+    };
+    std::map<std::string, Acc> acc;
+    HostTrace()
+    {
+        const char* v = std::getenv("SLGPU_HOST_TRACE");
+        on = v != nullptr && std::strcmp(v, "1") == 0;
+    }
+    ~HostTrace()
+    {
+        if (!on || acc.empty())
+            return;
+        std::fprintf(stderr, "slgpu host trace (label: calls, mean us, max us, total ms)\n");
+        for (auto& [k, v] : acc)
+            std::fprintf(stderr, "  %-30s %9lld %10.2f %10.2f %10.2f\n", k.c_str(), (long long)v.n, v.total * 1e6 / std::max<int64_t>(v.n, 1),
+                         v.max * 1e6, v.total * 1e3);
+    }
+};
+HostTrace g_htrace;
+double host_seconds() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+}  // namespace
+
+void htrace_begin(Ctx* ctx)
+{
+    if (g_htrace.on)
+        ctx->x->trace_t = host_seconds();
+}
+
+void htrace_mark(Ctx* ctx, const char* label)
+{
+    if (!g_htrace.on)
+        return;
+    const double t = host_seconds();
+    {
+        std::lock_guard<std::mutex> lk(g_htrace.mu);
+        auto& a = g_htrace.acc[label];
+        a.total += t - ctx->x->trace_t;
+        a.max = std::max(a.max, t - ctx->x->trace_t);
+        a.n++;
+    }
+    ctx->x->trace_t = t;
 }
 
 // Kernel-family timers: kstat_start/kstat_stop bracket launches with an
@@ -1090,10 +1156,13 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     const int NE = split_tile_width();
     const int64_t ntiles = (int64_t)g.tiles.size();
     const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
-    if (ctx->x->split_cols.bytes() < colbytes)
-        ctx->x->split_cols.alloc(ctx, colbytes);
-    if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
-        ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
+    {
+        ArenaPause keep(*ctx->x);  // per-state scratch, kept between requests
+        if (ctx->x->split_cols.bytes() < colbytes)
+            ctx->x->split_cols.alloc(ctx, colbytes);
+        if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
+            ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
+    }
     ColSliceParams cs{};
     cs.C = C;
     cs.elemexp = elemexp;
@@ -1284,8 +1353,10 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     DevBuf C;
     C.alloc(ctx, std::max<int64_t>(ctot, 1) * 8);
     if (precision != SLGPU_PREC_FP64) {
-        if (ctx->x->split_error.empty())
+        if (ctx->x->split_error.empty()) {
+            ArenaPause keep(*ctx->x);
             ctx->x->split_error.alloc(ctx, 16);
+        }
         cuda_check(cudaMemsetAsync(ctx->x->split_error.as<void>(), 0, 16, ctx->x->stream), "memset");
     }
     while (ctx->x->evpool.size() < 3) {
@@ -1408,8 +1479,33 @@ void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::v
     }
 }
 
+// Everything the value path creates lazily (split-precision row slices,
+// column-slice buffers, the error flag), made ahead of time on the current
+// execution state so that the value path itself allocates none of it.
+void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
+{
+    if (precision == SLGPU_PREC_FP64)
+        return;
+    const int tier = precision == SLGPU_PREC_SPLIT ? 0 : 1;
+    size_t colbytes = 0, expbytes = 0;
+    for (auto& g : M.groups)
+        if (g->nelem > 0 && uses_split(*g, precision)) {
+            const GroupDev::Split& sp = ensure_split(ctx, *g, tier);
+            colbytes = std::max(colbytes, (size_t)sp.S * sp.Qpad * g->tiles.size() * 64);
+            expbytes = std::max(expbytes, g->tiles.size() * 64 * 4);
+        }
+    Exec& x = *ctx->x;
+    if (x.split_cols.bytes() < colbytes)
+        x.split_cols.alloc(ctx, colbytes);
+    if (x.split_colexp.bytes() < expbytes)
+        x.split_colexp.alloc(ctx, expbytes);
+    if (x.split_error.empty())
+        x.split_error.alloc(ctx, 16);
+}
+
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
 {
+    htrace_begin(ctx);
     ctx->x->kev_tag.clear();
     stage_reset(*ctx->x);
     if (ctx->record_only) {

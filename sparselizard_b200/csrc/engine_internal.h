@@ -37,6 +37,7 @@ private:
     cudaStream_t s_ = nullptr;  // allocated (and freed) in this stream's order
     void* p_ = nullptr;
     size_t n_ = 0;
+    bool arena_ = false;  // carved from an execution state's arena (nothing to free)
 };
 
 struct Error {
@@ -187,6 +188,16 @@ struct Exec {
     char* stage = nullptr;
     size_t stage_bytes = 0, stage_used = 0;
     std::vector<char*> stage_old;  // outgrown blocks, freed when the state is
+    double trace_t = 0;            // host time of the last trace mark (SLGPU_HOST_TRACE)
+    // Request arena (serving slots): while arena_on, DevBuf::alloc carves
+    // buffers from `arena` (bump allocation, reset per request; the slot's
+    // previous request has completed) instead of the stream-ordered pool,
+    // whose growth under concurrent streams stalls the launching thread.
+    // Allocations that do not fit go to the pool and are counted in
+    // arena_miss, by which the arena grows before the next request.
+    DevBuf arena;
+    size_t arena_off = 0, arena_miss = 0;
+    bool arena_on = false;
 };
 
 struct Ctx {
@@ -238,7 +249,24 @@ void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::v
 void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes);
 void stage_reset(Exec& x);
 void stage_free(Exec& x);
+// Allocations that outlive the current request (per-state scratch kept
+// between requests) bypass the arena while one of these is alive.
+struct ArenaPause {
+    Exec& x;
+    bool was;
+    explicit ArenaPause(Exec& e) : x(e), was(e.arena_on) { x.arena_on = false; }
+    ~ArenaPause() { x.arena_on = was; }
+};
 int kstat_start(Ctx* ctx, const char* family, double work);
+// Host-side launch tracing (SLGPU_HOST_TRACE=1): htrace_begin starts the
+// clock of the current execution state; htrace_mark adds the host time since
+// the previous mark to `label`.  The totals are printed to stderr at exit.
+void htrace_begin(Ctx* ctx);
+void htrace_mark(Ctx* ctx, const char* label);
+// Split-precision operands of the matrix's groups (built once) and the
+// current execution state's split scratch grown to fit them, so that the
+// value path allocates nothing for them.
+void prepare_value_path(Ctx* ctx, const Matrix& M, int precision);
 void kstat_stop(Ctx* ctx, int i);
 void kstat_collect(Ctx* ctx);
 

@@ -52,6 +52,13 @@ struct Request {
     double* in = nullptr;  // page-locked block with every update's values
     size_t in_cap = 0;
     int64_t nin = 0;
+    // Caller arrays already page-locked: read in place (host pointer, offset
+    // in doubles, count), no copy at submit.
+    struct DirectIn {
+        const double* host;
+        int64_t offset, n;
+    };
+    std::vector<DirectIn> direct_in;
     double* Aout = nullptr;
     double* Dout = nullptr;
     bool pinned_out = false;
@@ -71,6 +78,7 @@ struct Request {
 
 struct Slot {
     Exec ex;
+    size_t arena_need = 0;  // largest arena use (fitted or missed) of a request so far
     cudaEvent_t start = nullptr, done = nullptr;
     std::shared_ptr<Request> req;
     void* pinned = nullptr;  // staging for inputs and pageable outputs
@@ -100,8 +108,9 @@ struct Server {
 
 namespace {
 
-// Device bytes a request allocates while it runs.
-int64_t estimate_bytes(const Matrix& M, int precision, const Request& r)
+// Device bytes a request allocates while it runs (r == nullptr: a request
+// that updates every per-element array of every group).
+int64_t estimate_bytes(const Matrix& M, int precision, const Request* r)
 {
     int64_t vals = 0, coef = 0, exps = 0, split = 0;
     for (auto& g : M.groups) {
@@ -112,10 +121,16 @@ int64_t estimate_bytes(const Matrix& M, int precision, const Request& r)
         split = std::max<int64_t>(split, 7 * Qpad * (int64_t)g->tiles.size() * 64 + (int64_t)g->tiles.size() * 256);
     }
     for (auto& f : M.frags) vals += (int64_t)f->nr * f->nc;
-    int64_t upd = r.nin, over = 0;
-    for (auto& u : r.updates) {
-        const GroupDev& g = *M.groups[u.group];
-        over += (u.kind == SLGPU_UPDATE_ELEMDATA ? (int64_t)g.elemdata.bytes() : (int64_t)g.fielddata.bytes()) / 8;
+    int64_t upd = 0, over = 0;
+    if (r != nullptr) {
+        upd = r->nin;
+        for (auto& u : r->updates) {
+            const GroupDev& g = *M.groups[u.group];
+            over += (u.kind == SLGPU_UPDATE_ELEMDATA ? (int64_t)g.elemdata.bytes() : (int64_t)g.fielddata.bytes()) / 8;
+        }
+    } else {
+        for (auto& g : M.groups) over += (int64_t)(g->elemdata.bytes() + g->fielddata.bytes()) / 8;
+        upd = over;
     }
     const int64_t csr = M.pattern ? M.pattern->nnzA + M.pattern->nnzD : 0;
     int64_t b = 8 * (vals + coef + csr + upd + over) + 4 * exps;
@@ -145,7 +160,19 @@ void launch(Server& S, Slot& s, Request& r)
     const double t0 = S.now();
     ctx->x = &s.ex;
     stage_reset(s.ex);
+    htrace_begin(ctx);
     cudaStream_t st = s.ex.stream;
+    // Request buffers come from the slot's arena, grown (rarely, on this
+    // slot's stream) to the largest request seen.
+    {
+        const size_t want = std::max<size_t>(s.arena_need, (size_t)r.est_bytes);
+        if (s.ex.arena.bytes() < want)
+            s.ex.arena.alloc(ctx, want + want / 8);
+        s.ex.arena_off = 0;
+        s.ex.arena_miss = 0;
+        s.ex.arena_on = true;
+    }
+    htrace_mark(ctx, "request: arena");
     cuda_check_srv(cudaEventRecord(s.start, st), "cudaEventRecord");
     // Inputs: every update's values are in the request's page-locked block
     // (filled at submit): one copy to the device, then per updated group a
@@ -163,7 +190,14 @@ void launch(Server& S, Slot& s, Request& r)
     r.fd.resize(M.groups.size());
     if (r.nin > 0) {
         r.upd.alloc(ctx, (size_t)r.nin * 8);
-        cuda_check_srv(cudaMemcpyAsync(r.upd.as<void>(), r.in, (size_t)r.nin * 8, cudaMemcpyHostToDevice, st), "H2D request inputs");
+        if (!r.direct_in.empty()) {
+            for (const auto& d : r.direct_in)
+                cuda_check_srv(cudaMemcpyAsync(r.upd.as<double>() + d.offset, d.host, (size_t)d.n * 8, cudaMemcpyHostToDevice, st),
+                               "H2D request inputs");
+        } else {
+            cuda_check_srv(cudaMemcpyAsync(r.upd.as<void>(), r.in, (size_t)r.nin * 8, cudaMemcpyHostToDevice, st),
+                           "H2D request inputs");
+        }
         for (auto& u : r.updates) {
             GroupDev& g = *M.groups[u.group];
             const bool elem = u.kind == SLGPU_UPDATE_ELEMDATA;
@@ -188,6 +222,7 @@ void launch(Server& S, Slot& s, Request& r)
         }
     }
     const double t1 = S.now();
+    htrace_mark(ctx, "request: inputs");
     std::vector<int64_t> gvb;
     int64_t total_vals = 0;
     std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
@@ -209,6 +244,9 @@ void launch(Server& S, Slot& s, Request& r)
     if (r.precision != SLGPU_PREC_FP64 && !s.ex.split_error.empty())
         cuda_check_srv(cudaMemcpyAsync(s.err_host, s.ex.split_error.as<void>(), 4, cudaMemcpyDeviceToHost, st), "D2H split error");
     cuda_check_srv(cudaEventRecord(s.done, st), "cudaEventRecord");
+    htrace_mark(ctx, "request: outputs");
+    s.ex.arena_on = false;
+    s.arena_need = std::max(s.arena_need, s.ex.arena_off + s.ex.arena_miss);
     ctx->x = &ctx->main;
     const double t3 = S.now();
     r.parts_ms[0] = (t1 - t0) * 1e3;
@@ -297,7 +335,9 @@ void server_loop(Server& S)
                 r = S.queue.front();
             }
             std::lock_guard<std::recursive_mutex> cl(ctx->mu);
-            if (ctx->in_use + r->est_bytes > (int64_t)ctx->budget) {
+            // Device memory the request adds: what its slot's arena lacks.
+            const int64_t extra = std::max<int64_t>(0, r->est_bytes - (int64_t)free_slot->ex.arena.bytes());
+            if (ctx->in_use + extra > (int64_t)ctx->budget) {
                 bool busy = false;
                 for (Slot& s : S.slots) busy = busy || (bool)s.req;
                 if (busy)
@@ -325,6 +365,7 @@ void server_loop(Server& S)
                 msg = e.what();
             }
             if (code != SLGPU_OK) {
+                free_slot->ex.arena_on = false;
                 ctx->x = &ctx->main;
                 cudaStreamSynchronize(free_slot->ex.stream);
                 std::lock_guard<std::mutex> lk(S.mu);
@@ -412,6 +453,7 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
         return SLGPU_E_ARG;
     Ctx* ctx = S->ctx;
     auto r = std::make_shared<Request>();
+    std::map<std::pair<const double*, int64_t>, int64_t> seen_arrays;  // (values, doubles) -> offset
     {
         std::lock_guard<std::recursive_mutex> cl(ctx->mu);
         auto it = ctx->matrices.find(rq->handle);
@@ -440,7 +482,7 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
         t->frags = M.frags;
         t->pattern = M.pattern;
         r->tmpl = t;
-        std::map<std::pair<const double*, int64_t>, int64_t> seen;  // identical arrays are sent once
+        auto& seen = seen_arrays;  // identical arrays are sent once
         for (int i = 0; i < rq->nupdates; i++) {
             const slgpu_update& u = rq->updates[i];
             if (u.group < 0 || u.group >= (int)M.groups.size()) {
@@ -489,14 +531,26 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
                         (cudaPointerGetAttributes(&pd, rq->Dvals) == cudaSuccess && pd.type == cudaMemoryTypeHost);
         cudaGetLastError();
         r->pinned_out = pA && pD;
-        r->est_bytes = estimate_bytes(M, rq->precision, *r);
+        r->est_bytes = estimate_bytes(M, rq->precision, r.get());
         if (r->est_bytes > (int64_t)ctx->budget) {
             ctx->last_error = "a request needs more device memory than the whole HBM budget";
             return SLGPU_E_BUDGET;
         }
     }
-    // Inputs into a page-locked block (outside the context lock).
+    // Inputs: page-locked caller arrays are read in place by the request's
+    // copy; others are copied into a page-locked block here (outside the
+    // context lock), so that the caller may reuse them at once.
     if (r->nin > 0) {
+        bool pinned = true;
+        for (const auto& kv : seen_arrays) {
+            cudaPointerAttributes a{};
+            pinned = pinned && cudaPointerGetAttributes(&a, kv.first.first) == cudaSuccess && a.type == cudaMemoryTypeHost;
+        }
+        cudaGetLastError();
+        if (pinned)
+            for (const auto& kv : seen_arrays) r->direct_in.push_back(Request::DirectIn{kv.first.first, kv.second, kv.first.second});
+    }
+    if (r->nin > 0 && r->direct_in.empty()) {
         const size_t need = (size_t)r->nin * 8;
         size_t cap = size_t(1) << 16;
         while (cap < need) cap <<= 1;
@@ -606,6 +660,50 @@ int64_t slgpu_server_pending(slgpu_server* S)
 
 double slgpu_server_clock(slgpu_server* S) { return S == nullptr ? 0.0 : S->now(); }
 
+int slgpu_server_prepare(slgpu_server* S, int handle, int precision)
+{
+    if (S == nullptr)
+        return SLGPU_E_ARG;
+    Ctx* ctx = S->ctx;
+    std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->running > 0) {
+            ctx->last_error = "a server is prepared while it has no requests";
+            return SLGPU_E_ARG;
+        }
+    }
+    auto it = ctx->matrices.find(handle);
+    if (it == ctx->matrices.end() || !it->second->pattern) {
+        ctx->last_error = "prepare: unknown or unprocessed template " + std::to_string(handle);
+        return SLGPU_E_ARG;
+    }
+    if (precision != SLGPU_PREC_FP64 && precision != SLGPU_PREC_SPLIT && precision != SLGPU_PREC_FP32) {
+        ctx->last_error = "unknown precision mode";
+        return SLGPU_E_ARG;
+    }
+    const Matrix& M = *it->second;
+    try {
+        cudaSetDevice(ctx->device);
+        const size_t est = (size_t)estimate_bytes(M, precision, nullptr);
+        for (Slot& s : S->slots) {
+            ctx->x = &s.ex;
+            prepare_value_path(ctx, M, precision);
+            const size_t want = std::max(s.arena_need, est);
+            if (s.ex.arena.bytes() < want)
+                s.ex.arena.alloc(ctx, want + want / 8);
+            s.arena_need = want;
+            ctx->x = &ctx->main;
+        }
+        for (Slot& s : S->slots) cuda_check_srv(cudaStreamSynchronize(s.ex.stream), "prepare");
+    } catch (const SlgpuException& e) {
+        ctx->x = &ctx->main;
+        ctx->last_error = e.e.msg;
+        return e.e.code;
+    }
+    return SLGPU_OK;
+}
+
 void slgpu_server_destroy(slgpu_server* S)
 {
     if (S == nullptr)
@@ -627,6 +725,7 @@ void slgpu_server_destroy(slgpu_server* S)
         s.ex.split_cols.release();
         s.ex.split_colexp.release();
         s.ex.split_error.release();
+        s.ex.arena.release();
         if (s.ex.stream != nullptr)
             cudaStreamSynchronize(s.ex.stream);
         for (auto& e : s.ex.ev)

@@ -470,22 +470,26 @@ int slz_serve_add(int kind, const char* msh, int dim, int order, long long* info
 // [5] mean ms a request waited in the queue, [6..8] mean host ms of the
 // launch parts (inputs, contractions, values and copies).
 int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency_out,
-                       double* done_out, double* device_out, int* problem_out, double* summary);
+                       double* done_out, double* device_out, int* problem_out, double* detail_out, double* summary);
 
 int slz_serve_run(int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency, double* done_s,
                   double* device_ms, int* problem, double* summary)
 {
-    return slz_serve_run_warm(0, nreq, rate, nslots, precision, seed, ngen, latency, done_s, device_ms, problem, summary);
+    return slz_serve_run_warm(0, nreq, rate, nslots, precision, seed, ngen, latency, done_s, device_ms, problem, nullptr, summary);
 }
 
 // As slz_serve_run, with `nwarm` requests of the same stream before the
 // measured ones (same server, so page-locked pools and split-precision
 // tables are warm); the outputs and summary cover the last `nreq` requests.
+// detail_out (optional): per measured request, server-thread launch time and
+// its three parts (ms), queueing time (ms) and submission delay behind the
+// scheduled arrival (ms).
 int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precision, unsigned long long seed, int ngen, double* latency_out,
-                       double* done_out, double* device_out, int* problem_out, double* summary)
+                       double* done_out, double* device_out, int* problem_out, double* detail_out, double* summary)
 {
     const int ntot = nwarm + nreq;
-    std::vector<double> latency(ntot), done_s(ntot), device_ms(ntot);
+    constexpr int kDetail = 6;
+    std::vector<double> latency(ntot), done_s(ntot), device_ms(ntot), detail((size_t)ntot * kDetail);
     std::vector<int> problem(ntot);
     g_error.clear();
     const int np = (int)g_serve.size();
@@ -499,6 +503,15 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
         g_error = "slgpu_server_create failed";
         return -1;
     }
+    // Every slot's device scratch sized for every problem before the stream.
+    for (int p = 0; p < np; p++)
+        if (slgpu_server_prepare(srv, g_serve[p]->handle, precision) != SLGPU_OK) {
+            char buf[512];
+            slgpu_last_error(ctx, buf, sizeof(buf));
+            g_error = std::string("slgpu_server_prepare: ") + buf;
+            slgpu_server_destroy(srv);
+            return -1;
+        }
     // Schedule.
     Normal rs(seed);
     std::vector<double> arrival(ntot);
@@ -508,18 +521,35 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
         arrival[k] = t;
         problem[k] = (int)(rs.next() % (uint64_t)np);
     }
-    // Output buffers: a few page-locked pairs per problem.
-    const int B = 4;
+    // Output buffers: page-locked pairs per problem, enough for about half a
+    // second of its arrivals (at least 4), so that a slow request does not
+    // hold back the submission of later ones.  Input buffers likewise:
+    // page-locked, so that the server reads them in place (no copy at submit).
+    std::vector<int> nbuf(np);
+    for (int p = 0; p < np; p++) nbuf[p] = std::max(4, (int)std::ceil(0.5 * rate / np) + 2);
     std::vector<std::vector<std::pair<double*, double*>>> free_out(np);
+    std::vector<std::vector<double*>> free_in(np);
     std::vector<void*> pinned;
     for (int p = 0; p < np; p++)
-        for (int b = 0; b < B; b++) {
-            void *a = nullptr, *d = nullptr;
+        for (int b = 0; b < nbuf[p]; b++) {
+            void *a = nullptr, *d = nullptr, *in = nullptr;
             slgpu_host_alloc(ctx, (size_t)std::max(1LL, g_serve[p]->nnzA) * 8, &a);
             slgpu_host_alloc(ctx, (size_t)std::max(1LL, g_serve[p]->nnzD) * 8, &d);
+            slgpu_host_alloc(ctx, (size_t)std::max(1LL, g_serve[p]->nmesh) * 8, &in);
+            if (a == nullptr || d == nullptr || in == nullptr) {
+                g_error = "page-locked request buffers";
+                for (void* q : {a, d, in})
+                    if (q != nullptr)
+                        slgpu_host_free(q);
+                for (void* q : pinned) slgpu_host_free(q);
+                slgpu_server_destroy(srv);
+                return -1;
+            }
             pinned.push_back(a);
             pinned.push_back(d);
+            pinned.push_back(in);
             free_out[p].push_back({(double*)a, (double*)d});
+            free_in[p].push_back((double*)in);
         }
     lognormal_table();
     // Time origin of the arrivals: after the set-up above.
@@ -527,26 +557,33 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
     const double offset = slgpu_server_clock(srv);  // server time at t_create
     std::mutex mu;
     std::condition_variable cv;
-    // Prepared inputs (lookahead window of L requests).
+    // Prepared inputs (lookahead window of L requests).  Input buffers are
+    // taken in request order (next_take), so that the earliest unsubmitted
+    // request never waits for a buffer held by a later one.
     const int L = 64;
-    std::vector<std::vector<double>> inputs(L);
+    std::vector<double*> inputs(ntot, nullptr);
     std::vector<int> ready(ntot, 0);
     std::atomic<int> consumed{0};
+    int next_take = 0;
     std::vector<std::thread> gens;
     for (int gth = 0; gth < ngen; gth++)
         gens.emplace_back([&, gth] {
             for (int k = gth; k < ntot; k += ngen) {
+                double* v = nullptr;
                 {
                     std::unique_lock<std::mutex> lk(mu);
-                    cv.wait(lk, [&] { return k < consumed.load() + L; });
+                    cv.wait(lk, [&] { return k < consumed.load() + L && next_take == k && !free_in[problem[k]].empty(); });
+                    v = free_in[problem[k]].back();
+                    free_in[problem[k]].pop_back();
+                    next_take = k + 1;
+                    cv.notify_all();
                 }
                 const ServeProblem& S = *g_serve[problem[k]];
-                std::vector<double> v((size_t)S.nmesh);
                 Normal r(seed * 1000003ull + (uint64_t)k * 7919ull + 17);
                 const double* T = lognormal_table().data();
-                for (double& x : v) x = S.median * T[r.next() >> 48];
+                for (int64_t i = 0; i < S.nmesh; i++) v[i] = S.median * T[r.next() >> 48];
                 std::lock_guard<std::mutex> lk(mu);
-                inputs[k % L] = std::move(v);
+                inputs[k] = v;
                 ready[k] = 1;
                 cv.notify_all();
             }
@@ -555,36 +592,63 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
     std::vector<std::pair<double*, double*>> outs(ntot);
     std::vector<int> submitted(ntot, 0);
     double late = 0, late_measured = 0, launch_ms_sum = 0, queue_s_sum = 0, parts_sum[3] = {0, 0, 0};
-    // Waiter: completions in submission order; frees output buffers.
+    // Waiter: collects completions in any order (a long request does not
+    // hold back the buffers of shorter ones behind it) and frees buffers.
     std::thread waiter([&] {
-        for (int k = 0; k < ntot; k++) {
+        std::vector<int> open;  // submitted, not yet collected
+        int next = 0, collected = 0;
+        while (collected < ntot) {
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv.wait(lk, [&] { return submitted[k] != 0; });
+                if (open.empty())
+                    cv.wait(lk, [&] { return next < ntot && submitted[next] != 0; });
+                while (next < ntot && submitted[next] != 0) open.push_back(next++);
             }
-            slgpu_request_stats st{};
-            int rc = slgpu_server_wait(srv, tickets[k], -1.0, &st);
-            latency[k] = rc == SLGPU_OK ? st.done_s - (arrival[k] + offset) : -1.0;
-            done_s[k] = st.done_s;
-            device_ms[k] = st.device_ms;
-            launch_ms_sum += st.launch_ms;
-            for (int i = 0; i < 3; i++) parts_sum[i] += st.launch_parts_ms[i];
-            queue_s_sum += st.start_s - st.submit_s;
-            slgpu_server_release(srv, tickets[k]);
-            std::lock_guard<std::mutex> lk(mu);
-            free_out[problem[k]].push_back(outs[k]);
-            cv.notify_all();
+            bool any = false;
+            for (size_t i = 0; i < open.size();) {
+                const int k = open[i];
+                slgpu_request_stats st{};
+                st.status = -1;
+                if (tickets[k] <= 0)  // rejected at submit
+                    st.status = SLGPU_E_ARG;
+                else  // oldest open request: a short blocking wait; the rest are polled
+                    slgpu_server_wait(srv, tickets[k], i == 0 && !any ? 2e-3 : 0.0, &st);
+                if (st.status < 0) {
+                    i++;
+                    continue;
+                }
+                any = true;
+                latency[k] = st.status == SLGPU_OK ? st.done_s - (arrival[k] + offset) : -1.0;
+                done_s[k] = st.done_s;
+                device_ms[k] = st.device_ms;
+                launch_ms_sum += st.launch_ms;
+                for (int j = 0; j < 3; j++) parts_sum[j] += st.launch_parts_ms[j];
+                queue_s_sum += st.start_s - st.submit_s;
+                double* d = &detail[(size_t)k * kDetail];
+                d[0] = st.launch_ms;
+                for (int j = 0; j < 3; j++) d[1 + j] = st.launch_parts_ms[j];
+                d[4] = (st.start_s - st.submit_s) * 1e3;
+                d[5] = std::max(0.0, (st.submit_s - (arrival[k] + offset)) * 1e3);
+                if (tickets[k] > 0)
+                    slgpu_server_release(srv, tickets[k]);
+                open.erase(open.begin() + (long)i);
+                collected++;
+                std::lock_guard<std::mutex> lk(mu);
+                free_out[problem[k]].push_back(outs[k]);
+                free_in[problem[k]].push_back(inputs[k]);
+                cv.notify_all();
+            }
         }
     });
     // Submitter: on the server clock (t_create ~ the server's start).
     for (int k = 0; k < ntot; k++) {
         const ServeProblem& S = *g_serve[problem[k]];
-        std::vector<double> v;
+        const double* v = nullptr;
         std::pair<double*, double*> o;
         {
             std::unique_lock<std::mutex> lk(mu);
             cv.wait(lk, [&] { return ready[k] != 0 && !free_out[problem[k]].empty(); });
-            v = std::move(inputs[k % L]);
+            v = inputs[k];
             o = free_out[problem[k]].back();
             free_out[problem[k]].pop_back();
         }
@@ -597,7 +661,7 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
                 late_measured += 1;
         }
         std::vector<slgpu_update> ups;
-        for (int gi : S.groups) ups.push_back(slgpu_update{gi, SLGPU_UPDATE_FIELDDATA, 0, 1, v.data(), S.nmesh});
+        for (int gi : S.groups) ups.push_back(slgpu_update{gi, SLGPU_UPDATE_FIELDDATA, 0, 1, v, S.nmesh});
         slgpu_request rq{S.handle, precision, (int32_t)ups.size(), 0, ups.data(), o.first, o.second};
         int64_t tk = 0;
         if (slgpu_server_submit(srv, &rq, &tk) != SLGPU_OK) {
@@ -623,6 +687,8 @@ int slz_serve_run_warm(int nwarm, int nreq, double rate, int nslots, int precisi
         done_out[k - nwarm] = done_s[k];
         device_out[k - nwarm] = device_ms[k];
         problem_out[k - nwarm] = problem[k];
+        if (detail_out != nullptr)
+            for (int j = 0; j < kDetail; j++) detail_out[(size_t)(k - nwarm) * kDetail + j] = detail[(size_t)k * kDetail + j];
     }
     summary[0] = last - (arrival[nwarm] + offset);
     summary[1] = nnz;

@@ -93,6 +93,14 @@ class Server:
         self._keep.pop(ticket, None)
         return s
 
+    def prepare(self, handle: int, precision: int):
+        """Grows every slot's device scratch for requests on a template (no requests pending)."""
+        st = self.lib.slgpu_server_prepare(self.h, handle, precision)
+        if st != abi.OK:
+            buf = ctypes.create_string_buffer(2048)
+            self.lib.slgpu_last_error(self.ctx, buf, 2048)
+            raise abi.SlgpuError(st, buf.value.decode(errors="replace"))
+
     def pending(self) -> int:
         return int(self.lib.slgpu_server_pending(self.h))
 

@@ -146,3 +146,33 @@ def test_pinned_outputs_and_pending_count(ctx):
         srv.close()
         for p in pins:
             p.close()
+
+
+def test_prepare_and_page_locked_inputs(ctx):
+    """slgpu_server_prepare sizes every slot ahead of the stream; inputs in
+    page-locked memory are read in place.  Results equal process()."""
+    rng = np.random.Generator(np.random.PCG64(10))
+    t = _template(ctx, rng, 6, 70, 9, 9, 3, 3, 2500)
+    srv = serving.Server(ctx.lib, ctx.h, 3)
+    pins = []
+    try:
+        for prec in (abi.PREC_FP64, abi.PREC_SPLIT):
+            srv.prepare(t["handle"], prec)
+        tickets = []
+        for k in range(6):
+            prec = abi.PREC_SPLIT if k % 2 else abi.PREC_FP64
+            vin = serving.PinnedArray(ctx.lib, ctx.h, t["nmesh"])
+            vin.array[:] = rng.lognormal(0.0, 0.3, t["nmesh"])
+            A = np.full(t["nnzA"], np.nan)
+            D = np.full(max(1, t["nnzD"]), np.nan)[: t["nnzD"]]
+            pins.append(vin)
+            tk = srv.submit(t["handle"], prec, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vin.array)], A, D)
+            tickets.append((tk, prec, vin.array.copy(), A, D))
+        for tk, prec, vals, A, D in tickets:
+            assert srv.wait(tk).status == abi.OK
+            pA, pD = _plain(ctx, t, vals, prec)
+            assert np.array_equal(A, pA) and np.array_equal(D, pD)
+    finally:
+        srv.close()
+        for p in pins:
+            p.close()
