@@ -330,6 +330,7 @@ def run_ours(args, spec):
     phase = np.zeros(5)
     stats = {}
     launches0 = lib.slgpu_kernel_launches(ctx)
+    graphs0 = lib.slgpu_graph_launches(ctx)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         if world > 1:
@@ -345,6 +346,7 @@ def run_ours(args, spec):
             torch.distributed.barrier()
         torch.cuda.synchronize()
     launches = lib.slgpu_kernel_launches(ctx) - launches0
+    graph_replays = lib.slgpu_graph_launches(ctx) - graphs0
     dev_ms = phase[4] / args.steps
     dev_ms_max, = allreduce([dev_ms], torch.distributed.ReduceOp.MAX) if world > 1 else [dev_ms]
     total_nnz, = allreduce([float(nnz)], torch.distributed.ReduceOp.SUM) if world > 1 else [float(nnz)]
@@ -453,6 +455,7 @@ def run_ours(args, spec):
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_s_max * 1e3,
                     "h2d_bytes_per_step": int(24 * nnodes), "d2h_bytes_per_step": int(8 * (info.nnzA + info.nnzD))},
             "gpu_launches": int(launches),
+            "graph_replays": int(graph_replays),
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -245,8 +245,22 @@ int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_
  * A family that did not run reports zeros.  No counterpart in the reference
  * (a measurement hook). */
 int slgpu_kernel_stats(const slgpu_ctx* ctx, const char* family, double* total_ms, int64_t* launches, double* work);
-/* Number of kernels this context has launched so far. */
+/* Number of kernels this context has launched so far (kernels of replayed
+ * graphs included). */
 int64_t slgpu_kernel_launches(const slgpu_ctx* ctx);
+
+/* CUDA graphs for the value path of process() on a resident pattern
+ * (default on; SLGPU_GRAPHS=0 in the environment turns them off at context
+ * creation).  The second process() of a matrix whose launches would be the
+ * same as the first's (same pattern, buffers and kernels) captures the
+ * coefficient, contraction and CSR value launches into one graph; later ones
+ * replay it.  Per-element data, field data, term scales, destination
+ * multipliers and node coordinates changed in place are seen by the replay.
+ * No counterpart in the reference (rawmat::process runs on the host,
+ * rawmat.cpp:127-299). */
+int slgpu_ctx_set_graphs(slgpu_ctx* ctx, int enable);
+/* Number of graph replays of process() so far. */
+int64_t slgpu_graph_launches(const slgpu_ctx* ctx);
 
 /* Algorithmic work of one process() of a matrix, for roofline accounting:
  * contraction_flops = sum over groups of nelem * sum over terms of

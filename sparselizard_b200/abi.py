@@ -112,6 +112,8 @@ SIGNATURES = {
     "slgpu_matrix_set_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_matrix_get_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
+    "slgpu_ctx_set_graphs": (c_int, [c_void_p, c_int]),
+    "slgpu_graph_launches": (c_int64, [c_void_p]),
     "slgpu_kernel_stats": (c_int, [c_void_p, c_char_p, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]),
     "slgpu_check_coefficient_kernels": (c_int, [c_void_p, c_int, c_char_p, c_size_t]),
     "slgpu_matrix_work": (c_int, [c_void_p, c_int, c_void_p]),

@@ -57,7 +57,10 @@ std::string jit_coef_source(const std::vector<const GroupDev*>& batch)
     const int dim = g0.problemdim, ncn = g0.ncn, ngp = g0.ngp;
     std::ostringstream s;
     s << kPrelude;
-    s << "extern \"C\" __global__ void __launch_bounds__(128) slgpu_coef(JitGeom p, const JitGroup* __restrict__ grp)\n{\n";
+    // The batch's group descriptors are passed by value (kernel parameter
+    // space), so that a launch needs no argument upload.
+    s << "struct JitGroups { JitGroup g[" << batch.size() << "]; };\n";
+    s << "extern \"C\" __global__ void __launch_bounds__(128) slgpu_coef(JitGeom p, const JitGroups grp)\n{\n";
     s << "  const i64 n = blockIdx.x * (i64)blockDim.x + threadIdx.x;\n";
     s << "  if (n >= p.nelem * " << ngp << ") return;\n";
     s << "  const int g = (int)(n / p.nelem);\n  const i64 e = n - (i64)g * p.nelem;\n";
@@ -92,7 +95,7 @@ std::string jit_coef_source(const std::vector<const GroupDev*>& batch)
     s << "  (void)o; (void)X0; (void)X1; (void)X2;\n";
     for (size_t k = 0; k < batch.size(); k++) {
         const GroupDev& G = *batch[k];
-        s << "  {\n    const JitGroup q = grp[" << k << "];\n";
+        s << "  {\n    const JitGroup q = grp.g[" << k << "];\n";
         const int n = (int)G.nodes.size();
         std::vector<char> needed(n, 0);
         for (int t = 0; t < G.nterms; t++) needed[G.term_node[t]] = 1;

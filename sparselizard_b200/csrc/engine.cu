@@ -20,6 +20,7 @@
 #include "engine_internal.h"
 #include "engine_kernels.cuh"
 #include "split_tc.cuh"
+#include "row_stream.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -557,8 +558,13 @@ void stage_free(Exec& x)
 
 void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes)
 {
-    Exec& x = *ctx->x;
     buf.alloc(ctx, bytes);
+    upload_staged_into(ctx, buf.as<void>(), src, bytes);
+}
+
+void upload_staged_into(Ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    Exec& x = *ctx->x;
     if (bytes == 0)
         return;
     const size_t need = (bytes + 255) & ~size_t(255);
@@ -576,7 +582,7 @@ void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes)
     char* p = x.stage + x.stage_used;
     x.stage_used += need;
     std::memcpy(p, src, bytes);
-    cuda_check(cudaMemcpyAsync(buf.as<void>(), p, bytes, cudaMemcpyHostToDevice, x.stream), "cudaMemcpyAsync H2D staged");
+    cuda_check(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, x.stream), "cudaMemcpyAsync H2D staged");
 }
 
 namespace {
@@ -638,12 +644,19 @@ int kstat_start(Ctx* ctx, const char* family, double work)
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         ctx->x->kev.push_back(e);
     }
-    cuda_check(cudaEventRecord(ctx->x->kev[2 * i], ctx->x->stream), "cudaEventRecord");
+    record_event(ctx, ctx->x->kev[2 * i]);
     ctx->x->kev_tag.emplace_back(family, work);
     return (int)i;
 }
 
-void kstat_stop(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->kev[2 * i + 1], ctx->x->stream), "cudaEventRecord"); }
+void kstat_stop(Ctx* ctx, int i) { record_event(ctx, ctx->x->kev[2 * i + 1]); }
+
+void record_event(Ctx* ctx, cudaEvent_t e)
+{
+    const cudaError_t err = ctx->x->capturing ? cudaEventRecordWithFlags(e, ctx->x->stream, cudaEventRecordExternal)
+                                              : cudaEventRecord(e, ctx->x->stream);
+    cuda_check(err, "cudaEventRecord");
+}
 
 void kstat_collect(Ctx* ctx)
 {
@@ -659,7 +672,7 @@ void kstat_collect(Ctx* ctx)
     ctx->x->kev_tag.clear();
 }
 
-static void ev_record(Ctx* ctx, int i) { cuda_check(cudaEventRecord(ctx->x->ev[i], ctx->x->stream), "cudaEventRecord"); }
+static void ev_record(Ctx* ctx, int i) { record_event(ctx, ctx->x->ev[i]); }
 
 static float ev_ms(Ctx* ctx, int a, int b)
 {
@@ -1250,6 +1263,10 @@ struct JitGroup {
 // groups with the same geometry key run as one runtime-compiled kernel; the
 // interpreter kernel is used when SLGPU_COEF_INTERPRETER=1 or when a kernel
 // cannot be compiled.
+// Groups per runtime-compiled coefficient kernel: their descriptors (48 bytes
+// each) are one by-value kernel parameter.
+constexpr int kJitBatch = 64;
+
 static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std::vector<int64_t>& coff, int32_t* elemexp,
                                 const std::vector<int64_t>& eoff, const std::vector<GroupData>* ov)
 {
@@ -1262,7 +1279,7 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
     while (k < ng) {
         const GroupDev& g0 = *M.groups[k];
         size_t k1 = k + 1;
-        while (k1 < ng && M.groups[k1]->geom_hash == g0.geom_hash) k1++;
+        while (k1 < ng && k1 - k < kJitBatch && M.groups[k1]->geom_hash == g0.geom_hash) k1++;
         if (g0.nelem == 0) {
             k = k1;
             continue;
@@ -1292,13 +1309,10 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                     jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, G.term_scale_d.as<double>(), C + coff[j],
                                           eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
                 }
-                DevBuf djg;
-                upload_staged(ctx, djg, jg.data(), jg.size() * sizeof(JitGroup));
                 const MeshDev& m = ctx->meshes.at(g0.mesh);
                 JitGeom geom{m.xyz.as<double>(), m.types.at(g0.elemtype).conn.as<int32_t>(), g0.elems.as<int32_t>(), g0.orient.as<int32_t>(),
                              (long long)g0.nelem, g0.weights.as<double>(), g0.lagrange.as<double>()};
-                const JitGroup* gp = djg.as<JitGroup>();
-                void* args[] = {&geom, &gp};
+                void* args[] = {&geom, jg.data()};  // the group array is one by-value parameter
                 const int64_t n = g0.nelem * (int64_t)g0.ngp;
                 double cbytes = 0;
                 for (size_t j = k; j < k1; j++) cbytes += 8.0 * M.groups[j]->nterms * M.groups[j]->ngp * M.groups[j]->nelem;
@@ -1378,9 +1392,9 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
         E.alloc(ctx, (size_t)etot * 4);
         cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
     }
-    cuda_check(cudaEventRecord(ctx->x->evpool[0], ctx->x->stream), "cudaEventRecord");
+    record_event(ctx, ctx->x->evpool[0]);
     launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov);
-    cuda_check(cudaEventRecord(ctx->x->evpool[1], ctx->x->stream), "cudaEventRecord");
+    record_event(ctx, ctx->x->evpool[1]);
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
@@ -1406,18 +1420,26 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
             kp.tiles = g->tiles_d.as<Tile>();
             kp.out = vals + gvb[gi];
             const int64_t P = (int64_t)g->ntf * g->ndof;
-            dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
-            if (grid.y > 65535)
-                fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
+            const size_t small_smem = ((size_t)g->norient * g->nterms * g->ngp * P + (size_t)kSmallE * (P + 1)) * 8;
             const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
-            k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
+            if (P <= kSmallP && small_smem <= kSmallSmem) {
+                static std::once_flag attr;
+                std::call_once(attr, [] { cudaFuncSetAttribute(k_contract_small, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmallSmem); });
+                k_contract_small<<<(unsigned)((g->nelem + kSmallE - 1) / kSmallE), kSmallE, small_smem, ctx->x->stream>>>(
+                    kp, g->orient.as<int32_t>(), g->norient);
+            } else {
+                dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
+                if (grid.y > 65535)
+                    fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
+                k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
+            }
             kstat_stop(ctx, kt);
             cuda_check(cudaGetLastError(), "k_contract_fp64");
             ctx->launches++;
         }
         gi++;
     }
-    cuda_check(cudaEventRecord(ctx->x->evpool[2], ctx->x->stream), "cudaEventRecord");
+    record_event(ctx, ctx->x->evpool[2]);
     C.release();
     {
         int64_t vb = 0;
@@ -1432,51 +1454,169 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     }
 }
 
-// Step 4 on the current execution state's stream: A/D values (or the dense
-// right-hand side) from the element values through the resident pattern.
-void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::vector<Segment>& segs, bool rhs, const double* vals,
-                       double* Avals, double* Dvals)
+// CSR value kernel: -1 = chosen per pattern by timing both (default),
+// 0 = streaming warps (SLGPU_ROW_KERNEL=stream), 1 = one warp per row
+// (SLGPU_ROW_KERNEL=warp).
+static int row_kernel_forced()
+{
+    static const int k = [] {
+        const char* v = std::getenv("SLGPU_ROW_KERNEL");
+        if (v != nullptr && std::strcmp(v, "warp") == 0)
+            return 1;
+        if (v != nullptr && std::strcmp(v, "stream") == 0)
+            return 0;
+        return -1;
+    }();
+    return k;
+}
+
+std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs)
 {
     std::vector<RowSeg> rsegs(segs.size());
+    size_t s = 0;
+    for (auto& g : M.groups)
+        for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
+    for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
+    return rsegs;
+}
+
+namespace {
+// Launch shape of the streaming value kernel for a pattern and segment widths.
+struct StreamLaunch {
+    RowStreamParams sp{};
+    size_t smem = 0;
+    bool ok = false;
+    unsigned grid = 0;
+    void (*kern)(RowStreamParams) = nullptr;
+};
+
+StreamLaunch stream_launch(Ctx* ctx, const RowParams& rp, const std::vector<RowSeg>& rsegs)
+{
+    StreamLaunch L;
+    int wmax = 1;
+    for (const RowSeg& sg : rsegs) wmax = std::max(wmax, (int)sg.width);
+    RowStreamParams& sp = L.sp;
+    const int ring = wmax <= 32 ? 16 : 8;
+    sp.r = rp;
+    sp.vw = (wmax + 2 + 1) & ~1;
+    sp.sw = (wmax + 15 + 7) & ~7;
+    sp.lpad = (rp.lmax + 1) & ~1;
+    sp.rows_per_chunk = 31;  // its 32 row bounds fit one per lane
+    sp.nchunks = (rp.nrows + sp.rows_per_chunk - 1) / sp.rows_per_chunk;
+    L.smem = row_stream_warp_bytes(ring, sp.vw, sp.sw, sp.lpad) * kStreamWarps;
+    if (wmax > 64 || L.smem > 227 * 1024)
+        return L;
+    L.kern = ring == 16 ? k_row_stream<16> : k_row_stream<8>;
+    // Occupancy by ring depth and shared memory size; the kernels' shared
+    // memory limit only ever grows (launches on other streams may use a
+    // larger one).
+    static std::mutex occ_mu;
+    static std::map<std::pair<int, size_t>, int> blocks_per_sm;
+    static size_t attr_max = 48 * 1024;
+    int nblk = 1;
     {
-        size_t s = 0;
-        for (auto& g : M.groups)
-            for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
-        for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
-    }
-    DevBuf drsegs;
-    upload_staged(ctx, drsegs, rsegs.data(), rsegs.size() * sizeof(RowSeg));
-    if (P.nA > 0) {
-        RowParams rp{};
-        rp.inc_ptr = P.inc_ptr.as<uint32_t>();
-        rp.inc = P.inc.as<unsigned long long>();
-        rp.segs = drsegs.as<RowSeg>();
-        rp.slotmap = P.slotmap.as<int16_t>();
-        rp.vals = vals;
-        rp.Arows = P.Arows.as<uint32_t>();
-        rp.Drows = P.Drows.as<uint32_t>();
-        rp.nrows = P.nA;
-        rp.lmax = std::max(1, P.lmax);
-        rp.Avals = Avals;
-        rp.Dvals = rhs ? nullptr : Dvals;
-        rp.dense = rhs ? Avals : nullptr;
-        const size_t per_warp = (size_t)rp.lmax * 8;
-        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
-        size_t smem = per_warp * wpb;
-        if (smem > 48 * 1024) {
-            if (smem > 227 * 1024)
-                fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
-            cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        std::lock_guard<std::mutex> lk(occ_mu);
+        if (L.smem > attr_max) {
+            for (auto k : {k_row_stream<16>, k_row_stream<8>})
+                cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem), "smem attribute");
+            attr_max = L.smem;
         }
-        // Bytes: kept element values and their slots, incidences, row
-        // pointers read; A and D values written.
-        const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
-        const int kt = kstat_start(ctx, "row_values", rbytes);
-        k_row_values<<<grid_for(P.nA, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
-        kstat_stop(ctx, kt);
-        cuda_check(cudaGetLastError(), "k_row_values");
-        ctx->launches++;
+        const auto key = std::make_pair(ring, L.smem);
+        auto bi = blocks_per_sm.find(key);
+        if (bi == blocks_per_sm.end()) {
+            int nb = 0;
+            cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, L.kern, kStreamWarps * 32, L.smem), "occupancy");
+            bi = blocks_per_sm.emplace(key, std::max(nb, 1)).first;
+        }
+        nblk = bi->second;
     }
+    sp.nwarps = std::min<int64_t>(sp.nchunks, (int64_t)std::max(ctx->nsm, 1) * nblk * kStreamWarps);
+    L.grid = (unsigned)((sp.nwarps + kStreamWarps - 1) / kStreamWarps);
+    L.ok = sp.nwarps > 0;
+    return L;
+}
+
+void launch_stream_rows(Ctx* ctx, const StreamLaunch& L)
+{
+    L.kern<<<L.grid, kStreamWarps * 32, L.smem, ctx->x->stream>>>(L.sp);
+    cuda_check(cudaGetLastError(), "k_row_stream");
+    ctx->launches++;
+}
+
+void launch_warp_rows(Ctx* ctx, const RowParams& rp)
+{
+    const size_t per_warp = (size_t)rp.lmax * 8;
+    int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
+    size_t smem = per_warp * wpb;
+    if (smem > 48 * 1024) {
+        if (smem > 227 * 1024)
+            fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
+        cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    }
+    k_row_values<<<grid_for(rp.nrows, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
+    cuda_check(cudaGetLastError(), "k_row_values");
+    ctx->launches++;
+}
+}  // namespace
+
+// Step 4 on the current execution state's stream: A/D values (or the dense
+// right-hand side) from the element values through the resident pattern.
+// `dsegs` is the device copy of `rsegs`.  The two value kernels add in the
+// same order (bit-identical results); the first process() of a pattern on
+// the context's own stream times both on its data and keeps the faster one
+// for the pattern.
+void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<RowSeg>& rsegs, const RowSeg* dsegs, bool rhs,
+                       const double* vals, double* Avals, double* Dvals)
+{
+    if (P.nA <= 0)
+        return;
+    RowParams rp{};
+    rp.inc_ptr = P.inc_ptr.as<uint32_t>();
+    rp.inc = P.inc.as<unsigned long long>();
+    rp.segs = dsegs;
+    rp.slotmap = P.slotmap.as<int16_t>();
+    rp.vals = vals;
+    rp.Arows = P.Arows.as<uint32_t>();
+    rp.Drows = P.Drows.as<uint32_t>();
+    rp.nrows = P.nA;
+    rp.lmax = std::max(1, P.lmax);
+    rp.Avals = Avals;
+    rp.Dvals = rhs ? nullptr : Dvals;
+    rp.dense = rhs ? Avals : nullptr;
+    // Bytes: kept element values and their slots, incidences, row
+    // pointers read; A and D values written.
+    const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
+    const StreamLaunch sl = stream_launch(ctx, rp, rsegs);
+    int choice = row_kernel_forced();
+    if (!sl.ok)
+        choice = 1;
+    else if (choice < 0)
+        choice = P.row_kernel;
+    if (choice < 0 && !ctx->x->capturing && ctx->x == &ctx->main) {
+        // Both, timed on this call's data (their outputs are identical).
+        cudaEvent_t ev[3];
+        for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        const int kt = kstat_start(ctx, "row_values", 2 * rbytes);
+        cuda_check(cudaEventRecord(ev[0], ctx->x->stream), "cudaEventRecord");
+        launch_stream_rows(ctx, sl);
+        cuda_check(cudaEventRecord(ev[1], ctx->x->stream), "cudaEventRecord");
+        launch_warp_rows(ctx, rp);
+        cuda_check(cudaEventRecord(ev[2], ctx->x->stream), "cudaEventRecord");
+        kstat_stop(ctx, kt);
+        cuda_check(cudaEventSynchronize(ev[2]), "sync");
+        float ts = 0, tw = 0;
+        cudaEventElapsedTime(&ts, ev[0], ev[1]);
+        cudaEventElapsedTime(&tw, ev[1], ev[2]);
+        for (auto& e : ev) cudaEventDestroy(e);
+        P.row_kernel = ts < tw ? 0 : 1;
+        return;
+    }
+    const int kt = kstat_start(ctx, "row_values", rbytes);
+    if (choice == 0)
+        launch_stream_rows(ctx, sl);
+    else
+        launch_warp_rows(ctx, rp);
+    kstat_stop(ctx, kt);
 }
 
 // Everything the value path creates lazily (split-precision row slices,
@@ -1501,6 +1641,131 @@ void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
         x.split_colexp.alloc(ctx, expbytes);
     if (x.split_error.empty())
         x.split_error.alloc(ctx, 16);
+}
+
+ValueGraph::~ValueGraph()
+{
+    if (exec != nullptr)
+        cudaGraphExecDestroy(exec);
+    if (graph != nullptr)
+        cudaGraphDestroy(graph);
+    for (char* p : stage) cudaFreeHost(p);
+}
+
+// What the value path's launches take from host state: device pointers,
+// kernel handles and sizes.  Contents that can change in place (per-element
+// data, field data, term scales, the destination multipliers of the resident
+// segment array, node coordinates) are read by the kernels at run time and
+// are not part of it.  A group's own buffers and sizes are fixed at creation,
+// so its serial number stands for them.
+static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int precision, bool rhs, const Pattern& P,
+                                             const std::vector<Segment>& segs)
+{
+    std::vector<uint64_t> s;
+    auto u = [&](uint64_t v) { s.push_back(v); };
+    auto p = [&](const void* q) { s.push_back((uint64_t)(uintptr_t)q); };
+    const Exec& x = *ctx->x;
+    u((uint64_t)precision);
+    u(rhs ? 1 : 0);
+    p(&P);
+    u((uint64_t)P.row_kernel + 1);
+    u((uint64_t)M.ndofs);
+    p(M.vals.as<void>());
+    p(M.Avals.as<void>());
+    p(M.Dvals.as<void>());
+    p(M.rsegs_dev.as<void>());
+    u((uint64_t)split_tile_width());
+    u((uint64_t)ctx->nsm);
+    u(ctx->jit_broken ? 1 : 0);
+    p(x.split_cols.as<void>());
+    p(x.split_colexp.as<void>());
+    p(x.split_error.as<void>());
+    for (auto& gp : M.groups) {
+        const GroupDev& g = *gp;
+        u(g.serial);
+        p(g.jit_kernel);
+        u(g.jit_members.size());
+        for (uint64_t id : g.jit_members) u(id);
+        for (int t = 0; t < 2; t++) {
+            p(g.split[t] ? g.split[t]->slices.as<void>() : nullptr);
+            p(g.split[t] ? g.split[t]->rowexp.as<void>() : nullptr);
+        }
+        auto mi = ctx->meshes.find(g.mesh);
+        if (mi == ctx->meshes.end()) {
+            u(~0ull);
+            continue;
+        }
+        p(mi->second.xyz.as<void>());
+        auto ti = mi->second.types.find(g.elemtype);
+        p(ti == mi->second.types.end() ? nullptr : ti->second.conn.as<void>());
+    }
+    for (auto& f : M.frags) {
+        p(f->vals.as<void>());
+        u((uint64_t)f->nr);
+        u((uint64_t)f->nc);
+    }
+    for (const Segment& sg : segs) {
+        u((uint64_t)sg.coo_base);
+        u((uint64_t)sg.val_base);
+    }
+    return s;
+}
+
+// Captures the value path into M.vgraph.  Copies the captured launches make
+// from page-locked staging read blocks that the graph owns.  A capture the
+// driver refuses leaves the matrix ungraphed (graph_failed).
+static void capture_value_graph(Ctx* ctx, Matrix& M, int precision, bool rhs, const std::vector<int64_t>& gvb, std::vector<uint64_t> sig,
+                                double* Av, double* Dv)
+{
+    Exec& x = *ctx->x;
+    char* save_stage = x.stage;
+    const size_t save_bytes = x.stage_bytes, save_used = x.stage_used, nold = x.stage_old.size();
+    x.stage = nullptr;
+    x.stage_bytes = x.stage_used = 0;
+    auto G = std::make_unique<ValueGraph>();
+    const int64_t l0 = ctx->launches;
+    x.kev_tag.clear();
+    cuda_check(cudaStreamBeginCapture(x.stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    x.capturing = true;
+    std::string err;
+    try {
+        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
+        ev_record(ctx, 2);
+        launch_row_values(ctx, M, *M.pattern, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
+    } catch (const std::exception& e) {
+        err = e.what();
+    }
+    x.capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(x.stream, &graph);
+    // Staging blocks used while capturing belong to the graph.
+    if (x.stage != nullptr)
+        G->stage.push_back(x.stage);
+    for (size_t i = nold; i < x.stage_old.size(); i++) G->stage.push_back(x.stage_old[i]);
+    x.stage_old.resize(nold);
+    x.stage = save_stage;
+    x.stage_bytes = save_bytes;
+    x.stage_used = save_used;
+    const int64_t nlaunch = ctx->launches - l0;
+    ctx->launches = l0;
+    if (err.empty() && ec == cudaSuccess && graph != nullptr) {
+        G->graph = graph;
+        if (cudaGraphInstantiate(&G->exec, graph, 0) == cudaSuccess) {
+            G->kev_tag = x.kev_tag;
+            G->launches = nlaunch;
+            G->sig = std::move(sig);
+            G->pattern = M.pattern;
+            M.vgraph = std::move(G);
+            return;
+        }
+        G->exec = nullptr;
+    } else if (graph != nullptr) {
+        cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+    M.graph_failed = true;
+    M.vgraph.reset();
+    x.kev_tag.clear();
 }
 
 static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, int precision, bool rhs, slgpu_csr_info* info)
@@ -1559,26 +1824,73 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         key1 = mix64(key1 + f->addr_hash[1]);
     }
 
-    // 1+2: geometry, coefficients and contraction into the value buffer.
-    if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
-        M.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
-    launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
-    ev_record(ctx, 1);
-
-    // 3: pattern.
+    // 3: pattern (symbolic; cached while addresses and constraints are unchanged).
     bool reused = false;
     M.pattern = get_pattern(ctx, M, segs, dconstr, rhs, key0, key1, &reused);
     Pattern& P = *M.pattern;
-    ev_record(ctx, 2);
+    ev_record(ctx, 1);
 
-    // 4: values, one warp per row.
+    // Output buffers, kept between calls while their sizes are unchanged.
+    if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
+        M.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
+    auto keep_or_alloc = [&](DevBuf& b, int64_t n) {
+        const size_t want = (((size_t)std::max<int64_t>(n, 1) * 8) + 255) & ~size_t(255);
+        if (b.bytes() != want)
+            b.alloc(ctx, want);
+    };
     if (rhs) {
-        M.Avals.alloc(ctx, (size_t)std::max<int64_t>(M.ndofs, 1) * 8);
+        keep_or_alloc(M.Avals, M.ndofs);
     } else {
-        M.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
-        M.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
+        keep_or_alloc(M.Avals, P.nnzA);
+        keep_or_alloc(M.Dvals, P.nnzD);
     }
-    launch_row_values(ctx, M, P, segs, rhs, M.vals.as<double>(), M.Avals.as<double>(), rhs ? nullptr : M.Dvals.as<double>());
+    double* Av = M.Avals.as<double>();
+    double* Dv = rhs ? nullptr : M.Dvals.as<double>();
+    // Resident segment array of the value kernels (updated in place while its
+    // size is unchanged, so that captured graphs stay valid).
+    {
+        std::vector<RowSeg> rsegs = row_segments(M, segs);
+        const size_t nb = rsegs.size() * sizeof(RowSeg);
+        const bool same = rsegs.size() == M.rsegs_host.size() && std::memcmp(rsegs.data(), M.rsegs_host.data(), nb) == 0;
+        if (!same || M.rsegs_dev.empty()) {
+            if (M.rsegs_dev.empty() || M.rsegs_dev.bytes() < std::max<size_t>(nb, 16))
+                M.rsegs_dev.alloc(ctx, std::max<size_t>(nb, 16));
+            if (nb > 0)
+                upload_staged_into(ctx, M.rsegs_dev.as<void>(), rsegs.data(), nb);
+            M.rsegs_host = std::move(rsegs);
+        }
+    }
+
+    // 1+2 (coefficients, contractions into the value buffer) and 4 (CSR
+    // values): replayed from a graph when the launches are the same as last
+    // time's.
+    bool graphed = false;
+    if (ctx->graphs && reused && ctx->x == &ctx->main && !M.graph_failed) {
+        prepare_value_path(ctx, M, precision);
+        std::vector<uint64_t> sig = value_signature(ctx, M, precision, rhs, P, segs);
+        if (!(M.vgraph && M.vgraph->sig == sig)) {
+            M.vgraph.reset();
+            if (M.vsig_prev == sig)
+                capture_value_graph(ctx, M, precision, rhs, gvb, std::move(sig), Av, Dv);
+            else
+                M.vsig_prev = std::move(sig);
+        }
+        if (M.vgraph) {
+            cuda_check(cudaGraphLaunch(M.vgraph->exec, ctx->x->stream), "cudaGraphLaunch");
+            ctx->x->kev_tag = M.vgraph->kev_tag;
+            ctx->launches += M.vgraph->launches;
+            ctx->graph_launches++;
+            graphed = true;
+        }
+    } else {
+        M.vgraph.reset();
+        M.vsig_prev.clear();
+    }
+    if (!graphed) {
+        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
+        ev_record(ctx, 2);
+        launch_row_values(ctx, M, P, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
+    }
     ev_record(ctx, 3);
     cuda_check(cudaEventSynchronize(ctx->x->ev[3]), "sync");
     kstat_collect(ctx);
@@ -1593,7 +1905,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     cudaEventElapsedTime(&contract_ms, ctx->x->evpool[1], ctx->x->evpool[2]);
     ctx->x->timings[0] = coef_ms;
     ctx->x->timings[1] = contract_ms;
-    ctx->x->timings[2] = ev_ms(ctx, 1, 2);
+    ctx->x->timings[2] = ev_ms(ctx, 0, 1);
     ctx->x->timings[3] = ev_ms(ctx, 2, 3);
     ctx->x->timings[4] = ev_ms(ctx, 0, 3);
     if (info != nullptr) {
@@ -1674,6 +1986,8 @@ int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** 
         }
         for (auto& e : ctx->x->ev) cudaEventCreate(&e);
         cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+        const char* gv = std::getenv("SLGPU_GRAPHS");
+        ctx->graphs = !(gv != nullptr && std::strcmp(gv, "0") == 0);
         // Keep freed blocks in the stream-ordered pool between assemblies.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -1733,8 +2047,12 @@ int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double*
         if (nnodes < 0 || (nnodes > 0 && xyz == nullptr))
             fail(SLGPU_E_ARG, "invalid node array");
         MeshDev& m = ctx->meshes[mesh];
+        const bool same = !ctx->record_only && m.nnodes == nnodes && !m.xyz.empty();
         m.nnodes = nnodes;
-        if (!ctx->record_only)
+        if (same && nnodes > 0)  // in place: buffers (and captured graphs) stay valid
+            cuda_check(cudaMemcpyAsync(m.xyz.as<void>(), xyz, (size_t)3 * nnodes * 8, cudaMemcpyHostToDevice, ctx->x->stream),
+                       "upload nodes");
+        else if (!ctx->record_only)
             upload(ctx, m.xyz, xyz, (size_t)3 * nnodes);
         else
             m.hxyz.assign(xyz, xyz + 3 * nnodes);
@@ -1922,6 +2240,20 @@ int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const 
 
 int64_t slgpu_kernel_launches(const slgpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int slgpu_ctx_set_graphs(slgpu_ctx* ctx, int enable)
+{
+    return guarded(ctx, [&] {
+        ctx->graphs = enable != 0;
+        if (!ctx->graphs)
+            for (auto& [h, m] : ctx->matrices) {
+                m->vgraph.reset();
+                m->vsig_prev.clear();
+            }
+    });
+}
+
+int64_t slgpu_graph_launches(const slgpu_ctx* ctx) { return ctx ? ctx->graph_launches : 0; }
+
 int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_t len)
 {
     int st = guarded(ctx, [&] {
@@ -1929,7 +2261,7 @@ int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_
         size_t k = 0;
         while (k < M.groups.size()) {
             size_t k1 = k + 1;
-            while (k1 < M.groups.size() && M.groups[k1]->geom_hash == M.groups[k]->geom_hash) k1++;
+            while (k1 < M.groups.size() && k1 - k < (size_t)kJitBatch && M.groups[k1]->geom_hash == M.groups[k]->geom_hash) k1++;
             std::vector<const GroupDev*> batch;
             for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
             try {

@@ -137,6 +137,7 @@ struct Pattern {
     uint64_t key[2] = {0, 0};
     int64_t ndofs = 0, nA = 0, nD = 0, nnzA = 0, nnzD = 0, ncoo = 0, nvalid = 0, ninc = 0;
     int lmax = 0;          // longest row (A and D entries)
+    int row_kernel = -1;   // CSR value kernel chosen by timing: 0 streaming warps, 1 warp per row, -1 not yet
     DevBuf Arows, Acols, Drows, Dcols;
     DevBuf slotmap;        // int16 [ncoo]: position in the row's [A | D] segment, -1 = dropped
     DevBuf inc_ptr;        // uint32 [nA+1]: incidences of each row
@@ -144,11 +145,39 @@ struct Pattern {
     uint64_t last_use = 0;
 };
 
+// Per COO segment, as the CSR value kernels read it: where its entries
+// values start in the element-value buffer, its destination multiplier and
+// the width of its incidences (ndof of a group, 1 for a raw fragment).
+struct RowSeg {
+    int64_t coo_base;
+    int64_t val_base;
+    double mult;
+    int32_t width, pad;
+};
+
 struct Segment {
     int64_t coo_base;
     int64_t count;
     int64_t val_base;
     double mult;
+};
+
+// The value path of one matrix's process() on a resident pattern
+// (coefficients, contractions, CSR values) captured as one CUDA graph.  It is
+// replayed while `sig` -- every device pointer and host value that the
+// captured launches bake in -- is unchanged.
+struct ValueGraph {
+    std::vector<uint64_t> sig;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char*> stage;  // page-locked blocks read by the graph's copies
+    std::vector<std::pair<std::string, double>> kev_tag;  // kernel-family timers recorded by the graph
+    int64_t launches = 0;                                 // kernels per replay
+    std::shared_ptr<Pattern> pattern;                     // kept resident while the graph exists
+    ValueGraph() = default;
+    ValueGraph(const ValueGraph&) = delete;
+    ValueGraph& operator=(const ValueGraph&) = delete;
+    ~ValueGraph();
 };
 
 struct Matrix {
@@ -160,6 +189,15 @@ struct Matrix {
     DevBuf Avals, Dvals;
     std::vector<uint8_t> rec_constrained;  // record-only
     slgpu_csr_info info{};
+    // Graph of the value path, and the signature of the last ungraphed run
+    // (a graph is captured when two consecutive runs have equal signatures).
+    std::unique_ptr<ValueGraph> vgraph;
+    std::vector<uint64_t> vsig_prev;
+    bool graph_failed = false;  // capture was refused: this matrix runs ungraphed
+    // Segments of the value kernels, resident (replayed graphs read them);
+    // updated in place when multipliers change.
+    std::vector<RowSeg> rsegs_host;
+    DevBuf rsegs_dev;
 };
 
 // Per kernel family: device time (CUDA events around each launch on the
@@ -189,6 +227,7 @@ struct Exec {
     size_t stage_bytes = 0, stage_used = 0;
     std::vector<char*> stage_old;  // outgrown blocks, freed when the state is
     double trace_t = 0;            // host time of the last trace mark (SLGPU_HOST_TRACE)
+    bool capturing = false;        // launches are being captured into a graph
     // Request arena (serving slots): while arena_on, DevBuf::alloc carves
     // buffers from `arena` (bump allocation, reset per request; the slot's
     // previous request has completed) instead of the stream-ordered pool,
@@ -221,6 +260,8 @@ struct Ctx {
     DevBuf constr_dev;
     uint64_t constr_key[2] = {0, 0};
     int64_t launches = 0;              // kernels launched by this context
+    bool graphs = true;                // value-path graphs for process() (slgpu_ctx_set_graphs)
+    int64_t graph_launches = 0;
     uint64_t next_serial = 1;          // group serial numbers
     std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source
     std::vector<cudaLibrary_t> jit_libs;
@@ -242,11 +283,15 @@ struct GroupData {
 std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals);
 void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::vector<int64_t>& gvb, double* vals,
                          const std::vector<GroupData>* ov);
-void launch_row_values(Ctx* ctx, const Matrix& M, const Pattern& P, const std::vector<Segment>& segs, bool rhs, const double* vals,
-                       double* Avals, double* Dvals);
+std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs);
+void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<RowSeg>& rsegs, const RowSeg* dsegs, bool rhs,
+                       const double* vals, double* Avals, double* Dvals);
 // Copies `bytes` from host memory to a new device buffer through the current
 // execution state's page-locked staging (asynchronous, stream-ordered).
 void upload_staged(Ctx* ctx, DevBuf& buf, const void* src, size_t bytes);
+// Copies `bytes` from host memory to existing device memory through the
+// current execution state's page-locked staging (asynchronous, stream-ordered).
+void upload_staged_into(Ctx* ctx, void* dst, const void* src, size_t bytes);
 void stage_reset(Exec& x);
 void stage_free(Exec& x);
 // Allocations that outlive the current request (per-state scratch kept
@@ -258,6 +303,9 @@ struct ArenaPause {
     ~ArenaPause() { x.arena_on = was; }
 };
 int kstat_start(Ctx* ctx, const char* family, double work);
+// Records an event on the current execution state's stream (as an event
+// node of the graph when the stream is being captured).
+void record_event(Ctx* ctx, cudaEvent_t e);
 // Host-side launch tracing (SLGPU_HOST_TRACE=1): htrace_begin starts the
 // clock of the current execution state; htrace_mark adds the host time since
 // the previous mark to `label`.  The totals are printed to stderr at exit.

@@ -250,6 +250,67 @@ __global__ void __launch_bounds__(256) k_contract_fp64(ContractParams p)
     }
 }
 
+// FP64 contraction for small element matrices (ntf*ndof <= 32): one thread
+// per element, M of every orientation in shared memory.  Each output is
+// accumulated in (term, Gauss point) order with the same fma operands as
+// k_contract_fp64, so both kernels give the same values.  The block's outputs
+// are staged in shared memory and stored as contiguous [e][p] rows.
+constexpr int kSmallE = 128;
+constexpr int kSmallP = 32;
+constexpr int kSmallSmem = 96 * 1024;
+
+__global__ void __launch_bounds__(kSmallE) k_contract_small(ContractParams p, const int32_t* __restrict__ orient, int norient)
+{
+    extern __shared__ double sm_small[];
+    const int P = p.ntf * p.ndof, Q = p.nterms * p.ngp;
+    double* Ms = sm_small;                             // [norient][Q][P]
+    double* Os = sm_small + (int64_t)norient * Q * P;  // [kSmallE][P + 1]
+    for (int idx = threadIdx.x; idx < norient * Q * P; idx += blockDim.x) {
+        const int o = idx / (Q * P), rem = idx - o * (Q * P), q = rem / P, pe = rem - q * P;
+        const int t = q / p.ngp, g = q - t * p.ngp;
+        const int i = pe / p.ndof, j = pe - i * p.ndof;
+        const double tv = p.tables[p.tab_off[p.term_tf[t]] + ((int64_t)o * p.ntf + i) * p.ngp + g];
+        const int dt = p.term_dof[t];
+        const double dv = dt >= 0 ? p.tables[p.tab_off[dt] + ((int64_t)o * p.ndof + j) * p.ngp + g] : 1.0;
+        Ms[idx] = tv * dv;
+    }
+    __syncthreads();
+    const int64_t e0 = (int64_t)blockIdx.x * kSmallE;
+    const int64_t e = e0 + threadIdx.x;
+    double acc[kSmallP];
+#pragma unroll
+    for (int pe = 0; pe < kSmallP; pe++) acc[pe] = 0.0;
+    if (e < p.nelem) {
+        const double* M = Ms + (int64_t)orient[e] * Q * P;
+        // Coefficients eight at a time, all loads issued before their use.
+        for (int q0 = 0; q0 < Q; q0 += 8) {
+            double c[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) c[u] = q0 + u < Q ? p.C[(int64_t)(q0 + u) * p.nelem + e] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                if (q0 + u >= Q)
+                    break;
+                const double* Mq = M + (q0 + u) * P;
+#pragma unroll
+                for (int pe = 0; pe < kSmallP; pe++)
+                    if (pe < P)
+                        acc[pe] = fma(Mq[pe], c[u], acc[pe]);
+            }
+        }
+    }
+#pragma unroll
+    for (int pe = 0; pe < kSmallP; pe++)
+        if (pe < P)
+            Os[threadIdx.x * (P + 1) + pe] = acc[pe];
+    __syncthreads();
+    const int ne = (int)min((int64_t)kSmallE, p.nelem - e0);
+    for (int idx = threadIdx.x; idx < ne * P; idx += blockDim.x) {
+        const int ee = idx / P, pe = idx - ee * P;
+        p.out[(e0 + ee) * P + pe] = Os[ee * (P + 1) + pe];
+    }
+}
+
 struct KeyParams {
     const int32_t* tfaddr;
     const int32_t* dofaddr;  // null: right-hand side (column 0)
@@ -557,13 +618,6 @@ __global__ void k_max_rowlen(const uint32_t* Arows, const uint32_t* Drows, int64
     if ((threadIdx.x & 31) == 0)
         atomicMax(out, len);
 }
-
-struct RowSeg {
-    int64_t coo_base;
-    int64_t val_base;
-    double mult;
-    int32_t width, pad;
-};
 
 struct RowParams {
     const uint32_t* inc_ptr;

@@ -156,7 +156,7 @@ void launch(Server& S, Slot& s, Request& r)
 {
     Ctx* ctx = S.ctx;
     const Matrix& M = *r.tmpl;
-    const Pattern& P = *M.pattern;
+    Pattern& P = *M.pattern;
     const double t0 = S.now();
     ctx->x = &s.ex;
     stage_reset(s.ex);
@@ -232,7 +232,10 @@ void launch(Server& S, Slot& s, Request& r)
     const double t2 = S.now();
     r.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
     r.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
-    launch_row_values(ctx, M, P, segs, false, r.vals.as<double>(), r.Avals.as<double>(), r.Dvals.as<double>());
+    const std::vector<RowSeg> rsegs = row_segments(M, segs);
+    DevBuf dsegs;
+    upload_staged(ctx, dsegs, rsegs.data(), rsegs.size() * sizeof(RowSeg));
+    launch_row_values(ctx, M, P, rsegs, dsegs.as<RowSeg>(), false, r.vals.as<double>(), r.Avals.as<double>(), r.Dvals.as<double>());
     r.vals.release();  // stream-ordered: after the value kernel
     double* hA = r.pinned_out ? r.Aout : static_cast<double*>(s.pinned);
     double* hD = r.pinned_out ? r.Dout : static_cast<double*>(s.pinned) + r.nnzA;

@@ -1,0 +1,143 @@
+"""CUDA-graph replay of process() on a resident pattern.
+
+The value path (coefficients, contractions, CSR values) of a matrix is
+captured into a graph on the second process() with unchanged launches and
+replayed afterwards.  Replays must give the same values bit for bit as the
+ungraphed path, also after in-place changes of per-element data, node
+coordinates, term scales and destination multipliers (read by the kernels at
+run time).  Both CSR value kernels (streaming warps, warp per row) must agree
+bit for bit as well.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import _synthetic as S
+from sparselizard_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = abi.Context(0)
+    yield c
+    c.close()
+
+
+def _setup(ctx, rng, mesh_id, grid, ntf, ndof, nterms, ngp1, ndofs):
+    gb, xyz, conn = S.group(rng, nelem_grid=grid, ntf=ntf, ndof=ndof, nterms=nterms, ngp1=ngp1, norient=2, ndests=2,
+                            ndofs=ndofs)
+    g = gb.g
+    g.mesh = mesh_id
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, mesh_id, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, mesh_id, 3, 4, conn.size // 4, abi.i32p(conn)))
+    h = ctypes.c_int()
+    ctx.check(L.slgpu_matrix_create(ctx.h, ndofs, ctypes.byref(h)))
+    ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g), None))
+    con = (rng.random(ndofs) < 0.1).astype(np.uint8)
+    return dict(gb=gb, h=h.value, con=con, xyz=xyz, nelem=g.nelem, nterms=g.nterms, ndests=g.ndests, mesh=mesh_id)
+
+
+def _process(ctx, t, precision):
+    L = ctx.lib
+    info = abi.CsrInfo()
+    ctx.check(L.slgpu_matrix_process(ctx.h, t["h"], t["con"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), precision,
+                                     ctypes.byref(info)))
+    A, D = np.zeros(max(1, info.nnzA)), np.zeros(max(1, info.nnzD))
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, t["h"], abi.f64p(A), abi.f64p(D)))
+    return A[: info.nnzA].copy(), D[: info.nnzD].copy()
+
+
+def _run(ctx, t, precision, graphs, edits):
+    """process() after each edit (a callable or None); returns the values."""
+    ctx.check(ctx.lib.slgpu_ctx_set_graphs(ctx.h, 1 if graphs else 0))
+    out = []
+    for e in edits:
+        if e is not None:
+            e()
+        out.append(_process(ctx, t, precision))
+    return out
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_SPLIT])
+def test_graph_replay_matches_ungraphed(ctx, precision):
+    rng = np.random.Generator(np.random.PCG64(21))
+    t = _setup(ctx, rng, 11 + precision, 60, 9, 9, 4, 3, 3000)
+    L = ctx.lib
+    e1 = rng.lognormal(0.0, 0.4, t["nelem"])
+    e2 = rng.lognormal(0.0, 0.4, t["nelem"])
+    xyz2 = t["xyz"] * 1.01
+    scales = rng.uniform(0.5, 2.0, t["nterms"])
+    mults = rng.uniform(-2.0, 2.0, t["ndests"])
+
+    def set_e(v):
+        return lambda: ctx.check(L.slgpu_matrix_set_elemdata(ctx.h, t["h"], 0, 0, abi.f64p(v)))
+
+    def set_nodes(v):
+        return lambda: ctx.check(L.slgpu_mesh_set_nodes(ctx.h, t["mesh"], v.size // 3, abi.f64p(v)))
+
+    def set_scales(ts, dm):
+        return lambda: ctx.check(L.slgpu_matrix_set_scales(ctx.h, t["h"], 0, abi.f64p(ts) if ts is not None else None,
+                                                           abi.f64p(dm) if dm is not None else None))
+
+    orig_scales = np.zeros(t["nterms"])
+    orig_mults = np.zeros(t["ndests"])
+    ctx.check(L.slgpu_matrix_get_scales(ctx.h, t["h"], 0, abi.f64p(orig_scales), abi.f64p(orig_mults)))
+    edits = [set_e(e1), None, None, set_e(e2), set_nodes(xyz2), set_scales(scales, None), None,
+             set_scales(None, mults), None, set_nodes(t["xyz"]), set_scales(orig_scales, orig_mults)]
+    g0 = L.slgpu_graph_launches(ctx.h)
+    with_graph = _run(ctx, t, precision, True, edits)
+    replays = L.slgpu_graph_launches(ctx.h) - g0
+    without = _run(ctx, t, precision, False, edits)
+    ctx.check(L.slgpu_ctx_set_graphs(ctx.h, 1))
+    assert replays >= 8, f"only {replays} graph replays"
+    for i, ((a, d), (a0, d0)) in enumerate(zip(with_graph, without)):
+        assert np.all(np.isfinite(a)) and np.all(np.isfinite(d)), f"call {i}: non-finite values"
+        assert np.array_equal(a, a0) and np.array_equal(d, d0), f"call {i}: graph != ungraphed"
+    # The edits changed the values (the replays are not stale copies).
+    assert not np.array_equal(with_graph[2][0], with_graph[3][0])
+    assert not np.array_equal(with_graph[3][0], with_graph[4][0])
+    assert not np.array_equal(with_graph[6][0], with_graph[7][0])
+
+
+def test_graph_kernel_stats_and_launch_count(ctx):
+    rng = np.random.Generator(np.random.PCG64(22))
+    t = _setup(ctx, rng, 13, 40, 4, 4, 3, 2, 1200)
+    L = ctx.lib
+    ctx.check(L.slgpu_ctx_set_graphs(ctx.h, 1))
+    for _ in range(3):
+        _process(ctx, t, abi.PREC_FP64)
+    k0 = L.slgpu_kernel_launches(ctx.h)
+    g0 = L.slgpu_graph_launches(ctx.h)
+    _process(ctx, t, abi.PREC_FP64)
+    assert L.slgpu_graph_launches(ctx.h) == g0 + 1
+    # coefficients, contraction, CSR values
+    assert L.slgpu_kernel_launches(ctx.h) - k0 == 3
+    ms, n, w = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+    for fam in ("coefficients", "contract_fp64", "row_values"):
+        ctx.check(L.slgpu_kernel_stats(ctx.h, fam.encode(), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(w)))
+        assert n.value == 1 and ms.value > 0 and w.value > 0, fam
+
+
+def test_value_kernels_agree(tmp_path):
+    """The streaming-warp and warp-per-row CSR value kernels, each forced in a
+    child process, give the same values bit for bit (incidence widths 4, 9
+    and 40)."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    res = {}
+    for k in ("stream", "warp"):
+        out = str(tmp_path / f"{k}.npz")
+        env = dict(os.environ, SLGPU_ROW_KERNEL=k)
+        subprocess.run([sys.executable, os.path.join(here, "_rowkernel_child.py"), out], env=env, check=True, timeout=600)
+        res[k] = np.load(out)
+    for key in res["warp"].files:
+        a, b = res["stream"][key], res["warp"][key]
+        assert np.all(np.isfinite(a)), key
+        assert np.array_equal(a, b), f"{key}: streaming and warp-per-row value kernels differ"
