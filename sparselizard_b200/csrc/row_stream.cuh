@@ -32,17 +32,21 @@ struct RowStreamParams {
     int64_t nwarps;       // warps in the grid (the chunk stride)
 };
 
-struct RowStreamMeta {
+// Decoded incidence: where its values and slots start (16-byte units from
+// the value buffer and the slot map) and how to copy and add them.
+struct RowStreamDesc {
     double mult;
-    int32_t info;  // width | serial << 16 | value shift << 17 | slot shift << 18
-    int32_t pad;
+    uint32_t va16, sa16;  // first 16-byte unit of the values / slots superset
+    uint32_t info;        // width | serial << 7 | value shift << 8 | slot shift << 9 | nv << 12 | ns << 18
+    uint32_t pad;
+    uint64_t pad2;
 };
-
-constexpr int kStreamWarps = 8;
+constexpr int kStreamDescs = 48;  // per warp: decoded incidences (>= ring + 32)
+constexpr int kStreamWarps = 4;
 
 __host__ __device__ constexpr size_t row_stream_warp_bytes(int ring, int vw, int sw, int lpad)
 {
-    return (size_t)ring * 16 + (size_t)ring * vw * 8 + (size_t)ring * sw * 2 + (size_t)lpad * 8;
+    return (size_t)kStreamDescs * sizeof(RowStreamDesc) + (size_t)ring * vw * 8 + (size_t)ring * sw * 2 + (size_t)lpad * 8;
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
@@ -61,6 +65,7 @@ __device__ __forceinline__ void cp_async_wait()
 template <int R>
 __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParams sp)
 {
+    static_assert(kStreamDescs >= R + 32, "descriptor ring too small");
     extern __shared__ __align__(16) unsigned char stream_smem[];
     const RowParams& p = sp.r;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -68,92 +73,95 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
     if (gw >= sp.nwarps)
         return;
     unsigned char* base = stream_smem + (size_t)wib * row_stream_warp_bytes(R, sp.vw, sp.sw, sp.lpad);
-    RowStreamMeta* meta = reinterpret_cast<RowStreamMeta*>(base);
-    double* rv = reinterpret_cast<double*>(base + (size_t)R * 16);
-    int16_t* rs = reinterpret_cast<int16_t*>(base + (size_t)R * 16 + (size_t)R * sp.vw * 8);
-    double* buf = reinterpret_cast<double*>(base + (size_t)R * 16 + (size_t)R * sp.vw * 8 + (size_t)R * sp.sw * 2);
+    RowStreamDesc* desc = reinterpret_cast<RowStreamDesc*>(base);
+    unsigned char* rv = base + (size_t)kStreamDescs * sizeof(RowStreamDesc);
+    unsigned char* rs = rv + (size_t)R * sp.vw * 8;
+    double* buf = reinterpret_cast<double*>(rs + (size_t)R * sp.sw * 2);
+    const unsigned char* vals16 = reinterpret_cast<const unsigned char*>(p.vals);
+    const unsigned char* slots16 = reinterpret_cast<const unsigned char*>(p.slotmap);
+    // The row buffer is kept zero between rows (the write-back clears it).
+    for (int s = lane; s < sp.lpad; s += 32) buf[s] = 0.0;
 
-    // ---- producer state: next incidence to fetch (pk) within chunk pc
+    // ---- producer: decodes incidences 32 at a time (pk), issues copies
     int64_t pc = gw;
     uint32_t pk = 0, pk_end = 0;
-    auto chunk_incidences = [&](int64_t c, uint32_t& a, uint32_t& b) {
+    auto chunk_incidences = [&](int64_t c) {
         const int64_t r0 = c * sp.rows_per_chunk;
         const int64_t r1 = min(r0 + sp.rows_per_chunk, p.nrows);
-        a = p.inc_ptr[r0];
-        b = p.inc_ptr[r1];
+        pk = p.inc_ptr[r0];
+        pk_end = p.inc_ptr[r1];
     };
     bool pdone = pc >= sp.nchunks;
     if (!pdone)
-        chunk_incidences(pc, pk, pk_end);
-    // Decoded headers of incidences hb .. hb+31 (lane l holds hb + l).
-    uint32_t hb = 0;
-    bool hvalid = false;
-    long long h_voff = 0, h_coo = 0;
-    double h_mult = 0.0;
-    int h_info = 0;
-    uint32_t issued = 0, consumed = 0;
+        chunk_incidences(pc);
+    uint32_t decoded = 0, issued = 0, consumed = 0;  // stream sequence numbers
 
-    // Warp-collective: fetches the next incidence of the stream into entry
-    // issued % R (every lane commits one group, possibly empty).  Returns
-    // false at the end of the stream.
-    auto issue_next = [&]() -> bool {
+    auto decode = [&]() -> bool {
         while (!pdone && pk == pk_end) {
             pc += sp.nwarps;
-            hvalid = false;
-            if (pc >= sp.nchunks) {
+            if (pc >= sp.nchunks)
                 pdone = true;
-                break;
-            }
-            chunk_incidences(pc, pk, pk_end);
+            else
+                chunk_incidences(pc);
         }
         if (pdone)
             return false;
-        if (!hvalid || pk >= hb + 32) {
-            hb = pk;
-            hvalid = true;
-            const uint32_t k = hb + lane;
-            if (k < pk_end) {
-                const unsigned long long pkd = p.inc[k];
-                const RowSeg sg = p.segs[(pkd >> 40) & ((1ull << 23) - 1)];
-                h_coo = (long long)(pkd & ((1ull << 40) - 1));
-                h_voff = sg.val_base + (h_coo - sg.coo_base);
-                h_mult = sg.mult;
-                h_info = sg.width | ((pkd >> 63) != 0 ? (1 << 16) : 0);
-            }
+        const uint32_t n = min(32u, pk_end - pk);
+        if ((uint32_t)lane < n) {
+            const unsigned long long pkd = p.inc[pk + lane];
+            const RowSeg sg = p.segs[(pkd >> 40) & ((1ull << 23) - 1)];
+            const long long co = (long long)(pkd & ((1ull << 40) - 1));
+            const long long vo = sg.val_base + (co - sg.coo_base);
+            const int width = sg.width;
+            const uint64_t vbyte = (uint64_t)vo * 8, sbyte = (uint64_t)co * 2;
+            const uint32_t nv = (uint32_t)(((vbyte + (uint64_t)width * 8 + 15) >> 4) - (vbyte >> 4));
+            const uint32_t ns = (uint32_t)(((sbyte + (uint64_t)width * 2 + 15) >> 4) - (sbyte >> 4));
+            RowStreamDesc d;
+            d.mult = sg.mult;
+            d.va16 = (uint32_t)(vbyte >> 4);
+            d.sa16 = (uint32_t)(sbyte >> 4);
+            d.info = (uint32_t)width | ((pkd >> 63) != 0 ? (1u << 7) : 0u) | (uint32_t)((vbyte >> 3) & 1) << 8 |
+                     (uint32_t)((sbyte >> 1) & 7) << 9 | nv << 12 | ns << 18;
+            d.pad = 0;
+            d.pad2 = 0;
+            desc[(decoded + lane) % kStreamDescs] = d;
         }
-        const int src = (int)(pk - hb);
-        const long long vo = __shfl_sync(0xffffffffu, h_voff, src);
-        const long long co = __shfl_sync(0xffffffffu, h_coo, src);
-        const double m = __shfl_sync(0xffffffffu, h_mult, src);
-        const int inf = __shfl_sync(0xffffffffu, h_info, src);
-        const uint32_t e = issued % (uint32_t)R;
-        const int width = inf & 0xffff;
-        const uintptr_t v0 = reinterpret_cast<uintptr_t>(p.vals + vo);
-        const uintptr_t va = v0 & ~uintptr_t(15), vb = (v0 + (uintptr_t)width * 8 + 15) & ~uintptr_t(15);
-        const uintptr_t s0 = reinterpret_cast<uintptr_t>(p.slotmap + co);
-        const uintptr_t sa = s0 & ~uintptr_t(15), sb = (s0 + (uintptr_t)width * 2 + 15) & ~uintptr_t(15);
-        const int nv = (int)((vb - va) >> 4), ns = (int)((sb - sa) >> 4);
-        unsigned char* dv = reinterpret_cast<unsigned char*>(rv + (size_t)e * sp.vw);
-        unsigned char* ds = reinterpret_cast<unsigned char*>(rs + (size_t)e * sp.sw);
+        decoded += n;
+        pk += n;
+        __syncwarp();
+        return true;
+    };
+
+    // Warp-collective: copies incidence `issued` into ring entry issued % R
+    // (every lane commits one group, possibly empty).
+    auto issue = [&]() -> bool {
+        if (issued == decoded && !decode())
+            return false;
+        const RowStreamDesc& d = desc[issued % kStreamDescs];
+        const uint32_t info = d.info;
+        const int nv = (int)((info >> 12) & 63), ns = (int)((info >> 18) & 63);
+        unsigned char* dv = rv + (size_t)(issued % R) * sp.vw * 8;
+        unsigned char* ds = rs + (size_t)(issued % R) * sp.sw * 2;
         for (int i = lane; i < nv + ns; i += 32) {
             if (i < nv)
-                cp_async16(dv + 16 * i, reinterpret_cast<const void*>(va + 16 * (uintptr_t)i));
+                cp_async16(dv + 16 * i, vals16 + 16 * ((uint64_t)d.va16 + i));
             else
-                cp_async16(ds + 16 * (i - nv), reinterpret_cast<const void*>(sa + 16 * (uintptr_t)(i - nv)));
+                cp_async16(ds + 16 * (i - nv), slots16 + 16 * ((uint64_t)d.sa16 + (i - nv)));
         }
         cp_async_commit();
-        if (lane == 0) {
-            meta[e].mult = m;
-            meta[e].info = inf | (int)(((v0 - va) >> 3) << 17) | (int)(((s0 - sa) >> 1) << 18);
-        }
-        pk++;
         issued++;
         return true;
     };
 
     for (int i = 0; i < R; i++)
-        if (!issue_next())
+        if (!issue())
             break;
+    // Entry of the first incidence in place for every lane.
+    if (issued - consumed >= (uint32_t)R)
+        cp_async_wait<R - 1>();
+    else
+        cp_async_wait<0>();
+    __syncwarp();
 
     for (int64_t cc = gw; cc < sp.nchunks; cc += sp.nwarps) {
         const int64_t r0 = cc * sp.rows_per_chunk;
@@ -170,22 +178,16 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
             const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
             const uint32_t k0 = __shfl_sync(0xffffffffu, i_lo, rr), k1 = __shfl_sync(0xffffffffu, i_lo, rr + 1);
             const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
-            for (int s = lane; s < L; s += 32) buf[s] = 0.0;
-            __syncwarp();
             for (uint32_t k = k0; k < k1; k++) {
-                const uint32_t e = consumed % (uint32_t)R;
-                // The oldest of the groups in flight is incidence `consumed`.
-                if (issued - consumed >= (uint32_t)R)
-                    cp_async_wait<R - 1>();
-                else
-                    cp_async_wait<0>();
-                __syncwarp();
-                const double m = meta[e].mult;
-                const int inf = meta[e].info;
-                const int width = inf & 0xffff;
-                const double* v = rv + (size_t)e * sp.vw + ((inf >> 17) & 1);
-                const int16_t* sl = rs + (size_t)e * sp.sw + ((inf >> 18) & 7);
-                if (inf & (1 << 16)) {
+                // Incidence `consumed` is in ring entry consumed % R (waited for
+                // before the barrier that ended the previous step).
+                const RowStreamDesc& d = desc[consumed % kStreamDescs];
+                const uint32_t info = d.info;
+                const double m = d.mult;
+                const int width = (int)(info & 127);
+                const double* v = reinterpret_cast<const double*>(rv + (size_t)(consumed % R) * sp.vw * 8) + ((info >> 8) & 1);
+                const int16_t* sl = reinterpret_cast<const int16_t*>(rs + (size_t)(consumed % R) * sp.sw * 2) + ((info >> 9) & 7);
+                if (info & (1u << 7)) {
                     if (lane == 0)
                         for (int j = 0; j < width; j++) {
                             const int s = sl[j];
@@ -199,20 +201,29 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
                             buf[s] = fma(v[j], m, buf[s]);
                     }
                 }
-                __syncwarp();
                 consumed++;
-                issue_next();
+                // The next incidence's group (the oldest still pending) done.
+                if (issued - consumed >= (uint32_t)(R - 1))
+                    cp_async_wait<R - 2>();
+                else
+                    cp_async_wait<0>();
+                __syncwarp();  // additions ordered, next entry visible, this entry free
+                issue();
             }
             const int64_t r = r0 + rr;
             if (p.dense != nullptr) {
                 if (lane == 0)
                     p.dense[r] = L > 0 ? -buf[0] : 0.0;
+                __syncwarp();
+                for (int s = lane; s < L; s += 32) buf[s] = 0.0;
             } else {
                 for (int s = lane; s < L; s += 32) {
+                    const double x = buf[s];
+                    buf[s] = 0.0;
                     if (s < la)
-                        p.Avals[a0 + s] = buf[s];
+                        p.Avals[a0 + s] = x;
                     else
-                        p.Dvals[d0 + (s - la)] = buf[s];
+                        p.Dvals[d0 + (s - la)] = x;
                 }
             }
             __syncwarp();
