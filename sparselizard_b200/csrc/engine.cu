@@ -1496,17 +1496,18 @@ StreamLaunch stream_launch(Ctx* ctx, const RowParams& rp, const std::vector<RowS
     int wmax = 1;
     for (const RowSeg& sg : rsegs) wmax = std::max(wmax, (int)sg.width);
     RowStreamParams& sp = L.sp;
-    const int ring = wmax <= 32 ? 16 : 8;
+    const bool narrow = wmax <= StreamNarrow::WMAX;
+    const int ring = narrow ? StreamNarrow::R : StreamWide::R;
     sp.r = rp;
-    sp.vw = (wmax + 2 + 1) & ~1;
-    sp.sw = (wmax + 15 + 7) & ~7;
     sp.lpad = (rp.lmax + 1) & ~1;
     sp.rows_per_chunk = 31;  // its 32 row bounds fit one per lane
     sp.nchunks = (rp.nrows + sp.rows_per_chunk - 1) / sp.rows_per_chunk;
-    L.smem = row_stream_warp_bytes(ring, sp.vw, sp.sw, sp.lpad) * kStreamWarps;
-    if (wmax > 64 || L.smem > 227 * 1024)
+    L.smem = (narrow ? row_stream_warp_bytes(StreamNarrow::R, StreamNarrow::VSH, StreamNarrow::SSH, sp.lpad)
+                     : row_stream_warp_bytes(StreamWide::R, StreamWide::VSH, StreamWide::SSH, sp.lpad)) *
+             kStreamWarps;
+    if (wmax > StreamWide::WMAX || L.smem > 227 * 1024)
         return L;
-    L.kern = ring == 16 ? k_row_stream<16> : k_row_stream<8>;
+    L.kern = narrow ? k_row_stream<StreamNarrow> : k_row_stream<StreamWide>;
     // Occupancy by ring depth and shared memory size; the kernels' shared
     // memory limit only ever grows (launches on other streams may use a
     // larger one).
@@ -1517,7 +1518,7 @@ StreamLaunch stream_launch(Ctx* ctx, const RowParams& rp, const std::vector<RowS
     {
         std::lock_guard<std::mutex> lk(occ_mu);
         if (L.smem > attr_max) {
-            for (auto k : {k_row_stream<16>, k_row_stream<8>})
+            for (auto k : {k_row_stream<StreamNarrow>, k_row_stream<StreamWide>})
                 cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem), "smem attribute");
             attr_max = L.smem;
         }

@@ -25,7 +25,6 @@ namespace slgpu {
 
 struct RowStreamParams {
     RowParams r;
-    int vw, sw;           // ring entry capacity: doubles of values, int16 of slots
     int lpad;             // row buffer doubles per warp (>= longest row, even)
     int rows_per_chunk;   // <= 31 (a chunk's row bounds are held one per lane)
     int64_t nchunks;
@@ -41,12 +40,25 @@ struct RowStreamDesc {
     uint32_t pad;
     uint64_t pad2;
 };
-constexpr int kStreamDescs = 48;  // per warp: decoded incidences (>= ring + 32)
+constexpr int kStreamDescs = 64;  // per warp: decoded incidences (>= ring + 32, a power of two)
 constexpr int kStreamWarps = 4;
 
-__host__ __device__ constexpr size_t row_stream_warp_bytes(int ring, int vw, int sw, int lpad)
+// Ring shapes by incidence width: R entries, 2^VSH bytes of values and 2^SSH
+// bytes of slots per entry (at least 8 width + 16 and 2 width + 30: the
+// 16-byte aligned supersets).  Narrow (width <= 30): one copy and one
+// addition per lane and incidence.  Wide (width <= 62): loops over the lanes.
+struct StreamNarrow {
+    static constexpr int R = 16, VSH = 8, SSH = 7, WMAX = 30;
+    static constexpr bool kNarrow = true;
+};
+struct StreamWide {
+    static constexpr int R = 8, VSH = 9, SSH = 8, WMAX = 62;
+    static constexpr bool kNarrow = false;
+};
+
+__host__ __device__ constexpr size_t row_stream_warp_bytes(int ring, int vsh, int ssh, int lpad)
 {
-    return (size_t)kStreamDescs * sizeof(RowStreamDesc) + (size_t)ring * vw * 8 + (size_t)ring * sw * 2 + (size_t)lpad * 8;
+    return (size_t)kStreamDescs * sizeof(RowStreamDesc) + ((size_t)ring << vsh) + ((size_t)ring << ssh) + (size_t)lpad * 8;
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
@@ -62,21 +74,23 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int R>
+template <class Shape>
 __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParams sp)
 {
-    static_assert(kStreamDescs >= R + 32, "descriptor ring too small");
+    constexpr int R = Shape::R, VSH = Shape::VSH, SSH = Shape::SSH;
+    static_assert(kStreamDescs >= R + 32 && (kStreamDescs & (kStreamDescs - 1)) == 0, "descriptor ring");
+    static_assert((R & (R - 1)) == 0, "ring size a power of two");
     extern __shared__ __align__(16) unsigned char stream_smem[];
     const RowParams& p = sp.r;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t gw = (int64_t)blockIdx.x * kStreamWarps + wib;
     if (gw >= sp.nwarps)
         return;
-    unsigned char* base = stream_smem + (size_t)wib * row_stream_warp_bytes(R, sp.vw, sp.sw, sp.lpad);
+    unsigned char* base = stream_smem + (size_t)wib * row_stream_warp_bytes(R, VSH, SSH, sp.lpad);
     RowStreamDesc* desc = reinterpret_cast<RowStreamDesc*>(base);
     unsigned char* rv = base + (size_t)kStreamDescs * sizeof(RowStreamDesc);
-    unsigned char* rs = rv + (size_t)R * sp.vw * 8;
-    double* buf = reinterpret_cast<double*>(rs + (size_t)R * sp.sw * 2);
+    unsigned char* rs = rv + ((size_t)R << VSH);
+    double* buf = reinterpret_cast<double*>(rs + ((size_t)R << SSH));
     const unsigned char* vals16 = reinterpret_cast<const unsigned char*>(p.vals);
     const unsigned char* slots16 = reinterpret_cast<const unsigned char*>(p.slotmap);
     // The row buffer is kept zero between rows (the write-back clears it).
@@ -124,7 +138,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
                      (uint32_t)((sbyte >> 1) & 7) << 9 | nv << 12 | ns << 18;
             d.pad = 0;
             d.pad2 = 0;
-            desc[(decoded + lane) % kStreamDescs] = d;
+            desc[(decoded + lane) & (kStreamDescs - 1)] = d;
         }
         decoded += n;
         pk += n;
@@ -137,16 +151,23 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
     auto issue = [&]() -> bool {
         if (issued == decoded && !decode())
             return false;
-        const RowStreamDesc& d = desc[issued % kStreamDescs];
+        const RowStreamDesc& d = desc[issued & (kStreamDescs - 1)];
         const uint32_t info = d.info;
         const int nv = (int)((info >> 12) & 63), ns = (int)((info >> 18) & 63);
-        unsigned char* dv = rv + (size_t)(issued % R) * sp.vw * 8;
-        unsigned char* ds = rs + (size_t)(issued % R) * sp.sw * 2;
-        for (int i = lane; i < nv + ns; i += 32) {
-            if (i < nv)
-                cp_async16(dv + 16 * i, vals16 + 16 * ((uint64_t)d.va16 + i));
-            else
-                cp_async16(ds + 16 * (i - nv), slots16 + 16 * ((uint64_t)d.sa16 + (i - nv)));
+        unsigned char* dv = rv + ((issued & (R - 1)) << VSH);
+        unsigned char* ds = rs + ((issued & (R - 1)) << SSH);
+        if (Shape::kNarrow) {  // nv + ns <= 24
+            if (lane < nv)
+                cp_async16(dv + 16 * lane, vals16 + 16 * ((uint64_t)d.va16 + lane));
+            else if (lane < nv + ns)
+                cp_async16(ds + 16 * (lane - nv), slots16 + 16 * ((uint64_t)d.sa16 + (lane - nv)));
+        } else {
+            for (int i = lane; i < nv + ns; i += 32) {
+                if (i < nv)
+                    cp_async16(dv + 16 * i, vals16 + 16 * ((uint64_t)d.va16 + i));
+                else
+                    cp_async16(ds + 16 * (i - nv), slots16 + 16 * ((uint64_t)d.sa16 + (i - nv)));
+            }
         }
         cp_async_commit();
         issued++;
@@ -181,12 +202,12 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
             for (uint32_t k = k0; k < k1; k++) {
                 // Incidence `consumed` is in ring entry consumed % R (waited for
                 // before the barrier that ended the previous step).
-                const RowStreamDesc& d = desc[consumed % kStreamDescs];
+                const RowStreamDesc& d = desc[consumed & (kStreamDescs - 1)];
                 const uint32_t info = d.info;
                 const double m = d.mult;
                 const int width = (int)(info & 127);
-                const double* v = reinterpret_cast<const double*>(rv + (size_t)(consumed % R) * sp.vw * 8) + ((info >> 8) & 1);
-                const int16_t* sl = reinterpret_cast<const int16_t*>(rs + (size_t)(consumed % R) * sp.sw * 2) + ((info >> 9) & 7);
+                const double* v = reinterpret_cast<const double*>(rv + ((consumed & (R - 1)) << VSH)) + ((info >> 8) & 1);
+                const int16_t* sl = reinterpret_cast<const int16_t*>(rs + ((consumed & (R - 1)) << SSH)) + ((info >> 9) & 7);
                 if (info & (1u << 7)) {
                     if (lane == 0)
                         for (int j = 0; j < width; j++) {
@@ -194,6 +215,12 @@ __global__ void __launch_bounds__(kStreamWarps * 32) k_row_stream(RowStreamParam
                             if (s >= 0)
                                 buf[s] = fma(v[j], m, buf[s]);
                         }
+                } else if (Shape::kNarrow) {
+                    if (lane < width) {
+                        const int s = sl[lane];
+                        if (s >= 0)
+                            buf[s] = fma(v[lane], m, buf[s]);
+                    }
                 } else {
                     for (int j = lane; j < width; j += 32) {
                         const int s = sl[j];
