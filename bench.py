@@ -273,6 +273,47 @@ def run_reference(args, spec):
     print(json.dumps(line), flush=True)
 
 
+KERNEL_NAMES = {"coefficients": "slgpu_coef (runtime-compiled)", "contract_fp64": "k_contract_fp64 / k_contract_small",
+                "slice_cols": "k_slice_cols", "contract_split": "k_contract_split<7,8>",
+                "contract_split_fp32": "k_contract_split<5,6>", "row_values": "k_row_values / k_row_stream (chosen per pattern)"}
+
+
+def roofline_of(stats, workload, n):
+    """Roofline entry of the kernel family with the most device time in `stats`
+    (CUDA-event times and algorithmic work summed over launches)."""
+    hbm, bf16, peak_kind = peaks()
+    dom = max(stats, key=lambda f: stats[f]["ms"])
+    k = stats[dom]
+    rate = k["work"] / (k["ms"] * 1e-3)
+    if dom.startswith("contract_split"):
+        peak = 2.0 * bf16
+        roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_kind": f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops",
+                "frac": rate / 1e12 / peak}
+    elif dom == "contract_fp64":
+        roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": 40.0, "unit": "TFLOP/s",
+                "peak_kind": "nominal B200 FP64 40 TFLOP/s (FP64 vector and tensor rates are equal; not measured here)",
+                "frac": rate / 1e12 / 40.0}
+    else:
+        roof = {"kernel": KERNEL_NAMES[dom], "bound": "hbm", "achieved": rate / 1e9, "peak": hbm, "unit": "GB/s",
+                "peak_kind": peak_kind, "frac": rate / 1e9 / hbm}
+    roof["ms_per_launch"] = k["ms"] / k["launches"]
+    roof["traffic"] = traffic_per_launch(workload, dom, n, k["launches"])
+    return roof
+
+
+def cpu_baseline(args, spec, rank, world):
+    """Stock sparselizard (oracle/_ref) on the host cores, on the workload's
+    bounded sample size, rank 0 of a one-GPU run only."""
+    if rank != 0 or world != 1 or args.no_cpu_baseline or not os.path.exists(REF_LIB):
+        return None
+    threads = os.cpu_count() or 1
+    cnnz, per = cpu_reference_run(spec, spec["ref_n"], 2, 1, threads)
+    return {"value": cnnz / float(np.mean(per)), "unit": "nnz/s", "cores": threads, "kind": "reference",
+            "sample": f"stock sparselizard generate()+A()+b(), {spec['name']} at n={spec['ref_n']} ({cnnz} nnz), "
+                      f"mean of 2 after 1 warm-up"}
+
+
 def run_ours(args, spec):
     import torch
 
@@ -409,36 +450,9 @@ def run_ours(args, spec):
         prec = prec_run
 
     # ---- roofline of the dominant kernel (per-kernel events over the timed steps)
-    hbm, bf16, peak_kind = peaks()
     ph = phase / args.steps
-    dom = max(stats, key=lambda f: stats[f]["ms"])
-    k = stats[dom]
-    rate = k["work"] / (k["ms"] * 1e-3)
-    kernel_names = {"coefficients": "slgpu_coef (runtime-compiled)", "contract_fp64": "k_contract_fp64",
-                    "slice_cols": "k_slice_cols", "contract_split": "k_contract_split<7,8>",
-                    "contract_split_fp32": "k_contract_split<5,6>", "row_values": "k_row_values"}
-    if dom.startswith("contract_split"):
-        peak = 2.0 * bf16
-        roof = {"kernel": kernel_names[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_kind": f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops",
-                "frac": rate / 1e12 / peak}
-    elif dom == "contract_fp64":
-        roof = {"kernel": kernel_names[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": 40.0, "unit": "TFLOP/s",
-                "peak_kind": "nominal B200 FP64 40 TFLOP/s (FP64 vector and tensor rates are equal; not measured here)",
-                "frac": rate / 1e12 / 40.0}
-    else:
-        roof = {"kernel": kernel_names[dom], "bound": "hbm", "achieved": rate / 1e9, "peak": hbm, "unit": "GB/s",
-                "peak_kind": peak_kind, "frac": rate / 1e9 / hbm}
-    roof["ms_per_launch"] = k["ms"] / k["launches"]
-    roof["traffic"] = traffic_per_launch(args.workload, dom, n, k["launches"])
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
-        threads = os.cpu_count() or 1
-        cnnz, per = cpu_reference_run(spec, spec["ref_n"], 2, 1, threads)
-        cpu = {"value": cnnz / float(np.mean(per)), "unit": "nnz/s", "cores": threads, "kind": "reference",
-               "sample": f"stock sparselizard generate()+A()+b(), {spec['name']} at n={spec['ref_n']} ({cnnz} nnz), "
-                         f"mean of 2 after 1 warm-up"}
+    roof = roofline_of(stats, args.workload, n)
+    cpu = cpu_baseline(args, spec, rank, world)
 
     if rank == 0:
         line = {
@@ -498,13 +512,19 @@ def run_sweep(args, spec):
     nf = spec["sweep"]
     freqs = np.logspace(0.0, 6.0, nf)
     dev, host = np.zeros(nf), np.zeros(nf)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
     for _ in range(args.warmup):
         lib.slz_sweep_run(min(nf, 3), abi.f64p(freqs), prec, abi.f64p(dev), abi.f64p(host))
+    launches0, graphs0 = lib.slgpu_kernel_launches(ctx), lib.slgpu_graph_launches(ctx)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         if lib.slz_sweep_run(nf, abi.f64p(freqs), prec, abi.f64p(dev), abi.f64p(host)) != 0:
             raise RuntimeError("sweep failed: " + lib.slz_last_error().decode(errors="replace"))
         torch.cuda.synchronize()
+    launches = lib.slgpu_kernel_launches(ctx) - launches0
+    graph_replays = lib.slgpu_graph_launches(ctx) - graphs0
+    stats = kernel_stats(lib, ctx, {})  # the last frequency's process()
     dev_s = dev.sum() * 1e-3
     dev_s_max, = allreduce([dev_s], torch.distributed.ReduceOp.MAX) if world > 1 else [dev_s]
     total, = allreduce([float(nnz) * nf], torch.distributed.ReduceOp.SUM) if world > 1 else [float(nnz) * nf]
@@ -519,6 +539,8 @@ def run_sweep(args, spec):
         lib.slz_sweep_values(abi.f64p(A), abi.f64p(D))
     e2e_s = time.perf_counter() - t0
     lib.slz_sweep_release()
+    roof = roofline_of(stats, args.workload, n)
+    cpu = cpu_baseline(args, spec, rank, world)
     if rank == 0:
         line = {
             "metric": "assembled_nnz_per_s", "value": total / dev_s_max, "unit": "nnz/s", "n_gpus": world, "steps": nf,
@@ -528,6 +550,11 @@ def run_sweep(args, spec):
                        "prepare_s": prep_s, "parallelism": f"replicas{world}", "l2": "inputs larger than L2"},
             "e2e": {"value": total / e2e_s, "unit": "nnz/s", "ms_per_step": e2e_s * 1e3 / nf, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 8 * nnz},
+            "kernels_last_frequency": stats,
+            "gpu_launches": int(launches),
+            "graph_replays": int(graph_replays),
+            "roofline": roof,
+            "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
