@@ -1544,8 +1544,13 @@ void launch_stream_rows(Ctx* ctx, const StreamLaunch& L)
     ctx->launches++;
 }
 
-void launch_warp_rows(Ctx* ctx, const RowParams& rp)
+void launch_warp_rows(Ctx* ctx, RowParams rp)
 {
+    // Consecutive rows per warp: up to kRowsPerWarp (the row buffer stays
+    // clean between them), fewer when the rows are too few to fill the
+    // device with about 48 warps per multiprocessor.
+    const int64_t target = (int64_t)std::max(ctx->nsm, 1) * 48;
+    rp.rows_per_warp = (int)std::min<int64_t>(kRowsPerWarp, std::max<int64_t>(1, rp.nrows / target));
     const size_t per_warp = (size_t)rp.lmax * 8;
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / per_warp));
     size_t smem = per_warp * wpb;
@@ -1554,7 +1559,7 @@ void launch_warp_rows(Ctx* ctx, const RowParams& rp)
             fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
         cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
     }
-    k_row_values<<<grid_for(rp.nrows, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
+    k_row_values<<<grid_for((rp.nrows + rp.rows_per_warp - 1) / rp.rows_per_warp, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_row_values");
     ctx->launches++;
 }

@@ -632,6 +632,7 @@ struct RowParams {
     double* Avals;
     double* Dvals;
     double* dense;  // right-hand side: dense[row] = -value (Avals unused)
+    int rows_per_warp;  // k_row_values: consecutive rows per warp (1 .. kRowsPerWarp)
 };
 
 // CSR values, one warp per row: the row's incidences are visited in a fixed
@@ -668,79 +669,107 @@ __device__ __forceinline__ void row_add_generic(double* buf, int width, double m
     }
 }
 
-__global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
+// Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
+constexpr int kRowsPerWarp = 31;
+
+__global__ void __launch_bounds__(256, 3) k_row_values(RowParams p)
 {
     extern __shared__ double rowbuf[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-    if (r >= p.nrows)
+    const int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * p.rows_per_warp;
+    if (r0 >= p.nrows)
         return;
+    const int nr = (int)min((int64_t)p.rows_per_warp, p.nrows - r0);
     double* buf = rowbuf + (int64_t)warp * p.lmax;
-    const int la = (int)(p.Arows[r + 1] - p.Arows[r]);
-    const int ld = p.Drows ? (int)(p.Drows[r + 1] - p.Drows[r]) : 0;
-    const int L = la + ld;
-    for (int s = lane; s < L; s += 32) buf[s] = 0.0;
+    // The row buffer is kept zero between rows (the write-back clears it).
+    for (int s = lane; s < p.lmax; s += 32) buf[s] = 0.0;
+    // Row bounds of the warp's rows, one per lane (lane nr: the end).
+    uint32_t a_lo = 0, d_lo = 0, i_lo = 0;
+    if (lane <= nr) {
+        a_lo = p.Arows[r0 + lane];
+        d_lo = p.Drows ? p.Drows[r0 + lane] : 0u;
+        i_lo = p.inc_ptr[r0 + lane];
+    }
     __syncwarp();
-    const uint32_t k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
     constexpr int kGeneric = 1 << 17, kSerial = 1 << 16;
-    for (uint32_t kb = k0; kb < k1; kb += 32) {
-        const int nkb = (int)min(32u, k1 - kb);
-        long long voff = 0, coo = 0;
-        double mult = 0.0;
-        int info = 0;  // width | kSerial | kGeneric
-        if (lane < nkb) {
-            const unsigned long long pk = p.inc[kb + lane];
-            const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-            coo = (long long)(pk & ((1ull << 40) - 1));
-            voff = sg.val_base + (coo - sg.coo_base);
-            mult = sg.mult;
-            const bool serial = (pk >> 63) != 0;
-            info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
-        }
-        for (int u = 0; u < nkb; u += kRowBatch) {
-            double val[kRowBatch];
-            int slot[kRowBatch];
-#pragma unroll
-            for (int x = 0; x < kRowBatch; x++) {
-                const int src = (u + x) & 31;
-                const long long vo = __shfl_sync(0xffffffffu, voff, src);
-                const long long co = __shfl_sync(0xffffffffu, coo, src);
-                const int inf = __shfl_sync(0xffffffffu, info, src);
-                slot[x] = -1;
-                val[x] = 0.0;
-                if (u + x < nkb && !(inf & kGeneric) && lane < (inf & 0xffff)) {
-                    slot[x] = p.slotmap[co + lane];
-                    val[x] = p.vals[vo + lane];
-                }
+    for (int rr = 0; rr < nr; rr++) {
+        const uint32_t a0 = __shfl_sync(0xffffffffu, a_lo, rr), a1 = __shfl_sync(0xffffffffu, a_lo, rr + 1);
+        const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
+        const uint32_t k0 = __shfl_sync(0xffffffffu, i_lo, rr), k1 = __shfl_sync(0xffffffffu, i_lo, rr + 1);
+        const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
+        for (uint32_t kb = k0; kb < k1; kb += 32) {
+            const int nkb = (int)min(32u, k1 - kb);
+            // Lane l decodes incidence kb + l.  Value and COO offsets fit 32
+            // bits (fewer than 2^32 COO entries per matrix).
+            uint32_t voff = 0, coo = 0;
+            double mult = 0.0;
+            int info = 0;  // width | kSerial | kGeneric
+            if (lane < nkb) {
+                const unsigned long long pk = p.inc[kb + lane];
+                const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+                coo = (uint32_t)(pk & ((1ull << 40) - 1));
+                voff = (uint32_t)(sg.val_base + ((long long)coo - sg.coo_base));
+                mult = sg.mult;
+                const bool serial = (pk >> 63) != 0;
+                info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
             }
+            if (!__any_sync(0xffffffffu, (info & kGeneric) != 0)) {
+                // Batches of kRowBatch incidences: every load issued before
+                // the ordered additions.
+                for (int u = 0; u < nkb; u += kRowBatch) {
+                    double val[kRowBatch];
+                    int slot[kRowBatch];
 #pragma unroll
-            for (int x = 0; x < kRowBatch; x++) {
-                if (u + x < nkb) {
-                    const int src = (u + x) & 31;
-                    const double m = __shfl_sync(0xffffffffu, mult, src);
-                    const int inf = __shfl_sync(0xffffffffu, info, src);
-                    if (inf & kGeneric) {
-                        const long long vo = __shfl_sync(0xffffffffu, voff, src);
-                        const long long co = __shfl_sync(0xffffffffu, coo, src);
-                        row_add_generic(buf, inf & 0xffff, m, p.vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
-                    } else if (slot[x] >= 0) {
-                        buf[slot[x]] = fma(val[x], m, buf[slot[x]]);
+                    for (int x = 0; x < kRowBatch; x++) {
+                        const int src = (u + x) & 31;
+                        const uint32_t vo = __shfl_sync(0xffffffffu, voff, src);
+                        const uint32_t co = __shfl_sync(0xffffffffu, coo, src);
+                        const int inf = __shfl_sync(0xffffffffu, info, src);
+                        slot[x] = -1;
+                        val[x] = 0.0;
+                        if (u + x < nkb && lane < (inf & 0xffff)) {
+                            slot[x] = p.slotmap[(uint64_t)co + lane];
+                            val[x] = p.vals[(uint64_t)vo + lane];
+                        }
+                    }
+#pragma unroll
+                    for (int x = 0; x < kRowBatch; x++) {
+                        if (u + x < nkb) {
+                            const double m = __shfl_sync(0xffffffffu, mult, (u + x) & 31);
+                            if (slot[x] >= 0)
+                                buf[slot[x]] = fma(val[x], m, buf[slot[x]]);
+                            __syncwarp();
+                        }
                     }
                 }
-                __syncwarp();
+            } else {
+                for (int x = 0; x < nkb; x++) {
+                    const uint32_t vo = __shfl_sync(0xffffffffu, voff, x);
+                    const uint32_t co = __shfl_sync(0xffffffffu, coo, x);
+                    const double m = __shfl_sync(0xffffffffu, mult, x);
+                    const int inf = __shfl_sync(0xffffffffu, info, x);
+                    row_add_generic(buf, inf & 0xffff, m, p.vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
+                    __syncwarp();
+                }
             }
         }
-    }
-    if (p.dense != nullptr) {
-        if (lane == 0)
-            p.dense[r] = L > 0 ? -buf[0] : 0.0;
-        return;
-    }
-    for (int s = lane; s < L; s += 32) {
-        if (s < la)
-            p.Avals[p.Arows[r] + s] = buf[s];
-        else
-            p.Dvals[p.Drows[r] + (s - la)] = buf[s];
+        const int64_t r = r0 + rr;
+        if (p.dense != nullptr) {
+            if (lane == 0)
+                p.dense[r] = L > 0 ? -buf[0] : 0.0;
+            __syncwarp();
+            for (int s = lane; s < L; s += 32) buf[s] = 0.0;
+        } else {
+            for (int s = lane; s < L; s += 32) {
+                const double v = buf[s];
+                buf[s] = 0.0;
+                if (s < la)
+                    p.Avals[a0 + s] = v;
+                else
+                    p.Dvals[d0 + (s - la)] = v;
+            }
+        }
+        __syncwarp();
     }
 }
 
