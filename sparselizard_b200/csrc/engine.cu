@@ -1599,22 +1599,25 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
     else if (choice < 0)
         choice = P.row_kernel;
     if (choice < 0 && !ctx->x->capturing && ctx->x == &ctx->main) {
-        // Both, timed on this call's data (their outputs are identical).
-        cudaEvent_t ev[3];
+        // Both, twice each in turn, timed on this call's data (their outputs
+        // are identical); the faster of each kernel's runs is compared, so
+        // that a first, cold run decides nothing.
+        cudaEvent_t ev[5];
         for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        const int kt = kstat_start(ctx, "row_values", 2 * rbytes);
+        const int kt = kstat_start(ctx, "row_values", 4 * rbytes);
         cuda_check(cudaEventRecord(ev[0], ctx->x->stream), "cudaEventRecord");
-        launch_stream_rows(ctx, sl);
-        cuda_check(cudaEventRecord(ev[1], ctx->x->stream), "cudaEventRecord");
-        launch_warp_rows(ctx, rp);
-        cuda_check(cudaEventRecord(ev[2], ctx->x->stream), "cudaEventRecord");
+        for (int r = 0; r < 2; r++) {
+            launch_stream_rows(ctx, sl);
+            cuda_check(cudaEventRecord(ev[1 + 2 * r], ctx->x->stream), "cudaEventRecord");
+            launch_warp_rows(ctx, rp);
+            cuda_check(cudaEventRecord(ev[2 + 2 * r], ctx->x->stream), "cudaEventRecord");
+        }
         kstat_stop(ctx, kt);
-        cuda_check(cudaEventSynchronize(ev[2]), "sync");
-        float ts = 0, tw = 0;
-        cudaEventElapsedTime(&ts, ev[0], ev[1]);
-        cudaEventElapsedTime(&tw, ev[1], ev[2]);
+        cuda_check(cudaEventSynchronize(ev[4]), "sync");
+        float t[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
         for (auto& e : ev) cudaEventDestroy(e);
-        P.row_kernel = ts < tw ? 0 : 1;
+        P.row_kernel = std::min(t[0], t[2]) < std::min(t[1], t[3]) ? 0 : 1;
         return;
     }
     const int kt = kstat_start(ctx, "row_values", rbytes);

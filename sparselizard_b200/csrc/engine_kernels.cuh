@@ -672,7 +672,7 @@ __device__ __forceinline__ void row_add_generic(double* buf, int width, double m
 // Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
 constexpr int kRowsPerWarp = 31;
 
-__global__ void __launch_bounds__(256, 3) k_row_values(RowParams p)
+__global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
 {
     extern __shared__ double rowbuf[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

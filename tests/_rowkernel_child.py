@@ -1,5 +1,6 @@
-"""Child process for test_gpu_graphs: assembles a synthetic matrix with the
-CSR value kernel named by SLGPU_ROW_KERNEL and saves the values (argv[1])."""
+"""Child process for tests that compare engine variants chosen by environment
+(SLGPU_ROW_KERNEL, SLGPU_FUSED_SPLIT): assembles synthetic matrices in FP64
+and split precision and saves the values (argv[1])."""
 import os
 import sys
 
