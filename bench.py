@@ -167,9 +167,9 @@ TRAFFIC_PER_ELEMENT = {
     # profiles/k_contract_split_elasticity_hex32.md: 60.29 MB read + 135.83 MB
     # written by one group launch over 32768 elements.
     ("c2", "contract_split"): (60.287488e6 + 135.8272e6) / 32768,
-    # profiles/k_row_values_elasticity_hex32.md: 2.487 GB read + 1.182 GB
+    # profiles/k_row_values_elasticity_hex32.md: 2.859 GB read + 1.202 GB
     # written by the launch over all 9 groups of 32768 elements.
-    ("c2", "row_values"): (2.487337e9 + 1.182009e9) / 32768,
+    ("c2", "row_values"): (2.858950e9 + 1.201917e9) / 32768,
 }
 
 
