@@ -261,6 +261,12 @@ int64_t slgpu_kernel_launches(const slgpu_ctx* ctx);
 int slgpu_ctx_set_graphs(slgpu_ctx* ctx, int enable);
 /* Number of graph replays of process() so far. */
 int64_t slgpu_graph_launches(const slgpu_ctx* ctx);
+/* Per-kernel and per-phase CUDA events inside process() (default on;
+ * SLGPU_KERNEL_TIMERS=0 in the environment turns them off at context
+ * creation).  Off, slgpu_kernel_stats reports nothing and
+ * slgpu_last_timings only the total, and a replayed graph holds no event
+ * nodes between its kernels.  No counterpart in the reference. */
+int slgpu_ctx_set_kernel_timers(slgpu_ctx* ctx, int enable);
 
 /* Algorithmic work of one process() of a matrix, for roofline accounting:
  * contraction_flops = sum over groups of nelem * sum over terms of

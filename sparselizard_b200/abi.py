@@ -114,6 +114,7 @@ SIGNATURES = {
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
     "slgpu_ctx_set_graphs": (c_int, [c_void_p, c_int]),
     "slgpu_graph_launches": (c_int64, [c_void_p]),
+    "slgpu_ctx_set_kernel_timers": (c_int, [c_void_p, c_int]),
     "slgpu_kernel_stats": (c_int, [c_void_p, c_char_p, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]),
     "slgpu_check_coefficient_kernels": (c_int, [c_void_p, c_int, c_char_p, c_size_t]),
     "slgpu_matrix_work": (c_int, [c_void_p, c_int, c_void_p]),

@@ -638,6 +638,8 @@ void htrace_mark(Ctx* ctx, const char* label)
 // event pair; kstat_collect sums them once the stream has been synchronised.
 int kstat_start(Ctx* ctx, const char* family, double work)
 {
+    if (!ctx->timers)
+        return -1;
     const size_t i = ctx->x->kev_tag.size();
     while (ctx->x->kev.size() < 2 * (i + 1)) {
         cudaEvent_t e;
@@ -649,7 +651,18 @@ int kstat_start(Ctx* ctx, const char* family, double work)
     return (int)i;
 }
 
-void kstat_stop(Ctx* ctx, int i) { record_event(ctx, ctx->x->kev[2 * i + 1]); }
+void kstat_stop(Ctx* ctx, int i)
+{
+    if (i >= 0)
+        record_event(ctx, ctx->x->kev[2 * i + 1]);
+}
+
+// Phase boundary events (within a process()), recorded only with timers on.
+static void phase_event(Ctx* ctx, cudaEvent_t e)
+{
+    if (ctx->timers)
+        record_event(ctx, e);
+}
 
 void record_event(Ctx* ctx, cudaEvent_t e)
 {
@@ -1392,9 +1405,9 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
         E.alloc(ctx, (size_t)etot * 4);
         cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
     }
-    record_event(ctx, ctx->x->evpool[0]);
+    phase_event(ctx, ctx->x->evpool[0]);
     launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov);
-    record_event(ctx, ctx->x->evpool[1]);
+    phase_event(ctx, ctx->x->evpool[1]);
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
@@ -1439,7 +1452,7 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
         }
         gi++;
     }
-    record_event(ctx, ctx->x->evpool[2]);
+    phase_event(ctx, ctx->x->evpool[2]);
     C.release();
     {
         int64_t vb = 0;
@@ -1685,6 +1698,7 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
     p(M.rsegs_dev.as<void>());
     u((uint64_t)split_tile_width());
     u((uint64_t)ctx->nsm);
+    u(ctx->timers ? 1 : 0);
     u(ctx->jit_broken ? 1 : 0);
     p(x.split_cols.as<void>());
     p(x.split_colexp.as<void>());
@@ -1739,7 +1753,7 @@ static void capture_value_graph(Ctx* ctx, Matrix& M, int precision, bool rhs, co
     std::string err;
     try {
         launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
-        ev_record(ctx, 2);
+        phase_event(ctx, ctx->x->ev[2]);
         launch_row_values(ctx, M, *M.pattern, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
     } catch (const std::exception& e) {
         err = e.what();
@@ -1837,7 +1851,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     bool reused = false;
     M.pattern = get_pattern(ctx, M, segs, dconstr, rhs, key0, key1, &reused);
     Pattern& P = *M.pattern;
-    ev_record(ctx, 1);
+    phase_event(ctx, ctx->x->ev[1]);
 
     // Output buffers, kept between calls while their sizes are unchanged.
     if (M.vals.bytes() < (size_t)std::max<int64_t>(total_vals, 1) * 8)
@@ -1897,7 +1911,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     }
     if (!graphed) {
         launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
-        ev_record(ctx, 2);
+        phase_event(ctx, ctx->x->ev[2]);
         launch_row_values(ctx, M, P, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
     }
     ev_record(ctx, 3);
@@ -1910,12 +1924,14 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
             fail(SLGPU_E_TIMEOUT, "a split-precision contraction tile timed out waiting for its data");
     }
     float coef_ms = 0, contract_ms = 0;
-    cudaEventElapsedTime(&coef_ms, ctx->x->evpool[0], ctx->x->evpool[1]);
-    cudaEventElapsedTime(&contract_ms, ctx->x->evpool[1], ctx->x->evpool[2]);
+    if (ctx->timers) {
+        cudaEventElapsedTime(&coef_ms, ctx->x->evpool[0], ctx->x->evpool[1]);
+        cudaEventElapsedTime(&contract_ms, ctx->x->evpool[1], ctx->x->evpool[2]);
+    }
     ctx->x->timings[0] = coef_ms;
     ctx->x->timings[1] = contract_ms;
-    ctx->x->timings[2] = ev_ms(ctx, 0, 1);
-    ctx->x->timings[3] = ev_ms(ctx, 2, 3);
+    ctx->x->timings[2] = ctx->timers ? ev_ms(ctx, 0, 1) : 0.0;
+    ctx->x->timings[3] = ctx->timers ? ev_ms(ctx, 2, 3) : 0.0;
     ctx->x->timings[4] = ev_ms(ctx, 0, 3);
     if (info != nullptr) {
         info->nA = P.nA;
@@ -1997,6 +2013,8 @@ int slgpu_ctx_create(int device, size_t hbm_budget, unsigned flags, slgpu_ctx** 
         cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
         const char* gv = std::getenv("SLGPU_GRAPHS");
         ctx->graphs = !(gv != nullptr && std::strcmp(gv, "0") == 0);
+        const char* tv = std::getenv("SLGPU_KERNEL_TIMERS");
+        ctx->timers = !(tv != nullptr && std::strcmp(tv, "0") == 0);
         // Keep freed blocks in the stream-ordered pool between assemblies.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -2262,6 +2280,11 @@ int slgpu_ctx_set_graphs(slgpu_ctx* ctx, int enable)
 }
 
 int64_t slgpu_graph_launches(const slgpu_ctx* ctx) { return ctx ? ctx->graph_launches : 0; }
+
+int slgpu_ctx_set_kernel_timers(slgpu_ctx* ctx, int enable)
+{
+    return guarded(ctx, [&] { ctx->timers = enable != 0; });
+}
 
 int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_t len)
 {

@@ -261,6 +261,7 @@ struct Ctx {
     uint64_t constr_key[2] = {0, 0};
     int64_t launches = 0;              // kernels launched by this context
     bool graphs = true;                // value-path graphs for process() (slgpu_ctx_set_graphs)
+    bool timers = true;                // per-kernel and per-phase events (slgpu_ctx_set_kernel_timers)
     int64_t graph_launches = 0;
     uint64_t next_serial = 1;          // group serial numbers
     std::map<std::string, cudaKernel_t> jit_kernels;  // runtime-compiled coefficient kernels by source
