@@ -1467,9 +1467,10 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     }
 }
 
-// CSR value kernel: -1 = chosen per pattern by timing both (default),
-// 0 = streaming warps (SLGPU_ROW_KERNEL=stream), 1 = one warp per row
-// (SLGPU_ROW_KERNEL=warp).
+// CSR value kernel: -1 = chosen per pattern by timing the candidates
+// (default), 0 = streaming warps (SLGPU_ROW_KERNEL=stream), 1 = warp per row
+// (SLGPU_ROW_KERNEL=warp), 2 = thread per row, rows of at most 32 entries
+// (SLGPU_ROW_KERNEL=thread).
 static int row_kernel_forced()
 {
     static const int k = [] {
@@ -1478,6 +1479,8 @@ static int row_kernel_forced()
             return 1;
         if (v != nullptr && std::strcmp(v, "stream") == 0)
             return 0;
+        if (v != nullptr && std::strcmp(v, "thread") == 0)
+            return 2;
         return -1;
     }();
     return k;
@@ -1557,6 +1560,14 @@ void launch_stream_rows(Ctx* ctx, const StreamLaunch& L)
     ctx->launches++;
 }
 
+void launch_thread_rows(Ctx* ctx, const RowParams& rp)
+{
+    const size_t smem = (size_t)rp.lmax * kThreadRows * 8;
+    k_row_thread<<<grid_for(rp.nrows, kThreadRows), kThreadRows, smem, ctx->x->stream>>>(rp);
+    cuda_check(cudaGetLastError(), "k_row_thread");
+    ctx->launches++;
+}
+
 void launch_warp_rows(Ctx* ctx, RowParams rp)
 {
     // Consecutive rows per warp: up to kRowsPerWarp (the row buffer stays
@@ -1606,38 +1617,63 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
     // pointers read; A and D values written.
     const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
     const StreamLaunch sl = stream_launch(ctx, rp, rsegs);
+    const bool thread_ok = rp.lmax <= kThreadRowMax;
+    // Candidates: warp per row always, streaming warps and thread per row
+    // where their shapes allow.
+    std::vector<int> cand{1};
+    if (sl.ok)
+        cand.push_back(0);
+    if (thread_ok)
+        cand.push_back(2);
+    auto launch = [&](int c) {
+        if (c == 0)
+            launch_stream_rows(ctx, sl);
+        else if (c == 2)
+            launch_thread_rows(ctx, rp);
+        else
+            launch_warp_rows(ctx, rp);
+    };
     int choice = row_kernel_forced();
-    if (!sl.ok)
+    if (choice >= 0 && std::find(cand.begin(), cand.end(), choice) == cand.end())
         choice = 1;
-    else if (choice < 0)
+    if (choice < 0)
         choice = P.row_kernel;
     if (choice < 0 && !ctx->x->capturing && ctx->x == &ctx->main) {
-        // Both, twice each in turn, timed on this call's data (their outputs
-        // are identical); the faster of each kernel's runs is compared, so
-        // that a first, cold run decides nothing.
-        cudaEvent_t ev[5];
+        // Every candidate, twice each in turn, timed on this call's data
+        // (their outputs are identical); the best run of each is compared,
+        // so that a first, cold run decides nothing.
+        const size_t nc = cand.size();
+        std::vector<cudaEvent_t> ev(2 * nc + 1);
         for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        const int kt = kstat_start(ctx, "row_values", 4 * rbytes);
+        const int kt = kstat_start(ctx, "row_values", 2.0 * nc * rbytes);
         cuda_check(cudaEventRecord(ev[0], ctx->x->stream), "cudaEventRecord");
-        for (int r = 0; r < 2; r++) {
-            launch_stream_rows(ctx, sl);
-            cuda_check(cudaEventRecord(ev[1 + 2 * r], ctx->x->stream), "cudaEventRecord");
-            launch_warp_rows(ctx, rp);
-            cuda_check(cudaEventRecord(ev[2 + 2 * r], ctx->x->stream), "cudaEventRecord");
-        }
+        for (size_t r = 0; r < 2; r++)
+            for (size_t c = 0; c < nc; c++) {
+                launch(cand[c]);
+                cuda_check(cudaEventRecord(ev[1 + r * nc + c], ctx->x->stream), "cudaEventRecord");
+            }
         kstat_stop(ctx, kt);
-        cuda_check(cudaEventSynchronize(ev[4]), "sync");
-        float t[4] = {0, 0, 0, 0};
-        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
+        cuda_check(cudaEventSynchronize(ev[2 * nc]), "sync");
+        float best_t = 0;
+        int best = 1;
+        for (size_t c = 0; c < nc; c++) {
+            float t0 = 0, t1 = 0;
+            cudaEventElapsedTime(&t0, ev[c], ev[c + 1]);
+            cudaEventElapsedTime(&t1, ev[nc + c], ev[nc + c + 1]);
+            const float t = std::min(t0, t1);
+            if (c == 0 || t < best_t) {
+                best_t = t;
+                best = cand[c];
+            }
+        }
         for (auto& e : ev) cudaEventDestroy(e);
-        P.row_kernel = std::min(t[0], t[2]) < std::min(t[1], t[3]) ? 0 : 1;
+        P.row_kernel = best;
         return;
     }
+    if (choice < 0)
+        choice = 1;
     const int kt = kstat_start(ctx, "row_values", rbytes);
-    if (choice == 0)
-        launch_stream_rows(ctx, sl);
-    else
-        launch_warp_rows(ctx, rp);
+    launch(choice);
     kstat_stop(ctx, kt);
 }
 

@@ -669,6 +669,50 @@ __device__ __forceinline__ void row_add_generic(double* buf, int width, double m
     }
 }
 
+// CSR values for short rows (lmax <= kThreadRowMax): one thread per row, its
+// row buffer a column of a [lmax][kThreadRows] shared array.  The thread adds
+// its incidences in order and each incidence's columns in order, so the
+// results equal the warp kernels' (every slot is touched once per incidence
+// except in serial incidences, which every kernel adds in column order).
+constexpr int kThreadRows = 128;
+constexpr int kThreadRowMax = 32;
+
+__global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
+{
+    extern __shared__ double tbuf[];
+    const int64_t r = (int64_t)blockIdx.x * kThreadRows + threadIdx.x;
+    if (r >= p.nrows)
+        return;
+    double* buf = tbuf + threadIdx.x;  // slot s at buf[s * kThreadRows]
+    const uint32_t a0 = p.Arows[r], a1 = p.Arows[r + 1];
+    const uint32_t d0 = p.Drows ? p.Drows[r] : 0u, d1 = p.Drows ? p.Drows[r + 1] : 0u;
+    const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
+    for (int s = 0; s < L; s++) buf[s * kThreadRows] = 0.0;
+    const uint32_t k0 = p.inc_ptr[r], k1 = p.inc_ptr[r + 1];
+    for (uint32_t k = k0; k < k1; k++) {
+        const unsigned long long pk = p.inc[k];
+        const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+        const long long co = (long long)(pk & ((1ull << 40) - 1));
+        const double* v = p.vals + (sg.val_base + (co - sg.coo_base));
+        const int16_t* sl = p.slotmap + co;
+        for (int j = 0; j < sg.width; j++) {
+            const int s = sl[j];
+            if (s >= 0)
+                buf[s * kThreadRows] = fma(v[j], sg.mult, buf[s * kThreadRows]);
+        }
+    }
+    if (p.dense != nullptr) {
+        p.dense[r] = L > 0 ? -buf[0] : 0.0;
+        return;
+    }
+    for (int s = 0; s < L; s++) {
+        if (s < la)
+            p.Avals[a0 + s] = buf[s * kThreadRows];
+        else
+            p.Dvals[d0 + (s - la)] = buf[s * kThreadRows];
+    }
+}
+
 // Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
 constexpr int kRowsPerWarp = 31;
 

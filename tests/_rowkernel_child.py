@@ -16,7 +16,7 @@ import test_gpu_graphs as T  # noqa: E402
 ctx = abi.Context(0)
 out = {}
 for name, (grid, ntf, ndof, nterms, ngp1, ndofs) in {"narrow": (60, 9, 9, 4, 3, 3000), "wide": (30, 20, 40, 3, 3, 4000),
-                                                      "small": (80, 4, 4, 3, 2, 5000)}.items():
+                                                      "small": (80, 4, 4, 3, 2, 5000), "short": (40, 4, 4, 2, 2, 20000)}.items():
     rng = np.random.Generator(np.random.PCG64(31))
     t = T._setup(ctx, rng, 20 + len(out), grid, ntf, ndof, nterms, ngp1, ndofs)
     for prec in (abi.PREC_FP64, abi.PREC_SPLIT):

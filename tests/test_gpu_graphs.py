@@ -123,21 +123,22 @@ def test_graph_kernel_stats_and_launch_count(ctx):
 
 
 def test_value_kernels_agree(tmp_path):
-    """The streaming-warp and warp-per-row CSR value kernels, each forced in a
-    child process, give the same values bit for bit (incidence widths 4, 9
-    and 40)."""
+    """The streaming-warp, warp-per-row and thread-per-row CSR value kernels,
+    each forced in a child process, give the same values bit for bit
+    (incidence widths 4, 9 and 40; the thread kernel on the short rows)."""
     import os
     import subprocess
     import sys
 
     here = os.path.dirname(os.path.abspath(__file__))
     res = {}
-    for k in ("stream", "warp"):
+    for k in ("stream", "warp", "thread"):
         out = str(tmp_path / f"{k}.npz")
         env = dict(os.environ, SLGPU_ROW_KERNEL=k)
         subprocess.run([sys.executable, os.path.join(here, "_rowkernel_child.py"), out], env=env, check=True, timeout=600)
         res[k] = np.load(out)
     for key in res["warp"].files:
-        a, b = res["stream"][key], res["warp"][key]
-        assert np.all(np.isfinite(a)), key
-        assert np.array_equal(a, b), f"{key}: streaming and warp-per-row value kernels differ"
+        for k in ("stream", "thread"):
+            a, b = res[k][key], res["warp"][key]
+            assert np.all(np.isfinite(a)), key
+            assert np.array_equal(a, b), f"{key}: {k} and warp-per-row value kernels differ"
