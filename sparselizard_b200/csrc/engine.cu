@@ -1173,22 +1173,15 @@ static int split_tile_width()
     return ne;
 }
 
-// Split contraction of one group: column slices of C (exponents per element
-// from the coefficient kernel), then the tcgen05 kernel.
-static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out)
+// Column slices of one group's coefficients (k_slice_cols) into `slices` /
+// `colexp`, on the current execution state's stream.
+static void slice_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const double* C, const int32_t* elemexp, int8_t* slices,
+                        int32_t* colexp)
 {
-    GroupDev::Split& sp = ensure_split(ctx, g, tier);
-    const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+    const int Q = g.nterms * g.ngp;
     const int NE = split_tile_width();
     const int64_t ntiles = (int64_t)g.tiles.size();
     const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
-    {
-        ArenaPause keep(*ctx->x);  // per-state scratch, kept between requests
-        if (ctx->x->split_cols.bytes() < colbytes)
-            ctx->x->split_cols.alloc(ctx, colbytes);
-        if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
-            ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
-    }
     ColSliceParams cs{};
     cs.C = C;
     cs.elemexp = elemexp;
@@ -1197,8 +1190,8 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     cs.Qpad = sp.Qpad;
     cs.nelem = g.nelem;
     cs.ntiles = ntiles;
-    cs.slices = ctx->x->split_cols.as<int8_t>();
-    cs.colexp = ctx->x->split_colexp.as<int32_t>();
+    cs.slices = slices;
+    cs.colexp = colexp;
     const dim3 cgrid = grid_for(ntiles * 64, 128);
     const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + 4.0 * g.nelem + (double)colbytes + 4.0 * ntiles * 64);
     if (sp.S == 7 && NE == 64)
@@ -1214,6 +1207,14 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     kstat_stop(ctx, kt);
     cuda_check(cudaGetLastError(), "k_slice_cols");
     ctx->launches++;
+}
+
+// The tcgen05 contraction of one group from its column slices.
+static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const int8_t* slices, const int32_t* colexp, double* out)
+{
+    const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+    const int NE = split_tile_width();
+    const int64_t ntiles = (int64_t)g.tiles.size();
     SplitParams p{};
     p.P = P;
     p.Ppad = sp.Ppad;
@@ -1222,9 +1223,9 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     p.nwork = (int64_t)p.ntp * ntiles * (64 / NE);
     p.tiles = g.tiles_d.as<Tile>();
     p.A = sp.slices.as<int8_t>();
-    p.B = ctx->x->split_cols.as<int8_t>();
+    p.B = slices;
     p.rowexp = sp.rowexp.as<int32_t>();
-    p.colexp = ctx->x->split_colexp.as<int32_t>();
+    p.colexp = colexp;
     p.out = out;
     p.error = ctx->x->split_error.as<unsigned int>();
     // Algorithmic INT8 operations: 2 per product, pairs (a, b) with a + b <= L.
@@ -1243,6 +1244,25 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
     kstat_stop(ctx, kc);
     cuda_check(cudaGetLastError(), "k_contract_split");
     ctx->launches++;
+}
+
+// Split contraction of one group: column slices of C (exponents per element
+// from the coefficient kernel) into the execution state's scratch, then the
+// tcgen05 kernel.
+static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out)
+{
+    const GroupDev::Split& sp = ensure_split(ctx, g, tier);
+    const int64_t ntiles = (int64_t)g.tiles.size();
+    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
+    {
+        ArenaPause keep(*ctx->x);  // per-state scratch, kept between requests
+        if (ctx->x->split_cols.bytes() < colbytes)
+            ctx->x->split_cols.alloc(ctx, colbytes);
+        if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
+            ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
+    }
+    slice_group(ctx, g, sp, C, elemexp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>());
+    split_group(ctx, g, sp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>(), out);
 }
 
 // Whether a group's contraction runs in split precision: element matrices
