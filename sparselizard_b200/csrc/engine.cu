@@ -33,6 +33,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <stdexcept>
 
 namespace slgpu {
@@ -2108,6 +2109,12 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
         for (auto& e : ctx->x->ev) cudaEventDestroy(e);
         for (auto& e : ctx->x->evpool) cudaEventDestroy(e);
         for (auto& e : ctx->x->kev) cudaEventDestroy(e);
+        for (int b = 0; b < 2; b++) {
+            if (ctx->dl_stage[b] != nullptr)
+                cudaFreeHost(ctx->dl_stage[b]);
+            if (ctx->dl_ev[b] != nullptr)
+                cudaEventDestroy(ctx->dl_ev[b]);
+        }
         stage_free(ctx->main);
         cudaStreamDestroy(ctx->x->stream);
     }
@@ -2430,6 +2437,70 @@ int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstraine
     });
 }
 
+namespace {
+constexpr size_t kDlChunk = size_t(64) << 20;
+
+// Host copy spread over threads (large destinations in pageable memory are
+// also first touched here, so the page faults are spread as well).
+void parallel_memcpy(char* dst, const char* src, size_t n)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(1, n >> 22));
+    if (nt <= 1) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (n + nt - 1) / nt;
+    for (size_t t = 0; t < nt; t++) {
+        const size_t a = t * part, b = std::min(n, a + part);
+        if (a < b)
+            th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// Device -> host copy on the context's stream.  Page-locked or small
+// destinations: one asynchronous copy (the caller synchronises).  Large
+// pageable ones: 64 MB chunks through two page-locked blocks, the copy of
+// chunk i+1 in flight while chunk i is copied on the host (synchronous).
+void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
+{
+    if (n == 0)
+        return;
+    cudaPointerAttributes a{};
+    const bool pinned = cudaPointerGetAttributes(&a, dst) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned || n < 2 * kDlChunk) {
+        cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        return;
+    }
+    for (int b = 0; b < 2; b++) {
+        if (ctx->dl_stage[b] == nullptr)
+            cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&ctx->dl_stage[b]), kDlChunk, cudaHostAllocDefault), "cudaHostAlloc");
+        if (ctx->dl_ev[b] == nullptr)
+            cuda_check(cudaEventCreateWithFlags(&ctx->dl_ev[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    const size_t nch = (n + kDlChunk - 1) / kDlChunk;
+    auto issue = [&](size_t i) {
+        const size_t off = i * kDlChunk, len = std::min(kDlChunk, n - off);
+        cuda_check(cudaMemcpyAsync(ctx->dl_stage[i & 1], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, ctx->x->stream),
+                   "D2H chunk");
+        cuda_check(cudaEventRecord(ctx->dl_ev[i & 1], ctx->x->stream), "cudaEventRecord");
+    };
+    issue(0);
+    if (nch > 1)
+        issue(1);
+    for (size_t i = 0; i < nch; i++) {
+        cuda_check(cudaEventSynchronize(ctx->dl_ev[i & 1]), "D2H chunk wait");
+        const size_t off = i * kDlChunk, len = std::min(kDlChunk, n - off);
+        parallel_memcpy(static_cast<char*>(dst) + off, ctx->dl_stage[i & 1], len);
+        if (i + 2 < nch)
+            issue(i + 2);
+    }
+}
+}  // namespace
+
 int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* Acols, double* Avals, int32_t* Drows, int32_t* Dcols,
                           double* Dvals)
 {
@@ -2438,16 +2509,12 @@ int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* A
         if (!M.pattern)
             fail(SLGPU_E_STATE, "matrix not processed");
         Pattern& P = *M.pattern;
-        auto d2h = [&](void* dst, const void* src, size_t n) {
-            if (n > 0)
-                cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H csr");
-        };
-        d2h(Arows, P.Arows.as<void>(), (P.nA + 1) * 4);
-        d2h(Acols, P.Acols.as<void>(), P.nnzA * 4);
-        d2h(Avals, M.Avals.as<void>(), P.nnzA * 8);
-        d2h(Drows, P.Drows.as<void>(), (P.nA + 1) * 4);
-        d2h(Dcols, P.Dcols.as<void>(), P.nnzD * 4);
-        d2h(Dvals, M.Dvals.as<void>(), P.nnzD * 8);
+        d2h(ctx, Arows, P.Arows.as<void>(), (P.nA + 1) * 4);
+        d2h(ctx, Acols, P.Acols.as<void>(), P.nnzA * 4);
+        d2h(ctx, Avals, M.Avals.as<void>(), P.nnzA * 8);
+        d2h(ctx, Drows, P.Drows.as<void>(), (P.nA + 1) * 4);
+        d2h(ctx, Dcols, P.Dcols.as<void>(), P.nnzD * 4);
+        d2h(ctx, Dvals, M.Dvals.as<void>(), P.nnzD * 8);
         cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync download");
     });
 }
@@ -2459,10 +2526,8 @@ int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, doub
         if (!M.pattern)
             fail(SLGPU_E_STATE, "matrix not processed");
         Pattern& P = *M.pattern;
-        if (P.nnzA > 0)
-            cuda_check(cudaMemcpyAsync(Avals, M.Avals.as<void>(), P.nnzA * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
-        if (P.nnzD > 0)
-            cuda_check(cudaMemcpyAsync(Dvals, M.Dvals.as<void>(), P.nnzD * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
+        d2h(ctx, Avals, M.Avals.as<void>(), P.nnzA * 8);
+        d2h(ctx, Dvals, M.Dvals.as<void>(), P.nnzD * 8);
         cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync download");
     });
 }

@@ -268,6 +268,10 @@ struct Ctx {
     std::vector<cudaLibrary_t> jit_libs;
     bool jit_broken = false;  // a coefficient kernel failed to compile: interpreter from then on
     std::string jit_error;
+    // Page-locked blocks and events of the pipelined download into pageable
+    // host memory (slgpu_matrix_download*).
+    char* dl_stage[2] = {nullptr, nullptr};
+    cudaEvent_t dl_ev[2] = {nullptr, nullptr};
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;
