@@ -206,6 +206,19 @@ int slgpu_matrix_group_desc(slgpu_ctx* ctx, int handle, int gi, slgpu_group_desc
 int slgpu_matrix_set_scales(slgpu_ctx* ctx, int handle, int gi, const double* term_scales, const double* dest_multipliers);
 /* Current term scales (nterms) and destination multipliers (ndests) of group `gi`. */
 int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_scales, double* dest_multipliers);
+/* Symmetry of group `gi`'s element matrices.  mirror (nterms values, may be
+ * NULL) receives each term's mirror term: the term whose test-function and
+ * dof tables hold the values of this term's dof and test-function tables,
+ * with a coefficient of the same expression; all -1 when some term has none.
+ * Coefficients match up to the order of the factors of a product.
+ * *symmetric (may be NULL) is nonzero when the split-precision contraction
+ * currently computes only the upper triangle and mirrors it (mirror terms
+ * with equal scales): 1 when every coefficient equals its mirror's bit for
+ * bit (the mirrored result is then the unmirrored one bit for bit), 2 when
+ * some differ in the order of their factors (a few units in the last place).
+ * The reference computes full element matrices
+ * (src/formulation/contribution.cpp:155-249). */
+int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric);
 /* isconstrained [ndofs] (dofmanager::isconstrained, src/formulation/dofmanager.cpp:366-382). */
 int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstrained, int precision, slgpu_csr_info* info);
 /* Copies the processed CSR blocks to host memory: Arows/Drows [nA+1], Acols/Avals [nnzA], Dcols/Dvals [nnzD]. */

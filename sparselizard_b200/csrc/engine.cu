@@ -27,11 +27,13 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <stdexcept>
@@ -308,6 +310,129 @@ static void validate_group(const slgpu_group& g)
         fail(SLGPU_E_UNSUPPORTED, "group too large");
 }
 
+// Mirror term of each term when the group's element matrices are symmetric
+// (empty otherwise).  The condition: ntf == ndof, and every term t has a
+// partner u (t itself allowed) whose test-function table holds the values of
+// t's dof table and whose dof table holds those of t's test-function table,
+// with a coefficient node that computes the same expression: the same
+// operations on the same inputs, the operands of + in either order and the
+// factors of a chain of products in any order.  Entry (j, i) of term u is
+// then the product of entry (i, j) of term t with u's coefficient.
+//
+// `exact`: every coefficient also equals its mirror's bit for bit (IEEE
+// addition and multiplication commute exactly, so this holds when only the
+// two operands of single operations are swapped); the split contraction's
+// exact integer sums then give M[i][j] == M[j][i] with or without the
+// mirroring.  Otherwise a reordered product of n factors differs from its
+// mirror by at most about n units in the last place, far below the split
+// tiers' error bounds.  The scales are checked where the contraction is
+// launched (they can change).
+struct Mirror {
+    std::vector<int32_t> term;
+    bool exact = false;
+};
+
+static Mirror mirror_terms(const slgpu_group& g)
+{
+    if (g.ntf != g.ndof || g.terms[0].dof_table < 0)
+        return {};
+    // Tables with equal values share a class.
+    std::vector<int> tcls(g.ntables);
+    for (int k = 0; k < g.ntables; k++) {
+        tcls[k] = k;
+        const size_t n = (size_t)g.norient * g.tables[k].rows * g.ngp;
+        for (int k2 = 0; k2 < k; k2++)
+            if (tcls[k2] == k2 && g.tables[k2].rows == g.tables[k].rows &&
+                std::memcmp(g.tables[k2].vals, g.tables[k].vals, n * sizeof(double)) == 0) {
+                tcls[k] = k2;
+                break;
+            }
+    }
+    // Two classes per node by hash-consing over the program order: `ecls`
+    // (same value bit for bit: + and * with operands in either order) and
+    // `rcls` (same value up to the order of factors: a chain of products is
+    // keyed by the sorted classes of its factors).
+    std::map<std::vector<int64_t>, int> eids, rids;
+    std::vector<int> ecls(g.nnodes), rcls(g.nnodes);
+    std::vector<std::vector<int64_t>> factors(g.nnodes);
+    for (int k = 0; k < g.nnodes; k++) {
+        const slgpu_node& nd = g.nodes[k];
+        const bool ref_a = nd.op == SLGPU_OP_ADD || nd.op == SLGPU_OP_MUL || nd.op == SLGPU_OP_POW || nd.op == SLGPU_OP_INV ||
+                           nd.op == SLGPU_OP_NEG;
+        const bool ref_b = nd.op == SLGPU_OP_ADD || nd.op == SLGPU_OP_MUL || nd.op == SLGPU_OP_POW;
+        if ((ref_a && (nd.a < 0 || nd.a >= k)) || (ref_b && (nd.b < 0 || nd.b >= k)))
+            return {};
+        std::vector<int64_t> ek{nd.op, nd.a, ref_b ? nd.b : (int64_t)nd.b, nd.c}, rk;
+        switch (nd.op) {
+        case SLGPU_OP_CONST:
+            if (nd.a < 0 || nd.a >= g.nconsts)
+                return {};
+            std::memcpy(&ek[1], &g.consts[nd.a], 8);
+            ek[2] = 0;
+            break;
+        case SLGPU_OP_FIELD:
+            if (nd.b < 0 || nd.b >= g.ntables)
+                return {};
+            ek[2] = tcls[nd.b];
+            break;
+        default:
+            break;
+        }
+        rk = ek;
+        if (ref_a) {
+            ek[1] = ecls[nd.a];
+            rk[1] = rcls[nd.a];
+        }
+        if (ref_b) {
+            ek[2] = ecls[nd.b];
+            rk[2] = rcls[nd.b];
+        }
+        if (nd.op == SLGPU_OP_ADD || nd.op == SLGPU_OP_MUL) {
+            if (ek[1] > ek[2])
+                std::swap(ek[1], ek[2]);
+            if (rk[1] > rk[2])
+                std::swap(rk[1], rk[2]);
+        }
+        if (nd.op == SLGPU_OP_MUL) {
+            std::vector<int64_t>& f = factors[k];
+            for (int x : {nd.a, nd.b}) {
+                if (g.nodes[x].op == SLGPU_OP_MUL)
+                    f.insert(f.end(), factors[x].begin(), factors[x].end());
+                else
+                    f.push_back(rcls[x]);
+            }
+            std::sort(f.begin(), f.end());
+            rk.assign(1, SLGPU_OP_MUL);
+            rk.insert(rk.end(), f.begin(), f.end());
+        }
+        ecls[k] = eids.emplace(ek, (int)eids.size()).first->second;
+        rcls[k] = rids.emplace(rk, (int)rids.size()).first->second;
+    }
+    Mirror m;
+    m.term.assign(g.nterms, -1);
+    m.exact = true;
+    for (int t = 0; t < g.nterms; t++) {
+        if (m.term[t] >= 0)
+            continue;
+        const slgpu_term& a = g.terms[t];
+        if (a.coef_node < 0 || a.coef_node >= g.nnodes)
+            return {};
+        for (int u = t; u < g.nterms; u++) {
+            const slgpu_term& b = g.terms[u];
+            if (m.term[u] < 0 && b.coef_node >= 0 && b.coef_node < g.nnodes && tcls[b.tf_table] == tcls[a.dof_table] &&
+                tcls[b.dof_table] == tcls[a.tf_table] && rcls[b.coef_node] == rcls[a.coef_node]) {
+                m.term[t] = u;
+                m.term[u] = t;
+                m.exact = m.exact && ecls[b.coef_node] == ecls[a.coef_node];
+                break;
+            }
+        }
+        if (m.term[t] < 0)
+            return {};
+    }
+    return m;
+}
+
 static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
 {
     validate_group(g);
@@ -329,6 +454,11 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     gd->prog = compile_program(g, g.nterms);
     gd->nodes.assign(g.nodes, g.nodes + g.nnodes);
     for (int t = 0; t < g.nterms; t++) gd->term_node.push_back(g.terms[t].coef_node);
+    {
+        Mirror m = mirror_terms(g);
+        gd->mirror = std::move(m.term);
+        gd->mirror_exact = m.exact;
+    }
     gd->hconsts.assign(g.consts, g.consts + g.nconsts);
     {
         // Geometry key: groups with the same key share elements, orientations,
@@ -1080,20 +1210,50 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 // Tier 0: 7 slices, levels <= 8 (28 INT8 products; about 1e-12 relative per
 // element matrix, well inside 1e-10); tier 1: 5 slices, levels <= 6 (15
 // products; about 1e-8, inside the FP32-level 1e-6).
-static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int tier)
+// Whether the split contraction of a group computes only the upper triangle
+// of its element matrices: the group has mirror terms with equal scales
+// (SLGPU_SPLIT_SYMMETRY=0 turns this off).
+static bool split_symmetric(const GroupDev& g)
 {
-    std::unique_ptr<GroupDev::Split>& sp = g.split[tier];
+    static const bool enabled = [] {
+        const char* v = std::getenv("SLGPU_SPLIT_SYMMETRY");
+        return v == nullptr || std::strcmp(v, "0") != 0;
+    }();
+    if (!enabled || g.mirror.empty())
+        return false;
+    for (int t = 0; t < g.nterms; t++)
+        if (std::memcmp(&g.term_scale[t], &g.term_scale[g.mirror[t]], sizeof(double)) != 0)
+            return false;
+    return true;
+}
+
+static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int slot)
+{
+    std::unique_ptr<GroupDev::Split>& sp = g.split[slot];
     if (sp)
         return *sp;
+    const int tier = slot & 1;
+    const bool sym = slot >= 2;
     sp.reset(new GroupDev::Split());
     sp->S = tier == 0 ? 7 : 5;
     sp->L = tier == 0 ? 8 : 6;
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
     sp->Qpad = std::max(kSplitKStep, (Q + kSplitKStep - 1) / kSplitKStep * kSplitKStep);
-    sp->Ppad = (P + kSplitM - 1) / kSplitM * kSplitM;
+    sp->nrows = sym ? g.ntf * (g.ntf + 1) / 2 : P;
+    sp->Ppad = (sp->nrows + kSplitM - 1) / kSplitM * kSplitM;
+    if (sym) {
+        // Rows (i, j), i <= j, row-major: entry i ndof + j and its mirror.
+        std::vector<int2> map;
+        map.reserve(sp->nrows);
+        for (int i = 0; i < g.ntf; i++)
+            for (int j = i; j < g.ntf; j++) map.push_back(make_int2(i * g.ndof + j, j * g.ndof + i));
+        upload(ctx, sp->rowmap, map);
+    }
     sp->slices.alloc(ctx, (size_t)sp->S * g.norient * sp->Qpad * sp->Ppad);
     sp->rowexp.alloc(ctx, (size_t)g.norient * sp->Ppad * 4);
     RowSliceParams rp{};
+    rp.rowmap = sp->rowmap.empty() ? nullptr : sp->rowmap.as<int2>();
+    rp.nrows = sp->nrows;
     rp.tables = g.tables.as<double>();
     rp.tab_off = g.tab_off_d.as<int64_t>();
     rp.term_tf = g.term_tf_d.as<int32_t>();
@@ -1120,12 +1280,13 @@ static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int tier)
 // execution state's stream order; a request stream waits for them.
 static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
 {
-    if (g.split[tier])
-        return *g.split[tier];
+    const int slot = tier + (split_symmetric(g) ? 2 : 0);
+    if (g.split[slot])
+        return *g.split[slot];
     Exec* cur = ctx->x;
     ctx->x = &ctx->main;
     try {
-        build_split(ctx, g, tier);
+        build_split(ctx, g, slot);
     } catch (...) {
         ctx->x = cur;
         throw;
@@ -1138,7 +1299,7 @@ static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
         cuda_check(cudaStreamWaitEvent(cur->stream, e, 0), "cudaStreamWaitEvent");
         cudaEventDestroy(e);
     }
-    return *g.split[tier];
+    return *g.split[slot];
 }
 
 // Whether a group's contraction can take the split path: level sums stay
@@ -1218,6 +1379,8 @@ static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, 
     const int64_t ntiles = (int64_t)g.tiles.size();
     SplitParams p{};
     p.P = P;
+    p.nrows = sp.nrows;
+    p.rowmap = sp.rowmap.empty() ? nullptr : sp.rowmap.as<int2>();
     p.Ppad = sp.Ppad;
     p.ntp = sp.Ppad / kSplitM;
     p.nk = sp.Qpad / kSplitKStep;
@@ -1233,7 +1396,7 @@ static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, 
     int pairs = 0;
     for (int a = 1; a <= sp.S; a++)
         for (int b = 1; b <= sp.S; b++) pairs += (a + b <= sp.L);
-    const int kc = kstat_start(ctx, sp.S == 7 ? "contract_split" : "contract_split_fp32", 2.0 * pairs * P * Q * g.nelem);
+    const int kc = kstat_start(ctx, sp.S == 7 ? "contract_split" : "contract_split_fp32", 2.0 * pairs * sp.nrows * Q * g.nelem);
     if (sp.S == 7 && NE == 64)
         launch_split<7, 8, 64>(ctx, p);
     else if (sp.S == 7)
@@ -1766,7 +1929,8 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
         p(g.jit_kernel);
         u(g.jit_members.size());
         for (uint64_t id : g.jit_members) u(id);
-        for (int t = 0; t < 2; t++) {
+        u(split_symmetric(g) ? 1 : 0);
+        for (int t = 0; t < 4; t++) {
             p(g.split[t] ? g.split[t]->slices.as<void>() : nullptr);
             p(g.split[t] ? g.split[t]->rowexp.as<void>() : nullptr);
         }
@@ -2424,6 +2588,20 @@ int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_sca
             std::copy(g.term_scale.begin(), g.term_scale.end(), term_scales);
         if (dest_multipliers != nullptr)
             std::copy(g.dest_mult.begin(), g.dest_mult.end(), dest_multipliers);
+    });
+}
+
+int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (gi < 0 || gi >= (int)M.groups.size())
+            fail(SLGPU_E_ARG, "group index out of range");
+        const GroupDev& g = *M.groups[gi];
+        if (mirror != nullptr)
+            for (int t = 0; t < g.nterms; t++) mirror[t] = g.mirror.empty() ? -1 : g.mirror[t];
+        if (symmetric != nullptr)
+            *symmetric = split_symmetric(g) ? (g.mirror_exact ? 1 : 2) : 0;
     });
 }
 

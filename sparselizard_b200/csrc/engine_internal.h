@@ -109,12 +109,21 @@ struct GroupDev {
         tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
     std::vector<DevBuf> tfaddr, dofaddr;  // per destination
 
-    // Split-precision operand A (row slices of M), built on first use per tier.
+    // Mirror of each term for symmetric element matrices (empty: none), and
+    // whether mirror coefficients are equal bit for bit; see mirror_terms in
+    // engine.cu.
+    std::vector<int32_t> mirror;
+    bool mirror_exact = false;
+
+    // Split-precision operand A (row slices of M), built on first use per
+    // tier (0 split, 1 FP32 level) and form: slot tier + 2 holds the upper
+    // triangle of a symmetric group, each row mapped to an entry and its
+    // mirror.
     struct Split {
-        int S = 0, L = 0, Qpad = 0, Ppad = 0;
-        DevBuf slices, rowexp;
+        int S = 0, L = 0, Qpad = 0, Ppad = 0, nrows = 0;
+        DevBuf slices, rowexp, rowmap;
     };
-    std::unique_ptr<Split> split[2];
+    std::unique_ptr<Split> split[4];
 
     // Record-only copy of the original description (for inspection).
     struct Record;

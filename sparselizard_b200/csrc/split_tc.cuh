@@ -54,7 +54,9 @@ struct SplitShape {
 };
 
 struct SplitParams {
-    int P, Ppad, ntp, nk;   // entries, padded entries, row tiles, K steps
+    int P, Ppad, ntp, nk;   // entries, padded rows, row tiles, K steps
+    int nrows;              // rows of A computed (P, or the upper triangle)
+    const int2* rowmap;     // [nrows]: the entry and its mirror; null: row r is entry r
     int64_t nwork;          // row tiles x element units
     const Tile* tiles;      // 64-element tiles; unit u = tile u / kUnits, part u % kUnits
     const int8_t* A;        // row slices
@@ -80,20 +82,24 @@ __device__ __forceinline__ Tile split_unit(const Tile* tiles, int64_t u)
 
 // Row slices of M for one orientation: block per row p, threads over q.
 // M[p][q] = T_t[o][i][g] * D_t[o][j][g] as in the FP64 contraction.
+// Row r of A holds entry rowmap[r].x of M (entry r without a map); rows
+// from nrows to Ppad are zero.
 struct RowSliceParams {
     const double* tables;
     const int64_t* tab_off;
     const int32_t* term_tf;
     const int32_t* term_dof;
-    int nterms, ngp, ntf, ndof, norient, S, Qpad, Ppad;
+    const int2* rowmap;
+    int nterms, ngp, ntf, ndof, norient, S, Qpad, Ppad, nrows;
     int8_t* slices;   // [orient][ptile][kstep][S][2][128][16]
     int32_t* rowexp;  // [norient][Ppad]
 };
 
+// M[pe][q] (pe < 0: zero).
 __device__ __forceinline__ double m_entry(const RowSliceParams& p, int o, int pe, int q)
 {
     const int Q = p.nterms * p.ngp;
-    if (q >= Q || pe >= p.ntf * p.ndof)
+    if (q >= Q || pe < 0)
         return 0.0;
     const int t = q / p.ngp, g = q - t * p.ngp;
     const int i = pe / p.ndof, j = pe - i * p.ndof;
@@ -118,9 +124,10 @@ __device__ __forceinline__ void split7(double x, int S, int8_t* out)
 __global__ void k_slice_rows(RowSliceParams p)
 {
     const int pe = blockIdx.x, o = blockIdx.y;
+    const int src = pe >= p.nrows ? -1 : p.rowmap != nullptr ? p.rowmap[pe].x : pe;
     __shared__ double red[256];
     double mx = 0;
-    for (int q = threadIdx.x; q < p.Qpad; q += blockDim.x) mx = fmax(mx, fabs(m_entry(p, o, pe, q)));
+    for (int q = threadIdx.x; q < p.Qpad; q += blockDim.x) mx = fmax(mx, fabs(m_entry(p, o, src, q)));
     red[threadIdx.x] = mx;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
@@ -137,7 +144,7 @@ __global__ void k_slice_rows(RowSliceParams p)
     const int pt = pe / kSplitM, r = pe % kSplitM;
     for (int q = threadIdx.x; q < p.Qpad; q += blockDim.x) {
         int8_t sl[kSplitMaxS];
-        split7(ldexp(m_entry(p, o, pe, q), -ex), p.S, sl);
+        split7(ldexp(m_entry(p, o, src, q), -ex), p.S, sl);
         const int ks = q / kSplitKStep, c = (q / 16) & 1;
         for (int s = 0; s < p.S; s++)
             p.slices[(((((int64_t)o * ntp + pt) * nk + ks) * p.S + s) * 2 + c) * (kSplitM * 16) + r * 16 + (q & 15)] = sl[s];
@@ -525,10 +532,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
             if (lane == 0)
                 mbar_arrive(&sm.tmem_empty[buf]);
             const int pe = pt * kSplitM + quarter * 32 + lane;
-            if (pe < p.P) {
+            if (pe < p.nrows) {
                 const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
                 const int32_t* ce = p.colexp + u * NE + c0;
-                double* outp = p.out + (int64_t)(unit.e0 + c0) * p.P + pe;
+                // Row pe is entry m.x and, for a symmetric group, also its
+                // mirror m.y (the same entry on the diagonal).
+                const int2 m = p.rowmap != nullptr ? p.rowmap[pe] : make_int2(pe, pe);
+                double* outp = p.out + (int64_t)(unit.e0 + c0) * p.P + m.x;
+                double* outm = m.y != m.x ? p.out + (int64_t)(unit.e0 + c0) * p.P + m.y : nullptr;
                 const int nj = min(16, unit.ne - c0);
 #pragma unroll
                 for (int j = 0; j < 16; j += 4) {
@@ -541,8 +552,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                         for (int l = 0; l < L - 5; l++) Lo = Lo * 128 + r[l][j + jj];
                         Lo <<= 7 * (8 - L);
                         const double d = fma((double)Lo, 0x1p-21, (double)H[j + jj]);
-                        if (j + jj < nj)
-                            outp[(int64_t)(j + jj) * p.P] = scale2(d, rex + cx[jj]);
+                        if (j + jj < nj) {
+                            const double v = scale2(d, rex + cx[jj]);
+                            outp[(int64_t)(j + jj) * p.P] = v;
+                            if (outm != nullptr)
+                                outm[(int64_t)(j + jj) * p.P] = v;
+                        }
                     }
                 }
             }

@@ -47,6 +47,9 @@ def _child_main(mode, workload, msh, params, out, reps):
     elif mode == "record":
         np.savez(out, **record_oracle_inproc(workload, msh, params))
         return
+    elif mode == "symmetry":
+        np.savez(out, **symmetry_inproc(workload, msh, params))
+        return
     elif mode.startswith("sweep"):
         np.savez(out, **sweep_inproc(msh, params, mode.split(":")[1]))
         return
@@ -98,9 +101,49 @@ def reference(workload, msh, params, reps=1):
         return _child("ref", workload, msh, params, os.path.join(d, "o.npz"), reps=reps)
 
 
-def gpu(workload, msh, params, precision="fp64", reps=1):
+def gpu(workload, msh, params, precision="fp64", reps=1, env=None):
     with tempfile.TemporaryDirectory() as d:
-        return _child("gpu", workload, msh, params, os.path.join(d, "o.npz"), {"SLGPU_PRECISION": precision}, reps=reps)
+        return _child("gpu", workload, msh, params, os.path.join(d, "o.npz"), dict(env or {}, SLGPU_PRECISION=precision),
+                      reps=reps)
+
+
+def record_symmetry(workload, msh, params):
+    """Lowers the workload on a record-only context (no GPU) and returns, per
+    matrix group, its term count, the mirror term of each term
+    (slgpu_matrix_group_symmetry) and whether the split contraction would
+    compute only the upper triangle."""
+    with tempfile.TemporaryDirectory() as d:
+        return _child("symmetry", workload, msh, params, os.path.join(d, "o.npz"), {"SLGPU_RECORD_ONLY": "1"})
+
+
+def symmetry_inproc(workload, msh, params):
+    from sparselizard_b200 import abi
+    from sparselizard_b200 import workloads as W
+
+    assert os.environ.get("SLGPU_RECORD_ONLY") == "1"
+    lib = W.load(GPU_LIB)
+    try:
+        W.run(GPU_LIB, workload, msh, params)
+    except RuntimeError as e:
+        assert "record-only" in str(e), str(e)
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+    h = lib.slgpu_adapter_last_handle()
+    ng = ctypes.c_int()
+    assert lib.slgpu_matrix_group_count(ctx, h, ctypes.byref(ng)) == 0
+    nterms, mirror, sym = [], [], []
+    for gi in range(ng.value):
+        desc = abi.GroupDesc()
+        assert lib.slgpu_matrix_group_desc(ctx, h, gi, ctypes.byref(desc)) == 0
+        m = np.zeros(desc.nterms, np.int32)
+        s = ctypes.c_int32()
+        assert lib.slgpu_matrix_group_symmetry(ctx, h, gi, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s)) == 0
+        nterms.append(desc.nterms)
+        mirror.append(m)
+        sym.append(s.value)
+    return dict(nterms=np.array(nterms, np.int32), mirror=np.concatenate(mirror) if mirror else np.zeros(0, np.int32),
+                symmetric=np.array(sym, np.int32))
 
 
 def record_oracle(workload, msh, params):

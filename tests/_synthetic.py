@@ -41,8 +41,16 @@ def quad_mesh_arrays(n, rng, jitter=0.2):
 
 
 def group(rng, nelem_grid=8, ntf=5, ndof=3, nterms=3, ngp1=3, norient=2, ndests=2, ndofs=60, rhs=False, p_neg=0.1,
-          with_elemdata=True):
-    """Returns (GroupBuilder, xyz, conn, extra) for a random quad group."""
+          with_elemdata=True, symmetric=False):
+    """Returns (GroupBuilder, xyz, conn, extra) for a random quad group.
+
+    symmetric: element matrices symmetric by construction (ntf == ndof).
+    Terms 2k and 2k+1 are mirrors: each one's dof table is a copy of the
+    other's test-function table, and their coefficients are the same
+    expression with the operands of one product swapped; equal scales.  An
+    odd last term is its own mirror."""
+    if symmetric:
+        assert ntf == ndof and not rhs
     xyz, conn = quad_mesh_arrays(nelem_grid, rng)
     nelem = nelem_grid * nelem_grid
     x, w = gauss_1d(ngp1)
@@ -53,7 +61,10 @@ def group(rng, nelem_grid=8, ntf=5, ndof=3, nterms=3, ngp1=3, norient=2, ndests=
     elems = rng.permutation(nelem).astype(np.int32)
     orient = np.sort(rng.integers(0, norient, nelem)).astype(np.int32)
     tables = [rng.standard_normal((norient, ntf, ngp)) for _ in range(nterms)]
-    if not rhs:
+    mirror = [t ^ 1 if (t ^ 1) < nterms else t for t in range(nterms)]
+    if symmetric:
+        tables += [tables[mirror[t]].copy() for t in range(nterms)]
+    elif not rhs:
         tables += [rng.standard_normal((norient, ndof, ngp)) for _ in range(nterms)]
     consts = rng.standard_normal(4)
     # coef_t = c0*invJ(0,t%2)*invJ(1,(t+1)%2) + c1*E/(detJ) + x coordinate, E per element.
@@ -71,12 +82,13 @@ def group(rng, nelem_grid=8, ntf=5, ndof=3, nterms=3, ngp1=3, norient=2, ndests=
     base = len(nodes)
     coef_nodes = []
     for t in range(nterms):
-        a, b = t % 2, (t + 1) % 2
+        k = t // 2 if symmetric else t
+        a, b = k % 2, (k + 1) % 2
         nodes.append((abi.OP_INVJAC, 0, a, 0))
         i1 = len(nodes) - 1
         nodes.append((abi.OP_INVJAC, 1, b, 0))
         i2 = len(nodes) - 1
-        nodes.append((abi.OP_MUL, i1, i2, 0))
+        nodes.append((abi.OP_MUL, i2, i1, 0) if symmetric and t % 2 else (abi.OP_MUL, i1, i2, 0))
         m = len(nodes) - 1
         nodes.append((abi.OP_MUL, m, 0, 0))
         m0 = len(nodes) - 1
@@ -89,8 +101,9 @@ def group(rng, nelem_grid=8, ntf=5, ndof=3, nterms=3, ngp1=3, norient=2, ndests=
         nodes.append((abi.OP_ADD, s, 4, 0))
         coef_nodes.append(len(nodes) - 1)
     terms = []
+    scales = [float(rng.choice([1.0, -0.5, 2.0])) for _ in range(nterms)]
     for t in range(nterms):
-        terms.append((t, -1 if rhs else nterms + t, coef_nodes[t], float(rng.choice([1.0, -0.5, 2.0]))))
+        terms.append((t, -1 if rhs else nterms + t, coef_nodes[t], scales[min(t, mirror[t])] if symmetric else scales[t]))
 
     def addr(rows):
         a = rng.integers(0, ndofs, (rows, nelem)).astype(np.int32)

@@ -93,3 +93,85 @@ def test_meshgen_tets_positive_and_conforming(tmp_path):
             faces[k] = faces.get(k, 0) + 1
     assert max(faces.values()) == 2
     assert sum(1 for v in faces.values() if v == 1) == 6 * 2 * n * n
+
+
+def _add_record_group(c, gb, xyz, conn):
+    L = c.lib
+    c.check(L.slgpu_mesh_set_nodes(c.h, 0, xyz.size // 3, abi.f64p(xyz)))
+    c.check(L.slgpu_mesh_set_elements(c.h, 0, 3, 4, conn.size // 4, abi.i32p(conn)))
+    h = ctypes.c_int()
+    c.check(L.slgpu_matrix_create(c.h, 60, ctypes.byref(h)))
+    c.check(L.slgpu_matrix_add_group(c.h, h, ctypes.byref(gb.g), None))
+    return h.value
+
+
+def _symmetry(c, h, nterms):
+    m = np.zeros(nterms, np.int32)
+    s = ctypes.c_int32()
+    c.check(c.lib.slgpu_matrix_group_symmetry(c.h, h, 0, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s)))
+    return m, s.value
+
+
+def test_symmetry_detection_synthetic():
+    """Mirror terms: copied tables and coefficients that differ only in the
+    operand order of a product are found; scales that differ turn the
+    symmetric contraction off and back on; one changed constant, or distinct
+    tables, leave a group without mirrors."""
+    from _synthetic import group
+
+    c = abi.Context(0, flags=abi.CTX_RECORD_ONLY)
+    L = c.lib
+    gb, xyz, conn = group(np.random.Generator(np.random.PCG64(3)), ntf=6, ndof=6, nterms=5, symmetric=True, ndests=1)
+    h = _add_record_group(c, gb, xyz, conn)
+    m, s = _symmetry(c, h, 5)
+    assert m.tolist() == [1, 0, 3, 2, 4] and s == 1
+    sc = np.zeros(5)
+    c.check(L.slgpu_matrix_get_scales(c.h, h, 0, abi.f64p(sc), None))
+    sc2 = sc.copy()
+    sc2[1] *= 1.0000001
+    c.check(L.slgpu_matrix_set_scales(c.h, h, 0, abi.f64p(sc2), None))
+    assert _symmetry(c, h, 5)[1] == 0
+    c.check(L.slgpu_matrix_set_scales(c.h, h, 0, abi.f64p(sc), None))
+    assert _symmetry(c, h, 5)[1] == 1
+
+    # A different constant in one mirror's coefficient: no mirror for it.
+    gb, xyz, conn = group(np.random.Generator(np.random.PCG64(3)), ntf=6, ndof=6, nterms=4, symmetric=True, ndests=1)
+    nodes = [(gb.g.nodes[k].op, gb.g.nodes[k].a, gb.g.nodes[k].b, gb.g.nodes[k].c) for k in range(gb.g.nnodes)]
+    t3 = gb.g.terms[3].coef_node
+    gb.g.nodes[t3].b = 2  # x + detJ instead of x + coordinate
+    h = _add_record_group(c, gb, xyz, conn)
+    m, s = _symmetry(c, h, 4)
+    assert (m == -1).all() and s == 0
+    assert nodes[t3][0] == abi.OP_ADD
+
+    # Independent random tables: not symmetric.
+    gb, xyz, conn = group(np.random.Generator(np.random.PCG64(3)), ntf=6, ndof=6, nterms=4, ndests=1)
+    h = _add_record_group(c, gb, xyz, conn)
+    m, s = _symmetry(c, h, 4)
+    assert (m == -1).all() and s == 0
+    c.close()
+
+
+def test_symmetry_detection_workloads(gpu_lib, tmp_path):
+    """On the drop-in's lowering (record-only context): every group of the
+    p-adaptive Helmholtz problem (grad-grad and mass terms) has mirror terms,
+    pairing d/dx_a with d/dx_b; of the nine component blocks of the
+    order-2 elasticity problem, the three diagonal ones do."""
+    n = 2
+    rng = np.random.Generator(np.random.PCG64(7))
+    tags = meshgen.ORDER_REGION_BASE + rng.integers(1, 6, size=6 * n ** 3)
+    msh = str(tmp_path / "t.msh")
+    meshgen.tet_mesh(msh, n, jitter=0.1, seed=2, element_tags=tags)
+    from sparselizard_b200 import workloads as W
+
+    r = P.record_symmetry(W.HELMHOLTZ_TET, msh, [])
+    assert len(r["symmetric"]) >= 3 and (r["symmetric"] == 1).all()
+    off = 0
+    for nt in r["nterms"]:
+        m = r["mirror"][off:off + nt]
+        assert (m[m] == np.arange(nt)).all() and (m != np.arange(nt)).sum() == 6  # three swapped pairs
+        off += nt
+    msh = str(tmp_path / "h.msh")
+    meshgen.hex_mesh(msh, 2, jitter=0.15, seed=1)
+    r = P.record_symmetry(W.ELASTICITY_HEX, msh, [2, -2])
+    assert r["symmetric"].tolist() == [2, 0, 0, 0, 2, 0, 0, 0, 2]

@@ -77,6 +77,52 @@ def test_split_many_tiles(ctx, seed, grid, ntf, ndof, norient, nterms, ngp1):
         assert err.max() <= tol, f"precision {prec}: per-element Frobenius error {err.max():.3e} > {tol:g}"
 
 
+@pytest.mark.parametrize("seed,grid,n,norient,nterms,ngp1", [(6, 14, 9, 2, 5, 3), (7, 60, 20, 3, 4, 4), (8, 30, 27, 1, 9, 3)])
+def test_split_symmetric_group(ctx, seed, grid, n, norient, nterms, ngp1):
+    """A group with mirror terms: the split contraction computes the upper
+    triangle (1 to 3 row tiles, the last one partly filled) and mirrors it.
+    The element matrices are symmetric bit for bit and within the split
+    tiers' bounds of the FP64 path."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gb, xyz, conn = S.group(rng, nelem_grid=grid, ntf=n, ndof=n, nterms=nterms, ngp1=ngp1, norient=norient, ndests=1,
+                            symmetric=True)
+    ref = _element_matrices(ctx, gb, xyz, conn, abi.PREC_FP64)
+    for prec, tol in ((abi.PREC_SPLIT, 1e-10), (abi.PREC_FP32, 1e-6)):
+        got = _element_matrices(ctx, gb, xyz, conn, prec)
+        m = got.reshape(-1, n, n)
+        assert np.array_equal(m, m.transpose(0, 2, 1)), f"precision {prec}: element matrices not symmetric"
+        err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert err.max() <= tol, f"precision {prec}: per-element Frobenius error {err.max():.3e} > {tol:g}"
+
+
+def test_split_symmetry_matches_full_contraction(ref_lib, gpu_lib, tmp_path):
+    """The mirrored split contraction against the full one
+    (SLGPU_SPLIT_SYMMETRY=0) through the drop-in.  p-adaptive Helmholtz
+    tetrahedra, whose mirror coefficients are equal bit for bit: the same
+    matrix bit for bit.  Order-2 elasticity, whose diagonal blocks' mirror
+    coefficients differ in the order of their factors: within 1e-14 of the
+    largest entry.  Both within 1e-10 of the reference."""
+    n = 3
+    rng = np.random.Generator(np.random.PCG64(7))
+    tags = meshgen.ORDER_REGION_BASE + rng.integers(1, 6, size=6 * n ** 3)
+    tmsh = str(tmp_path / "t.msh")
+    meshgen.tet_mesh(tmsh, n, jitter=0.1, seed=2, element_tags=tags)
+    hmsh = str(tmp_path / "h.msh")
+    meshgen.hex_mesh(hmsh, 3, jitter=0.15, seed=1)
+    for args, exact in (((W.HELMHOLTZ_TET, tmsh, []), True), ((W.ELASTICITY_HEX, hmsh, [2, -2]), False)):
+        sym = P.gpu(*args, precision="split")
+        full = P.gpu(*args, precision="split", env={"SLGPU_SPLIT_SYMMETRY": "0"})
+        P.check_pattern(full, sym)
+        for k in ("Avals", "Dvals", "b"):
+            if exact:
+                assert np.array_equal(sym[k], full[k]), f"workload {args[0]}: {k} differs"
+            elif full[k].size:
+                d = np.abs(sym[k] - full[k]).max() / max(np.abs(full[k]).max(), 1e-300)
+                assert d <= 1e-14, f"workload {args[0]}: {k} differs by {d:.3e}"
+        _, _, fro = P.scaled_errors(P.reference(*args), sym)
+        assert fro <= 1e-10, f"workload {args[0]}: assembled Frobenius-relative error {fro:.3e}"
+
+
 def test_split_dropin_elasticity(ref_lib, gpu_lib, tmp_path):
     msh = str(tmp_path / "h.msh")
     meshgen.hex_mesh(msh, 4, jitter=0.15, seed=1)
