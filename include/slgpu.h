@@ -216,9 +216,13 @@ int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_sca
  * with equal scales): 1 when every coefficient equals its mirror's bit for
  * bit (the mirrored result is then the unmirrored one bit for bit), 2 when
  * some differ in the order of their factors (a few units in the last place).
- * The reference computes full element matrices
- * (src/formulation/contribution.cpp:155-249). */
-int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric);
+ * *partner (may be NULL) is the group whose element matrices are the
+ * transposes of this group's (same elements and data, ntf and ndof swapped,
+ * terms matched with tables swapped, coefficients of the same expression and
+ * equal scales), so that one split-precision contraction writes both; -1
+ * when there is none.  The reference computes full element matrices for
+ * every group (src/formulation/contribution.cpp:155-249). */
+int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric, int32_t* partner);
 /* isconstrained [ndofs] (dofmanager::isconstrained, src/formulation/dofmanager.cpp:366-382). */
 int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstrained, int precision, slgpu_csr_info* info);
 /* Copies the processed CSR blocks to host memory: Arows/Drows [nA+1], Acols/Avals [nnzA], Dcols/Dvals [nnzD]. */

@@ -111,7 +111,7 @@ SIGNATURES = {
     "slgpu_matrix_set_fielddata": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double)]),
     "slgpu_matrix_set_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_matrix_get_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
-    "slgpu_matrix_group_symmetry": (c_int, [c_void_p, c_int, c_int, POINTER(c_int32), POINTER(c_int32)]),
+    "slgpu_matrix_group_symmetry": (c_int, [c_void_p, c_int, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
     "slgpu_ctx_set_graphs": (c_int, [c_void_p, c_int]),
     "slgpu_graph_launches": (c_int64, [c_void_p]),

@@ -433,6 +433,94 @@ static Mirror mirror_terms(const slgpu_group& g)
     return m;
 }
 
+// 128-bit content keys (two independent 64-bit mixes).
+static GroupDev::Key key_mix(GroupDev::Key k, uint64_t v)
+{
+    return {mix64(k.a ^ v), mix64(k.b + (v ^ 0xD6E8FEB86659FD93ull) * 0x9E3779B97F4A7C15ull)};
+}
+
+static GroupDev::Key key_of(const double* v, size_t n, uint64_t tag)
+{
+    GroupDev::Key k{tag, ~tag};
+    k = key_mix(k, n);
+    for (size_t i = 0; i < n; i++) {
+        uint64_t w;
+        std::memcpy(&w, &v[i], 8);
+        k = key_mix(k, w);
+    }
+    return k;
+}
+
+// Per-term content keys (tables by value, coefficient nodes by expression with
+// + operands and product factors in any order) and data array keys.
+static void content_keys(const slgpu_group& g, GroupDev& gd)
+{
+    gd.term_keys.clear();
+    gd.data_keys.clear();
+    for (int k = 0; k < g.nelemdata; k++) gd.data_keys.push_back(key_of(g.elemdata[k], (size_t)g.nelem, 1));
+    for (int k = 0; k < g.nfielddata; k++)
+        gd.data_keys.push_back(key_of(g.fielddata[k], (size_t)g.fieldrows[k] * g.nelem, 2));
+    if (g.terms[0].dof_table < 0)
+        return;
+    std::vector<GroupDev::Key> tk(g.ntables);
+    for (int k = 0; k < g.ntables; k++)
+        tk[k] = key_mix(key_of(g.tables[k].vals, (size_t)g.norient * g.tables[k].rows * g.ngp, 3), (uint64_t)g.tables[k].rows);
+    std::vector<GroupDev::Key> nk(g.nnodes);
+    std::vector<std::vector<GroupDev::Key>> factors(g.nnodes);
+    auto less = [](const GroupDev::Key& x, const GroupDev::Key& y) { return x.a != y.a ? x.a < y.a : x.b < y.b; };
+    for (int k = 0; k < g.nnodes; k++) {
+        const slgpu_node& nd = g.nodes[k];
+        // Operands precede their node (checked by the program compiler for
+        // the nodes it uses); others key as zero.
+        auto at = [&](int x) { return x >= 0 && x < k ? nk[x] : GroupDev::Key{}; };
+        GroupDev::Key h{(uint64_t)nd.op * 0x100000001B3ull, (uint64_t)nd.op};
+        switch (nd.op) {
+        case SLGPU_OP_CONST: {
+            uint64_t w = 0;
+            if (nd.a >= 0 && nd.a < g.nconsts)
+                std::memcpy(&w, &g.consts[nd.a], 8);
+            h = key_mix(h, w);
+            break;
+        }
+        case SLGPU_OP_FIELD:
+            h = key_mix(key_mix(h, (uint64_t)nd.a), nd.b >= 0 && nd.b < g.ntables ? tk[nd.b].a : 0);
+            h = key_mix(h, nd.b >= 0 && nd.b < g.ntables ? tk[nd.b].b : 0);
+            break;
+        case SLGPU_OP_ADD: {
+            GroupDev::Key x = at(nd.a), y = at(nd.b);
+            if (less(y, x))
+                std::swap(x, y);
+            h = key_mix(key_mix(key_mix(key_mix(h, x.a), x.b), y.a), y.b);
+            break;
+        }
+        case SLGPU_OP_MUL: {
+            std::vector<GroupDev::Key>& f = factors[k];
+            for (int x : {nd.a, nd.b}) {
+                if (x >= 0 && x < k && g.nodes[x].op == SLGPU_OP_MUL)
+                    f.insert(f.end(), factors[x].begin(), factors[x].end());
+                else
+                    f.push_back(at(x));
+            }
+            std::sort(f.begin(), f.end(), less);
+            for (const GroupDev::Key& x : f) h = key_mix(key_mix(h, x.a), x.b);
+            break;
+        }
+        case SLGPU_OP_POW:
+            h = key_mix(key_mix(key_mix(key_mix(h, at(nd.a).a), at(nd.a).b), at(nd.b).a), at(nd.b).b);
+            break;
+        case SLGPU_OP_INV:
+        case SLGPU_OP_NEG:
+            h = key_mix(key_mix(h, at(nd.a).a), at(nd.a).b);
+            break;
+        default:
+            h = key_mix(key_mix(key_mix(h, (uint64_t)(uint32_t)nd.a), (uint64_t)(uint32_t)nd.b), (uint64_t)(uint32_t)nd.c);
+            break;
+        }
+        nk[k] = h;
+    }
+    for (int t = 0; t < g.nterms; t++) gd.term_keys.push_back({tk[g.terms[t].tf_table], tk[g.terms[t].dof_table], nk[g.terms[t].coef_node]});
+}
+
 static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
 {
     validate_group(g);
@@ -459,6 +547,7 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
         gd->mirror = std::move(m.term);
         gd->mirror_exact = m.exact;
     }
+    content_keys(g, *gd);
     gd->hconsts.assign(g.consts, g.consts + g.nconsts);
     {
         // Geometry key: groups with the same key share elements, orientations,
@@ -1213,13 +1302,18 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 // Whether the split contraction of a group computes only the upper triangle
 // of its element matrices: the group has mirror terms with equal scales
 // (SLGPU_SPLIT_SYMMETRY=0 turns this off).
-static bool split_symmetric(const GroupDev& g)
+static bool split_symmetry_enabled()
 {
     static const bool enabled = [] {
         const char* v = std::getenv("SLGPU_SPLIT_SYMMETRY");
         return v == nullptr || std::strcmp(v, "0") != 0;
     }();
-    if (!enabled || g.mirror.empty())
+    return enabled;
+}
+
+static bool split_symmetric(const GroupDev& g)
+{
+    if (!split_symmetry_enabled() || g.mirror.empty())
         return false;
     for (int t = 0; t < g.nterms; t++)
         if (std::memcmp(&g.term_scale[t], &g.term_scale[g.mirror[t]], sizeof(double)) != 0)
@@ -1227,28 +1321,43 @@ static bool split_symmetric(const GroupDev& g)
     return true;
 }
 
+// Rows of A for the mirrored forms (the upper triangle of a symmetric group,
+// or every entry of a group with a transposed partner), each with the entry
+// it is and the entry its value also goes to: (j, i) of the same matrix, or
+// (j, i) of the partner's.  They come in blocks of 4 rows i by 8 columns j
+// (row-major inside a block), so that a warp's 32 stores of one element
+// cover 4 runs of 8 entries and their mirrors 8 runs of 4, rather than one
+// run of 32 and 32 scattered entries.
+static std::vector<int2> mirrored_rows(int ntf, int ndof, bool upper)
+{
+    std::vector<int2> map;
+    for (int bi = 0; bi < ntf; bi += 4)
+        for (int bj = 0; bj < ndof; bj += 8)
+            for (int i = bi; i < std::min(bi + 4, ntf); i++)
+                for (int j = bj; j < std::min(bj + 8, ndof); j++)
+                    if (!upper || j >= i)
+                        map.push_back(make_int2(i * ndof + j, j * ntf + i));
+    return map;
+}
+
+// Row slices of a group for a tier (0 split, 1 FP32 level) and form (0 every
+// entry, 1 upper triangle of a symmetric group, 2 every entry with its
+// transposed partner's): slot tier + 2 form.
 static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int slot)
 {
     std::unique_ptr<GroupDev::Split>& sp = g.split[slot];
     if (sp)
         return *sp;
-    const int tier = slot & 1;
-    const bool sym = slot >= 2;
+    const int tier = slot & 1, form = slot >> 1;
     sp.reset(new GroupDev::Split());
     sp->S = tier == 0 ? 7 : 5;
     sp->L = tier == 0 ? 8 : 6;
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
     sp->Qpad = std::max(kSplitKStep, (Q + kSplitKStep - 1) / kSplitKStep * kSplitKStep);
-    sp->nrows = sym ? g.ntf * (g.ntf + 1) / 2 : P;
+    sp->nrows = form == 1 ? g.ntf * (g.ntf + 1) / 2 : P;
     sp->Ppad = (sp->nrows + kSplitM - 1) / kSplitM * kSplitM;
-    if (sym) {
-        // Rows (i, j), i <= j, row-major: entry i ndof + j and its mirror.
-        std::vector<int2> map;
-        map.reserve(sp->nrows);
-        for (int i = 0; i < g.ntf; i++)
-            for (int j = i; j < g.ntf; j++) map.push_back(make_int2(i * g.ndof + j, j * g.ndof + i));
-        upload(ctx, sp->rowmap, map);
-    }
+    if (form != 0)
+        upload(ctx, sp->rowmap, mirrored_rows(g.ntf, g.ndof, form == 1));
     sp->slices.alloc(ctx, (size_t)sp->S * g.norient * sp->Qpad * sp->Ppad);
     sp->rowexp.alloc(ctx, (size_t)g.norient * sp->Ppad * 4);
     RowSliceParams rp{};
@@ -1278,9 +1387,9 @@ static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int slot)
 
 // The row slices are resident with the group, so they are built in the main
 // execution state's stream order; a request stream waits for them.
-static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier)
+static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier, bool paired)
 {
-    const int slot = tier + (split_symmetric(g) ? 2 : 0);
+    const int slot = tier + 2 * (paired ? 2 : split_symmetric(g) ? 1 : 0);
     if (g.split[slot])
         return *g.split[slot];
     Exec* cur = ctx->x;
@@ -1372,7 +1481,8 @@ static void slice_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, 
 }
 
 // The tcgen05 contraction of one group from its column slices.
-static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const int8_t* slices, const int32_t* colexp, double* out)
+static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const int8_t* slices, const int32_t* colexp, double* out,
+                        double* out2)
 {
     const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
     const int NE = split_tile_width();
@@ -1381,6 +1491,7 @@ static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, 
     p.P = P;
     p.nrows = sp.nrows;
     p.rowmap = sp.rowmap.empty() ? nullptr : sp.rowmap.as<int2>();
+    p.out2 = out2;
     p.Ppad = sp.Ppad;
     p.ntp = sp.Ppad / kSplitM;
     p.nk = sp.Qpad / kSplitKStep;
@@ -1412,10 +1523,11 @@ static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, 
 
 // Split contraction of one group: column slices of C (exponents per element
 // from the coefficient kernel) into the execution state's scratch, then the
-// tcgen05 kernel.
-static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out)
+// tcgen05 kernel (which also writes the transposed partner's element matrices
+// into out2, if given).
+static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out, double* out2)
 {
-    const GroupDev::Split& sp = ensure_split(ctx, g, tier);
+    const GroupDev::Split& sp = ensure_split(ctx, g, tier, out2 != nullptr);
     const int64_t ntiles = (int64_t)g.tiles.size();
     const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
     {
@@ -1426,7 +1538,7 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
             ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
     }
     slice_group(ctx, g, sp, C, elemexp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>());
-    split_group(ctx, g, sp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>(), out);
+    split_group(ctx, g, sp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>(), out, out2);
 }
 
 // Whether a group's contraction runs in split precision: element matrices
@@ -1435,6 +1547,72 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
 static bool uses_split(const GroupDev& g, int precision)
 {
     return precision != SLGPU_PREC_FP64 && !g.rhs && (int64_t)g.ntf * g.ndof >= 64 && split_supported(g);
+}
+
+// Transposed pairs among a matrix's split-precision groups: group j is the
+// partner of group i when its element matrices are the transposes of i's:
+// same elements, orientations and geometry, ntf and ndof swapped, the same
+// element and field data, and a one-to-one map of terms u = pi(t) with u's
+// test-function table holding the values of t's dof table, u's dof table
+// those of t's test-function table, the same coefficient expression (factors
+// in any order) and the same scale.  The contraction of the lower-numbered
+// group then also writes the other's element matrices, transposed, and the
+// other's contraction is skipped.  Groups whose data are replaced for one
+// assembly (`ov`) and groups contracted as symmetric are not paired.
+// Returns the partner of each group (-1: none).
+static std::vector<int> cross_pairs(const Matrix& M, int precision, const std::vector<GroupData>* ov)
+{
+    const size_t n = M.groups.size();
+    std::vector<int> pair(n, -1);
+    static const bool enabled = [] {
+        const char* v = std::getenv("SLGPU_SPLIT_PAIRS");
+        return v == nullptr || std::strcmp(v, "0") != 0;
+    }();
+    if (precision == SLGPU_PREC_FP64 || !enabled || !split_symmetry_enabled())
+        return pair;
+    auto eligible = [&](size_t i) {
+        const GroupDev& g = *M.groups[i];
+        if (g.nelem == 0 || !uses_split(g, precision) || split_symmetric(g) || g.term_keys.empty())
+            return false;
+        return ov == nullptr || ((*ov)[i].elemdata == nullptr && (*ov)[i].fielddata == nullptr);
+    };
+    std::vector<char> used;
+    for (size_t i = 0; i < n; i++) {
+        if (pair[i] >= 0 || !eligible(i))
+            continue;
+        const GroupDev& a = *M.groups[i];
+        for (size_t j = i + 1; j < n; j++) {
+            if (pair[j] >= 0 || !eligible(j))
+                continue;
+            const GroupDev& b = *M.groups[j];
+            if (b.mesh != a.mesh || b.elemtype != a.elemtype || b.geom_hash != a.geom_hash || b.nelem != a.nelem ||
+                b.ngp != a.ngp || b.norient != a.norient || b.ntf != a.ndof || b.ndof != a.ntf || b.nterms != a.nterms ||
+                !(b.data_keys == a.data_keys))
+                continue;
+            used.assign(b.nterms, 0);
+            bool ok = true;
+            for (int t = 0; t < a.nterms && ok; t++) {
+                const GroupDev::TermKey& ka = a.term_keys[t];
+                int found = -1;
+                for (int u = 0; u < b.nterms && found < 0; u++) {
+                    const GroupDev::TermKey& kb = b.term_keys[u];
+                    if (!used[u] && kb.tf == ka.dof && kb.dof == ka.tf && kb.coef == ka.coef &&
+                        std::memcmp(&b.term_scale[u], &a.term_scale[t], sizeof(double)) == 0)
+                        found = u;
+                }
+                if (found < 0)
+                    ok = false;
+                else
+                    used[found] = 1;
+            }
+            if (ok) {
+                pair[i] = (int)j;
+                pair[j] = (int)i;
+                break;
+            }
+        }
+    }
+    return pair;
 }
 
 // Host mirror of the runtime-compiled kernel's parameter structs (coef_jit.cu).
@@ -1592,14 +1770,18 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     phase_event(ctx, ctx->x->evpool[0]);
     launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov);
     phase_event(ctx, ctx->x->evpool[1]);
+    const std::vector<int> pair = cross_pairs(M, precision, ov);
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
             double* Cg = C.as<double>() + coff[gi];
             // Split precision for the larger element matrices (order >= 2);
-            // right-hand sides and small matrices stay in FP64.
+            // right-hand sides and small matrices stay in FP64.  The second
+            // group of a transposed pair is written by the first's contraction.
             if (uses_split(*g, precision)) {
-                contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], vals + gvb[gi]);
+                if (pair[gi] < 0 || pair[gi] > (int)gi)
+                    contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], vals + gvb[gi],
+                                   pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr);
                 gi++;
                 continue;
             }
@@ -1870,12 +2052,19 @@ void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
         return;
     const int tier = precision == SLGPU_PREC_SPLIT ? 0 : 1;
     size_t colbytes = 0, expbytes = 0;
-    for (auto& g : M.groups)
+    // Both the unpaired form (assemblies with replaced data) and, for the
+    // first group of a transposed pair, the paired one.
+    const std::vector<int> pair = cross_pairs(M, precision, nullptr);
+    for (size_t gi = 0; gi < M.groups.size(); gi++) {
+        GroupDev* g = M.groups[gi].get();
         if (g->nelem > 0 && uses_split(*g, precision)) {
-            const GroupDev::Split& sp = ensure_split(ctx, *g, tier);
+            const GroupDev::Split& sp = ensure_split(ctx, *g, tier, false);
+            if (pair[gi] > (int)gi)
+                ensure_split(ctx, *g, tier, true);
             colbytes = std::max(colbytes, (size_t)sp.S * sp.Qpad * g->tiles.size() * 64);
             expbytes = std::max(expbytes, g->tiles.size() * 64 * 4);
         }
+    }
     Exec& x = *ctx->x;
     if (x.split_cols.bytes() < colbytes)
         x.split_cols.alloc(ctx, colbytes);
@@ -1923,6 +2112,8 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
     p(x.split_cols.as<void>());
     p(x.split_colexp.as<void>());
     p(x.split_error.as<void>());
+    const std::vector<int> pair = cross_pairs(M, precision, nullptr);
+    size_t gi = 0;
     for (auto& gp : M.groups) {
         const GroupDev& g = *gp;
         u(g.serial);
@@ -1930,7 +2121,8 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
         u(g.jit_members.size());
         for (uint64_t id : g.jit_members) u(id);
         u(split_symmetric(g) ? 1 : 0);
-        for (int t = 0; t < 4; t++) {
+        u((uint64_t)(pair[gi++] + 1));
+        for (int t = 0; t < 6; t++) {
             p(g.split[t] ? g.split[t]->slices.as<void>() : nullptr);
             p(g.split[t] ? g.split[t]->rowexp.as<void>() : nullptr);
         }
@@ -2463,6 +2655,7 @@ int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const d
         GroupDev& g = *M.groups[gi];
         if (k < 0 || k >= (int)g.elemdata_off.size())
             fail(SLGPU_E_ARG, "element data index out of range");
+        g.data_keys[k] = key_of(values, (size_t)g.nelem, 1);
         if (ctx->record_only) {
             std::copy(values, values + g.nelem, g.rec->elemdata[k].begin());
             return;
@@ -2483,6 +2676,7 @@ int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const 
         if (k < 0 || k >= (int)g.field_off.size())
             fail(SLGPU_E_ARG, "field data index out of range");
         const size_t n = (size_t)g.field_rows[k] * g.nelem;
+        g.data_keys[g.elemdata_off.size() + k] = key_of(values, n, 2);
         if (ctx->record_only) {
             std::copy(values, values + n, g.rec->fielddata[k].begin());
             return;
@@ -2591,7 +2785,7 @@ int slgpu_matrix_get_scales(slgpu_ctx* ctx, int handle, int gi, double* term_sca
     });
 }
 
-int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric)
+int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mirror, int32_t* symmetric, int32_t* partner)
 {
     return guarded(ctx, [&] {
         Matrix& M = get_matrix(ctx, handle);
@@ -2602,6 +2796,8 @@ int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mir
             for (int t = 0; t < g.nterms; t++) mirror[t] = g.mirror.empty() ? -1 : g.mirror[t];
         if (symmetric != nullptr)
             *symmetric = split_symmetric(g) ? (g.mirror_exact ? 1 : 2) : 0;
+        if (partner != nullptr)
+            *partner = cross_pairs(M, SLGPU_PREC_SPLIT, nullptr)[gi];
     });
 }
 

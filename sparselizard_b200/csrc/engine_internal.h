@@ -114,16 +114,30 @@ struct GroupDev {
     // engine.cu.
     std::vector<int32_t> mirror;
     bool mirror_exact = false;
+    // Content keys for transposed pairs of groups (cross_pairs in engine.cu):
+    // per term its test-function table, dof table and coefficient expression
+    // (up to the order of factors), and per element / field data array its
+    // values (updated when an array is replaced).
+    struct Key {
+        uint64_t a = 0, b = 0;
+        bool operator==(const Key& o) const { return a == o.a && b == o.b; }
+    };
+    struct TermKey {
+        Key tf, dof, coef;
+    };
+    std::vector<TermKey> term_keys;
+    std::vector<Key> data_keys;  // elemdata arrays, then fielddata arrays
 
     // Split-precision operand A (row slices of M), built on first use per
-    // tier (0 split, 1 FP32 level) and form: slot tier + 2 holds the upper
-    // triangle of a symmetric group, each row mapped to an entry and its
-    // mirror.
+    // tier (0 split, 1 FP32 level) and form (0 every entry; 1 the upper
+    // triangle of a symmetric group and 2 every entry of a group with a
+    // transposed partner, each row mapped to an entry and its mirror):
+    // slot tier + 2 form.
     struct Split {
         int S = 0, L = 0, Qpad = 0, Ppad = 0, nrows = 0;
         DevBuf slices, rowexp, rowmap;
     };
-    std::unique_ptr<Split> split[4];
+    std::unique_ptr<Split> split[6];
 
     // Record-only copy of the original description (for inspection).
     struct Record;

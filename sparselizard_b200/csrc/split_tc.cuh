@@ -57,6 +57,8 @@ struct SplitParams {
     int P, Ppad, ntp, nk;   // entries, padded rows, row tiles, K steps
     int nrows;              // rows of A computed (P, or the upper triangle)
     const int2* rowmap;     // [nrows]: the entry and its mirror; null: row r is entry r
+    double* out2;           // null, or [nelem][P]: the transposed partner group's
+                            // element matrices (entry rowmap[r].y from row r)
     int64_t nwork;          // row tiles x element units
     const Tile* tiles;      // 64-element tiles; unit u = tile u / kUnits, part u % kUnits
     const int8_t* A;        // row slices
@@ -536,10 +538,13 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                 const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
                 const int32_t* ce = p.colexp + u * NE + c0;
                 // Row pe is entry m.x and, for a symmetric group, also its
-                // mirror m.y (the same entry on the diagonal).
+                // mirror m.y (the same entry on the diagonal); with a
+                // transposed partner, entry (i, j) is also the partner's
+                // entry (j, i).
                 const int2 m = p.rowmap != nullptr ? p.rowmap[pe] : make_int2(pe, pe);
-                double* outp = p.out + (int64_t)(unit.e0 + c0) * p.P + m.x;
-                double* outm = m.y != m.x ? p.out + (int64_t)(unit.e0 + c0) * p.P + m.y : nullptr;
+                const int64_t ebase = (int64_t)(unit.e0 + c0) * p.P;
+                double* outp = p.out + ebase + m.x;
+                double* outm = p.out2 != nullptr ? p.out2 + ebase + m.y : m.y != m.x ? p.out + ebase + m.y : nullptr;
                 const int nj = min(16, unit.ne - c0);
 #pragma unroll
                 for (int j = 0; j < 16; j += 4) {

@@ -110,8 +110,8 @@ def gpu(workload, msh, params, precision="fp64", reps=1, env=None):
 def record_symmetry(workload, msh, params):
     """Lowers the workload on a record-only context (no GPU) and returns, per
     matrix group, its term count, the mirror term of each term
-    (slgpu_matrix_group_symmetry) and whether the split contraction would
-    compute only the upper triangle."""
+    (slgpu_matrix_group_symmetry), whether the split contraction would
+    compute only the upper triangle, and its transposed partner group."""
     with tempfile.TemporaryDirectory() as d:
         return _child("symmetry", workload, msh, params, os.path.join(d, "o.npz"), {"SLGPU_RECORD_ONLY": "1"})
 
@@ -132,18 +132,20 @@ def symmetry_inproc(workload, msh, params):
     h = lib.slgpu_adapter_last_handle()
     ng = ctypes.c_int()
     assert lib.slgpu_matrix_group_count(ctx, h, ctypes.byref(ng)) == 0
-    nterms, mirror, sym = [], [], []
+    nterms, mirror, sym, partner = [], [], [], []
     for gi in range(ng.value):
         desc = abi.GroupDesc()
         assert lib.slgpu_matrix_group_desc(ctx, h, gi, ctypes.byref(desc)) == 0
         m = np.zeros(desc.nterms, np.int32)
-        s = ctypes.c_int32()
-        assert lib.slgpu_matrix_group_symmetry(ctx, h, gi, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s)) == 0
+        s, pt = ctypes.c_int32(), ctypes.c_int32()
+        assert lib.slgpu_matrix_group_symmetry(ctx, h, gi, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s),
+                                               ctypes.byref(pt)) == 0
         nterms.append(desc.nterms)
         mirror.append(m)
         sym.append(s.value)
+        partner.append(pt.value)
     return dict(nterms=np.array(nterms, np.int32), mirror=np.concatenate(mirror) if mirror else np.zeros(0, np.int32),
-                symmetric=np.array(sym, np.int32))
+                symmetric=np.array(sym, np.int32), partner=np.array(partner, np.int32))
 
 
 def record_oracle(workload, msh, params):

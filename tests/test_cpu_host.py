@@ -105,11 +105,12 @@ def _add_record_group(c, gb, xyz, conn):
     return h.value
 
 
-def _symmetry(c, h, nterms):
+def _symmetry(c, h, nterms, gi=0):
     m = np.zeros(nterms, np.int32)
-    s = ctypes.c_int32()
-    c.check(c.lib.slgpu_matrix_group_symmetry(c.h, h, 0, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s)))
-    return m, s.value
+    s, pt = ctypes.c_int32(), ctypes.c_int32()
+    c.check(c.lib.slgpu_matrix_group_symmetry(c.h, h, gi, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(s),
+                                              ctypes.byref(pt)))
+    return m, s.value, pt.value
 
 
 def test_symmetry_detection_synthetic():
@@ -123,8 +124,8 @@ def test_symmetry_detection_synthetic():
     L = c.lib
     gb, xyz, conn = group(np.random.Generator(np.random.PCG64(3)), ntf=6, ndof=6, nterms=5, symmetric=True, ndests=1)
     h = _add_record_group(c, gb, xyz, conn)
-    m, s = _symmetry(c, h, 5)
-    assert m.tolist() == [1, 0, 3, 2, 4] and s == 1
+    m, s, pt = _symmetry(c, h, 5)
+    assert m.tolist() == [1, 0, 3, 2, 4] and s == 1 and pt == -1
     sc = np.zeros(5)
     c.check(L.slgpu_matrix_get_scales(c.h, h, 0, abi.f64p(sc), None))
     sc2 = sc.copy()
@@ -140,15 +141,57 @@ def test_symmetry_detection_synthetic():
     t3 = gb.g.terms[3].coef_node
     gb.g.nodes[t3].b = 2  # x + detJ instead of x + coordinate
     h = _add_record_group(c, gb, xyz, conn)
-    m, s = _symmetry(c, h, 4)
+    m, s, _ = _symmetry(c, h, 4)
     assert (m == -1).all() and s == 0
     assert nodes[t3][0] == abi.OP_ADD
 
     # Independent random tables: not symmetric.
     gb, xyz, conn = group(np.random.Generator(np.random.PCG64(3)), ntf=6, ndof=6, nterms=4, ndests=1)
     h = _add_record_group(c, gb, xyz, conn)
-    m, s = _symmetry(c, h, 4)
+    m, s, _ = _symmetry(c, h, 4)
     assert (m == -1).all() and s == 0
+    c.close()
+
+
+def test_transposed_partner_detection():
+    """Two groups with ntf and ndof swapped and the tables of each term
+    swapped are partners; replacing one group's element data or scaling one
+    term of one group ends the pairing, and restoring it brings it back."""
+    from _synthetic import group
+
+    c = abi.Context(0, flags=abi.CTX_RECORD_ONLY)
+    L = c.lib
+    rng = np.random.Generator(np.random.PCG64(9))
+    gb, xyz, conn = group(rng, ntf=12, ndof=8, nterms=4, ndests=1)
+    g1 = gb.g
+    g2 = abi.Group.from_buffer_copy(g1)
+    g2.ntf, g2.ndof = g1.ndof, g1.ntf
+    terms2 = (abi.Term * g1.nterms)(*[abi.Term(g1.terms[t].dof_table, g1.terms[t].tf_table, g1.terms[t].coef_node, 0,
+                                               g1.terms[t].scale) for t in range(g1.nterms)])
+    g2.terms = terms2
+    c.check(L.slgpu_mesh_set_nodes(c.h, 0, xyz.size // 3, abi.f64p(xyz)))
+    c.check(L.slgpu_mesh_set_elements(c.h, 0, 3, 4, conn.size // 4, abi.i32p(conn)))
+    h = ctypes.c_int()
+    c.check(L.slgpu_matrix_create(c.h, 60, ctypes.byref(h)))
+    c.check(L.slgpu_matrix_add_group(c.h, h, ctypes.byref(g1), None))
+    c.check(L.slgpu_matrix_add_group(c.h, h, ctypes.byref(g2), None))
+    h = h.value
+    partners = lambda: [_symmetry(c, h, 4, gi)[2] for gi in (0, 1)]
+    assert partners() == [1, 0]
+    e_new = rng.lognormal(0.0, 0.4, g1.nelem)
+    e_old = np.ctypeslib.as_array(g1.elemdata[0], (g1.nelem,)).copy()
+    c.check(L.slgpu_matrix_set_elemdata(c.h, h, 1, 0, abi.f64p(e_new)))
+    assert partners() == [-1, -1]
+    c.check(L.slgpu_matrix_set_elemdata(c.h, h, 1, 0, abi.f64p(e_old)))
+    assert partners() == [1, 0]
+    sc = np.zeros(4)
+    c.check(L.slgpu_matrix_get_scales(c.h, h, 0, abi.f64p(sc), None))
+    sc2 = sc.copy()
+    sc2[2] *= 2.0
+    c.check(L.slgpu_matrix_set_scales(c.h, h, 0, abi.f64p(sc2), None))
+    assert partners() == [-1, -1]
+    c.check(L.slgpu_matrix_set_scales(c.h, h, 1, abi.f64p(sc2), None))
+    assert partners() == [1, 0]
     c.close()
 
 
@@ -175,3 +218,5 @@ def test_symmetry_detection_workloads(gpu_lib, tmp_path):
     meshgen.hex_mesh(msh, 2, jitter=0.15, seed=1)
     r = P.record_symmetry(W.ELASTICITY_HEX, msh, [2, -2])
     assert r["symmetric"].tolist() == [2, 0, 0, 0, 2, 0, 0, 0, 2]
+    # Off-diagonal blocks (u_a, u_b) and (u_b, u_a) are transposed partners.
+    assert r["partner"].tolist() == [-1, 3, 6, 1, -1, 7, 2, 5, -1]

@@ -123,6 +123,84 @@ def test_split_symmetry_matches_full_contraction(ref_lib, gpu_lib, tmp_path):
         assert fro <= 1e-10, f"workload {args[0]}: assembled Frobenius-relative error {fro:.3e}"
 
 
+def _pair_matrices(ctx, groups, xyz, conn, precision, edit=None):
+    """Element matrices of several groups of one matrix, each group's rows in
+    a block of its own (row = block base + e ntf + i, column = j).  `edit(h)`
+    runs before processing.  Also returns each group's transposed partner."""
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, 0, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, 0, 3, 4, conn.size // 4, abi.i32p(conn)))
+    keep, base = [], 0
+    for g in groups:
+        tfaddr = (base + np.arange(g.nelem)[None, :] * g.ntf + np.arange(g.ntf)[:, None]).astype(np.int32)
+        dofaddr = np.repeat(np.arange(g.ndof, dtype=np.int32)[:, None], g.nelem, axis=1)
+        dest = (abi.Dest * 1)()
+        dest[0].tfaddr, dest[0].dofaddr, dest[0].multiplier = abi.i32p(tfaddr), abi.i32p(dofaddr), 1.0
+        g.ndests, g.dests = 1, dest
+        keep += [tfaddr, dofaddr, dest]
+        base += g.nelem * g.ntf
+    ndofs = base
+    h = ctypes.c_int()
+    ctx.check(L.slgpu_matrix_create(ctx.h, ndofs, ctypes.byref(h)))
+    for g in groups:
+        ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g), None))
+    if edit is not None:
+        edit(h.value)
+    partners = []
+    for gi in range(len(groups)):
+        pt = ctypes.c_int32()
+        ctx.check(L.slgpu_matrix_group_symmetry(ctx.h, h, gi, None, None, ctypes.byref(pt)))
+        partners.append(pt.value)
+    info = abi.CsrInfo()
+    con = np.zeros(ndofs, np.uint8)
+    ctx.check(L.slgpu_matrix_process(ctx.h, h, con.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), precision,
+                                     ctypes.byref(info)))
+    rows, cols = np.zeros(ndofs + 1, np.int32), np.zeros(info.nnzA, np.int32)
+    vals = np.zeros(info.nnzA)
+    ctx.check(L.slgpu_matrix_download(ctx.h, h, abi.i32p(rows), abi.i32p(cols), abi.f64p(vals),
+                                      abi.i32p(np.zeros(ndofs + 1, np.int32)), abi.i32p(np.zeros(1, np.int32)),
+                                      abi.f64p(np.zeros(1))))
+    ctx.check(L.slgpu_matrix_destroy(ctx.h, h))
+    out, base = [], 0
+    for g in groups:
+        n = g.nelem * g.ntf * g.ndof
+        assert np.array_equal(cols[base:base + n], np.tile(np.arange(g.ndof), g.nelem * g.ntf))
+        out.append(vals[base:base + n].reshape(g.nelem, g.ntf, g.ndof))
+        base += n
+    return out, partners
+
+
+def test_split_transposed_pair(ctx):
+    """Two groups whose element matrices are transposes of each other (ntf 12
+    and ndof 8 swapped, tables of each term swapped, the same coefficients and
+    data): one split contraction writes both, and the second group's matrices
+    are the first's transposed bit for bit, within the split bound of its own
+    FP64 result.  Replacing one group's element data ends the pairing; the
+    same data in both restores it."""
+    rng = np.random.Generator(np.random.PCG64(9))
+    gb, xyz, conn = S.group(rng, nelem_grid=30, ntf=12, ndof=8, nterms=4, ngp1=3, norient=2, ndests=1)
+    g1 = gb.g
+    g2 = abi.Group.from_buffer_copy(g1)
+    g2.ntf, g2.ndof = g1.ndof, g1.ntf
+    terms2 = (abi.Term * g1.nterms)(*[abi.Term(g1.terms[t].dof_table, g1.terms[t].tf_table, g1.terms[t].coef_node, 0,
+                                               g1.terms[t].scale) for t in range(g1.nterms)])
+    g2.terms = terms2
+    new_e = rng.lognormal(0.0, 0.4, g1.nelem)
+
+    def set_e(groups):
+        return lambda h: [ctx.check(ctx.lib.slgpu_matrix_set_elemdata(ctx.h, h, gi, 0, abi.f64p(new_e))) for gi in groups]
+
+    for edit, paired in ((None, True), (set_e([1]), False), (set_e([0, 1]), True)):
+        (r1, r2), _ = _pair_matrices(ctx, [g1, g2], xyz, conn, abi.PREC_FP64, edit)
+        (m1, m2), partners = _pair_matrices(ctx, [g1, g2], xyz, conn, abi.PREC_SPLIT, edit)
+        assert partners == ([1, 0] if paired else [-1, -1])
+        if paired:
+            assert np.array_equal(m2, m1.transpose(0, 2, 1))
+        for got, ref in ((m1, r1), (m2, r2)):
+            err = np.linalg.norm((got - ref).reshape(len(got), -1), axis=1) / np.linalg.norm(ref.reshape(len(ref), -1), axis=1)
+            assert err.max() <= 1e-10, f"paired={paired}: per-element Frobenius error {err.max():.3e}"
+
+
 def test_split_dropin_elasticity(ref_lib, gpu_lib, tmp_path):
     msh = str(tmp_path / "h.msh")
     meshgen.hex_mesh(msh, 4, jitter=0.15, seed=1)
