@@ -167,7 +167,9 @@ std::string jit_coef_source(const std::vector<const GroupDev*>& batch)
     s << "  (void)o; (void)X0; (void)X1; (void)X2;\n";
     for (size_t k = 0; k < batch.size(); k++) {
         const GroupDev& G = *batch[k];
-        s << "  {\n    const JitGroup q = grp.g[" << k << "];\n";
+        // A group whose coefficients are not needed in this launch (the
+        // second group of a transposed pair) gets C = null.
+        s << "  if (grp.g[" << k << "].C != nullptr) {\n    const JitGroup q = grp.g[" << k << "];\n";
         emit_nodes(s, G, node_closure(G, all_terms(G)), ngp, "    ");
         s << "    double cmax = 0;\n";
         for (int t = 0; t < G.nterms; t++) {

@@ -1643,8 +1643,10 @@ struct JitGroup {
 constexpr int kJitBatch = 64;
 
 static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std::vector<int64_t>& coff, int32_t* elemexp,
-                                const std::vector<int64_t>& eoff, const std::vector<GroupData>* ov)
+                                const std::vector<int64_t>& eoff, const std::vector<GroupData>* ov, const std::vector<int>& pair)
 {
+    // The second group of a transposed pair needs no coefficients.
+    auto skip = [&](size_t j) { return pair[j] >= 0 && pair[j] < (int)j; };
     static const bool interp_only = [] {
         const char* v = std::getenv("SLGPU_COEF_INTERPRETER");
         return v != nullptr && std::strcmp(v, "1") == 0;
@@ -1681,8 +1683,8 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                     GroupDev& G = *M.groups[j];
                     const double* ed = ov != nullptr && (*ov)[j].elemdata != nullptr ? (*ov)[j].elemdata : G.elemdata.as<double>();
                     const double* fd = ov != nullptr && (*ov)[j].fielddata != nullptr ? (*ov)[j].fielddata : G.fielddata.as<double>();
-                    jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, G.term_scale_d.as<double>(), C + coff[j],
-                                          eoff[j] >= 0 ? elemexp + eoff[j] : nullptr});
+                    jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, G.term_scale_d.as<double>(), skip(j) ? nullptr : C + coff[j],
+                                          eoff[j] >= 0 && !skip(j) ? elemexp + eoff[j] : nullptr});
                 }
                 const MeshDev& m = ctx->meshes.at(g0.mesh);
                 JitGeom geom{m.xyz.as<double>(), m.types.at(g0.elemtype).conn.as<int32_t>(), g0.elems.as<int32_t>(), g0.orient.as<int32_t>(),
@@ -1690,7 +1692,9 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                 void* args[] = {&geom, jg.data()};  // the group array is one by-value parameter
                 const int64_t n = g0.nelem * (int64_t)g0.ngp;
                 double cbytes = 0;
-                for (size_t j = k; j < k1; j++) cbytes += 8.0 * M.groups[j]->nterms * M.groups[j]->ngp * M.groups[j]->nelem;
+                for (size_t j = k; j < k1; j++)
+                    if (!skip(j))
+                        cbytes += 8.0 * M.groups[j]->nterms * M.groups[j]->ngp * M.groups[j]->nelem;
                 const int kt = kstat_start(ctx, "coefficients", cbytes);
                 cuda_check(cudaLaunchKernel((const void*)kern, dim3(grid_for(n, 128)), dim3(128), args, 0, ctx->x->stream),
                            "coefficient kernel launch");
@@ -1706,6 +1710,8 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
         }
         if (!done) {
             for (size_t j = k; j < k1; j++) {
+                if (skip(j))
+                    continue;
                 GroupDev& G = *M.groups[j];
                 CoefParams cp = coef_params(ctx, G, C + coff[j]);
                 cp.elemexp = eoff[j] >= 0 ? elemexp + eoff[j] : nullptr;
@@ -1767,10 +1773,10 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
         E.alloc(ctx, (size_t)etot * 4);
         cuda_check(cudaMemsetAsync(E.as<void>(), 0x80, (size_t)etot * 4, ctx->x->stream), "memset");
     }
-    phase_event(ctx, ctx->x->evpool[0]);
-    launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov);
-    phase_event(ctx, ctx->x->evpool[1]);
     const std::vector<int> pair = cross_pairs(M, precision, ov);
+    phase_event(ctx, ctx->x->evpool[0]);
+    launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov, pair);
+    phase_event(ctx, ctx->x->evpool[1]);
     size_t gi = 0;
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
