@@ -142,3 +142,76 @@ def test_value_kernels_agree(tmp_path):
             a, b = res[k][key], res["warp"][key]
             assert np.all(np.isfinite(a)), key
             assert np.array_equal(a, b), f"{key}: {k} and warp-per-row value kernels differ"
+
+
+def test_graph_replay_with_transposed_pair(ctx):
+    """A matrix with two transposed-partner groups, edited so that the pairing
+    turns off and on again (a scale of one group; element data of one group,
+    then of both): replayed graphs give the ungraphed values bit for bit, and
+    the pairing follows the edits."""
+    rng = np.random.Generator(np.random.PCG64(23))
+    ndofs = 2500
+    gb, xyz, conn = S.group(rng, nelem_grid=40, ntf=12, ndof=8, nterms=4, ngp1=3, norient=2, ndests=1, ndofs=ndofs)
+    g1 = gb.g
+    g2 = abi.Group.from_buffer_copy(g1)
+    g2.ntf, g2.ndof = g1.ndof, g1.ntf
+    terms2 = (abi.Term * g1.nterms)(*[abi.Term(g1.terms[t].dof_table, g1.terms[t].tf_table, g1.terms[t].coef_node, 0,
+                                               g1.terms[t].scale) for t in range(g1.nterms)])
+    g2.terms = terms2
+    dest2 = (abi.Dest * 1)()
+    dest2[0].tfaddr, dest2[0].dofaddr, dest2[0].multiplier = g1.dests[0].dofaddr, g1.dests[0].tfaddr, 1.5
+    g2.dests = dest2
+    mesh_id = 31
+    g1.mesh = g2.mesh = mesh_id
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, mesh_id, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, mesh_id, 3, 4, conn.size // 4, abi.i32p(conn)))
+    h = ctypes.c_int()
+    ctx.check(L.slgpu_matrix_create(ctx.h, ndofs, ctypes.byref(h)))
+    ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g1), None))
+    ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g2), None))
+    t = dict(h=h.value, con=(rng.random(ndofs) < 0.1).astype(np.uint8))
+    sc = np.zeros(g1.nterms)
+    ctx.check(L.slgpu_matrix_get_scales(ctx.h, t["h"], 0, abi.f64p(sc), None))
+    sc2 = sc.copy()
+    sc2[1] *= 3.0
+    e_old = np.ctypeslib.as_array(g1.elemdata[0], (g1.nelem,)).copy()
+    e_new = rng.lognormal(0.0, 0.4, g1.nelem)
+
+    def set_scales(gi, v):
+        return lambda: ctx.check(L.slgpu_matrix_set_scales(ctx.h, t["h"], gi, abi.f64p(v), None))
+
+    def set_e(gi, v):
+        return lambda: ctx.check(L.slgpu_matrix_set_elemdata(ctx.h, t["h"], gi, 0, abi.f64p(v)))
+
+    def partner():
+        pt = ctypes.c_int32()
+        ctx.check(L.slgpu_matrix_group_symmetry(ctx.h, t["h"], 0, None, None, ctypes.byref(pt)))
+        return pt.value
+
+    edits = [None, None, set_scales(0, sc2), None, None, set_scales(1, sc2), None, None, set_e(1, e_new), None,
+             set_e(0, e_new), None, None, set_e(0, e_old), set_e(1, e_old), set_scales(0, sc), set_scales(1, sc), None]
+    paired = [True, True, False, False, False, True, True, True, False, False, True, True, True, False, True, False, True,
+              True]
+
+    def run(graphs):
+        ctx.check(L.slgpu_ctx_set_graphs(ctx.h, 1 if graphs else 0))
+        out = []
+        for e, p in zip(edits, paired):
+            if e is not None:
+                e()
+            assert (partner() == 1) == p
+            out.append(_process(ctx, t, abi.PREC_SPLIT))
+        return out
+
+    g0 = L.slgpu_graph_launches(ctx.h)
+    with_graph = run(True)
+    replays = L.slgpu_graph_launches(ctx.h) - g0
+    without = run(False)
+    ctx.check(L.slgpu_ctx_set_graphs(ctx.h, 1))
+    ctx.check(L.slgpu_matrix_destroy(ctx.h, t["h"]))
+    assert replays >= 5, f"only {replays} graph replays"
+    for i, ((a, d), (a0, d0)) in enumerate(zip(with_graph, without)):
+        assert np.all(np.isfinite(a)) and np.all(np.isfinite(d)), f"call {i}: non-finite values"
+        assert np.array_equal(a, a0) and np.array_equal(d, d0), f"call {i}: graph != ungraphed"
+    assert not np.array_equal(with_graph[1][0], with_graph[2][0])
