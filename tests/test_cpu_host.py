@@ -156,7 +156,8 @@ def test_symmetry_detection_synthetic():
 def test_transposed_partner_detection():
     """Two groups with ntf and ndof swapped and the tables of each term
     swapped are partners; replacing one group's element data or scaling one
-    term of one group ends the pairing, and restoring it brings it back."""
+    term of one group ends the pairing, and restoring it brings it back.  A
+    coefficient that reads another constant is not a partner's."""
     from _synthetic import group
 
     c = abi.Context(0, flags=abi.CTX_RECORD_ONLY)
@@ -192,6 +193,19 @@ def test_transposed_partner_detection():
     assert partners() == [-1, -1]
     c.check(L.slgpu_matrix_set_scales(c.h, h, 1, abi.f64p(sc2), None))
     assert partners() == [1, 0]
+
+    # A partner whose coefficients read another constant: no pair.
+    g3 = abi.Group.from_buffer_copy(g2)
+    nodes3 = (abi.Node * g1.nnodes)(*[abi.Node(g1.nodes[k].op, g1.nodes[k].a, g1.nodes[k].b, g1.nodes[k].c)
+                                      for k in range(g1.nnodes)])
+    assert nodes3[1].op == abi.OP_CONST
+    nodes3[1].a = 3
+    g3.nodes = nodes3
+    h3 = ctypes.c_int()
+    c.check(L.slgpu_matrix_create(c.h, 60, ctypes.byref(h3)))
+    c.check(L.slgpu_matrix_add_group(c.h, h3, ctypes.byref(g1), None))
+    c.check(L.slgpu_matrix_add_group(c.h, h3, ctypes.byref(g3), None))
+    assert [_symmetry(c, h3.value, 4, gi)[2] for gi in (0, 1)] == [-1, -1]
     c.close()
 
 
