@@ -213,7 +213,8 @@ def test_symmetry_detection_workloads(gpu_lib, tmp_path):
     """On the drop-in's lowering (record-only context): every group of the
     p-adaptive Helmholtz problem (grad-grad and mass terms) has mirror terms,
     pairing d/dx_a with d/dx_b; of the nine component blocks of the
-    order-2 elasticity problem, the three diagonal ones do."""
+    order-2 elasticity problem, the three diagonal ones do, and the others
+    form three transposed pairs; the harmonic hcurl groups are symmetric."""
     n = 2
     rng = np.random.Generator(np.random.PCG64(7))
     tags = meshgen.ORDER_REGION_BASE + rng.integers(1, 6, size=6 * n ** 3)
@@ -234,3 +235,11 @@ def test_symmetry_detection_workloads(gpu_lib, tmp_path):
     assert r["symmetric"].tolist() == [2, 0, 0, 0, 2, 0, 0, 0, 2]
     # Off-diagonal blocks (u_a, u_b) and (u_b, u_a) are transposed partners.
     assert r["partner"].tolist() == [-1, 3, 6, 1, -1, 7, 2, 5, -1]
+    # Harmonic hcurl eddy currents (curl-curl and sigma dt terms, two harmonics): both groups are
+    # symmetric up to the order of factors.
+    rng = np.random.Generator(np.random.PCG64(11))
+    tags = meshgen.MATERIAL_REGION_BASE + rng.integers(0, 4, size=6 * n ** 3)
+    msh = str(tmp_path / "e.msh")
+    meshgen.tet_mesh(msh, n, jitter=0.1, seed=4, element_tags=tags)
+    r = P.record_symmetry(W.EDDY_TET, msh, [2, 1.0e3, 1e3, 5e5, 2e6, 6e7])
+    assert len(r["symmetric"]) >= 1 and (r["symmetric"] > 0).all() and (r["partner"] == -1).all()
