@@ -164,9 +164,10 @@ def peaks():
 # launch's group (traffic grows in proportion to the elements).  Summaries
 # and the commands that made them are under profiles/.
 TRAFFIC_PER_ELEMENT = {
-    # profiles/k_contract_split_elasticity_hex32.md: 60.29 MB read + 135.83 MB
-    # written by one group launch over 32768 elements.
-    ("c2", "contract_split"): (60.287488e6 + 135.8272e6) / 32768,
+    # profiles/k_contract_split_elasticity_hex32.md, 32768 elements: a symmetric
+    # launch reads 59.91 MB and writes 138.28 MB, a paired one 70.26 + 338.40 MB;
+    # a step runs three of each, so a launch averages their mean.
+    ("c2", "contract_split"): ((59.910656e6 + 138.279168e6) + (70.263296e6 + 338.402048e6)) / 2 / 32768,
     # profiles/k_row_values_elasticity_hex32.md: 2.859 GB read + 1.202 GB
     # written by the launch over all 9 groups of 32768 elements.
     ("c2", "row_values"): (2.858950e9 + 1.201917e9) / 32768,

@@ -243,3 +243,23 @@ def test_symmetry_detection_workloads(gpu_lib, tmp_path):
     meshgen.tet_mesh(msh, n, jitter=0.1, seed=4, element_tags=tags)
     r = P.record_symmetry(W.EDDY_TET, msh, [2, 1.0e3, 1e3, 5e5, 2e6, 6e7])
     assert len(r["symmetric"]) >= 1 and (r["symmetric"] > 0).all() and (r["partner"] == -1).all()
+
+
+def test_bench_roofline_of_dominant_family():
+    """bench.roofline_of names the family with the most device time, divides
+    its algorithmic work by its event time, and scales the ncu traffic per
+    element to the launch (8x the 32^3 capture at 64^3)."""
+    import bench
+
+    stats = {"coefficients": {"ms": 8.2, "launches": 10, "work": 3.1e10},
+             "contract_split": {"ms": 75.0, "launches": 60, "work": 1.5e17},
+             "row_values": {"ms": 84.0, "launches": 10, "work": 2.73e11}}
+    r = bench.roofline_of(stats, "c2", 64)
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s" and "k_row_values" in r["kernel"]
+    assert abs(r["achieved"] - 2.73e11 / 84e-3 / 1e9) < 1e-6 and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert abs(r["ms_per_launch"] - 8.4) < 1e-12
+    assert abs(r["traffic"] - 8 * bench.traffic_per_launch("c2", "row_values", 32, 1)) < 1.0
+    stats["contract_split"]["ms"] = 100.0
+    r = bench.roofline_of(stats, "c2", 64)
+    assert r["bound"] == "tensor" and r["unit"] == "TFLOP/s" and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert bench.roofline_of(stats, "c3", 32)["traffic"] is None
