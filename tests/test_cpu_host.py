@@ -26,6 +26,20 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(abi.SIGNATURES), "python binding and header disagree"
 
 
+def test_binding_argument_counts_match_header():
+    """Each ctypes signature in abi.SIGNATURES takes as many arguments as
+    the header's prototype."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    protos = dict(re.findall(r"^\s*(?:int|void|int64_t|double|const char)\s*\**\s*(slgpu_\w+)\s*\(([^)]*)\)\s*;", text, re.M))
+    assert set(protos) == set(abi.SIGNATURES)
+    bad = []
+    for name, args in protos.items():
+        n = 0 if args.strip() in ("", "void") else args.count(",") + 1
+        if name in abi.SIGNATURES and len(abi.SIGNATURES[name][1]) != n:
+            bad.append((name, n, len(abi.SIGNATURES[name][1])))
+    assert not bad, f"argument counts differ (name, header, binding): {bad}"
+
+
 def test_no_device_is_a_clean_error():
     """Without a GPU the context refuses to start (there is no CPU fallback)."""
     import torch
