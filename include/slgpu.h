@@ -62,6 +62,10 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx);
 int slgpu_last_error(const slgpu_ctx* ctx, char* buf, size_t len);
 /* Bytes of device memory currently held by the context. */
 int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx);
+/* Host-to-device and device-to-host bytes the context's calls have copied so
+ * far (uploads of meshes, groups, data and constraints; downloads of CSR
+ * arrays and values).  No counterpart in the reference (no device there). */
+int slgpu_transfer_bytes(const slgpu_ctx* ctx, int64_t* h2d, int64_t* d2h);
 
 /*
  * Mesh geometry, resident on the device.  Replaces the node-coordinate and
@@ -233,6 +237,13 @@ int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, doub
 /* Device pointers to the processed CSR arrays (valid until the next process/destroy). */
 int slgpu_matrix_device_csr(slgpu_ctx* ctx, int handle, const int32_t** Arows, const int32_t** Acols, const double** Avals,
                             const int32_t** Drows, const int32_t** Dcols, const double** Dvals);
+/* Elimination of the constrained DOFs from a right-hand side on the device,
+ * for a solver that takes the CSR blocks without a download:
+ *   out[r] = b[Ainds[r]] - sum_j D[r][j] * b[Dinds[j]]
+ * (mat::eliminate, src/formulation/mat.cpp:78-103: ba - D*bd with the product
+ * summed over each row of D in column order).  b [ndofs] and out [nA] are
+ * device pointers on the context's device; returns when out is written. */
+int slgpu_matrix_eliminate(slgpu_ctx* ctx, int handle, const double* b, double* out);
 
 /*
  * Right-hand side (contribution.cpp:293-300 + rawvec::setvalues "add",
@@ -416,27 +427,36 @@ void slgpu_host_free(void* p);
  * that must not pay for cudaMalloc/cudaFree -- and already hold the mesh and
  * output buffers on the device.
  *   g          group description in host memory, as for slgpu_matrix_add_group
- *              (destinations are not used: no assembly happens here)
+ *              (destinations are not used and may be absent: ndests = 0)
  *   xyz        device pointer, [3*nnodes] node coordinates
+ *   nnodes     number of nodes in xyz; an element whose connectivity names a
+ *              node outside [0, nnodes) is not read and its matrix is NaN
  *   conn       device pointer, [mesh_nelem*ncurvednodes] curved-node
- *              connectivity of g->elemtype; every entry must index xyz
+ *              connectivity of g->elemtype
  *   K          device pointer, [nelem][ntf*ndof] output: K[e*ntf*ndof+i*ndof+j]
  *              = sum over terms of scale * element matrix entry (i, j) of
  *              element e (no destination multiplier)
  *   stream     cudaStream_t the work is queued on (0 = legacy default stream);
  *              the call returns once the work is queued
  *   err/errlen optional buffer for the error message
+ * The group's host arrays (tables, per-element and field data, element
+ * numbers, ...) are copied to the device on `stream`.  Arrays in pageable
+ * memory may be reused as soon as the call returns; arrays in page-locked
+ * memory are read when the stream reaches the copy, so they must stay
+ * allocated and unchanged until then.  While `stream` is capturing, the call
+ * returns SLGPU_E_UNSUPPORTED and queues nothing.
  * Working memory is a 32 MiB array compiled into this library's device image
  * (held on every GPU that loads the library until the process exits).
  * Groups needing more (program, tables, per-element data and
  * nterms*ngp*nelem doubles of coefficients) are rejected with SLGPU_E_BUDGET.
  * The first call on each device looks up the array's device address; make
- * that first call before any stream capture.  All calls share the array:
- * calls that may run at the same time on the GPU race and must be ordered
- * by the caller (same stream, or events).
+ * that first call before any stream capture, and do not use the library
+ * across a cudaDeviceReset.  All calls share the array: calls that may run
+ * at the same time on the GPU race and must be ordered by the caller (same
+ * stream, or events).
  */
-int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, const int32_t* conn, int64_t mesh_nelem,
-                                   double* K, void* stream, char* err, size_t errlen);
+int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, int64_t nnodes, const int32_t* conn,
+                                   int64_t mesh_nelem, double* K, void* stream, char* err, size_t errlen);
 
 #ifdef __cplusplus
 }

@@ -113,19 +113,21 @@ SIGNATURES = {
     "slgpu_matrix_get_scales": (c_int, [c_void_p, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_matrix_group_symmetry": (c_int, [c_void_p, c_int, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
+    "slgpu_transfer_bytes": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int64)]),
     "slgpu_ctx_set_graphs": (c_int, [c_void_p, c_int]),
     "slgpu_graph_launches": (c_int64, [c_void_p]),
     "slgpu_ctx_set_kernel_timers": (c_int, [c_void_p, c_int]),
     "slgpu_kernel_stats": (c_int, [c_void_p, c_char_p, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]),
     "slgpu_check_coefficient_kernels": (c_int, [c_void_p, c_int, c_char_p, c_size_t]),
     "slgpu_matrix_work": (c_int, [c_void_p, c_int, c_void_p]),
-    "slgpu_element_matrices_noalloc": (c_int, [POINTER(Group), c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
-                                               c_char_p, c_size_t]),
+    "slgpu_element_matrices_noalloc": (c_int, [POINTER(Group), c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                               c_void_p, c_char_p, c_size_t]),
     "slgpu_matrix_process": (c_int, [c_void_p, c_int, POINTER(c_uint8), c_int, POINTER(CsrInfo)]),
     "slgpu_matrix_download": (c_int, [c_void_p, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_double),
                                       POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),
     "slgpu_matrix_download_values": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_matrix_device_csr": (c_int, [c_void_p, c_int] + [POINTER(c_void_p)] * 6),
+    "slgpu_matrix_eliminate": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "slgpu_rhs_assemble": (c_int, [c_void_p, POINTER(Group), c_int64, c_int, POINTER(c_double)]),
     "slgpu_last_timings": (c_int, [c_void_p, POINTER(c_double)]),
     "slgpu_record_count": (c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),

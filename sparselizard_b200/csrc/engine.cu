@@ -117,6 +117,7 @@ template <class T>
 static void upload(Ctx* ctx, DevBuf& buf, const T* src, size_t count)
 {
     buf.alloc(ctx, count * sizeof(T));
+    ctx->bytes_h2d += (int64_t)(count * sizeof(T));
     if (count > 0)
         cuda_check(cudaMemcpyAsync(buf.as<void>(), src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->x->stream),
                    "cudaMemcpyAsync H2D");
@@ -279,9 +280,11 @@ struct GroupDev::Record {
     slgpu_group desc{};
 };
 
-static void validate_group(const slgpu_group& g)
+// `with_dests`: the group is assembled, so it needs at least one valid
+// destination (the allocation-free element-matrix call has none).
+static void validate_group(const slgpu_group& g, bool with_dests = true)
 {
-    if (g.nelem < 0 || g.ngp <= 0 || g.ntf <= 0 || g.ndof <= 0 || g.nterms <= 0 || g.ndests <= 0 || g.norient <= 0)
+    if (g.nelem < 0 || g.ngp <= 0 || g.ntf <= 0 || g.ndof <= 0 || g.nterms <= 0 || (with_dests && g.ndests <= 0) || g.norient <= 0)
         fail(SLGPU_E_ARG, "group sizes must be positive");
     if (g.elemdim != g.problemdim)
         fail(SLGPU_E_UNSUPPORTED, "only elements of the mesh dimension are supported (element dim " +
@@ -300,7 +303,7 @@ static void validate_group(const slgpu_group& g)
         if (!rhs_term && (tm.dof_table >= g.ntables || g.tables[tm.dof_table].rows != g.ndof))
             fail(SLGPU_E_ARG, "term dof table invalid or its rows differ from ndof");
     }
-    for (int d = 0; d < g.ndests; d++) {
+    for (int d = 0; with_dests && d < g.ndests; d++) {
         if (g.dests[d].tfaddr == nullptr)
             fail(SLGPU_E_ARG, "destination without test-function addresses");
         if (g.terms[0].dof_table >= 0 && g.dests[d].dofaddr == nullptr)
@@ -662,6 +665,7 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     upload(ctx, gd->weights, g.weights, (size_t)g.ngp);
     upload(ctx, gd->lagrange, g.lagrange, (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp);
     gd->tables.alloc(ctx, (size_t)tables_total * sizeof(double));
+    ctx->bytes_h2d += (int64_t)tables_total * 8 + (int64_t)g.nelemdata * g.nelem * 8 + field_total * 8;
     for (int k = 0; k < g.ntables; k++)
         cuda_check(cudaMemcpyAsync(gd->tables.as<double>() + gd->tab_off[k], g.tables[k].vals,
                                    (size_t)g.norient * g.tables[k].rows * g.ngp * sizeof(double), cudaMemcpyHostToDevice,
@@ -1085,6 +1089,13 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
         cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync");
         nA = tot[0];
         nD = tot[1];
+        P->ainds.alloc(ctx, std::max<int64_t>(nA, 1) * 4);
+        P->dinds.alloc(ctx, std::max<int64_t>(nD, 1) * 4);
+        if (M.ndofs > 0) {
+            k_dof_split<<<grid_for(M.ndofs, 256), 256, 0, ctx->x->stream>>>(dconstr, M.ndofs, scanA.as<uint32_t>(), scanD.as<uint32_t>(),
+                                                                          P->ainds.as<int32_t>(), P->dinds.as<int32_t>());
+            cuda_check(cudaGetLastError(), "k_dof_split");
+        }
     }
     P->nA = nA;
     P->nD = nD;
@@ -2244,6 +2255,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         ctx->constr_host.assign(hconstr, hconstr + M.ndofs);
         ctx->constr_dev.alloc(ctx, (size_t)M.ndofs + 1);
         cuda_check(cudaMemcpyAsync(ctx->constr_dev.as<void>(), hconstr, M.ndofs, cudaMemcpyHostToDevice, ctx->x->stream), "H2D constr");
+        ctx->bytes_h2d += M.ndofs;
         std::vector<int32_t> packed((M.ndofs + 3) / 4, 0);
         std::memcpy(packed.data(), hconstr, M.ndofs);
         uint64_t a = 0x12345, b = 0x6789;
@@ -2493,6 +2505,15 @@ int slgpu_last_error(const slgpu_ctx* ctx, char* buf, size_t len)
 
 int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx) { return ctx ? ctx->in_use : 0; }
 
+int slgpu_transfer_bytes(const slgpu_ctx* ctx, int64_t* h2d, int64_t* d2h)
+{
+    if (ctx == nullptr || h2d == nullptr || d2h == nullptr)
+        return SLGPU_E_ARG;
+    *h2d = ctx->bytes_h2d;
+    *d2h = ctx->bytes_d2h;
+    return SLGPU_OK;
+}
+
 int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double* xyz)
 {
     return guarded(ctx, [&] {
@@ -2501,9 +2522,11 @@ int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double*
         MeshDev& m = ctx->meshes[mesh];
         const bool same = !ctx->record_only && m.nnodes == nnodes && !m.xyz.empty();
         m.nnodes = nnodes;
-        if (same && nnodes > 0)  // in place: buffers (and captured graphs) stay valid
+        if (same && nnodes > 0) {  // in place: buffers (and captured graphs) stay valid
             cuda_check(cudaMemcpyAsync(m.xyz.as<void>(), xyz, (size_t)3 * nnodes * 8, cudaMemcpyHostToDevice, ctx->x->stream),
                        "upload nodes");
+            ctx->bytes_h2d += 24 * nnodes;
+        }
         else if (!ctx->record_only)
             upload(ctx, m.xyz, xyz, (size_t)3 * nnodes);
         else
@@ -2669,6 +2692,7 @@ int slgpu_matrix_set_elemdata(slgpu_ctx* ctx, int handle, int gi, int k, const d
         cuda_check(cudaMemcpyAsync(g.elemdata.as<double>() + g.elemdata_off[k], values, (size_t)g.nelem * 8, cudaMemcpyHostToDevice,
                                    ctx->x->stream),
                    "upload elemdata");
+        ctx->bytes_h2d += g.nelem * 8;
     });
 }
 
@@ -2689,6 +2713,7 @@ int slgpu_matrix_set_fielddata(slgpu_ctx* ctx, int handle, int gi, int k, const 
         }
         cuda_check(cudaMemcpyAsync(g.fielddata.as<double>() + g.field_off[k], values, n * 8, cudaMemcpyHostToDevice, ctx->x->stream),
                    "upload fielddata");
+        ctx->bytes_h2d += (int64_t)n * 8;
     });
 }
 
@@ -2848,6 +2873,7 @@ void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
 {
     if (n == 0)
         return;
+    ctx->bytes_d2h += (int64_t)n;
     cudaPointerAttributes a{};
     const bool pinned = cudaPointerGetAttributes(&a, dst) == cudaSuccess && a.type == cudaMemoryTypeHost;
     cudaGetLastError();
@@ -2926,6 +2952,33 @@ int slgpu_matrix_device_csr(slgpu_ctx* ctx, int handle, const int32_t** Arows, c
         *Drows = P.Drows.as<int32_t>();
         *Dcols = P.Dcols.as<int32_t>();
         *Dvals = M.Dvals.as<double>();
+    });
+}
+
+int slgpu_matrix_eliminate(slgpu_ctx* ctx, int handle, const double* b, double* out)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        if (!M.pattern)
+            fail(SLGPU_E_STATE, "matrix not processed");
+        if (b == nullptr || out == nullptr)
+            fail(SLGPU_E_ARG, "null argument");
+        Pattern& P = *M.pattern;
+        for (const void* p : {(const void*)b, (const void*)out}) {
+            cudaPointerAttributes a{};
+            const bool dev = cudaPointerGetAttributes(&a, p) == cudaSuccess &&
+                             (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == ctx->device;
+            cudaGetLastError();
+            if (!dev)
+                fail(SLGPU_E_ARG, "b and out must be device memory of the context's device");
+        }
+        if (P.nA > 0) {
+            k_eliminate<<<grid_for(P.nA, 256), 256, 0, ctx->x->stream>>>(P.Drows.as<uint32_t>(), P.Dcols.as<int32_t>(), M.Dvals.as<double>(),
+                                                                       P.ainds.as<int32_t>(), P.dinds.as<int32_t>(), P.nA, b, out);
+            cuda_check(cudaGetLastError(), "k_eliminate");
+            ctx->launches++;
+        }
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync eliminate");
     });
 }
 
@@ -3098,7 +3151,8 @@ static void* g_noalloc_addr[256] = {};  // device address of the scratch, per de
 // Device address of the scratch array on the current device.  In host code
 // the name g_noalloc_scratch is only a host-side stand-in, not a device
 // address, so the address is looked up once per device (with that device
-// current) and kept.
+// current) and kept.  The kept address belongs to the device's primary
+// context: the library must not be used across a cudaDeviceReset.
 static void* noalloc_scratch_address(int* status, std::string* msg)
 {
     int dev = -1;
@@ -3124,8 +3178,8 @@ static void* noalloc_scratch_address(int* status, std::string* msg)
 }
 }  // namespace slgpu
 
-extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, const int32_t* conn, int64_t mesh_nelem,
-                                              double* K, void* stream, char* err, size_t errlen)
+extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double* xyz, int64_t nnodes, const int32_t* conn,
+                                              int64_t mesh_nelem, double* K, void* stream, char* err, size_t errlen)
 {
     auto report = [&](int code, const std::string& m) {
         if (err != nullptr && errlen > 0)
@@ -3134,8 +3188,23 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
     };
     if (g == nullptr || xyz == nullptr || conn == nullptr || K == nullptr)
         return report(SLGPU_E_ARG, "null argument");
+    if (nnodes <= 0 || nnodes > INT32_MAX)
+        return report(SLGPU_E_ARG, "node count must be in [1, 2^31)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    {
+        // The copies below read host arrays, some of them temporaries of this
+        // call, so they must not be recorded for a later replay.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t ce = cudaStreamIsCapturing(s, &cs);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            return report(SLGPU_E_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+        }
+        if (cs != cudaStreamCaptureStatusNone)
+            return report(SLGPU_E_UNSUPPORTED, "the stream is capturing; this call copies host arrays that do not outlive it");
+    }
     try {
-        validate_group(*g);
+        validate_group(*g, false);
         for (int64_t e = 0; e < g->nelem; e++)
             if (g->elems[e] < 0 || g->elems[e] >= mesh_nelem)
                 return report(SLGPU_E_ARG, "element number outside the mesh");
@@ -3150,6 +3219,9 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
             tiles.push_back(Tile{(int32_t)e, (int32_t)(e1 - e), o, 0});
             e = e1;
         }
+        // Checked before anything is queued on the stream.
+        if (tiles.size() > 65535)
+            return report(SLGPU_E_UNSUPPORTED, "more than 65535 orientation-uniform runs of elements in one group");
         // Scratch layout: each block 256-byte aligned.
         struct Block {
             const void* src;
@@ -3211,7 +3283,6 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
         unsigned char* base = static_cast<unsigned char*>(noalloc_scratch_address(&status, &msg));
         if (base == nullptr)
             return report(status, msg);
-        cudaStream_t s = static_cast<cudaStream_t>(stream);
         auto h2d = [&](size_t off, const void* src, size_t bytes) {
             if (bytes > 0)
                 cuda_check(cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync to scratch");
@@ -3251,6 +3322,7 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
         cp.term_scale = (const double*)at(b_scale);
         cp.nterms = g->nterms;
         cp.C = (double*)at(b_C);
+        cp.nnodes = nnodes;
         const int64_t n = g->nelem * (int64_t)g->ngp;
         k_geometry_coef<<<grid_for(n, 128), 128, 0, s>>>(cp);
         cuda_check(cudaGetLastError(), "k_geometry_coef");
@@ -3269,8 +3341,6 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
         kp.out = K;
         const int64_t P = (int64_t)g->ntf * g->ndof;
         dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)tiles.size());
-        if (grid.y > 65535)
-            return report(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
         k_contract_fp64<<<grid, dim3(16, 16), 0, s>>>(kp);
         cuda_check(cudaGetLastError(), "k_contract_fp64");
         return report(SLGPU_OK, "");

@@ -162,6 +162,7 @@ struct Pattern {
     int lmax = 0;          // longest row (A and D entries)
     int row_kernel = -1;   // CSR value kernel chosen by timing: 0 streaming warps, 1 warp per row, -1 not yet
     DevBuf Arows, Acols, Drows, Dcols;
+    DevBuf ainds, dinds;   // int32 [nA], [nD]: global DOF of each local row of A / column of D
     DevBuf slotmap;        // int16 [ncoo]: position in the row's [A | D] segment, -1 = dropped
     DevBuf inc_ptr;        // uint32 [nA+1]: incidences of each row
     DevBuf inc;            // uint64 [ninc]: segment << 40 | COO index of the incidence's first entry
@@ -272,6 +273,7 @@ struct Ctx {
     Exec* x = &main;        // the execution state launches are issued on
     std::recursive_mutex mu;  // one thread at a time inside the context
     std::string last_error;
+    int64_t bytes_h2d = 0, bytes_d2h = 0;  // host <-> device bytes copied by the context's calls
     std::map<int, MeshDev> meshes;
     std::map<int, std::unique_ptr<Matrix>> matrices;
     int next_handle = 1;

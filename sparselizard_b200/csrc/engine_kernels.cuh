@@ -63,6 +63,7 @@ struct CoefParams {
     int nterms;
     double* C;  // [nterms][ngp][nelem]
     int32_t* elemexp;  // nullptr, or [nelem]: atomicMax of the frexp exponents of |C|
+    int64_t nnodes;    // > 0: node numbers outside [0, nnodes) are not read and give NaN coefficients
 };
 
 // Geometry (J, detJ, invJ; src/field/jacobian.cpp:248-349 and :396-504 for
@@ -83,8 +84,13 @@ __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
     double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     double X[3] = {0, 0, 0};
     const int32_t* cn = p.conn + (int64_t)elem * p.ncn;
+    bool bad_node = false;
     for (int k = 0; k < p.ncn; k++) {
         const int node = cn[k];
+        if (p.nnodes > 0 && (node < 0 || node >= p.nnodes)) {
+            bad_node = true;
+            continue;
+        }
         const double x0 = p.xyz[3 * (int64_t)node + 0], x1 = p.xyz[3 * (int64_t)node + 1], x2 = p.xyz[3 * (int64_t)node + 2];
         const double nv = p.lagrange[(int64_t)k * p.ngp + g];
         X[0] += nv * x0;
@@ -147,7 +153,7 @@ __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
         case SLGPU_OP_NEG: v = -s[in.a]; break;
         case SLGPU_OP_POW: v = pow(s[in.a], s[in.b]); break;
         case INSTR_STORE: {
-            const double c = s[in.a] * p.term_scale[in.b] * wdet;
+            const double c = bad_node ? __longlong_as_double(0x7ff8000000000000ll) : s[in.a] * p.term_scale[in.b] * wdet;
             p.C[((int64_t)in.b * p.ngp + g) * p.nelem + e] = c;
             cmax = fmax(cmax, fabs(c));
             continue;
@@ -431,6 +437,37 @@ __global__ void k_renumber(const uint8_t* c, int64_t ndofs, const uint32_t* sA, 
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < ndofs)
         renum[i] = c[i] ? (int32_t)sD[i] : (int32_t)sA[i];
+}
+
+// Ainds / Dinds of gentools::findtruefalse (src/formulation/rawmat.cpp:133):
+// the unconstrained and the constrained DOFs, each in increasing order.
+__global__ void k_dof_split(const uint8_t* c, int64_t ndofs, const uint32_t* sA, const uint32_t* sD, int32_t* ainds, int32_t* dinds)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= ndofs)
+        return;
+    if (c[i])
+        dinds[sD[i]] = (int32_t)i;
+    else
+        ainds[sA[i]] = (int32_t)i;
+}
+
+// mat::eliminate (src/formulation/mat.cpp:78-103) on the device:
+// out[r] = b[ainds[r]] - (D b_D)[r], (D b_D)[r] summed over the row in column
+// order with separate roundings (the sequential product-then-add of a CSR
+// SpMV on the host, MatMult_SeqAIJ), then subtracted as VecAXPY(ba, -1, prod).
+// A thread per row: rows of D hold the few constrained neighbours of a DOF.
+__global__ void k_eliminate(const uint32_t* __restrict__ Drows, const int32_t* __restrict__ Dcols, const double* __restrict__ Dvals,
+                            const int32_t* __restrict__ ainds, const int32_t* __restrict__ dinds, int64_t nA,
+                            const double* __restrict__ b, double* __restrict__ out)
+{
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= nA)
+        return;
+    double s = 0.0;
+    for (uint32_t k = Drows[r]; k < Drows[r + 1]; k++)
+        s = __dadd_rn(s, __dmul_rn(Dvals[k], b[dinds[Dcols[k]]]));
+    out[r] = __dadd_rn(b[ainds[r]], __dmul_rn(-1.0, s));
 }
 
 __global__ void k_classify_runs(const unsigned long long* sk, const uint32_t* run_start, int64_t nruns, int colbits, const uint8_t* c,

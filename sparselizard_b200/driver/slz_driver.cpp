@@ -35,6 +35,9 @@ struct Result {
 
 Result g_result;
 std::string g_error;
+// The last captured matrix and right-hand side (kept for slz_eliminate).
+mat g_lastA;
+vec g_lastb;
 
 double now_s(void)
 {
@@ -94,6 +97,8 @@ void capture(mat& A, vec& b)
     VecGetSize(bp, &blen);
     r.b.assign(slshim_vec_array(bp), slshim_vec_array(bp) + blen);
     g_result = std::move(r);
+    g_lastA = A;
+    g_lastb = b;
 }
 
 // Runs generate(), A(), b() `reps` times; times[3*i + {0,1,2}] receive the
@@ -274,6 +279,35 @@ void slz_result_copy(int* Arows, int* Acols, double* Avals, int* Drows, int* Dco
 
 void slz_set_threads(int n) { setmaxnumthreads(n); }
 
+// mat::eliminate (src/formulation/mat.cpp:78-103) of the last captured matrix
+// applied to the vector x [ndofs]: out [nA] = x_A - D x_D.  Returns nA, or -1.
+long long slz_eliminate(const double* x, double* out)
+{
+    g_error.clear();
+    try {
+        const int n = g_lastb.size();
+        vec xv = g_lastb.copy();
+        densemat vals(n, 1);
+        std::memcpy(vals.getvalues(), x, (size_t)n * sizeof(double));
+        xv.setvalues(indexmat(n, 1, 0, 1), vals);
+        vec e = g_lastA.eliminate(xv);
+        densemat ev = e.getallvalues();
+        if (out != nullptr)
+            std::memcpy(out, ev.getvalues(), (size_t)ev.count() * sizeof(double));
+        return ev.count();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// Releases the last captured matrix and right-hand side.
+void slz_release_last(void)
+{
+    g_lastA = mat();
+    g_lastb = vec();
+}
+
 }
 
 #ifdef SLZ_GPU_BUILD
@@ -326,6 +360,49 @@ int slz_bench_prepare(int workload, const char* msh, const double* params, doubl
         return 2;
     }
     return 0;
+}
+
+// Warm generate(), A(), b() of the resident problem, `reps` times: the drop-in's
+// repeated path (the pattern is found in the engine's resident cache).
+// times[3*i + {0,1,2}] receive the phase wall seconds of repetition i; info4
+// as for slz_bench_prepare (the matrix handle changes with every A()).
+int slz_bench_reassemble(int reps, double* times, long long* info4)
+{
+    g_error.clear();
+    try {
+        if (!g_bench)
+            throw std::runtime_error("no resident problem");
+        for (int i = 0; i < reps; i++) {
+            g_bench->A = mat();
+            g_bench->b = vec();
+            double t0 = now_s();
+            g_bench->P->f.generate();
+            double t1 = now_s();
+            g_bench->A = g_bench->P->f.A();
+            double t2 = now_s();
+            g_bench->b = g_bench->P->f.b();
+            double t3 = now_s();
+            times[3 * i + 0] = t1 - t0;
+            times[3 * i + 1] = t2 - t1;
+            times[3 * i + 2] = t3 - t2;
+        }
+        std::shared_ptr<rawmat> raw = g_bench->A.getpointer();
+        info4[0] = slgpu_adapter::find_matrix_handle(raw.get());
+        info4[1] = raw->countrows();
+        info4[2] = raw->countnnz();
+        info4[3] = g_bench->A.getdinds().count();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+    return 0;
+}
+
+// Engine handle of the last matrix captured by slz_run.
+int slz_last_matrix_handle(void)
+{
+    std::shared_ptr<rawmat> raw = g_lastA.getpointer();
+    return raw ? slgpu_adapter::find_matrix_handle(raw.get()) : 0;
 }
 
 const unsigned char* slz_bench_constraints(void) { return g_bench ? g_bench->constrained.data() : nullptr; }
@@ -455,6 +532,48 @@ int slz_serve_add(int kind, const char* msh, int dim, int order, long long* info
         g_error = e.what();
         return -2;
     }
+}
+
+// Relative Frobenius error of pool problem `idx`'s assembled values (A and D)
+// in split precision (err2[0]) and in the FP32-level tier (err2[1]) against
+// the plain FP64 path, each re-assembled on the resident pattern.
+int slz_serve_error(int idx, double* err2)
+{
+    g_error.clear();
+    try {
+        if (idx < 0 || idx >= (int)g_serve.size())
+            throw std::runtime_error("no such pool problem");
+        ServeProblem& S = *g_serve[idx];
+        slgpu_ctx* ctx = slgpu_adapter_ctx();
+        std::shared_ptr<rawmat> raw = S.A.getpointer();
+        std::vector<bool> cb = raw->getdofmanager()->isconstrained();
+        std::vector<unsigned char> con(cb.begin(), cb.end());
+        auto values = [&](int prec) {
+            slgpu_csr_info info{};
+            if (slgpu_matrix_process(ctx, S.handle, con.data(), prec, &info) != SLGPU_OK)
+                throw std::runtime_error("process failed");
+            std::vector<double> v((size_t)(info.nnzA + info.nnzD) + 1);
+            if (slgpu_matrix_download_values(ctx, S.handle, v.data(), v.data() + info.nnzA) != SLGPU_OK)
+                throw std::runtime_error("download failed");
+            v.pop_back();
+            return v;
+        };
+        const std::vector<double> ref = values(SLGPU_PREC_FP64);
+        const int precs[2] = {SLGPU_PREC_SPLIT, SLGPU_PREC_FP32};
+        for (int k = 0; k < 2; k++) {
+            const std::vector<double> v = values(precs[k]);
+            double num = 0, den = 0;
+            for (size_t i = 0; i < ref.size(); i++) {
+                num += (v[i] - ref[i]) * (v[i] - ref[i]);
+                den += ref[i] * ref[i];
+            }
+            err2[k] = den > 0 ? std::sqrt(num / den) : 0.0;
+        }
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+    return 0;
 }
 
 // Runs `nreq` requests arriving as a Poisson process of `rate` per second

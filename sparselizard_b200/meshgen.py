@@ -157,3 +157,26 @@ def tet_mesh(path, n, jitter=0.1, seed=1, element_tags=None):
         (2, np.full(tris.shape[0], CLAMP), tris),
     ])
     return {"nelem": tets.shape[0], "nnodes": nodes.shape[0]}
+
+
+def workload_mesh(kind, n, path):
+    """The seeded mesh of one benchmark workload at size n:
+    "quad"       n x n q4, jitter 0.2h (Poisson);
+    "hex"        n^3 hexahedra, jitter 0.15h (elasticity, z = 0 face clamped);
+    "tet_orders" n^3 x 6 tets, jitter 0.1h, each tet in region
+                 ORDER_REGION_BASE + p with p uniform in 1..5 (p-adaptive Helmholtz);
+    "tet_sigma"  n^3 x 6 tets, jitter 0.1h, each tet in one of the 4 material
+                 regions MATERIAL_REGION_BASE + 0..3 (eddy currents)."""
+    if kind == "quad":
+        return quad_mesh(path, n, jitter=0.2, seed=1)
+    if kind == "hex":
+        return hex_mesh(path, n, jitter=0.15, seed=1)
+    if kind == "tet_orders":
+        rng = np.random.Generator(np.random.PCG64(1))
+        tags = ORDER_REGION_BASE + rng.integers(1, 6, size=6 * n ** 3)
+        return tet_mesh(path, n, jitter=0.1, seed=1, element_tags=tags)
+    if kind == "tet_sigma":
+        rng = np.random.Generator(np.random.PCG64(1))
+        tags = MATERIAL_REGION_BASE + rng.integers(0, 4, size=6 * n ** 3)
+        return tet_mesh(path, n, jitter=0.1, seed=1, element_tags=tags)
+    raise ValueError(kind)

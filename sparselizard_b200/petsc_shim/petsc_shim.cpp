@@ -370,32 +370,45 @@ PetscErrorCode STGetKSP(ST, KSP*) { unsupported("STGetKSP"); }
 // ------------------------------------------------------------------ CBLAS
 typedef void (*dgemm_fn)(int, int, int, int, int, int, double, const double*, int, const double*, int, double, double*, int);
 
+// The BLAS behind cblas_dgemm: the library named by SLSHIM_OPENBLAS (an
+// OpenBLAS build exporting scipy_cblas_dgemm, e.g. the one bundled with scipy)
+// when it loads, else the plain loop below.  slshim_dgemm_name() reports which.
+static std::string g_dgemm_name = "loop (no BLAS library loaded)";
+
 static dgemm_fn load_openblas_dgemm(void)
 {
-    const char* candidates[] = {
-        std::getenv("SLSHIM_OPENBLAS"),
-        "/opt/prime-rl/.venv/lib/python3.12/site-packages/scipy.libs/libscipy_openblas-5f890258.so",
-    };
-    for (const char* path : candidates) {
-        if (path == nullptr || path[0] == 0)
-            continue;
-        void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
-        if (h == nullptr)
-            continue;
-        void* f = dlsym(h, "scipy_cblas_dgemm");
-        if (f != nullptr)
-            return (dgemm_fn)f;
-    }
-    return nullptr;
+    const char* path = std::getenv("SLSHIM_OPENBLAS");
+    if (path == nullptr || path[0] == 0)
+        return nullptr;
+    void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (h == nullptr)
+        return nullptr;
+    void* f = dlsym(h, "scipy_cblas_dgemm");
+    if (f == nullptr)
+        return nullptr;
+    g_dgemm_name = std::string("OpenBLAS scipy_cblas_dgemm from ") + path;
+    return (dgemm_fn)f;
+}
+
+static dgemm_fn dgemm_impl(void)
+{
+    static std::once_flag once;
+    static dgemm_fn fn = nullptr;
+    std::call_once(once, [] { fn = load_openblas_dgemm(); });
+    return fn;
+}
+
+extern "C" const char* slshim_dgemm_name(void)
+{
+    dgemm_impl();
+    return g_dgemm_name.c_str();
 }
 
 void cblas_dgemm(enum CBLAS_ORDER order, enum CBLAS_TRANSPOSE transa, enum CBLAS_TRANSPOSE transb,
                  int m, int n, int k, double alpha, const double* a, int lda, const double* b, int ldb,
                  double beta, double* c, int ldc)
 {
-    static std::once_flag once;
-    static dgemm_fn fn = nullptr;
-    std::call_once(once, [] { fn = load_openblas_dgemm(); });
+    dgemm_fn fn = dgemm_impl();
     if (fn != nullptr) {
         fn((int)order, (int)transa, (int)transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
         return;

@@ -44,8 +44,32 @@ class Assembled:
 _LIBS: dict[str, ctypes.CDLL] = {}
 
 
+def openblas_path() -> str | None:
+    """The OpenBLAS shared library bundled with scipy (it exports
+    scipy_cblas_dgemm), located through the installed scipy package."""
+    import glob
+    import importlib.util
+
+    spec = importlib.util.find_spec("scipy")
+    if spec is None or not spec.submodule_search_locations:
+        return None
+    site = os.path.dirname(list(spec.submodule_search_locations)[0])
+    hits = sorted(glob.glob(os.path.join(site, "scipy.libs", "libscipy_openblas*.so")))
+    return hits[0] if hits else None
+
+
+def dgemm_name(lib: ctypes.CDLL) -> str:
+    """Which dgemm the PETSc/CBLAS stand-in of a driver library uses."""
+    f = lib.slshim_dgemm_name
+    f.restype = ctypes.c_char_p
+    return f().decode(errors="replace")
+
+
 def load(path: str) -> ctypes.CDLL:
     path = os.path.abspath(path)
+    if not os.environ.get("SLSHIM_OPENBLAS"):
+        # The stand-in's cblas_dgemm dlopens SLSHIM_OPENBLAS on its first call.
+        os.environ["SLSHIM_OPENBLAS"] = openblas_path() or ""
     if path not in _LIBS:
         if not os.path.exists(path):
             raise FileNotFoundError(f"driver library {path} is not built")

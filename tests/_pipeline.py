@@ -53,6 +53,9 @@ def _child_main(mode, workload, msh, params, out, reps):
     elif mode.startswith("sweep"):
         np.savez(out, **sweep_inproc(msh, params, mode.split(":")[1]))
         return
+    elif mode in ("ref_elim", "gpu_elim"):
+        np.savez(out, **eliminate_inproc(mode, workload, msh, params))
+        return
     else:
         raise ValueError(mode)
     np.savez(out, ndofs=np.array(r.ndofs), times=r.times, **{k: getattr(r, k) for k in KEYS})
@@ -89,6 +92,64 @@ def sweep_inproc(msh, params, precision):
     A, D = np.zeros(max(1, nnzA)), np.zeros(max(1, nnz - nnzA))
     lib.slz_sweep_values(abi.f64p(A), abi.f64p(D))
     return dict(Avals=A[:nnzA], Dvals=D[: nnz - nnzA], device_ms=dev, host_ms=host)
+
+
+def elimination_vector(ndofs, seed=77):
+    return np.random.Generator(np.random.PCG64(seed)).standard_normal(ndofs)
+
+
+def eliminate_inproc(mode, workload, msh, params):
+    """Runs the workload, then eliminates the constrained DOFs from a seeded
+    random vector x: on the host through mat::eliminate (ref_elim, the stock
+    build) or on the device through slgpu_matrix_eliminate (gpu_elim, the
+    drop-in, which also checks slgpu_matrix_device_csr against the host CSR)."""
+    from sparselizard_b200 import abi, workloads as W
+
+    lib_path = REF_LIB if mode == "ref_elim" else GPU_LIB
+    r = W.run(lib_path, workload, msh, params)
+    lib = W.load(lib_path)
+    x = elimination_vector(r.ndofs)
+    out = {k: getattr(r, k) for k in ("Ainds", "Dinds", "Drows", "Dcols", "Dvals")}
+    out["x"] = x
+    if mode == "ref_elim":
+        lib.slz_eliminate.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.slz_eliminate.restype = ctypes.c_longlong
+        e = np.zeros(max(1, r.Ainds.size))
+        n = lib.slz_eliminate(x.ctypes.data, e.ctypes.data)
+        assert n == r.Ainds.size, lib.slz_last_error()
+        out["elim"] = e[:n]
+        return out
+    import torch
+
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+    h = lib.slz_last_matrix_handle()
+    assert h > 0
+    ptr = [ctypes.c_void_p() for _ in range(6)]
+    assert lib.slgpu_matrix_device_csr(ctx, h, *[ctypes.byref(q) for q in ptr]) == 0
+    cudart = ctypes.CDLL("libcudart.so.12")
+    cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    host = [r.Arows, r.Acols, r.Avals, r.Drows, r.Dcols, r.Dvals]
+    for q, a in zip(ptr, host):
+        got = np.empty_like(a)
+        if a.size:
+            assert cudart.cudaMemcpy(got.ctypes.data, q, a.nbytes, 2) == 0  # device to host
+        assert np.array_equal(got, a), "device CSR differs from the downloaded CSR"
+    xd = torch.from_numpy(x).cuda()
+    ed = torch.empty(max(1, r.Ainds.size), dtype=torch.float64, device="cuda")
+    st = lib.slgpu_matrix_eliminate(ctx, h, ctypes.c_void_p(xd.data_ptr()), ctypes.c_void_p(ed.data_ptr()))
+    assert st == 0, st
+    out["elim"] = ed.cpu().numpy()[: r.Ainds.size]
+    # Host memory is rejected with an error, not read by the device.
+    st = lib.slgpu_matrix_eliminate(ctx, h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(ed.data_ptr()))
+    assert st == abi.E_ARG, st
+    return out
+
+
+def eliminate(mode, workload, msh, params):
+    with tempfile.TemporaryDirectory() as d:
+        return _child(mode, workload, msh, params, os.path.join(d, "o.npz"))
 
 
 def sweep(msh, order, f1, f2, sigmas, freqs, precision="fp64"):
@@ -281,29 +342,35 @@ def scaled_errors(ref, other):
     error of the symmetrically scaled matrix D^-1/2 A D^-1/2: an entry that is
     exactly zero in exact arithmetic (e.g. curl-curl of a gradient form
     function) is judged against the scale of the terms that cancel in it, not
-    against its own rounding noise.  Also returns the Frobenius-relative error."""
-    Arows, Drows = np.asarray(ref["Arows"], np.int64), np.asarray(ref["Drows"], np.int64)
-    Acols, Dcols = np.asarray(ref["Acols"], np.int64), np.asarray(ref["Dcols"], np.int64)
-    Av, Dv = np.abs(np.asarray(ref["Avals"])), np.abs(np.asarray(ref["Dvals"]))
-    nA = Arows.size - 1
-    rowA = np.repeat(np.arange(nA), np.diff(Arows))
-    rowD = np.repeat(np.arange(nA), np.diff(Drows))
-    S = np.zeros(max(nA, 1))
-    if Av.size:
-        np.maximum.at(S, rowA, Av)
-        np.maximum.at(S, Acols, Av)
-    if Dv.size:
-        np.maximum.at(S, rowD, Dv)
-    Cd = np.zeros(int(Dcols.max()) + 1 if Dcols.size else 1)
-    if Dv.size:
-        np.maximum.at(Cd, Dcols, Dv)
+    against its own rounding noise.  Also returns the Frobenius-relative error.
+    Computed with torch's multi-threaded CPU kernels (full-size workloads hold
+    up to a few hundred million entries)."""
+    import torch
+
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dt))
+    Arows, Drows = t(ref["Arows"], np.int64), t(ref["Drows"], np.int64)
+    Acols, Dcols = t(ref["Acols"], np.int64), t(ref["Dcols"], np.int64)
+    Ar, Dr = t(ref["Avals"], np.float64), t(ref["Dvals"], np.float64)
+    Ao, Do = t(other["Avals"], np.float64), t(other["Dvals"], np.float64)
+    nA = Arows.numel() - 1
+    rowA = torch.repeat_interleave(torch.arange(nA), Arows.diff())
+    rowD = torch.repeat_interleave(torch.arange(nA), Drows.diff())
+    S = torch.zeros(max(nA, 1), dtype=torch.float64)
+    if Ar.numel():
+        S.scatter_reduce_(0, rowA, Ar.abs(), "amax")
+        S.scatter_reduce_(0, Acols, Ar.abs(), "amax")
+    if Dr.numel():
+        S.scatter_reduce_(0, rowD, Dr.abs(), "amax")
+    Cd = torch.zeros(int(Dcols.max()) + 1 if Dcols.numel() else 1, dtype=torch.float64)
+    if Dr.numel():
+        Cd.scatter_reduce_(0, Dcols, Dr.abs(), "amax")
     floor = 1e-300
-    eA = np.abs(np.asarray(other["Avals"]) - np.asarray(ref["Avals"])) / np.maximum(np.sqrt(S[rowA] * S[Acols]), floor) if Av.size else np.zeros(1)
-    eD = np.abs(np.asarray(other["Dvals"]) - np.asarray(ref["Dvals"])) / np.maximum(np.sqrt(S[rowD] * Cd[Dcols]), floor) if Dv.size else np.zeros(1)
-    allref = np.concatenate([np.asarray(ref["Avals"]), np.asarray(ref["Dvals"])])
-    alloth = np.concatenate([np.asarray(other["Avals"]), np.asarray(other["Dvals"])])
-    fro = float(np.linalg.norm(alloth - allref) / max(np.linalg.norm(allref), floor))
-    return float(eA.max()), float(eD.max()), fro
+    eA = ((Ao - Ar).abs() / (S[rowA] * S[Acols]).sqrt().clamp_min(floor)).max().item() if Ar.numel() else 0.0
+    eD = ((Do - Dr).abs() / (S[rowD] * Cd[Dcols]).sqrt().clamp_min(floor)).max().item() if Dr.numel() else 0.0
+    num = float(((Ao - Ar) ** 2).sum() + ((Do - Dr) ** 2).sum())
+    den = float((Ar ** 2).sum() + (Dr ** 2).sum())
+    fro = (num / den) ** 0.5 if den > 0 else (0.0 if num == 0 else float("inf"))
+    return float(eA), float(eD), float(fro)
 
 
 def magnitude_errors(ref, other, mag):

@@ -100,6 +100,28 @@ def test_dropin_poisson_full_size(ref_lib, gpu_lib, tmp):
     assert ref["Acols"].size == 582169 and ref["Dcols"].size == 3056
 
 
+@pytest.mark.parametrize("workload,kind,n,params", [(W.POISSON_QUAD, "quad", 64, [2]), (W.ELASTICITY_HEX, "hex", 6, [2, -2])])
+def test_device_csr_and_eliminate(ref_lib, gpu_lib, tmp, workload, kind, n, params):
+    """Device-resident handoff: slgpu_matrix_device_csr returns the same CSR
+    as the download, and slgpu_matrix_eliminate (x_A - D x_D on the device)
+    equals the reference's mat::eliminate of the same vector bit for bit."""
+    msh = str(tmp / f"elim_{kind}.msh")
+    meshgen.workload_mesh(kind, n, msh)
+    ref = P.eliminate("ref_elim", workload, msh, params)
+    got = P.eliminate("gpu_elim", workload, msh, params)
+    assert ref["Dcols"].size > 0
+    for k in ("Ainds", "Dinds", "Drows", "Dcols"):
+        assert np.array_equal(ref[k], got[k])
+    np.testing.assert_array_equal(ref["x"], got["x"])
+    # Bit-exact when D's values are; otherwise within the values' tolerance.
+    if np.array_equal(ref["Dvals"], got["Dvals"]):
+        np.testing.assert_array_equal(got["elim"], ref["elim"])
+    bd = ref["x"][ref["Dinds"]]
+    rows = np.repeat(np.arange(ref["Ainds"].size), np.diff(ref["Drows"]))
+    mag = np.abs(ref["x"][ref["Ainds"]]) + np.bincount(rows, np.abs(ref["Dvals"] * bd[ref["Dcols"]]), ref["Ainds"].size)
+    assert np.max(np.abs(got["elim"] - ref["elim"]) / np.maximum(mag, 1e-300)) <= TOL
+
+
 def _matrix(ctx, groups, ndofs, con, frags=(), precision=abi.PREC_FP64):
     L = ctx.lib
     h = ctypes.c_int()

@@ -52,9 +52,10 @@ def _regular_element_matrices(ctx, gb, xyz, conn):
     return vals.reshape(nelem, ntf * ndof)
 
 
-def _noalloc(gb, xyz_dev, conn_dev, mesh_nelem, out_dev, stream):
+def _noalloc(gb, xyz_dev, conn_dev, mesh_nelem, out_dev, stream, nnodes=None):
     err = ctypes.create_string_buffer(512)
-    st = abi.lib().slgpu_element_matrices_noalloc(ctypes.byref(gb.g), ctypes.c_void_p(xyz_dev.data_ptr()),
+    nnodes = xyz_dev.numel() // 3 if nnodes is None else nnodes
+    st = abi.lib().slgpu_element_matrices_noalloc(ctypes.byref(gb.g), ctypes.c_void_p(xyz_dev.data_ptr()), nnodes,
                                                   ctypes.c_void_p(conn_dev.data_ptr()), mesh_nelem,
                                                   ctypes.c_void_p(out_dev.data_ptr()), ctypes.c_void_p(stream), err, 512)
     return st, err.value.decode()
@@ -97,3 +98,33 @@ def test_noalloc_rejects_groups_beyond_its_scratch():
     out = torch.empty(16, dtype=torch.float64, device="cuda")
     st, msg = _noalloc(gb, xyz_dev, conn_dev, conn.size // 4, out, torch.cuda.current_stream().cuda_stream)
     assert st == abi.E_BUDGET and "scratch" in msg
+
+
+def test_noalloc_without_destinations_and_bad_nodes():
+    """A group with no destinations is accepted (nothing is assembled), and an
+    element whose connectivity names a node beyond `nnodes` gets a NaN matrix
+    while the other elements are unaffected."""
+    import torch
+
+    rng = np.random.Generator(np.random.PCG64(31))
+    gb, xyz, conn = S.group(rng, nelem_grid=6, ntf=4, ndof=4, nterms=2, norient=1, ndests=1)
+    g = gb.g
+    stream = torch.cuda.current_stream().cuda_stream
+    xyz_dev = torch.from_numpy(xyz).cuda()
+    conn_dev = torch.from_numpy(conn).cuda()
+    good = torch.empty((g.nelem, g.ntf * g.ndof), dtype=torch.float64, device="cuda")
+    st, msg = _noalloc(gb, xyz_dev, conn_dev, conn.size // 4, good, stream)
+    assert st == abi.OK, msg
+    g.ndests, g.dests = 0, None
+    bad_conn = conn.copy()
+    elems = np.ctypeslib.as_array(g.elems, (g.nelem,)).copy()
+    victim = int(elems[0])
+    bad_conn[victim * 4 + 1] = xyz.size // 3 + 7
+    out = torch.zeros_like(good)
+    st, msg = _noalloc(gb, xyz_dev, torch.from_numpy(bad_conn).cuda(), conn.size // 4, out, stream)
+    assert st == abi.OK, msg
+    torch.cuda.synchronize()
+    got, want = out.cpu().numpy(), good.cpu().numpy()
+    hit = elems == victim
+    assert np.isnan(got[hit]).all()
+    assert np.array_equal(got[~hit], want[~hit])
