@@ -21,6 +21,7 @@
 #include "engine_kernels.cuh"
 #include "split_tc.cuh"
 #include "row_stream.cuh"
+#include "contract_f64.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -1313,7 +1314,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
 // Whether the split contraction of a group computes only the upper triangle
 // of its element matrices: the group has mirror terms with equal scales
 // (SLGPU_SPLIT_SYMMETRY=0 turns this off).
-static bool split_symmetry_enabled()
+static bool mirror_forms_enabled()
 {
     static const bool enabled = [] {
         const char* v = std::getenv("SLGPU_SPLIT_SYMMETRY");
@@ -1322,9 +1323,9 @@ static bool split_symmetry_enabled()
     return enabled;
 }
 
-static bool split_symmetric(const GroupDev& g)
+static bool symmetric_form(const GroupDev& g)
 {
-    if (!split_symmetry_enabled() || g.mirror.empty())
+    if (!mirror_forms_enabled() || g.mirror.empty())
         return false;
     for (int t = 0; t < g.nterms; t++)
         if (std::memcmp(&g.term_scale[t], &g.term_scale[g.mirror[t]], sizeof(double)) != 0)
@@ -1400,7 +1401,7 @@ static GroupDev::Split& build_split(Ctx* ctx, GroupDev& g, int slot)
 // execution state's stream order; a request stream waits for them.
 static GroupDev::Split& ensure_split(Ctx* ctx, GroupDev& g, int tier, bool paired)
 {
-    const int slot = tier + 2 * (paired ? 2 : split_symmetric(g) ? 1 : 0);
+    const int slot = tier + 2 * (paired ? 2 : symmetric_form(g) ? 1 : 0);
     if (g.split[slot])
         return *g.split[slot];
     Exec* cur = ctx->x;
@@ -1445,111 +1446,212 @@ static void launch_split(Ctx* ctx, const SplitParams& p)
     k_contract_split<S, L, NE><<<(unsigned)grid, kSplitThreads, smem, ctx->x->stream>>>(p);
 }
 
-// Element-tile width of the split kernel: SLGPU_SPLIT_TILE=32 or 64 (default 64).
-static int split_tile_width()
+// Element-tile width of the split kernel forced by SLGPU_SPLIT_TILE=32 or 64;
+// 0: picked per group shape by timing (tile_choice).
+static int split_tile_forced()
 {
     static const int ne = [] {
         const char* v = std::getenv("SLGPU_SPLIT_TILE");
-        return (v != nullptr && std::strcmp(v, "32") == 0) ? 32 : 64;
+        if (v == nullptr)
+            return 0;
+        return std::strcmp(v, "32") == 0 ? 32 : std::strcmp(v, "64") == 0 ? 64 : 0;
     }();
     return ne;
 }
 
-// Column slices of one group's coefficients (k_slice_cols) into `slices` /
-// `colexp`, on the current execution state's stream.
-static void slice_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const double* C, const int32_t* elemexp, int8_t* slices,
-                        int32_t* colexp)
+// One split-precision contraction of a launch: group, tier, form and where
+// its coefficients, exponents and element matrices (and, for a transposed
+// pair, the partner's) are.
+struct SplitJob {
+    GroupDev* g;
+    int tier;
+    bool paired;
+    const double* C;
+    const int32_t* elemexp;
+    double* out;
+    double* out2;
+};
+
+static std::array<int, 5> split_shape_key(const GroupDev& g, int tier) { return {0, tier, g.ntf, g.ndof, g.ngp}; }
+
+// Column-slice bytes of one group in the scratch (256-byte aligned blocks).
+static size_t split_col_bytes(const GroupDev& g, const GroupDev::Split& sp)
 {
-    const int Q = g.nterms * g.ngp;
-    const int NE = split_tile_width();
-    const int64_t ntiles = (int64_t)g.tiles.size();
-    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
-    ColSliceParams cs{};
-    cs.C = C;
-    cs.elemexp = elemexp;
-    cs.tiles = g.tiles_d.as<Tile>();
-    cs.Q = Q;
-    cs.Qpad = sp.Qpad;
-    cs.nelem = g.nelem;
-    cs.ntiles = ntiles;
-    cs.slices = slices;
-    cs.colexp = colexp;
-    const dim3 cgrid = grid_for(ntiles * 64, 128);
-    const int kt = kstat_start(ctx, "slice_cols", 8.0 * Q * g.nelem + 4.0 * g.nelem + (double)colbytes + 4.0 * ntiles * 64);
-    if (sp.S == 7 && NE == 64)
-        k_slice_cols<7, 64><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
-    else if (sp.S == 7)
-        k_slice_cols<7, 32><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
-    else if (sp.S == 5 && NE == 64)
-        k_slice_cols<5, 64><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
-    else if (sp.S == 5)
-        k_slice_cols<5, 32><<<cgrid, 128, 0, ctx->x->stream>>>(cs);
-    else
-        fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
-    kstat_stop(ctx, kt);
-    cuda_check(cudaGetLastError(), "k_slice_cols");
-    ctx->launches++;
+    return ((size_t)sp.S * sp.Qpad * g.tiles.size() * 64 + 255) & ~size_t(255);
+}
+static size_t split_exp_bytes(const GroupDev& g) { return (g.tiles.size() * 64 * 4 + 255) & ~size_t(255); }
+
+template <int S, int NE>
+static void launch_slices(Ctx* ctx, const ColSliceParams& cs)
+{
+    k_slice_cols<S, NE><<<grid_for(cs.ntiles * 64, 128), 128, 0, ctx->x->stream>>>(cs);
 }
 
-// The tcgen05 contraction of one group from its column slices.
-static void split_group(Ctx* ctx, const GroupDev& g, const GroupDev::Split& sp, const int8_t* slices, const int32_t* colexp, double* out,
-                        double* out2)
+// Column slicing and the tcgen05 contraction of a set of jobs of one tier
+// with element-tile width NE: one slicing launch and one persistent
+// contraction launch per kSplitBatch jobs.  Every job's column slices and
+// exponents get their own block of the execution state's scratch.
+static void run_split_jobs(Ctx* ctx, const std::vector<SplitJob>& jobs, int NE)
 {
-    const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
-    const int NE = split_tile_width();
-    const int64_t ntiles = (int64_t)g.tiles.size();
-    SplitParams p{};
-    p.P = P;
-    p.nrows = sp.nrows;
-    p.rowmap = sp.rowmap.empty() ? nullptr : sp.rowmap.as<int2>();
-    p.out2 = out2;
-    p.Ppad = sp.Ppad;
-    p.ntp = sp.Ppad / kSplitM;
-    p.nk = sp.Qpad / kSplitKStep;
-    p.nwork = (int64_t)p.ntp * ntiles * (64 / NE);
-    p.tiles = g.tiles_d.as<Tile>();
-    p.A = sp.slices.as<int8_t>();
-    p.B = slices;
-    p.rowexp = sp.rowexp.as<int32_t>();
-    p.colexp = colexp;
-    p.out = out;
-    p.error = ctx->x->split_error.as<unsigned int>();
-    // Algorithmic INT8 operations: 2 per product, pairs (a, b) with a + b <= L.
-    int pairs = 0;
-    for (int a = 1; a <= sp.S; a++)
-        for (int b = 1; b <= sp.S; b++) pairs += (a + b <= sp.L);
-    const int kc = kstat_start(ctx, sp.S == 7 ? "contract_split" : "contract_split_fp32", 2.0 * pairs * sp.nrows * Q * g.nelem);
-    if (sp.S == 7 && NE == 64)
-        launch_split<7, 8, 64>(ctx, p);
-    else if (sp.S == 7)
-        launch_split<7, 8, 32>(ctx, p);
-    else if (NE == 64)
-        launch_split<5, 6, 64>(ctx, p);
-    else
-        launch_split<5, 6, 32>(ctx, p);
-    kstat_stop(ctx, kc);
-    cuda_check(cudaGetLastError(), "k_contract_split");
-    ctx->launches++;
-}
-
-// Split contraction of one group: column slices of C (exponents per element
-// from the coefficient kernel) into the execution state's scratch, then the
-// tcgen05 kernel (which also writes the transposed partner's element matrices
-// into out2, if given).
-static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, const int32_t* elemexp, double* out, double* out2)
-{
-    const GroupDev::Split& sp = ensure_split(ctx, g, tier, out2 != nullptr);
-    const int64_t ntiles = (int64_t)g.tiles.size();
-    const size_t colbytes = (size_t)sp.S * sp.Qpad * ntiles * 64;
+    if (jobs.empty())
+        return;
+    const int tier = jobs[0].tier;
+    size_t colb = 0, expb = 0;
+    for (const SplitJob& j : jobs) {
+        const GroupDev::Split& sp = ensure_split(ctx, *j.g, tier, j.paired);
+        colb += split_col_bytes(*j.g, sp);
+        expb += split_exp_bytes(*j.g);
+    }
     {
         ArenaPause keep(*ctx->x);  // per-state scratch, kept between requests
-        if (ctx->x->split_cols.bytes() < colbytes)
-            ctx->x->split_cols.alloc(ctx, colbytes);
-        if (ctx->x->split_colexp.bytes() < (size_t)ntiles * 64 * 4)
-            ctx->x->split_colexp.alloc(ctx, (size_t)ntiles * 64 * 4);
+        if (ctx->x->split_cols.bytes() < colb)
+            ctx->x->split_cols.alloc(ctx, colb);
+        if (ctx->x->split_colexp.bytes() < expb)
+            ctx->x->split_colexp.alloc(ctx, expb);
     }
-    slice_group(ctx, g, sp, C, elemexp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>());
-    split_group(ctx, g, sp, ctx->x->split_cols.as<int8_t>(), ctx->x->split_colexp.as<int32_t>(), out, out2);
+    int8_t* cols = ctx->x->split_cols.as<int8_t>();
+    int32_t* cexp = ctx->x->split_colexp.as<int32_t>();
+    for (size_t b0 = 0; b0 < jobs.size(); b0 += kSplitBatch) {
+        const size_t b1 = std::min(jobs.size(), b0 + kSplitBatch);
+        ColSliceParams cs{};
+        SplitParams sp{};
+        double slice_bytes = 0, ops = 0;
+        int S = 0;
+        for (size_t k = b0; k < b1; k++) {
+            const SplitJob& j = jobs[k];
+            const GroupDev& g = *j.g;
+            const GroupDev::Split& s = *g.split[tier + 2 * (j.paired ? 2 : symmetric_form(g) ? 1 : 0)];
+            S = s.S;
+            const int64_t ntiles = (int64_t)g.tiles.size();
+            const int Q = g.nterms * g.ngp;
+            ColSliceGroup& c = cs.g[cs.ngroups++];
+            c.C = j.C;
+            c.elemexp = j.elemexp;
+            c.tiles = g.tiles_d.as<Tile>();
+            c.Q = Q;
+            c.Qpad = s.Qpad;
+            c.nelem = g.nelem;
+            c.ntiles = ntiles;
+            c.slices = cols;
+            c.colexp = cexp;
+            c.t0 = cs.ntiles;
+            cs.ntiles += ntiles;
+            SplitGroup& G = sp.g[sp.ngroups++];
+            G.P = g.ntf * g.ndof;
+            G.Ppad = s.Ppad;
+            G.ntp = s.Ppad / kSplitM;
+            G.nk = s.Qpad / kSplitKStep;
+            G.nrows = s.nrows;
+            G.rowmap = s.rowmap.empty() ? nullptr : s.rowmap.as<int2>();
+            G.out2 = j.out2;
+            G.tiles = g.tiles_d.as<Tile>();
+            G.A = s.slices.as<int8_t>();
+            G.B = cols;
+            G.rowexp = s.rowexp.as<int32_t>();
+            G.colexp = cexp;
+            G.out = j.out;
+            G.w0 = sp.nwork;
+            G.nwork = (int64_t)G.ntp * ntiles * (64 / NE);
+            sp.nwork += G.nwork;
+            const size_t cb = split_col_bytes(g, s);
+            slice_bytes += 8.0 * Q * g.nelem + 4.0 * g.nelem + (double)cb + 4.0 * ntiles * 64;
+            // Algorithmic INT8 operations: 2 per product, pairs (a, b) with a + b <= L.
+            int pairs = 0;
+            for (int a = 1; a <= s.S; a++)
+                for (int bb = 1; bb <= s.S; bb++) pairs += (a + bb <= s.L);
+            ops += 2.0 * pairs * s.nrows * Q * g.nelem;
+            cols += cb;
+            cexp += split_exp_bytes(g) / 4;
+        }
+        sp.error = ctx->x->split_error.as<unsigned int>();
+        const int kt = kstat_start(ctx, "slice_cols", slice_bytes);
+        if (S == 7 && NE == 64)
+            launch_slices<7, 64>(ctx, cs);
+        else if (S == 7)
+            launch_slices<7, 32>(ctx, cs);
+        else if (S == 5 && NE == 64)
+            launch_slices<5, 64>(ctx, cs);
+        else if (S == 5)
+            launch_slices<5, 32>(ctx, cs);
+        else
+            fail(SLGPU_E_UNSUPPORTED, "unsupported slice count");
+        kstat_stop(ctx, kt);
+        cuda_check(cudaGetLastError(), "k_slice_cols");
+        ctx->launches++;
+        const int kc = kstat_start(ctx, S == 7 ? "contract_split" : "contract_split_fp32", ops);
+        if (S == 7 && NE == 64)
+            launch_split<7, 8, 64>(ctx, sp);
+        else if (S == 7)
+            launch_split<7, 8, 32>(ctx, sp);
+        else if (NE == 64)
+            launch_split<5, 6, 64>(ctx, sp);
+        else
+            launch_split<5, 6, 32>(ctx, sp);
+        kstat_stop(ctx, kc);
+        cuda_check(cudaGetLastError(), "k_contract_split");
+        ctx->launches++;
+    }
+}
+
+// Times each candidate (twice, in turn; best run kept) on the jobs' own data
+// and returns the fastest.  The candidates give identical element matrices.
+template <class Run>
+static int pick_by_timing(Ctx* ctx, const std::vector<int>& cand, Run run)
+{
+    const size_t nc = cand.size();
+    std::vector<cudaEvent_t> ev(2 * nc + 1);
+    for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    cuda_check(cudaEventRecord(ev[0], ctx->x->stream), "cudaEventRecord");
+    for (size_t r = 0; r < 2; r++)
+        for (size_t c = 0; c < nc; c++) {
+            run(cand[c]);
+            cuda_check(cudaEventRecord(ev[1 + r * nc + c], ctx->x->stream), "cudaEventRecord");
+        }
+    cuda_check(cudaEventSynchronize(ev[2 * nc]), "sync");
+    float best_t = 0;
+    int best = cand[0];
+    for (size_t c = 0; c < nc; c++) {
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, ev[c], ev[c + 1]);
+        cudaEventElapsedTime(&t1, ev[nc + c], ev[nc + c + 1]);
+        const float t = std::min(t0, t1);
+        if (c == 0 || t < best_t) {
+            best_t = t;
+            best = cand[c];
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return best;
+}
+
+// Element-tile width for a group shape: forced, tuned, or (while graph
+// capture or a request stream prevents timing) 64.
+static int split_ne_of(Ctx* ctx, const GroupDev& g, int tier)
+{
+    if (split_tile_forced() != 0)
+        return split_tile_forced();
+    auto it = ctx->tile_choice.find(split_shape_key(g, tier));
+    return it == ctx->tile_choice.end() ? 64 : it->second;
+}
+
+// All split jobs of one process: shapes without a tuned width are timed
+// first (their jobs at each width), then one launch pair per width.
+static void contract_split_all(Ctx* ctx, const std::vector<SplitJob>& jobs)
+{
+    if (jobs.empty())
+        return;
+    if (split_tile_forced() == 0 && !ctx->x->capturing && ctx->x == &ctx->main) {
+        std::map<std::array<int, 5>, std::vector<SplitJob>> untuned;
+        for (const SplitJob& j : jobs)
+            if (!ctx->tile_choice.count(split_shape_key(*j.g, j.tier)))
+                untuned[split_shape_key(*j.g, j.tier)].push_back(j);
+        for (auto& kv : untuned)
+            ctx->tile_choice[kv.first] = pick_by_timing(ctx, {64, 32}, [&](int ne) { run_split_jobs(ctx, kv.second, ne); });
+    }
+    std::vector<SplitJob> by[2];
+    for (const SplitJob& j : jobs) by[split_ne_of(ctx, *j.g, j.tier) == 32 ? 1 : 0].push_back(j);
+    run_split_jobs(ctx, by[0], 64);
+    run_split_jobs(ctx, by[1], 32);
 }
 
 // Whether a group's contraction runs in split precision: element matrices
@@ -1558,6 +1660,135 @@ static void contract_split(Ctx* ctx, GroupDev& g, int tier, const double* C, con
 static bool uses_split(const GroupDev& g, int precision)
 {
     return precision != SLGPU_PREC_FP64 && !g.rhs && (int64_t)g.ntf * g.ndof >= 64 && split_supported(g);
+}
+
+// Whether an FP64 contraction of a group may use the mirrored forms (upper
+// triangle of a symmetric group, transposed pairs): matrix groups with at
+// least 64 entries, as for split precision.
+static bool fp64_mirrored(const GroupDev& g) { return !g.rhs && (int64_t)g.ntf * g.ndof >= 64; }
+
+// Groups whose contraction may take a mirrored form at this precision.
+static bool mirror_eligible(const GroupDev& g, int precision)
+{
+    return precision == SLGPU_PREC_FP64 ? fp64_mirrored(g) : uses_split(g, precision);
+}
+
+// Resident M^T of a group for the FP64 tensor-core kernel, built on first use
+// in the main execution state's stream order (a request stream waits for it).
+static GroupDev::Fp64Mt& ensure_fmt(Ctx* ctx, GroupDev& g, int form)
+{
+    std::unique_ptr<GroupDev::Fp64Mt>& f = g.fmt[form];
+    if (f)
+        return *f;
+    Exec* cur = ctx->x;
+    ctx->x = &ctx->main;
+    try {
+        f.reset(new GroupDev::Fp64Mt());
+        const int Q = g.nterms * g.ngp, P = g.ntf * g.ndof;
+        f->nrows = form == 1 ? g.ntf * (g.ntf + 1) / 2 : P;
+        f->Qpad = (Q + kMmaBQ - 1) / kMmaBQ * kMmaBQ;
+        f->rpad = (f->nrows + kMmaBPMax - 1) / kMmaBPMax * kMmaBPMax;
+        if (form != 0)
+            upload(ctx, f->rowmap, mirrored_rows(g.ntf, g.ndof, form == 1));
+        f->Mt.alloc(ctx, (size_t)g.norient * f->Qpad * f->rpad * sizeof(double));
+        BuildMtParams bp{};
+        bp.tables = g.tables.as<double>();
+        bp.tab_off = g.tab_off_d.as<int64_t>();
+        bp.term_tf = g.term_tf_d.as<int32_t>();
+        bp.term_dof = g.term_dof_d.as<int32_t>();
+        bp.rowmap = f->rowmap.empty() ? nullptr : f->rowmap.as<int2>();
+        bp.nterms = g.nterms;
+        bp.ngp = g.ngp;
+        bp.ntf = g.ntf;
+        bp.ndof = g.ndof;
+        bp.norient = g.norient;
+        bp.nrows = f->nrows;
+        bp.Qpad = f->Qpad;
+        bp.rpad = f->rpad;
+        bp.Mt = f->Mt.as<double>();
+        const int64_t n = (int64_t)g.norient * f->Qpad * f->rpad;
+        k_build_mt<<<(unsigned)std::min<int64_t>((n + 255) / 256, 65536), 256, 0, ctx->x->stream>>>(bp);
+        cuda_check(cudaGetLastError(), "k_build_mt");
+        ctx->launches++;
+    } catch (...) {
+        f.reset();
+        ctx->x = cur;
+        throw;
+    }
+    ctx->x = cur;
+    if (cur != &ctx->main) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_check(cudaEventRecord(e, ctx->main.stream), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(cur->stream, e, 0), "cudaStreamWaitEvent");
+        cudaEventDestroy(e);
+    }
+    return *f;
+}
+
+template <int BP>
+static void launch_f64mma(Ctx* ctx, const GroupDev& g, MmaParams mp)
+{
+    static std::once_flag attr;
+    std::call_once(attr, [] {
+        cudaFuncSetAttribute(k_contract_f64mma<BP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MmaShape<BP>::Smem);
+    });
+    mp.nrt = mp.rpad / BP;
+    const int64_t nblocks = (int64_t)g.tiles.size() * mp.nrt;
+    if (nblocks > INT32_MAX)
+        fail(SLGPU_E_UNSUPPORTED, "group too large for one FP64 contraction launch");
+    k_contract_f64mma<BP><<<(unsigned)nblocks, 256, MmaShape<BP>::Smem, ctx->x->stream>>>(mp);
+    cuda_check(cudaGetLastError(), "k_contract_f64mma");
+    ctx->launches++;
+}
+
+// FP64 contraction of one group on the FP64 tensor cores: every entry, the
+// upper triangle of a symmetric group (mirrored into the lower), or every
+// entry with the transposed partner's element matrices written into out2.
+// Rows per block (128 or 64) are picked per group shape by timing on first
+// use (SLGPU_F64_TILE=128 or 64 forces one).
+static void contract_fp64_mma(Ctx* ctx, GroupDev& g, const double* C, double* out, double* out2)
+{
+    const int form = out2 != nullptr ? 2 : (fp64_mirrored(g) && symmetric_form(g)) ? 1 : 0;
+    GroupDev::Fp64Mt& f = ensure_fmt(ctx, g, form);
+    MmaParams mp{};
+    mp.Mt = f.Mt.as<double>();
+    mp.C = C;
+    mp.tiles = g.tiles_d.as<Tile>();
+    mp.rowmap = f.rowmap.empty() ? nullptr : f.rowmap.as<int2>();
+    mp.Q = g.nterms * g.ngp;
+    mp.Qpad = f.Qpad;
+    mp.rpad = f.rpad;
+    mp.nrows = f.nrows;
+    mp.P = g.ntf * g.ndof;
+    mp.mirror = form;
+    mp.nelem = g.nelem;
+    mp.out = out;
+    mp.out2 = out2;
+    static const int forced = [] {
+        const char* v = std::getenv("SLGPU_F64_TILE");
+        return v == nullptr ? 0 : std::strcmp(v, "64") == 0 ? 64 : std::strcmp(v, "128") == 0 ? 128 : 0;
+    }();
+    auto run = [&](int bp) {
+        if (bp == 64)
+            launch_f64mma<64>(ctx, g, mp);
+        else
+            launch_f64mma<128>(ctx, g, mp);
+    };
+    const std::array<int, 5> key{1, 0, g.ntf, g.ndof, g.ngp};
+    int bp = forced;
+    if (bp == 0) {
+        auto it = ctx->tile_choice.find(key);
+        if (it != ctx->tile_choice.end())
+            bp = it->second;
+        else if (!ctx->x->capturing && ctx->x == &ctx->main)
+            bp = ctx->tile_choice[key] = pick_by_timing(ctx, {128, 64}, run);
+        else
+            bp = 128;
+    }
+    const int kt = kstat_start(ctx, "contract_fp64", 2.0 * f.nrows * mp.Q * g.nelem);
+    run(bp);
+    kstat_stop(ctx, kt);
 }
 
 // Transposed pairs among a matrix's split-precision groups: group j is the
@@ -1579,11 +1810,11 @@ static std::vector<int> cross_pairs(const Matrix& M, int precision, const std::v
         const char* v = std::getenv("SLGPU_SPLIT_PAIRS");
         return v == nullptr || std::strcmp(v, "0") != 0;
     }();
-    if (precision == SLGPU_PREC_FP64 || !enabled || !split_symmetry_enabled())
+    if (!enabled || !mirror_forms_enabled())
         return pair;
     auto eligible = [&](size_t i) {
         const GroupDev& g = *M.groups[i];
-        if (g.nelem == 0 || !uses_split(g, precision) || split_symmetric(g) || g.term_keys.empty())
+        if (g.nelem == 0 || !mirror_eligible(g, precision) || symmetric_form(g) || g.term_keys.empty())
             return false;
         return ov == nullptr || ((*ov)[i].elemdata == nullptr && (*ov)[i].fielddata == nullptr);
     };
@@ -1789,6 +2020,7 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     launch_coefficients(ctx, M, C.as<double>(), coff, E.as<int32_t>(), eoff, ov, pair);
     phase_event(ctx, ctx->x->evpool[1]);
     size_t gi = 0;
+    std::vector<SplitJob> split_jobs;  // every split-precision group of the step, contracted together
     for (auto& g : M.groups) {
         if (g->nelem > 0) {
             double* Cg = C.as<double>() + coff[gi];
@@ -1797,44 +2029,48 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
             // group of a transposed pair is written by the first's contraction.
             if (uses_split(*g, precision)) {
                 if (pair[gi] < 0 || pair[gi] > (int)gi)
-                    contract_split(ctx, *g, precision == SLGPU_PREC_SPLIT ? 0 : 1, Cg, E.as<int32_t>() + eoff[gi], vals + gvb[gi],
-                                   pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr);
+                    split_jobs.push_back(SplitJob{g.get(), precision == SLGPU_PREC_SPLIT ? 0 : 1, pair[gi] > (int)gi, Cg,
+                                                  E.as<int32_t>() + eoff[gi], vals + gvb[gi],
+                                                  pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr});
                 gi++;
                 continue;
             }
-            ContractParams kp{};
-            kp.tables = g->tables.as<double>();
-            kp.tab_off = g->tab_off_d.as<int64_t>();
-            kp.term_tf = g->term_tf_d.as<int32_t>();
-            kp.term_dof = g->term_dof_d.as<int32_t>();
-            kp.nterms = g->nterms;
-            kp.ngp = g->ngp;
-            kp.ntf = g->ntf;
-            kp.ndof = g->ndof;
-            kp.nelem = g->nelem;
-            kp.C = Cg;
-            kp.tiles = g->tiles_d.as<Tile>();
-            kp.out = vals + gvb[gi];
+            // The second group of a transposed pair is written by the first's contraction.
+            if (pair[gi] >= 0 && pair[gi] < (int)gi) {
+                gi++;
+                continue;
+            }
             const int64_t P = (int64_t)g->ntf * g->ndof;
             const size_t small_smem = ((size_t)g->norient * g->nterms * g->ngp * P + (size_t)kSmallE * (P + 1)) * 8;
-            const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
             if (P <= kSmallP && small_smem <= kSmallSmem) {
+                ContractParams kp{};
+                kp.tables = g->tables.as<double>();
+                kp.tab_off = g->tab_off_d.as<int64_t>();
+                kp.term_tf = g->term_tf_d.as<int32_t>();
+                kp.term_dof = g->term_dof_d.as<int32_t>();
+                kp.nterms = g->nterms;
+                kp.ngp = g->ngp;
+                kp.ntf = g->ntf;
+                kp.ndof = g->ndof;
+                kp.nelem = g->nelem;
+                kp.C = Cg;
+                kp.tiles = g->tiles_d.as<Tile>();
+                kp.out = vals + gvb[gi];
                 static std::once_flag attr;
                 std::call_once(attr, [] { cudaFuncSetAttribute(k_contract_small, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmallSmem); });
+                const int kt = kstat_start(ctx, "contract_fp64", 2.0 * P * g->nterms * g->ngp * g->nelem);
                 k_contract_small<<<(unsigned)((g->nelem + kSmallE - 1) / kSmallE), kSmallE, small_smem, ctx->x->stream>>>(
                     kp, g->orient.as<int32_t>(), g->norient);
+                kstat_stop(ctx, kt);
+                cuda_check(cudaGetLastError(), "k_contract_small");
+                ctx->launches++;
             } else {
-                dim3 grid((unsigned)((P + kTileP - 1) / kTileP), (unsigned)g->tiles.size());
-                if (grid.y > 65535)
-                    fail(SLGPU_E_UNSUPPORTED, "more than 65535 contraction tiles in one group");
-                k_contract_fp64<<<grid, dim3(16, 16), 0, ctx->x->stream>>>(kp);
+                contract_fp64_mma(ctx, *g, Cg, vals + gvb[gi], pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr);
             }
-            kstat_stop(ctx, kt);
-            cuda_check(cudaGetLastError(), "k_contract_fp64");
-            ctx->launches++;
         }
         gi++;
     }
+    contract_split_all(ctx, split_jobs);
     phase_event(ctx, ctx->x->evpool[2]);
     C.release();
     {
@@ -2078,8 +2314,9 @@ void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
             const GroupDev::Split& sp = ensure_split(ctx, *g, tier, false);
             if (pair[gi] > (int)gi)
                 ensure_split(ctx, *g, tier, true);
-            colbytes = std::max(colbytes, (size_t)sp.S * sp.Qpad * g->tiles.size() * 64);
-            expbytes = std::max(expbytes, g->tiles.size() * 64 * 4);
+            // The groups of a step are sliced and contracted together.
+            colbytes += split_col_bytes(*g, sp);
+            expbytes += split_exp_bytes(*g);
         }
     }
     Exec& x = *ctx->x;
@@ -2122,7 +2359,7 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
     p(M.Avals.as<void>());
     p(M.Dvals.as<void>());
     p(M.rsegs_dev.as<void>());
-    u((uint64_t)split_tile_width());
+    u((uint64_t)split_tile_forced());
     u((uint64_t)ctx->nsm);
     u(ctx->timers ? 1 : 0);
     u(ctx->jit_broken ? 1 : 0);
@@ -2137,12 +2374,17 @@ static std::vector<uint64_t> value_signature(Ctx* ctx, const Matrix& M, int prec
         p(g.jit_kernel);
         u(g.jit_members.size());
         for (uint64_t id : g.jit_members) u(id);
-        u(split_symmetric(g) ? 1 : 0);
+        u(symmetric_form(g) ? 1 : 0);
         u((uint64_t)(pair[gi++] + 1));
+        for (int t = 0; t < 2; t++) {
+            auto it = ctx->tile_choice.find(split_shape_key(g, t));
+            u(it == ctx->tile_choice.end() ? 0 : (uint64_t)it->second);
+        }
         for (int t = 0; t < 6; t++) {
             p(g.split[t] ? g.split[t]->slices.as<void>() : nullptr);
             p(g.split[t] ? g.split[t]->rowexp.as<void>() : nullptr);
         }
+        for (int t = 0; t < 3; t++) p(g.fmt[t] ? g.fmt[t]->Mt.as<void>() : nullptr);
         auto mi = ctx->meshes.find(g.mesh);
         if (mi == ctx->meshes.end()) {
             u(~0ull);
@@ -2826,7 +3068,7 @@ int slgpu_matrix_group_symmetry(slgpu_ctx* ctx, int handle, int gi, int32_t* mir
         if (mirror != nullptr)
             for (int t = 0; t < g.nterms; t++) mirror[t] = g.mirror.empty() ? -1 : g.mirror[t];
         if (symmetric != nullptr)
-            *symmetric = split_symmetric(g) ? (g.mirror_exact ? 1 : 2) : 0;
+            *symmetric = symmetric_form(g) ? (g.mirror_exact ? 1 : 2) : 0;
         if (partner != nullptr)
             *partner = cross_pairs(M, SLGPU_PREC_SPLIT, nullptr)[gi];
     });

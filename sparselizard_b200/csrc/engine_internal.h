@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <exception>
 #include <map>
@@ -138,6 +139,13 @@ struct GroupDev {
         DevBuf slices, rowexp, rowmap;
     };
     std::unique_ptr<Split> split[6];
+    // FP64 tensor-core operand M^T per form (0 every entry, 1 upper triangle
+    // of a symmetric group, 2 every entry with its transposed partner's).
+    struct Fp64Mt {
+        int Qpad = 0, rpad = 0, nrows = 0;
+        DevBuf Mt, rowmap;
+    };
+    std::unique_ptr<Fp64Mt> fmt[3];
 
     // Record-only copy of the original description (for inspection).
     struct Record;
@@ -274,6 +282,10 @@ struct Ctx {
     std::recursive_mutex mu;  // one thread at a time inside the context
     std::string last_error;
     int64_t bytes_h2d = 0, bytes_d2h = 0;  // host <-> device bytes copied by the context's calls
+    // Tile shapes picked by timing on first use, per contraction kind and
+    // group shape {kind (0 split, 1 FP64), tier, ntf, ndof, ngp}: the split
+    // kernel's element-tile width NE, the FP64 kernel's rows per block.
+    std::map<std::array<int, 5>, int> tile_choice;
     std::map<int, MeshDev> meshes;
     std::map<int, std::unique_ptr<Matrix>> matrices;
     int next_handle = 1;

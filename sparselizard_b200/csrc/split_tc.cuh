@@ -53,21 +53,42 @@ struct SplitShape {
     static constexpr int kGroup = 256 / NE;              // B slices per MMA (N <= 256)
 };
 
-struct SplitParams {
+// One group of a batched contraction launch.  Its work items are
+// [w0, w0 + nwork) of the launch: item w0 + v is row tile v % ntp of element
+// unit v / ntp.
+struct SplitGroup {
     int P, Ppad, ntp, nk;   // entries, padded rows, row tiles, K steps
-    int nrows;              // rows of A computed (P, or the upper triangle)
+    int nrows, pad;         // rows of A computed (P, or the upper triangle)
     const int2* rowmap;     // [nrows]: the entry and its mirror; null: row r is entry r
     double* out2;           // null, or [nelem][P]: the transposed partner group's
                             // element matrices (entry rowmap[r].y from row r)
-    int64_t nwork;          // row tiles x element units
     const Tile* tiles;      // 64-element tiles; unit u = tile u / kUnits, part u % kUnits
     const int8_t* A;        // row slices
     const int8_t* B;        // column slices
     const int32_t* rowexp;  // [norient][Ppad]
     const int32_t* colexp;  // [ntiles][64]: exponent of each slot
     double* out;            // [nelem][P]
+    int64_t w0, nwork;
+};
+
+// Groups of one launch (same S, L and NE), passed by value: every element
+// group of a step runs in one persistent launch, whatever its entry count,
+// Gauss points or element count.
+constexpr int kSplitBatch = 24;
+struct SplitParams {
+    SplitGroup g[kSplitBatch];
+    int ngroups;
+    int64_t nwork;          // sum of the groups' work items
     unsigned int* error;    // set on a timed-out wait
 };
+
+// Group of work item w, advanced from the group of the CTA's previous item
+// (a CTA's items increase, so each role walks the groups once).
+__device__ __forceinline__ int split_group_of(const SplitParams& p, int gi, int64_t w)
+{
+    while (gi + 1 < p.ngroups && w >= p.g[gi + 1].w0) gi++;
+    return gi;
+}
 
 // Elements [e0, e0 + ne) and orientation of element unit u (ne <= 0: empty).
 template <int NE>
@@ -158,7 +179,7 @@ __global__ void k_slice_rows(RowSliceParams p)
 // are written coalesced over slots.  The exponent of each element (largest
 // |C[q][e]| = f 2^ex, f in [0.5, 1)) comes from the coefficient kernel.
 // Empty slots get zero slices.
-struct ColSliceParams {
+struct ColSliceGroup {
     const double* C;  // [Q][nelem]
     const int32_t* elemexp;  // [nelem]; below -1100: the column is zero
     const Tile* tiles;
@@ -166,16 +187,27 @@ struct ColSliceParams {
     int64_t nelem, ntiles;
     int8_t* slices;   // [unit][kstep][2][S][NE][16]
     int32_t* colexp;  // [ntiles][64]
+    int64_t t0;       // first tile of the group in the launch
+};
+
+struct ColSliceParams {
+    ColSliceGroup g[kSplitBatch];
+    int ngroups;
+    int64_t ntiles;   // sum over the groups
 };
 
 template <int S, int NE>
-__global__ void k_slice_cols(ColSliceParams p)
+__global__ void k_slice_cols(const __grid_constant__ ColSliceParams pb)
 {
     const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t t = gt / 64;
+    const int64_t tg = gt / 64;
     const int slot = (int)(gt % 64);
-    if (t >= p.ntiles)
+    if (tg >= pb.ntiles)
         return;
+    int gi = 0;
+    while (gi + 1 < pb.ngroups && tg >= pb.g[gi + 1].t0) gi++;
+    const ColSliceGroup& p = pb.g[gi];
+    const int64_t t = tg - p.t0;
     const Tile tile = p.tiles[t];
     const bool valid = slot < tile.ne;
     const int64_t e = tile.e0 + slot;
@@ -356,7 +388,7 @@ constexpr size_t split_smem_bytes() { return sizeof(SplitSmem<NE>) + 1024; }
 // timeout the CTA records the failure, the roles stop, outstanding copies and
 // MMAs are waited for (bounded), the TMEM is freed and the CTA returns.
 template <int S, int L, int NE>
-__global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams p)
+__global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __grid_constant__ SplitParams p)
 {
     static_assert(S <= kSplitMaxS && L - 1 <= S && L >= 6 && L <= 8, "level layout");
     using Sh = SplitShape<NE>;
@@ -398,15 +430,20 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         uint32_t phase = 0;
         uint32_t used = 0, last_parity = 0;  // per-stage bit sets
         bool ok = true;
+        int gi = 0;
         for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
-            const int pt = (int)(w % p.ntp);
-            const int64_t u = w / p.ntp;
-            const Tile unit = split_unit<NE>(p.tiles, u);
+            gi = split_group_of(p, gi, w);
+            const SplitGroup& G = p.g[gi];
+            const int64_t v = w - G.w0;
+            const int pt = (int)(v % G.ntp);
+            const int64_t u = v / G.ntp;
+            const Tile unit = split_unit<NE>(G.tiles, u);
             if (unit.ne <= 0)
                 continue;
-            const int8_t* srcA = p.A + ((int64_t)unit.orient * p.ntp + pt) * p.nk * kABytes;
-            const int8_t* srcB = p.B + u * p.nk * kBBytes;
-            for (int ks = 0; ks < p.nk; ks++) {
+            const int8_t* srcA = G.A + ((int64_t)unit.orient * G.ntp + pt) * G.nk * kABytes;
+            const int8_t* srcB = G.B + u * G.nk * kBBytes;
+            const int nk = G.nk;
+            for (int ks = 0; ks < nk; ks++) {
                 if (!mbar_wait(&sm.empty[stage], phase ^ 1, failed)) {
                     ok = false;
                     break;
@@ -438,9 +475,13 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         uint32_t phase = 0;
         bool ok = true;
         int64_t i = 0;  // units processed by this CTA
+        int gi = 0;
         for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
-            if (split_unit<NE>(p.tiles, w / p.ntp).ne <= 0)
+            gi = split_group_of(p, gi, w);
+            const SplitGroup& G = p.g[gi];
+            if (split_unit<NE>(G.tiles, (w - G.w0) / G.ntp).ne <= 0)
                 continue;
+            const int nk = G.nk;
             const int buf = (int)(i % Sh::kBufs);
             const int64_t use = i / Sh::kBufs;
             if (use > 0 && !mbar_wait(&sm.tmem_empty[buf], (uint32_t)((use - 1) & 1), failed)) {
@@ -449,7 +490,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t dbase = tmem + (uint32_t)(buf * 256);
-            for (int ks = 0; ks < p.nk; ks++) {
+            for (int ks = 0; ks < nk; ks++) {
                 if (!mbar_wait(&sm.full[stage], phase, failed)) {
                     ok = false;
                     break;
@@ -498,10 +539,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
         const int c0 = ((warp - 2) >> 2) * 16;
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         int64_t i = 0;
+        int gi = 0;
         for (int64_t w = blockIdx.x; w < p.nwork && c0 < NE; w += gridDim.x) {
-            const int pt = (int)(w % p.ntp);
-            const int64_t u = w / p.ntp;
-            const Tile unit = split_unit<NE>(p.tiles, u);
+            gi = split_group_of(p, gi, w);
+            const SplitGroup& G = p.g[gi];
+            const int64_t v = w - G.w0;
+            const int pt = (int)(v % G.ntp);
+            const int64_t u = v / G.ntp;
+            const Tile unit = split_unit<NE>(G.tiles, u);
             if (unit.ne <= 0)
                 continue;
             const int buf = (int)(i % Sh::kBufs);
@@ -534,17 +579,18 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
             if (lane == 0)
                 mbar_arrive(&sm.tmem_empty[buf]);
             const int pe = pt * kSplitM + quarter * 32 + lane;
-            if (pe < p.nrows) {
-                const int rex = p.rowexp[(int64_t)unit.orient * p.Ppad + pe] - 35;
-                const int32_t* ce = p.colexp + u * NE + c0;
+            if (pe < G.nrows) {
+                const int rex = G.rowexp[(int64_t)unit.orient * G.Ppad + pe] - 35;
+                const int32_t* ce = G.colexp + u * NE + c0;
                 // Row pe is entry m.x and, for a symmetric group, also its
                 // mirror m.y (the same entry on the diagonal); with a
                 // transposed partner, entry (i, j) is also the partner's
                 // entry (j, i).
-                const int2 m = p.rowmap != nullptr ? p.rowmap[pe] : make_int2(pe, pe);
-                const int64_t ebase = (int64_t)(unit.e0 + c0) * p.P;
-                double* outp = p.out + ebase + m.x;
-                double* outm = p.out2 != nullptr ? p.out2 + ebase + m.y : m.y != m.x ? p.out + ebase + m.y : nullptr;
+                const int2 m = G.rowmap != nullptr ? G.rowmap[pe] : make_int2(pe, pe);
+                const int P = G.P;
+                const int64_t ebase = (int64_t)(unit.e0 + c0) * P;
+                double* outp = G.out + ebase + m.x;
+                double* outm = G.out2 != nullptr ? G.out2 + ebase + m.y : m.y != m.x ? G.out + ebase + m.y : nullptr;
                 const int nj = min(16, unit.ne - c0);
 #pragma unroll
                 for (int j = 0; j < 16; j += 4) {
@@ -559,9 +605,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(SplitParams
                         const double d = fma((double)Lo, 0x1p-21, (double)H[j + jj]);
                         if (j + jj < nj) {
                             const double v = scale2(d, rex + cx[jj]);
-                            outp[(int64_t)(j + jj) * p.P] = v;
+                            outp[(int64_t)(j + jj) * P] = v;
                             if (outm != nullptr)
-                                outm[(int64_t)(j + jj) * p.P] = v;
+                                outm[(int64_t)(j + jj) * P] = v;
                         }
                     }
                 }
