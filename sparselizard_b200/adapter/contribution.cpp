@@ -259,8 +259,6 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
         unsupported("dof interpolation on another region (on())");
     if (numfftcoeffs > 0)
         unsupported("FFT-based multiharmonic coefficients");
-    if (isbarycentereval)
-        unsupported("barycenter evaluation");
     if (mymeshdeformation.size() > 0)
         unsupported("integration on a deformed mesh");
     if (universe::isaxisymmetric)
@@ -298,7 +296,11 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
         const int elemtype = universe::getrawmesh()->getdisjointregions()->getelementtypenumber(mydisjregs[0]);
         const int tforder = tffield->getinterpolationorder(mydisjregs[0]);
         const int doforder = doffield != NULL ? doffield->getinterpolationorder(mydisjregs[0]) : tforder;
-        const int integrationorder = doforder + tforder + 2 + integrationorderdelta;
+        // Barycenter evaluation (contribution.cpp:77-78,175-176,199-200): order 0,
+        // neither weights nor det J applied.  On point elements (the nodal
+        // Dirichlet projection, rawfield.cpp:134-162) that is the plain point
+        // value: one point of weight 1, identity Jacobian.
+        const int integrationorder = isbarycentereval ? 0 : doforder + tforder + 2 + integrationorderdelta;
         if (integrationorder < 0) {
             logs log;
             log.msg() << "Error in 'contribution' object: trying to integrate at negative order " << integrationorder << std::endl;
@@ -306,12 +308,14 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
         }
         element elemobj(elemtype);
         const int elemdim = elemobj.getelementdimension();
-        if (elemdim != meshdim)
-            unsupported("integration over elements of lower dimension than the mesh");
+        if (isbarycentereval && elemdim != 0)
+            unsupported("barycenter evaluation on elements other than points");
 
         gausspoints gps(elemtype, integrationorder);
         std::vector<double> gpcoords = gps.getcoordinates();
         std::vector<double> weights = gps.getweights();
+        if (isbarycentereval)
+            std::fill(weights.begin(), weights.end(), 1.0);
         const int ngp = (int)weights.size();
 
         std::shared_ptr<hierarchicalformfunction> tfff = selector::select(elemtype, tffield->gettypename());

@@ -13,6 +13,7 @@
 #include <string>
 
 class rawmat;
+class expression;
 
 namespace slgpu_adapter {
 
@@ -47,6 +48,14 @@ void forget_matrix(rawmat* m);
 bool record_only(void);
 // Remembers the engine matrix handed to the last rawmat::process call.
 void set_last_processed(rawmat* m);
+
+// Integral of a scalar expression over a physical region at a Gauss order
+// (what expression::integrate computes, src/expression/expression.cpp:808-889)
+// on the GPU: the expression is lowered to a coefficient program, evaluated
+// at the Gauss points with its weights and |det J| per element, and summed.
+// Field values inside the expression are interpolated on the device
+// (rawfield::interpolate, src/field/rawfield.cpp:2632-2686).
+double integrate(expression e, int physreg, int integrationorder);
 
 }  // namespace slgpu_adapter
 

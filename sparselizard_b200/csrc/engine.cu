@@ -287,9 +287,9 @@ static void validate_group(const slgpu_group& g, bool with_dests = true)
 {
     if (g.nelem < 0 || g.ngp <= 0 || g.ntf <= 0 || g.ndof <= 0 || g.nterms <= 0 || (with_dests && g.ndests <= 0) || g.norient <= 0)
         fail(SLGPU_E_ARG, "group sizes must be positive");
-    if (g.elemdim != g.problemdim)
-        fail(SLGPU_E_UNSUPPORTED, "only elements of the mesh dimension are supported (element dim " +
-                                      std::to_string(g.elemdim) + ", mesh dim " + std::to_string(g.problemdim) + ")");
+    if (g.elemdim < 0 || g.elemdim > g.problemdim)
+        fail(SLGPU_E_ARG, "element dimension must be in [0, mesh dimension] (element dim " + std::to_string(g.elemdim) +
+                              ", mesh dim " + std::to_string(g.problemdim) + ")");
     if (g.problemdim < 1 || g.problemdim > 3)
         fail(SLGPU_E_ARG, "problem dimension must be 1..3");
     if (g.ncurvednodes <= 0 || g.ncurvednodes > 64)
@@ -729,6 +729,7 @@ static CoefParams coef_params(Ctx* ctx, const GroupDev& g, double* C)
     p.weights = g.weights.as<double>();
     p.lagrange = g.lagrange.as<double>();
     p.dim = g.problemdim;
+    p.edim = g.elemdim;
     p.prog = g.prog_d.as<Instr>();
     p.nprog = (int)g.prog.size();
     p.consts = g.consts.as<double>();
@@ -1904,7 +1905,9 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
             continue;
         }
         bool done = false;
-        if (!interp_only && !ctx->jit_broken) {
+        // The runtime-compiled kernel covers elements of the mesh dimension;
+        // lower-dimensional ones (boundary projections) use the interpreter.
+        if (!interp_only && !ctx->jit_broken && g0.elemdim == g0.problemdim) {
             try {
                 std::vector<const GroupDev*> batch;
                 for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
@@ -2991,7 +2994,8 @@ int slgpu_check_coefficient_kernels(slgpu_ctx* ctx, int handle, char* log, size_
             std::vector<const GroupDev*> batch;
             for (size_t j = k; j < k1; j++) batch.push_back(M.groups[j].get());
             try {
-                jit_compile(jit_coef_source(batch));
+                if (M.groups[k]->elemdim == M.groups[k]->problemdim)
+                    jit_compile(jit_coef_source(batch));
             } catch (const std::exception& e) {
                 fail(SLGPU_E_CUDA, e.what());
             }
@@ -3552,6 +3556,7 @@ extern "C" int slgpu_element_matrices_noalloc(const slgpu_group* g, const double
         cp.weights = (const double*)at(b_weights);
         cp.lagrange = (const double*)at(b_lag);
         cp.dim = g->problemdim;
+        cp.edim = g->elemdim;
         cp.prog = (const Instr*)at(b_prog);
         cp.nprog = (int)prog.size();
         cp.consts = (const double*)at(b_consts);

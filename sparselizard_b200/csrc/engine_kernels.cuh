@@ -48,8 +48,9 @@ struct CoefParams {
     int64_t nelem;
     int ngp;
     const double* weights;
-    const double* lagrange;  // [1+dim][ncn][ngp]
-    int dim;
+    const double* lagrange;  // [1+edim][ncn][ngp]
+    int dim;                 // mesh (problem) dimension
+    int edim;                // element dimension (<= dim)
     const Instr* prog;
     int nprog;
     const double* consts;
@@ -66,10 +67,57 @@ struct CoefParams {
     int64_t nnodes;    // > 0: node numbers outside [0, nnodes) are not read and give NaN coefficients
 };
 
-// Geometry (J, detJ, invJ; src/field/jacobian.cpp:248-349 and :396-504 for
-// elements of the mesh dimension) and the coefficient program at one
-// (element, Gauss point).  Thread n handles g = n / nelem, e = n % nelem so
-// that the C writes are coalesced over elements.
+// Rows edim .. dim-1 of the Jacobian of an element of lower dimension than
+// the mesh, completed as src/field/jacobian.cpp:19-235 does: points get the
+// identity; a line in 2D the normed perpendicular of its tangent; a surface
+// in 3D the normed cross product of its two rows; a line in 3D a normed
+// perpendicular (the larger of [-b a 0] and [0 -c b] for row [a b c]), then
+// the normed cross product.
+__device__ __forceinline__ void complete_jacobian(double (&J)[3][3], int edim, int dim)
+{
+    if (edim == 0) {
+        for (int a = 0; a < dim; a++)
+            for (int b = 0; b < dim; b++) J[a][b] = a == b ? 1.0 : 0.0;
+        return;
+    }
+    if (dim == 2 && edim == 1) {
+        J[1][0] = -J[0][1];
+        J[1][1] = J[0][0];
+        const double nv = sqrt(J[1][0] * J[1][0] + J[1][1] * J[1][1]);
+        J[1][0] = J[1][0] / nv;
+        J[1][1] = J[1][1] / nv;
+        return;
+    }
+    if (dim == 3 && edim == 1) {
+        if (sqrt(J[0][0] * J[0][0] + J[0][1] * J[0][1]) > sqrt(J[0][1] * J[0][1] + J[0][2] * J[0][2])) {
+            J[1][0] = -J[0][1];
+            J[1][1] = J[0][0];
+            J[1][2] = 0;
+        } else {
+            J[1][0] = 0;
+            J[1][1] = -J[0][2];
+            J[1][2] = J[0][1];
+        }
+        const double nv = sqrt(J[1][0] * J[1][0] + J[1][1] * J[1][1] + J[1][2] * J[1][2]);
+        J[1][0] = J[1][0] / nv;
+        J[1][1] = J[1][1] / nv;
+        J[1][2] = J[1][2] / nv;
+    }
+    if (dim == 3 && edim <= 2) {
+        J[2][0] = J[0][1] * J[1][2] - J[1][1] * J[0][2];
+        J[2][1] = J[0][2] * J[1][0] - J[1][2] * J[0][0];
+        J[2][2] = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+        const double nv = sqrt(J[2][0] * J[2][0] + J[2][1] * J[2][1] + J[2][2] * J[2][2]);
+        J[2][0] = J[2][0] / nv;
+        J[2][1] = J[2][1] / nv;
+        J[2][2] = J[2][2] / nv;
+    }
+}
+
+// Geometry (J, detJ, invJ; src/field/jacobian.cpp:4-349 and :396-504) and
+// the coefficient program at one (element, Gauss point).  Thread n handles
+// g = n / nelem, e = n % nelem so that the C writes are coalesced over
+// elements.
 __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
 {
     const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -96,13 +144,15 @@ __global__ void __launch_bounds__(128) k_geometry_coef(CoefParams p)
         X[0] += nv * x0;
         X[1] += nv * x1;
         X[2] += nv * x2;
-        for (int a = 0; a < dim; a++) {
+        for (int a = 0; a < p.edim; a++) {
             const double dn = p.lagrange[((int64_t)(1 + a) * p.ncn + k) * p.ngp + g];
             J[a][0] += dn * x0;
             if (dim > 1) J[a][1] += dn * x1;
             if (dim > 2) J[a][2] += dn * x2;
         }
     }
+    if (p.edim < dim)
+        complete_jacobian(J, p.edim, dim);
     double det, inv[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (dim == 1) {
         det = J[0][0];

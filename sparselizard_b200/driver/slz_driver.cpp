@@ -9,6 +9,9 @@
 // b) and the per-phase wall times are exposed through the extern "C" functions
 // at the end of the file for the Python harness.
 #include "sparselizard.h"
+#ifdef SLZ_GPU_BUILD
+#include "slgpu_adapter.h"
+#endif
 
 #include <chrono>
 #include <memory>
@@ -208,6 +211,38 @@ void eddy_tet(Problem& P, const char* msh, int order, const double* sigmas, doub
     P.fields = {a};
 }
 
+// Poisson on quads as workload 1, with the non-zero Dirichlet value
+// v = 1 + x*y + 2*x^2 on the boundary: b() then projects it onto the
+// boundary form functions (rawvec::updatedisjregconstraints,
+// src/formulation/rawvec.cpp:142-214).
+void poisson_quad_dirichlet(Problem& P, const char* msh, int order)
+{
+    P.m = mesh(msh, 0);
+    field v("h1"), x("x"), y("y");
+    v.setorder(VOL, order);
+    v.setconstraint(BOUNDARY, 1 + x * y + 2 * x * x);
+    P.f += integral(VOL, -grad(dof(v)) * grad(tf(v)), -2);
+    P.f += integral(VOL, 1 * tf(v), -2);
+    P.fields = {v};
+}
+
+// Elasticity on hexes as workload 2 with a prescribed displacement
+// u = (1e-3 x y, 0, 2e-3 x) on the z = 0 face (projected onto the face,
+// edge and node form functions of that face).
+void elasticity_hex_dirichlet(Problem& P, const char* msh, int order)
+{
+    P.m = mesh(msh, 0);
+    field u("h1xyz"), E("one"), x("x"), y("y");
+    u.setorder(VOL, order);
+    u.setconstraint(CLAMP, array3x1(1e-3 * x * y, 0, 2e-3 * x));
+    Normal rng(12345);
+    std::vector<double> evals(1 << 16);
+    for (double& e : evals) e = 150e9 * std::exp(0.3 * rng.draw());
+    set_per_element(E, VOL, evals);
+    P.f += integral(VOL, predefinedelasticity(dof(u), tf(u), E, 0.3));
+    P.fields = {u, E};
+}
+
 std::unique_ptr<Problem> build(int workload, const char* msh, const double* params)
 {
     auto P = std::make_unique<Problem>();
@@ -216,6 +251,8 @@ std::unique_ptr<Problem> build(int workload, const char* msh, const double* para
     case 2: elasticity_hex(*P, msh, (int)params[0], (int)params[1]); break;
     case 3: helmholtz_tet(*P, msh); break;
     case 4: eddy_tet(*P, msh, (int)params[0], params + 2, params[1]); break;
+    case 5: poisson_quad_dirichlet(*P, msh, (int)params[0]); break;
+    case 6: elasticity_hex_dirichlet(*P, msh, (int)params[0]); break;
     default: throw std::runtime_error("unknown workload");
     }
     return P;
@@ -228,7 +265,9 @@ extern "C" {
 // Workload ids: 1 Poisson quads (param0 = order), 2 elasticity hexes
 // (param0 = order, param1 = integration delta), 3 p-adaptive Helmholtz tets,
 // 4 harmonic eddy current tets (param0 = order, param1 = frequency,
-// param2..5 = sigma per material region).
+// param2..5 = sigma per material region), 5 Poisson quads with a non-zero
+// Dirichlet value (param0 = order), 6 elasticity hexes with a prescribed
+// face displacement (param0 = order).
 int slz_run(int workload, const char* msh, const double* params, int reps, double* times)
 {
     g_error.clear();
@@ -299,6 +338,34 @@ long long slz_eliminate(const double* x, double* out)
         g_error = e.what();
         return -1;
     }
+}
+
+// Field interpolation and integration: v (h1, order `order`) is set on the
+// quadrangle mesh by projection (rawfield::setvalue), then
+// e = v*v*x + 3*y - 2 is integrated over the volume at Gauss order 4.
+// out[0]: expression::integrate (sparselizard's own, on the host); in the
+// GPU drop-in build out[1]: the same integral through the GPU lowering
+// (slgpu_adapter::integrate), else out[1] = out[0].
+int slz_integrate(const char* msh, int order, double* out)
+{
+    g_error.clear();
+    try {
+        mesh m(msh, 0);
+        field v("h1"), x("x"), y("y");
+        v.setorder(VOL, order);
+        v.setvalue(VOL, 1 + x * y + 2 * x * x);
+        expression e = v * v * x + 3 * y - 2;
+        out[0] = e.integrate(VOL, 4);
+#ifdef SLZ_GPU_BUILD
+        out[1] = slgpu_adapter::integrate(e, VOL, 4);
+#else
+        out[1] = out[0];
+#endif
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+    return 0;
 }
 
 // Releases the last captured matrix and right-hand side.

@@ -7,6 +7,7 @@
 #include "cblas.h"
 
 #include <dlfcn.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -252,8 +253,103 @@ PetscErrorCode MatView(Mat mat, PetscViewer)
 }
 PetscErrorCode MatMatMult(Mat, Mat, MatReuse, PetscReal, Mat*) { unsupported("MatMatMult"); }
 PetscErrorCode MatMatSolve(Mat, Mat, Mat) { unsupported("MatMatSolve"); }
-PetscErrorCode MatPermute(Mat, IS, IS, Mat*) { unsupported("MatPermute"); }
-PetscErrorCode MatInvertVariableBlockDiagonal(Mat, PetscInt, const PetscInt*, PetscScalar*) { unsupported("MatInvertVariableBlockDiagonal"); }
+// B(i, j) = A(rperm[i], cperm[j]) (each new row i is old row rperm[i], old
+// column c becomes column cinv[c]); rows of B sorted by column.
+PetscErrorCode MatPermute(Mat A, IS rperm, IS cperm, Mat* out)
+{
+    if (A->dense)
+        unsupported("MatPermute(dense)");
+    if ((PetscInt)rperm->idx.size() != A->m || (PetscInt)cperm->idx.size() != A->n)
+        unsupported("MatPermute(permutation size)");
+    std::vector<int> cinv(A->n);
+    for (int j = 0; j < A->n; j++) cinv[cperm->idx[j]] = j;
+    Mat M = new slshim_Mat();
+    M->m = A->m;
+    M->n = A->n;
+    M->own_rows.assign(A->m + 1, 0);
+    for (int i = 0; i < A->m; i++) {
+        const int r = rperm->idx[i];
+        M->own_rows[i + 1] = M->own_rows[i] + (A->rows[r + 1] - A->rows[r]);
+    }
+    M->own_cols.resize(M->own_rows[A->m]);
+    M->own_vals.resize(M->own_rows[A->m]);
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < A->m; i++) {
+        const int r = rperm->idx[i];
+        row.clear();
+        for (int k = A->rows[r]; k < A->rows[r + 1]; k++) row.emplace_back(cinv[A->cols[k]], A->vals[k]);
+        std::sort(row.begin(), row.end(), [](const std::pair<int, double>& a, const std::pair<int, double>& b) { return a.first < b.first; });
+        for (size_t k = 0; k < row.size(); k++) {
+            M->own_cols[M->own_rows[i] + k] = row[k].first;
+            M->own_vals[M->own_rows[i] + k] = row[k].second;
+        }
+    }
+    M->rows = M->own_rows.data();
+    M->cols = M->own_cols.data();
+    M->vals = M->own_vals.data();
+    *out = M;
+    return 0;
+}
+
+// Inverses of the consecutive diagonal blocks of sizes bsizes[0..nb), each
+// stored column-major one after the other (the layout
+// densemat::blockdiagonaltimesvector reads, src/densemat.cpp:788-818).
+// Gauss-Jordan elimination with partial pivoting.
+PetscErrorCode MatInvertVariableBlockDiagonal(Mat A, PetscInt nb, const PetscInt* bsizes, PetscScalar* diag)
+{
+    if (A->dense)
+        unsupported("MatInvertVariableBlockDiagonal(dense)");
+    long long r0 = 0, off = 0;
+    std::vector<double> a, inv;
+    for (PetscInt b = 0; b < nb; b++) {
+        const int n = bsizes[b];
+        a.assign((size_t)n * n, 0.0);  // row-major block
+        for (int i = 0; i < n; i++) {
+            const long long r = r0 + i;
+            for (int k = A->rows[r]; k < A->rows[r + 1]; k++) {
+                const long long c = A->cols[k];
+                if (c >= r0 && c < r0 + n)
+                    a[(size_t)i * n + (c - r0)] = A->vals[k];
+            }
+        }
+        inv.assign((size_t)n * n, 0.0);
+        for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
+        for (int col = 0; col < n; col++) {
+            int piv = col;
+            for (int i = col + 1; i < n; i++)
+                if (std::fabs(a[(size_t)i * n + col]) > std::fabs(a[(size_t)piv * n + col]))
+                    piv = i;
+            if (a[(size_t)piv * n + col] == 0.0)
+                unsupported("MatInvertVariableBlockDiagonal(singular block)");
+            if (piv != col)
+                for (int k = 0; k < n; k++) {
+                    std::swap(a[(size_t)piv * n + k], a[(size_t)col * n + k]);
+                    std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]);
+                }
+            const double d = a[(size_t)col * n + col];
+            for (int k = 0; k < n; k++) {
+                a[(size_t)col * n + k] /= d;
+                inv[(size_t)col * n + k] /= d;
+            }
+            for (int i = 0; i < n; i++) {
+                if (i == col)
+                    continue;
+                const double f = a[(size_t)i * n + col];
+                if (f == 0.0)
+                    continue;
+                for (int k = 0; k < n; k++) {
+                    a[(size_t)i * n + k] -= f * a[(size_t)col * n + k];
+                    inv[(size_t)i * n + k] -= f * inv[(size_t)col * n + k];
+                }
+            }
+        }
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) diag[off + (size_t)j * n + i] = inv[(size_t)i * n + j];
+        off += (long long)n * n;
+        r0 += n;
+    }
+    return 0;
+}
 
 int slshim_mat_csr(Mat m, PetscInt* nrows, PetscInt* ncols, const PetscInt** rows, const PetscInt** cols, const PetscScalar** vals)
 {

@@ -10,6 +10,8 @@ Workload ids and parameters follow ``slz_run``:
   2 elasticity on hexes         params = [order, integration delta]
   3 p-adaptive Helmholtz on tets params = []
   4 eddy currents on tets       params = [order, frequency, sigma0..sigma3]
+  5 Poisson on quads, non-zero Dirichlet value on the boundary   params = [order]
+  6 elasticity on hexes, prescribed displacement of the z = 0 face params = [order]
 """
 from __future__ import annotations
 
@@ -19,7 +21,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-POISSON_QUAD, ELASTICITY_HEX, HELMHOLTZ_TET, EDDY_TET = 1, 2, 3, 4
+POISSON_QUAD, ELASTICITY_HEX, HELMHOLTZ_TET, EDDY_TET, POISSON_DIRICHLET, ELASTICITY_DIRICHLET = 1, 2, 3, 4, 5, 6
 
 
 @dataclass

@@ -53,6 +53,14 @@ def _child_main(mode, workload, msh, params, out, reps):
     elif mode.startswith("sweep"):
         np.savez(out, **sweep_inproc(msh, params, mode.split(":")[1]))
         return
+    elif mode in ("ref_integrate", "gpu_integrate"):
+        lib = W.load(REF_LIB if mode == "ref_integrate" else GPU_LIB)
+        out3 = (ctypes.c_double * 2)()
+        rc = lib.slz_integrate(msh.encode(), int(params[0]), out3)
+        if rc != 0:
+            raise RuntimeError(lib.slz_last_error().decode(errors="replace"))
+        np.savez(out, host=np.array(out3[0]), gpu=np.array(out3[1]))
+        return
     elif mode in ("ref_elim", "gpu_elim"):
         np.savez(out, **eliminate_inproc(mode, workload, msh, params))
         return
@@ -145,6 +153,13 @@ def eliminate_inproc(mode, workload, msh, params):
     st = lib.slgpu_matrix_eliminate(ctx, h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(ed.data_ptr()))
     assert st == abi.E_ARG, st
     return out
+
+
+def integrate(mode, msh, order):
+    """slz_integrate of the reference build (ref_integrate) or the GPU drop-in
+    (gpu_integrate): {"host": expression::integrate, "gpu": the GPU integral}."""
+    with tempfile.TemporaryDirectory() as d:
+        return _child(mode, 0, msh, [order], os.path.join(d, "o.npz"))
 
 
 def eliminate(mode, workload, msh, params):

@@ -100,6 +100,40 @@ def test_dropin_poisson_full_size(ref_lib, gpu_lib, tmp):
     assert ref["Acols"].size == 582169 and ref["Dcols"].size == 3056
 
 
+@pytest.mark.parametrize("workload,kind,n,params", [(W.POISSON_DIRICHLET, "quad", 24, [1]), (W.POISSON_DIRICHLET, "quad", 24, [2]),
+                                                     (W.POISSON_DIRICHLET, "quad", 16, [3]), (W.ELASTICITY_DIRICHLET, "hex", 5, [2])])
+def test_dropin_nonzero_dirichlet(ref_lib, gpu_lib, tmp, workload, kind, n, params):
+    """Non-zero Dirichlet values: b() projects the constraint expression onto
+    the constrained form functions by secondary assemblies (barycenter values
+    on the nodes, then projections on the boundary edges / faces: elements of
+    lower dimension than the mesh), all through the drop-in on the GPU.  The
+    matrix, b and the constrained entries of b must match the reference."""
+    msh = str(tmp / f"dir_{kind}_{n}_{params[0]}.msh")
+    meshgen.workload_mesh(kind, n, msh)
+    ref = P.reference(workload, msh, params)
+    got = P.gpu(workload, msh, params)
+    P.check_pattern(ref, got)
+    assert np.array_equal(ref["Ainds"], got["Ainds"]) and np.array_equal(ref["Dinds"], got["Dinds"])
+    P.check_values(ref, got, TOL)
+    bd = ref["b"][ref["Dinds"]]
+    assert np.abs(bd).max() > 0, "the constraint values must be non-zero"
+    P.check_rhs(ref, got["b"], TOL)
+
+
+@pytest.mark.parametrize("order", [1, 3])
+def test_gpu_integrate_matches_expression_integrate(ref_lib, gpu_lib, tmp, order):
+    """Field interpolation and integration on the GPU: a field set by
+    projection, then the integral of an expression of it and of the
+    coordinates, against sparselizard's own expression::integrate."""
+    msh = str(tmp / f"int_{order}.msh")
+    meshgen.workload_mesh("quad", 32, msh)
+    ref = P.integrate("ref_integrate", msh, order)
+    got = P.integrate("gpu_integrate", msh, order)
+    r = float(ref["host"])
+    assert abs(float(got["gpu"]) - r) <= TOL * abs(r)
+    assert abs(float(got["host"]) - r) <= TOL * abs(r)
+
+
 @pytest.mark.parametrize("workload,kind,n,params", [(W.POISSON_QUAD, "quad", 64, [2]), (W.ELASTICITY_HEX, "hex", 6, [2, -2])])
 def test_device_csr_and_eliminate(ref_lib, gpu_lib, tmp, workload, kind, n, params):
     """Device-resident handoff: slgpu_matrix_device_csr returns the same CSR
