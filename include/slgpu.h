@@ -356,7 +356,13 @@ int slgpu_record_mesh(const slgpu_ctx* ctx, int mesh, int elemtype, int64_t* nno
  */
 typedef struct slgpu_server slgpu_server;
 
-enum { SLGPU_UPDATE_ELEMDATA = 0, SLGPU_UPDATE_FIELDDATA = 1 };
+/* SLGPU_UPDATE_SCALES: new term scales and destination multipliers of group
+ * `group` for this request only (a frequency of a harmonic problem, as
+ * slgpu_matrix_set_scales sets them on the template): values = [nterms] term
+ * scales then [ndests] multipliers, rows = nterms + ndests, count = 1,
+ * index unused.  On a group whose element matrices are contracted as
+ * symmetric, mirror terms must keep equal scales (else SLGPU_E_ARG). */
+enum { SLGPU_UPDATE_ELEMDATA = 0, SLGPU_UPDATE_FIELDDATA = 1, SLGPU_UPDATE_SCALES = 2 };
 
 typedef struct {
     int32_t group; /* group index in the template */
@@ -397,6 +403,15 @@ int slgpu_server_submit(slgpu_server* s, const slgpu_request* r, int64_t* ticket
 /* Waits up to timeout_s (< 0: no limit) for a request.  Returns SLGPU_OK when
  * it completed, SLGPU_E_TIMEOUT when still running, or the request's own
  * error code (message via slgpu_server_error).  stats may be NULL. */
+/* Queues a new template: a matrix whose groups and fragments were added but
+ * that was never processed (a new mesh, new orders, a new formulation).
+ * When admitted -- in arrival order, against the HBM budget like any request
+ * -- the server runs its first slgpu_matrix_process (pattern build and
+ * values) with these constraint flags (ndofs bytes, copied at submit; NULL:
+ * none constrained).  Once its ticket is done, requests may use the handle
+ * as a template.  The pattern build synchronises the context's main stream;
+ * requests already running on the slots continue meanwhile. */
+int slgpu_server_submit_template(slgpu_server* s, int handle, const uint8_t* isconstrained, int precision, int64_t* ticket);
 int slgpu_server_wait(slgpu_server* s, int64_t ticket, double timeout_s, slgpu_request_stats* stats);
 int slgpu_server_error(slgpu_server* s, int64_t ticket, char* buf, size_t len);
 /* Forgets a completed request. */

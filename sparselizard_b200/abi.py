@@ -68,7 +68,7 @@ class Work(ctypes.Structure):
                 ("nnz", c_int64), ("nA", c_int64), ("ngroups", c_int32), ("pad", c_int32)]
 
 
-UPDATE_ELEMDATA, UPDATE_FIELDDATA = 0, 1
+UPDATE_ELEMDATA, UPDATE_FIELDDATA, UPDATE_SCALES = 0, 1, 2
 
 
 class GroupDesc(ctypes.Structure):
@@ -145,6 +145,7 @@ SIGNATURES = {
     "slgpu_server_create": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     "slgpu_server_prepare": (c_int, [c_void_p, c_int, c_int]),
     "slgpu_server_submit": (c_int, [c_void_p, POINTER(Request), POINTER(c_int64)]),
+    "slgpu_server_submit_template": (c_int, [c_void_p, c_int, POINTER(c_uint8), c_int, POINTER(c_int64)]),
     "slgpu_server_wait": (c_int, [c_void_p, c_int64, c_double, POINTER(RequestStats)]),
     "slgpu_server_error": (c_int, [c_void_p, c_int64, c_char_p, c_size_t]),
     "slgpu_server_release": (c_int, [c_void_p, c_int64]),

@@ -1334,6 +1334,8 @@ static bool symmetric_form(const GroupDev& g)
     return true;
 }
 
+bool group_symmetric(const GroupDev& g) { return symmetric_form(g); }
+
 // Rows of A for the mirrored forms (the upper triangle of a symmetric group,
 // or every entry of a group with a transposed partner), each with the entry
 // it is and the entry its value also goes to: (j, i) of the same matrix, or
@@ -1663,6 +1665,16 @@ static bool uses_split(const GroupDev& g, int precision)
     return precision != SLGPU_PREC_FP64 && !g.rhs && (int64_t)g.ntf * g.ndof >= 64 && split_supported(g);
 }
 
+// Shared memory of k_contract_small for a group (M of every orientation and
+// the block's staged outputs), and whether its FP64 contraction uses it:
+// element matrices of at most 32 entries whose tables fit.
+static size_t small_kernel_smem(const GroupDev& g)
+{
+    const int64_t P = (int64_t)g.ntf * g.ndof;
+    return ((size_t)g.norient * g.nterms * g.ngp * P + (size_t)kSmallE * (P + 1)) * 8;
+}
+static bool uses_small_kernel(const GroupDev& g) { return (int64_t)g.ntf * g.ndof <= kSmallP && small_kernel_smem(g) <= kSmallSmem; }
+
 // Whether an FP64 contraction of a group may use the mirrored forms (upper
 // triangle of a symmetric group, transposed pairs): matrix groups with at
 // least 64 entries, as for split precision.
@@ -1817,7 +1829,7 @@ static std::vector<int> cross_pairs(const Matrix& M, int precision, const std::v
         const GroupDev& g = *M.groups[i];
         if (g.nelem == 0 || !mirror_eligible(g, precision) || symmetric_form(g) || g.term_keys.empty())
             return false;
-        return ov == nullptr || ((*ov)[i].elemdata == nullptr && (*ov)[i].fielddata == nullptr);
+        return ov == nullptr || ((*ov)[i].elemdata == nullptr && (*ov)[i].fielddata == nullptr && (*ov)[i].term_scale == nullptr);
     };
     std::vector<char> used;
     for (size_t i = 0; i < n; i++) {
@@ -1928,7 +1940,8 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                     GroupDev& G = *M.groups[j];
                     const double* ed = ov != nullptr && (*ov)[j].elemdata != nullptr ? (*ov)[j].elemdata : G.elemdata.as<double>();
                     const double* fd = ov != nullptr && (*ov)[j].fielddata != nullptr ? (*ov)[j].fielddata : G.fielddata.as<double>();
-                    jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, G.term_scale_d.as<double>(), skip(j) ? nullptr : C + coff[j],
+                    const double* ts = ov != nullptr && (*ov)[j].term_scale != nullptr ? (*ov)[j].term_scale : G.term_scale_d.as<double>();
+                    jg.push_back(JitGroup{G.tables.as<double>(), ed, fd, ts, skip(j) ? nullptr : C + coff[j],
                                           eoff[j] >= 0 && !skip(j) ? elemexp + eoff[j] : nullptr});
                 }
                 const MeshDev& m = ctx->meshes.at(g0.mesh);
@@ -1964,6 +1977,8 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
                     cp.elemdata = (*ov)[j].elemdata;
                 if (ov != nullptr && (*ov)[j].fielddata != nullptr)
                     cp.fielddata = (*ov)[j].fielddata;
+                if (ov != nullptr && (*ov)[j].term_scale != nullptr)
+                    cp.term_scale = (*ov)[j].term_scale;
                 const int64_t n = G.nelem * (int64_t)G.ngp;
                 const int kt = kstat_start(ctx, "coefficients", 8.0 * G.nterms * G.ngp * G.nelem);
                 k_geometry_coef<<<grid_for(n, 128), 128, 0, ctx->x->stream>>>(cp);
@@ -2044,8 +2059,8 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
                 continue;
             }
             const int64_t P = (int64_t)g->ntf * g->ndof;
-            const size_t small_smem = ((size_t)g->norient * g->nterms * g->ngp * P + (size_t)kSmallE * (P + 1)) * 8;
-            if (P <= kSmallP && small_smem <= kSmallSmem) {
+            const size_t small_smem = small_kernel_smem(*g);
+            if (uses_small_kernel(*g)) {
                 ContractParams kp{};
                 kp.tables = g->tables.as<double>();
                 kp.tab_off = g->tab_off_d.as<int64_t>();
@@ -2304,8 +2319,21 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
 // execution state so that the value path itself allocates none of it.
 void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
 {
-    if (precision == SLGPU_PREC_FP64)
+    if (precision == SLGPU_PREC_FP64) {
+        // The FP64 tensor-core operands of every tiled group, in the forms a
+        // step can use (the plain or symmetric form; the paired form for the
+        // first group of a transposed pair).
+        const std::vector<int> pair = cross_pairs(M, precision, nullptr);
+        for (size_t gi = 0; gi < M.groups.size(); gi++) {
+            GroupDev* g = M.groups[gi].get();
+            if (g->nelem == 0 || uses_small_kernel(*g))
+                continue;
+            ensure_fmt(ctx, *g, (fp64_mirrored(*g) && symmetric_form(*g)) ? 1 : 0);
+            if (pair[gi] > (int)gi)
+                ensure_fmt(ctx, *g, 2);
+        }
         return;
+    }
     const int tier = precision == SLGPU_PREC_SPLIT ? 0 : 1;
     size_t colbytes = 0, expbytes = 0;
     // Both the unpaired form (assemblies with replaced data) and, for the

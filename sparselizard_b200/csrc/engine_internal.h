@@ -319,7 +319,12 @@ struct Ctx {
 struct GroupData {
     const double* elemdata = nullptr;
     const double* fielddata = nullptr;
+    const double* term_scale = nullptr;  // device [nterms], replaces the group's term scales
 };
+
+// Whether a group's contraction takes the symmetric form (mirror terms with
+// equal scales; engine.cu).
+bool group_symmetric(const GroupDev& g);
 
 // Launch pieces of one assembly (engine.cu), issued on ctx->x's stream.
 std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals);

@@ -59,6 +59,13 @@ struct Request {
         int64_t offset, n;
     };
     std::vector<DirectIn> direct_in;
+    // Template requests (slgpu_server_submit_template): process the matrix
+    // once (pattern build and first values) with these constraint flags.
+    bool is_template = false;
+    std::vector<uint8_t> constr;
+    // SLGPU_UPDATE_SCALES: group and its term scales then multipliers.
+    std::vector<std::pair<int, std::vector<double>>> scales;
+    std::vector<DevBuf> ts;  // device term scales while running
     double* Aout = nullptr;
     double* Dout = nullptr;
     bool pinned_out = false;
@@ -117,8 +124,10 @@ int64_t estimate_bytes(const Matrix& M, int precision, const Request* r)
         vals += (int64_t)g->ntf * g->ndof * g->nelem;
         coef += (int64_t)g->nterms * g->ngp * g->nelem;
         exps += g->nelem;
+        // The split groups of a request are sliced and contracted together:
+        // their column slices coexist.
         const int64_t Qpad = ((int64_t)g->nterms * g->ngp + 31) / 32 * 32;
-        split = std::max<int64_t>(split, 7 * Qpad * (int64_t)g->tiles.size() * 64 + (int64_t)g->tiles.size() * 256);
+        split += 7 * Qpad * (int64_t)g->tiles.size() * 64 + (int64_t)g->tiles.size() * 256 + 512;
     }
     for (auto& f : M.frags) vals += (int64_t)f->nr * f->nc;
     int64_t upd = 0, over = 0;
@@ -221,6 +230,13 @@ void launch(Server& S, Slot& s, Request& r)
             (elem ? ov[u.group].elemdata : ov[u.group].fielddata) = dst.as<double>();
         }
     }
+    r.ts.clear();
+    r.ts.resize(r.scales.size());
+    for (size_t k = 0; k < r.scales.size(); k++) {
+        const int gi = r.scales[k].first;
+        upload_staged(ctx, r.ts[k], r.scales[k].second.data(), (size_t)M.groups[gi]->nterms * 8);
+        ov[gi].term_scale = r.ts[k].as<double>();
+    }
     const double t1 = S.now();
     htrace_mark(ctx, "request: inputs");
     std::vector<int64_t> gvb;
@@ -232,7 +248,17 @@ void launch(Server& S, Slot& s, Request& r)
     const double t2 = S.now();
     r.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
     r.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
-    const std::vector<RowSeg> rsegs = row_segments(M, segs);
+    std::vector<RowSeg> rsegs = row_segments(M, segs);
+    // Destination multipliers of the request's scale updates (segments are
+    // the groups' destinations in order).
+    if (!r.scales.empty()) {
+        std::vector<size_t> sbase(M.groups.size() + 1, 0);
+        for (size_t gi = 0; gi < M.groups.size(); gi++) sbase[gi + 1] = sbase[gi] + M.groups[gi]->ndests;
+        for (const auto& sc : r.scales) {
+            const GroupDev& g = *M.groups[sc.first];
+            for (int d = 0; d < g.ndests; d++) rsegs[sbase[sc.first] + d].mult = sc.second[g.nterms + d];
+        }
+    }
     DevBuf dsegs;
     upload_staged(ctx, dsegs, rsegs.data(), rsegs.size() * sizeof(RowSeg));
     launch_row_values(ctx, M, P, rsegs, dsegs.as<RowSeg>(), false, r.vals.as<double>(), r.Avals.as<double>(), r.Dvals.as<double>());
@@ -291,6 +317,7 @@ void finish(Server& S, Slot& s)
     r.upd.release();
     r.ed.clear();
     r.fd.clear();
+    r.ts.clear();
     r.tmpl.reset();
     ctx->x = &ctx->main;
     std::lock_guard<std::mutex> lk(S.mu);
@@ -352,6 +379,24 @@ void server_loop(Server& S)
                 r->t_start = S.now();
                 r->status = -2;
                 r->slot = (int)(free_slot - S.slots.data());
+            }
+            if (r->is_template) {
+                // A new template: its pattern build synchronises the main
+                // stream (the slots' streams keep running); it completes here.
+                const double tl = S.now();
+                slgpu_csr_info info{};
+                const int code = slgpu_matrix_process(reinterpret_cast<slgpu_ctx*>(ctx), r->handle, r->constr.data(), r->precision, &info);
+                std::lock_guard<std::mutex> lk(S.mu);
+                r->launch_ms = (S.now() - tl) * 1e3;
+                r->status = code;
+                if (code != SLGPU_OK)
+                    r->error = ctx->last_error;
+                r->t_done = S.now();
+                r->slot = -1;
+                S.running--;
+                S.done_cv.notify_all();
+                progress = true;
+                continue;
             }
             free_slot->req = r;
             int code = SLGPU_OK;
@@ -493,6 +538,21 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
                 return SLGPU_E_ARG;
             }
             const GroupDev& g = *M.groups[u.group];
+            if (u.kind == SLGPU_UPDATE_SCALES) {
+                if (u.rows != g.nterms + g.ndests || u.count != 1 || u.values == nullptr) {
+                    ctx->last_error = "update: scales need rows = nterms + ndests, count = 1";
+                    return SLGPU_E_ARG;
+                }
+                std::vector<double> v(u.values, u.values + u.rows);
+                if (group_symmetric(g))
+                    for (int t = 0; t < g.nterms; t++)
+                        if (std::memcmp(&v[t], &v[g.mirror[t]], sizeof(double)) != 0) {
+                            ctx->last_error = "update: the scales break the symmetry of a symmetric group (mirror terms differ)";
+                            return SLGPU_E_ARG;
+                        }
+                r->scales.emplace_back(u.group, std::move(v));
+                continue;
+            }
             const bool elem = u.kind == SLGPU_UPDATE_ELEMDATA;
             if (!elem && u.kind != SLGPU_UPDATE_FIELDDATA) {
                 ctx->last_error = "update: unknown kind";
@@ -577,16 +637,59 @@ int slgpu_server_submit(slgpu_server* S, const slgpu_request* rq, int64_t* ticke
             S->pin_all.push_back(p);
         }
         r->in_cap = cap;
-        std::map<int64_t, const double*> src;
-        for (int i = 0; i < rq->nupdates; i++) src[r->updates[i].offset] = rq->updates[i].values;
-        for (auto& kv : src) {
-            const Request::Update* u = nullptr;
-            for (auto& x : r->updates)
-                if (x.offset == kv.first) {
-                    u = &x;
-                    break;
-                }
-            std::memcpy(r->in + kv.first, kv.second, (size_t)u->rows * u->count * 8);
+        // Every distinct data array once, at its offset ((values, doubles) -> offset).
+        for (const auto& kv : seen_arrays) std::memcpy(r->in + kv.second, kv.first.first, (size_t)kv.first.second * 8);
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->ticket = S->next_ticket++;
+    r->t_submit = S->now();
+    S->reqs[r->ticket] = r;
+    S->queue.push_back(r);
+    S->running++;
+    *ticket = r->ticket;
+    S->wake.notify_one();
+    return SLGPU_OK;
+}
+
+int slgpu_server_submit_template(slgpu_server* S, int handle, const uint8_t* isconstrained, int precision, int64_t* ticket)
+{
+    if (S == nullptr || ticket == nullptr)
+        return SLGPU_E_ARG;
+    Ctx* ctx = S->ctx;
+    auto r = std::make_shared<Request>();
+    {
+        std::lock_guard<std::recursive_mutex> cl(ctx->mu);
+        auto it = ctx->matrices.find(handle);
+        if (it == ctx->matrices.end()) {
+            ctx->last_error = "unknown matrix handle " + std::to_string(handle);
+            return SLGPU_E_ARG;
+        }
+        const Matrix& M = *it->second;
+        if (precision != SLGPU_PREC_FP64 && precision != SLGPU_PREC_SPLIT && precision != SLGPU_PREC_FP32) {
+            ctx->last_error = "unknown precision mode";
+            return SLGPU_E_ARG;
+        }
+        r->is_template = true;
+        r->handle = handle;
+        r->precision = precision;
+        r->constr.assign((size_t)M.ndofs + 1, 0);
+        if (isconstrained != nullptr)
+            std::memcpy(r->constr.data(), isconstrained, (size_t)M.ndofs);
+        // The pattern build's device memory: sort keys and indices, runs,
+        // slot map and incidences of every COO entry, values and CSR arrays.
+        int64_t ncoo = 0, nvals = 0;
+        for (auto& g : M.groups) {
+            ncoo += (int64_t)g->ntf * g->ndof * g->nelem * g->ndests;
+            nvals += (int64_t)g->ntf * g->ndof * g->nelem;
+        }
+        for (auto& f : M.frags) {
+            ncoo += (int64_t)f->nr * f->nc;
+            nvals += (int64_t)f->nr * f->nc;
+        }
+        r->est_bytes = 40 * ncoo + 24 * nvals + 16 * M.ndofs + (int64_t(1) << 20);
+        if (r->est_bytes > (int64_t)ctx->budget) {
+            ctx->last_error = "the template's first assembly needs more device memory than the whole HBM budget";
+            return SLGPU_E_BUDGET;
         }
     }
     std::lock_guard<std::mutex> lk(S->mu);

@@ -20,9 +20,10 @@ class UpdateSpec:
     """New per-element data for one array of one group, in mesh element order."""
 
     group: int
-    kind: int          # abi.UPDATE_ELEMDATA or abi.UPDATE_FIELDDATA
+    kind: int          # abi.UPDATE_ELEMDATA, abi.UPDATE_FIELDDATA or abi.UPDATE_SCALES
     index: int
-    values: np.ndarray  # [rows][count] float64, count = mesh elements of the group's type
+    values: np.ndarray  # [rows][count] float64, count = mesh elements of the group's type;
+                        # scales: [nterms + ndests] term scales then destination multipliers
 
 
 class PinnedArray:
@@ -55,6 +56,19 @@ class Server:
         self.h = h
         self._keep = {}
 
+    def submit_template(self, handle: int, constrained, precision: int) -> int:
+        """Queues the first process() of an unprocessed matrix (pattern build)."""
+        c = np.ascontiguousarray(constrained, dtype=np.uint8) if constrained is not None else None
+        self._keep_c = c
+        t = ctypes.c_int64()
+        ptr = c.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if c is not None else None
+        st = self.lib.slgpu_server_submit_template(self.h, handle, ptr, precision, ctypes.byref(t))
+        if st != abi.OK:
+            buf = ctypes.create_string_buffer(2048)
+            self.lib.slgpu_last_error(self.ctx, buf, 2048)
+            raise abi.SlgpuError(st, buf.value.decode(errors="replace"))
+        return t.value
+
     def submit(self, handle: int, precision: int, updates, A_out, D_out) -> int:
         """A_out / D_out: float64 arrays (numpy or PinnedArray.array) of nnzA / nnzD values."""
         ups = (abi.Update * max(1, len(updates)))()
@@ -62,7 +76,7 @@ class Server:
         for i, u in enumerate(updates):
             v = np.ascontiguousarray(u.values, dtype=np.float64)
             if v.ndim == 1:
-                v = v[None, :]
+                v = v[:, None] if u.kind == abi.UPDATE_SCALES else v[None, :]
             vals.append(v)
             ups[i].group, ups[i].kind, ups[i].index = u.group, u.kind, u.index
             ups[i].rows, ups[i].count = v.shape[0], v.shape[1]

@@ -176,3 +176,113 @@ def test_prepare_and_page_locked_inputs(ctx):
         srv.close()
         for p in pins:
             p.close()
+
+
+def test_served_frequency_requests(ctx):
+    """Requests that carry new term scales and destination multipliers (a
+    frequency of a harmonic problem) next to requests with new coefficients,
+    in one mix: each result equals the template re-assembled with the same
+    scales through slgpu_matrix_set_scales + process(), bit for bit, and the
+    template's own scales are left unchanged."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    t = _template(ctx, rng, 5, 50, 9, 9, 4, 3, 2500)
+    g = t["gb"].g
+    L = ctx.lib
+    ts0, dm0 = np.zeros(g.nterms), np.zeros(g.ndests)
+    ctx.check(L.slgpu_matrix_get_scales(ctx.h, t["handle"], 0, abi.f64p(ts0), abi.f64p(dm0)))
+    reqs = []
+    for k in range(8):
+        prec = [abi.PREC_FP64, abi.PREC_SPLIT][k % 2]
+        w = 2 * np.pi * 10.0 ** (k - 2)
+        scales = np.concatenate([ts0 * (1.0 + 0.5 * w * (np.arange(g.nterms) % 2)), dm0 * (1.0 + 1e-3 * w)])
+        reqs.append((prec, scales))
+    srv = serving.Server(ctx.lib, ctx.h, 4)
+    outs, tickets = [], []
+    try:
+        for prec, scales in reqs:
+            A = np.full(t["nnzA"], np.nan)
+            D = np.full(max(1, t["nnzD"]), np.nan)[: t["nnzD"]]
+            tickets.append(srv.submit(t["handle"], prec, [serving.UpdateSpec(0, abi.UPDATE_SCALES, 0, scales)], A, D))
+            outs.append((A, D))
+            vals = rng.lognormal(0.0, 0.4, t["nmesh"])  # a coefficient request in between
+            A2, D2 = np.zeros(t["nnzA"]), np.zeros(max(1, t["nnzD"]))[: t["nnzD"]]
+            tickets.append(srv.submit(t["handle"], prec, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vals)], A2, D2))
+        for tk in tickets:
+            assert srv.wait(tk).status == abi.OK
+        with pytest.raises(abi.SlgpuError):  # wrong length
+            srv.submit(t["handle"], abi.PREC_FP64, [serving.UpdateSpec(0, abi.UPDATE_SCALES, 0, np.ones(3))], A, D)
+    finally:
+        srv.close()
+    ts1, dm1 = np.zeros(g.nterms), np.zeros(g.ndests)
+    ctx.check(L.slgpu_matrix_get_scales(ctx.h, t["handle"], 0, abi.f64p(ts1), abi.f64p(dm1)))
+    assert np.array_equal(ts0, ts1) and np.array_equal(dm0, dm1), "a request changed the template's scales"
+    # The template's element data as the plain path sees it: restore what
+    # _template set (the coefficient requests never touch it).
+    for (prec, scales), (A, D) in zip(reqs, outs):
+        ctx.check(L.slgpu_matrix_set_scales(ctx.h, t["handle"], 0, abi.f64p(np.ascontiguousarray(scales[: g.nterms])),
+                                            abi.f64p(np.ascontiguousarray(scales[g.nterms:]))))
+        info = abi.CsrInfo()
+        ctx.check(L.slgpu_matrix_process(ctx.h, t["handle"], t["con"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), prec,
+                                         ctypes.byref(info)))
+        pA, pD = np.zeros(max(1, t["nnzA"])), np.zeros(max(1, t["nnzD"]))
+        ctx.check(L.slgpu_matrix_download_values(ctx.h, t["handle"], abi.f64p(pA), abi.f64p(pD)))
+        assert np.array_equal(A, pA[: t["nnzA"]]) and np.array_equal(D, pD[: t["nnzD"]]), "served != set_scales + process()"
+    ctx.check(L.slgpu_matrix_set_scales(ctx.h, t["handle"], 0, abi.f64p(ts0), abi.f64p(dm0)))
+
+
+def test_server_admits_new_templates(ctx):
+    """A new template (groups added, never processed: a new mesh or order)
+    goes through the request queue: its first assembly runs when admitted,
+    while coefficient requests on another template are in flight, and the
+    new template then serves requests.  Its values equal a direct process()
+    of an identical matrix."""
+    rng = np.random.Generator(np.random.PCG64(23))
+    old = _template(ctx, rng, 6, 40, 9, 9, 3, 3, 1500)
+    gb, xyz, conn = S.group(rng, nelem_grid=30, ntf=8, ndof=8, nterms=3, ngp1=3, norient=2, ndests=2, ndofs=1200)
+    g = gb.g
+    g.mesh = 7
+    L = ctx.lib
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, 7, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, 7, 3, 4, conn.size // 4, abi.i32p(conn)))
+    hs = []
+    for _ in range(2):
+        h = ctypes.c_int()
+        ctx.check(L.slgpu_matrix_create(ctx.h, 1200, ctypes.byref(h)))
+        ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g), None))
+        hs.append(h.value)
+    con = (rng.random(1200) < 0.1).astype(np.uint8)
+    srv = serving.Server(ctx.lib, ctx.h, 3)
+    try:
+        tk = []
+        for k in range(4):
+            vals = rng.lognormal(0.0, 0.4, old["nmesh"])
+            A, D = np.zeros(old["nnzA"]), np.zeros(max(1, old["nnzD"]))[: old["nnzD"]]
+            tk.append(srv.submit(old["handle"], abi.PREC_SPLIT, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vals)], A, D))
+            if k == 1:
+                tt = srv.submit_template(hs[0], con, abi.PREC_FP64)
+        assert srv.wait(tt).status == abi.OK
+        for t in tk:
+            assert srv.wait(t).status == abi.OK
+        ref = _direct(ctx, hs[1], con)
+        nnzA, nnzD = ref[0].size, ref[1].size
+        A, D = np.full(nnzA, np.nan), np.full(max(1, nnzD), np.nan)[:nnzD]
+        vals = np.ones(conn.size // 4)
+        elems = np.ctypeslib.as_array(g.elems, (g.nelem,))
+        vals[elems] = np.ctypeslib.as_array(g.elemdata[0], (g.nelem,))
+        t2 = srv.submit(hs[0], abi.PREC_FP64, [serving.UpdateSpec(0, abi.UPDATE_ELEMDATA, 0, vals)], A, D)
+        assert srv.wait(t2).status == abi.OK
+        assert np.array_equal(A, ref[0]) and np.array_equal(D, ref[1])
+    finally:
+        srv.close()
+    A0, D0 = np.zeros(max(1, nnzA)), np.zeros(max(1, nnzD))
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, hs[0], abi.f64p(A0), abi.f64p(D0)))
+    assert np.array_equal(A0[:nnzA], ref[0]) and np.array_equal(D0[:nnzD], ref[1])
+
+
+def _direct(ctx, h, con):
+    L = ctx.lib
+    info = abi.CsrInfo()
+    ctx.check(L.slgpu_matrix_process(ctx.h, h, con.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), abi.PREC_FP64, ctypes.byref(info)))
+    A, D = np.zeros(max(1, info.nnzA)), np.zeros(max(1, info.nnzD))
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, h, abi.f64p(A), abi.f64p(D)))
+    return A[: info.nnzA], D[: info.nnzD]
