@@ -243,6 +243,23 @@ void elasticity_hex_dirichlet(Problem& P, const char* msh, int order)
     P.fields = {u, E};
 }
 
+// Per-element values for workload 7 (slz_set_element_values).
+std::vector<double> g_element_values;
+
+// Poisson on quads with a per-element coefficient field k (a "one" field set
+// from g_element_values): integral(VOL, -k*grad(dof(v))*grad(tf(v))), v = 0
+// on the boundary -- the formulation of the serving pool's Poisson templates.
+void poisson_quad_kfield(Problem& P, const char* msh, int order)
+{
+    P.m = mesh(msh, 0);
+    field v("h1"), k("one");
+    v.setorder(VOL, order);
+    v.setconstraint(BOUNDARY);
+    set_per_element(k, VOL, g_element_values.empty() ? std::vector<double>{1.0} : g_element_values);
+    P.f += integral(VOL, -k * grad(dof(v)) * grad(tf(v)));
+    P.fields = {v, k};
+}
+
 std::unique_ptr<Problem> build(int workload, const char* msh, const double* params)
 {
     auto P = std::make_unique<Problem>();
@@ -253,6 +270,7 @@ std::unique_ptr<Problem> build(int workload, const char* msh, const double* para
     case 4: eddy_tet(*P, msh, (int)params[0], params + 2, params[1]); break;
     case 5: poisson_quad_dirichlet(*P, msh, (int)params[0]); break;
     case 6: elasticity_hex_dirichlet(*P, msh, (int)params[0]); break;
+    case 7: poisson_quad_kfield(*P, msh, (int)params[0]); break;
     default: throw std::runtime_error("unknown workload");
     }
     return P;
@@ -267,7 +285,8 @@ extern "C" {
 // 4 harmonic eddy current tets (param0 = order, param1 = frequency,
 // param2..5 = sigma per material region), 5 Poisson quads with a non-zero
 // Dirichlet value (param0 = order), 6 elasticity hexes with a prescribed
-// face displacement (param0 = order).
+// face displacement (param0 = order), 7 Poisson quads with a per-element
+// coefficient field from slz_set_element_values (param0 = order).
 int slz_run(int workload, const char* msh, const double* params, int reps, double* times)
 {
     g_error.clear();
@@ -317,6 +336,9 @@ void slz_result_copy(int* Arows, int* Acols, double* Avals, int* Drows, int* Dco
 }
 
 void slz_set_threads(int n) { setmaxnumthreads(n); }
+
+// Per-element coefficient values of workload 7, in element order.
+void slz_set_element_values(const double* v, long long n) { g_element_values.assign(v, v + n); }
 
 // mat::eliminate (src/formulation/mat.cpp:78-103) of the last captured matrix
 // applied to the vector x [ndofs]: out [nA] = x_A - D x_D.  Returns nA, or -1.

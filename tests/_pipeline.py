@@ -53,6 +53,9 @@ def _child_main(mode, workload, msh, params, out, reps):
     elif mode.startswith("sweep"):
         np.savez(out, **sweep_inproc(msh, params, mode.split(":")[1]))
         return
+    elif mode in ("ref_kfield", "serve_kfield"):
+        np.savez(out, **kfield_inproc(mode, msh, params))
+        return
     elif mode in ("ref_integrate", "gpu_integrate"):
         lib = W.load(REF_LIB if mode == "ref_integrate" else GPU_LIB)
         out3 = (ctypes.c_double * 2)()
@@ -153,6 +156,62 @@ def eliminate_inproc(mode, workload, msh, params):
     st = lib.slgpu_matrix_eliminate(ctx, h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(ed.data_ptr()))
     assert st == abi.E_ARG, st
     return out
+
+
+def kfield_values(nelem, seed=29):
+    return np.random.Generator(np.random.PCG64(seed)).lognormal(0.0, 0.3, nelem)
+
+
+def kfield_inproc(mode, msh, params):
+    """Poisson with a per-element coefficient field k on quads.  ref_kfield:
+    stock sparselizard assembles it with k = kfield_values (element order).
+    serve_kfield: the drop-in assembles the same formulation once with k = 1
+    as a serving template (slz_serve_add), then one request through the
+    engine's server carries k = kfield_values (mesh element order); returns
+    the template's pattern and the request's values."""
+    from sparselizard_b200 import abi, serving, workloads as W
+
+    order, nelem, precision = int(params[0]), int(params[1]), int(params[2])
+    k = kfield_values(nelem)
+    if mode == "ref_kfield":
+        lib = W.load(REF_LIB)
+        lib.slz_set_element_values.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        lib.slz_set_element_values(k.ctypes.data, k.size)
+        r = W.run(REF_LIB, W.POISSON_KFIELD, msh, [order])
+        return {key: getattr(r, key) for key in ("Arows", "Acols", "Avals", "Drows", "Dcols", "Dvals")}
+    lib = W.load(GPU_LIB)
+    abi.bind(lib)
+    lib.slgpu_adapter_ctx.restype = ctypes.c_void_p
+    lib.slz_serve_add.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    info = (ctypes.c_longlong * 6)()
+    idx = lib.slz_serve_add(1, msh.encode(), 2, order, info)
+    if idx < 0:
+        raise RuntimeError(lib.slz_last_error().decode(errors="replace"))
+    ctx = ctypes.c_void_p(lib.slgpu_adapter_ctx())
+    h, nnzA, nnzD, nmesh, ngroups = int(info[0]), int(info[1]), int(info[2]), int(info[3]), int(info[4])
+    assert nmesh == nelem
+    # The template's pattern (its last process()).
+    ws = abi.Work()
+    assert lib.slgpu_matrix_work(ctx, h, ctypes.byref(ws)) == 0
+    nA = int(ws.nA)
+    pat = dict(Arows=np.zeros(nA + 1, np.int32), Acols=np.zeros(nnzA, np.int32), Avals=np.zeros(max(1, nnzA)),
+               Drows=np.zeros(nA + 1, np.int32), Dcols=np.zeros(nnzD, np.int32), Dvals=np.zeros(max(1, nnzD)))
+    assert lib.slgpu_matrix_download(ctx, h, *[abi.i32p(pat[x]) if pat[x].dtype == np.int32 else abi.f64p(pat[x])
+                                               for x in ("Arows", "Acols", "Avals", "Drows", "Dcols", "Dvals")]) == 0
+    srv = serving.Server(lib, ctx, 2)
+    try:
+        A, D = np.full(nnzA, np.nan), np.full(max(1, nnzD), np.nan)[:nnzD]
+        ups = [serving.UpdateSpec(gi, abi.UPDATE_FIELDDATA, 0, k) for gi in range(ngroups)]
+        st = srv.wait(srv.submit(h, precision, ups, A, D))
+        assert st.status == abi.OK
+    finally:
+        srv.close()
+    return dict(Arows=pat["Arows"], Acols=pat["Acols"], Avals=A, Drows=pat["Drows"], Dcols=pat["Dcols"], Dvals=D)
+
+
+def kfield(mode, msh, order, nelem, precision):
+    with tempfile.TemporaryDirectory() as d:
+        return _child(mode, 0, msh, [order, nelem, precision], os.path.join(d, "o.npz"))
 
 
 def integrate(mode, msh, order):

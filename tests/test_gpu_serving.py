@@ -286,3 +286,22 @@ def _direct(ctx, h, con):
     A, D = np.zeros(max(1, info.nnzA)), np.zeros(max(1, info.nnzD))
     ctx.check(L.slgpu_matrix_download_values(ctx.h, h, abi.f64p(A), abi.f64p(D)))
     return A[: info.nnzA], D[: info.nnzD]
+
+
+@pytest.mark.parametrize("order,precision,tol", [(1, abi.PREC_FP64, 1e-12), (3, abi.PREC_SPLIT, 1e-10)])
+def test_served_sparselizard_template_matches_reference(ref_lib, gpu_lib, tmp_path, order, precision, tol):
+    """A template built through sparselizard (the serving pool's Poisson
+    formulation with a per-element coefficient field, assembled once with
+    k = 1) serves a request carrying a new field k; the request's matrix must
+    equal stock sparselizard's assembly of the same formulation with that k:
+    bit-exact pattern, values within the tolerance of the precision."""
+    import _pipeline as P
+    from sparselizard_b200 import meshgen
+
+    n = 40
+    msh = str(tmp_path / "k.msh")
+    meshgen.workload_mesh("quad", n, msh)
+    ref = P.kfield("ref_kfield", msh, order, n * n, precision)
+    got = P.kfield("serve_kfield", msh, order, n * n, precision)
+    P.check_pattern(ref, got)
+    P.check_values(ref, got, tol)
