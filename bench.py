@@ -580,6 +580,9 @@ def run_ours(args, spec):
     lib.slgpu_ctx_set_kernel_timers(ctx, 0)
     ph = phase / args.steps
     roof = roofline_of(stats, args.workload, n, int8_tops)
+    tb = ctypes.create_string_buffer(8192)
+    lib.slgpu_tuned_tiles(ctx, tb, 8192)
+    tuned = [x for x in tb.value.decode().splitlines() if x]
 
     # ---- end to end through sparselizard's API: warm generate() + A() + b()
     # of the resident problem (one untimed warm repetition first)
@@ -635,6 +638,7 @@ def run_ours(args, spec):
             "gpu_launches": int(launches),
             "graph_replays": int(graph_replays),
             "roofline": roof,
+            "tuned": tuned,
             "int8_peak_tops": int8_tops,
             "cpu_baseline": cpu,
             "parity": parity,

@@ -66,6 +66,11 @@ int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx);
  * far (uploads of meshes, groups, data and constraints; downloads of CSR
  * arrays and values).  No counterpart in the reference (no device there). */
 int slgpu_transfer_bytes(const slgpu_ctx* ctx, int64_t* h2d, int64_t* d2h);
+/* The tile shapes the first-use tuner picked (one line each: kind, choice,
+ * group shape ntf/ndof/ngp) and the CSR value kernel of each resident
+ * pattern, as text.  No counterpart in the reference (a single fixed BLAS
+ * switch, src/densemat.cpp:264-306, picks between dgemm and a loop). */
+int slgpu_tuned_tiles(slgpu_ctx* ctx, char* buf, size_t len);
 
 /*
  * Mesh geometry, resident on the device.  Replaces the node-coordinate and

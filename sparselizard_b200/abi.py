@@ -114,6 +114,7 @@ SIGNATURES = {
     "slgpu_matrix_group_symmetry": (c_int, [c_void_p, c_int, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
     "slgpu_kernel_launches": (c_int64, [c_void_p]),
     "slgpu_transfer_bytes": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int64)]),
+    "slgpu_tuned_tiles": (c_int, [c_void_p, c_char_p, c_size_t]),
     "slgpu_ctx_set_graphs": (c_int, [c_void_p, c_int]),
     "slgpu_graph_launches": (c_int64, [c_void_p]),
     "slgpu_ctx_set_kernel_timers": (c_int, [c_void_p, c_int]),

@@ -23,6 +23,7 @@
 
 #include "dofinterpolate.h"
 #include "lagrangeformfunction.h"
+#include "opharmonic.h"
 #include "slgpu_adapter.h"
 
 #include <cmath>
@@ -65,6 +66,30 @@ std::string printed(const std::shared_ptr<operation>& op)
     std::cout.rdbuf(old);
     return ss.str();
 }
+
+// opharmonic (sl::moveharmonic, src/expression/operation/sl.cpp:555-601) keeps
+// its harmonic maps private and has no getters.  An explicit instantiation
+// may name private members (access is not checked there), which gives read
+// access through these pointers-to-member.
+template <class Tag, typename Tag::type M>
+struct MemberAccess {
+    friend typename Tag::type member(Tag) { return M; }
+};
+struct HarmOrig {
+    typedef std::vector<int> opharmonic::*type;
+    friend type member(HarmOrig);
+};
+struct HarmDest {
+    typedef std::vector<int> opharmonic::*type;
+    friend type member(HarmDest);
+};
+struct HarmFft {
+    typedef int opharmonic::*type;
+    friend type member(HarmFft);
+};
+template struct MemberAccess<HarmOrig, &opharmonic::myorigharms>;
+template struct MemberAccess<HarmDest, &opharmonic::mydestharms>;
+template struct MemberAccess<HarmFft, &opharmonic::mynumfftharms>;
 
 // Lowers coefficient operation trees of one disjoint-region group into an
 // slgpu coefficient program.  Shared subtrees (same operation object) become
@@ -170,7 +195,36 @@ private:
             return parameter(op);
         if (op->isfield())
             return fieldvalue(op);
+        if (auto* h = dynamic_cast<opharmonic*>(p))
+            return moved_harmonic(*h);
         unsupported(std::string("the coefficient operation '") + typeid(*p).name() + "'");
+    }
+
+    // opharmonic (opharmonic.cpp:12-57): harmonic dest_i of the result sums
+    // harmonic orig_i of the argument.  Coefficients here are constant in
+    // time (harmonic 1 only), so with every destination harmonic 1 and an
+    // argument of harmonic 1 the result is k times the argument, k the number
+    // of pairs (1 -> 1): what setvalue / setconstraint produce for a field
+    // that is not multiharmonic (sl::getharmonic(1, expr)).
+    int moved_harmonic(opharmonic& h)
+    {
+        const std::vector<int>& orig = h.*member(HarmOrig());
+        const std::vector<int>& dest = h.*member(HarmDest());
+        if (h.*member(HarmFft()) >= 0)
+            unsupported("FFT-based harmonic extraction in a coefficient");
+        std::shared_ptr<operation> arg = h.getarguments()[0];
+        if (!arg->isharmonicone(disjregs_))
+            unsupported("a harmonic of a multiharmonic coefficient");
+        int k = 0;
+        for (size_t i = 0; i < orig.size(); i++) {
+            if (dest[i] != 1)
+                unsupported("a coefficient moved to a harmonic other than 1");
+            k += orig[i] == 1 ? 1 : 0;
+        }
+        if (k == 0)
+            return constant(0.0);
+        const int a = lower(arg);
+        return k == 1 ? a : add(SLGPU_OP_MUL, constant((double)k), a);
     }
 
     // opparameter: one expression per disjoint region (opparameter.cpp:4).
