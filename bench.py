@@ -309,9 +309,12 @@ KERNEL_NAMES = {"coefficients": "slgpu_coef (runtime-compiled)", "contract_fp64"
                 "contract_split_fp32": "k_contract_split<5,6>", "row_values": "k_row_values / k_row_stream (chosen per pattern)"}
 
 
-def int8_peak_tops():
-    """Dense INT8 tensor throughput of this GPU, measured: torch._int_mm on
-    8192^3 int8 operands (2 N^3 ops), best of 10 after warm-up, CUDA events."""
+def int8_peak_tops(sustained_s=2.0):
+    """Dense INT8 tensor throughput of this GPU, measured with torch._int_mm on
+    8192^3 int8 operands (2 N^3 ops), CUDA events: the best of 10 single calls
+    after warm-up (burst), and the mean over back-to-back calls for
+    `sustained_s` seconds (sustained: what the power cap allows a kernel that
+    runs inside a long step).  Returns (burst, sustained) in TOPS."""
     import torch
 
     n = 8192
@@ -327,9 +330,18 @@ def int8_peak_tops():
         e1.record()
         e1.synchronize()
         best = min(best, e0.elapsed_time(e1))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(10, int(sustained_s / (best * 1e-3)))
+    e0.record()
+    for _ in range(reps):
+        torch._int_mm(a, b)
+    e1.record()
+    e1.synchronize()
+    mean = e0.elapsed_time(e1) / reps
     del a, b
     torch.cuda.empty_cache()
-    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    ops = 2.0 * n ** 3
+    return ops / (best * 1e-3) / 1e12, ops / (mean * 1e-3) / 1e12
 
 
 def roofline_of(stats, workload, n, int8_tops=None):
@@ -341,11 +353,15 @@ def roofline_of(stats, workload, n, int8_tops=None):
     rate = k["work"] / (k["ms"] * 1e-3)
     if dom.startswith("contract_split"):
         if int8_tops:
-            peak, kind = int8_tops, "measured INT8 dense (torch._int_mm 8192^3, best of 10, this run); achieved counts INT8 ops"
+            burst, sustained = int8_tops
+            peak = sustained
+            kind = ("measured INT8 dense, sustained (torch._int_mm 8192^3 back to back for 2 s, this run; the kernel "
+                    "is timed inside a long step); achieved counts INT8 ops")
         else:
-            peak, kind = 2.0 * bf16, f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops"
+            burst = peak = 2.0 * bf16
+            kind = f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops"
         roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_kind": kind, "frac": rate / 1e12 / peak}
+                "peak_kind": kind, "frac": rate / 1e12 / peak, "peak_burst": burst, "frac_of_burst": rate / 1e12 / burst}
     elif dom == "contract_fp64":
         roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": 40.0, "unit": "TFLOP/s",
                 "peak_kind": "nominal B200 FP64 40 TFLOP/s (FP64 vector and tensor rates are equal; not measured here)",
@@ -639,7 +655,7 @@ def run_ours(args, spec):
             "graph_replays": int(graph_replays),
             "roofline": roof,
             "tuned": tuned,
-            "int8_peak_tops": int8_tops,
+            "int8_peak_tops": {"burst": int8_tops[0], "sustained": int8_tops[1]},
             "cpu_baseline": cpu,
             "parity": parity,
             "per_config": per_config,

@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <map>
+#include <tuple>
 #include <sstream>
 #include <typeinfo>
 
@@ -45,6 +46,8 @@ void contribution::settfphysicalregion(int physreg) { tfphysreg = physreg; }
 void contribution::setintegrationorderdelta(int integrorderdelta) { integrationorderdelta = integrorderdelta; }
 void contribution::setnumfftcoeffs(int numcoeffs) { numfftcoeffs = numcoeffs; }
 void contribution::setbarycenterevalflag(void) { isbarycentereval = true; }
+
+
 
 namespace {
 
@@ -90,6 +93,52 @@ struct HarmFft {
 template struct MemberAccess<HarmOrig, &opharmonic::myorigharms>;
 template struct MemberAccess<HarmDest, &opharmonic::mydestharms>;
 template struct MemberAccess<HarmFft, &opharmonic::mynumfftharms>;
+
+// DOF addresses of one (dofmanager, field, order, element type, element list,
+// region), shared by the contributions of one assembly: the slices of a
+// vector field's formulation ask for the same test-function and dof
+// addresses many times (elasticity: 18 requests, 6 distinct tables).  Every
+// hit is checked against a fresh lookup of the list's first and last
+// elements; rawmat::process clears the cache (slgpu_adapter::clear_address_cache).
+struct AddressKey {
+    const void* dm;
+    const void* field;
+    int order, elemtype, physreg, meshnumber;
+    long long ndofs;
+    size_t n;
+    unsigned long long hash;
+    bool operator<(const AddressKey& o) const
+    {
+        return std::tie(dm, field, order, elemtype, physreg, meshnumber, ndofs, n, hash) <
+               std::tie(o.dm, o.field, o.order, o.elemtype, o.physreg, o.meshnumber, o.ndofs, o.n, o.hash);
+    }
+};
+std::map<AddressKey, indexmat> g_address_cache;
+
+indexmat cached_addresses(const std::shared_ptr<dofmanager>& dm, const std::shared_ptr<rawfield>& f, int order, int elemtype,
+                          std::vector<int>& elems, int physreg)
+{
+    unsigned long long h = 1469598103934665603ull;
+    for (int e : elems) h = (h ^ (unsigned long long)(unsigned)e) * 1099511628211ull;
+    const AddressKey key{dm.get(), f.get(), order, elemtype, physreg, universe::getrawmesh()->getmeshnumber(), dm->countdofs(),
+                         elems.size(), h};
+    auto it = g_address_cache.find(key);
+    if (it != g_address_cache.end() && !elems.empty()) {
+        std::vector<int> probe{elems.front(), elems.back()};
+        indexmat fresh = dm->getaddresses(f, order, elemtype, probe, physreg);
+        indexmat c = it->second;
+        const long long rows = c.countrows(), n = c.countcolumns();
+        bool same = fresh.countrows() == rows;
+        for (long long r = 0; same && r < rows; r++)
+            same = fresh.getvalues()[r * 2] == c.getvalues()[r * n] && fresh.getvalues()[r * 2 + 1] == c.getvalues()[r * n + n - 1];
+        if (same)
+            return c;
+        g_address_cache.erase(it);
+    }
+    indexmat a = dm->getaddresses(f, order, elemtype, elems, physreg);
+    g_address_cache[key] = a;
+    return a;
+}
 
 // Lowers coefficient operation trees of one disjoint-region group into an
 // slgpu coefficient program.  Shared subtrees (same operation object) become
@@ -532,11 +581,11 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
             std::vector<indexmat> addrkeep;
             std::vector<slgpu_dest> dests;
             for (auto& d : u.dests) {
-                indexmat tfa = mydofmanager->getaddresses(tffield->harmonic(d.first.first), tforder, elemtype, elems, tfphysreg);
+                indexmat tfa = cached_addresses(mydofmanager, tffield->harmonic(d.first.first), tforder, elemtype, elems, tfphysreg);
                 addrkeep.push_back(tfa);
                 const int32_t* dofp = nullptr;
                 if (doffield != NULL) {
-                    indexmat dfa = mydofmanager->getaddresses(doffield->harmonic(d.first.second), doforder, elemtype, elems, dofphysreg);
+                    indexmat dfa = cached_addresses(mydofmanager, doffield->harmonic(d.first.second), doforder, elemtype, elems, dofphysreg);
                     addrkeep.push_back(dfa);
                     dofp = dfa.getvalues();
                 }
@@ -589,3 +638,7 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
         }
     }
 }
+
+namespace slgpu_adapter {
+void clear_address_cache(void) { g_address_cache.clear(); }
+}  // namespace slgpu_adapter

@@ -26,7 +26,8 @@ double integrate(expression e, int physreg, int integrationorder)
     // Integration order of a contribution: dof order + tf order + 2 + delta,
     // with both orders 0 for a "one" field without dof.
     f += sl::integral(physreg, e * sl::tf(one), integrationorder - 2);
-    vec b = f.rhs();
+    f.generaterhs();
+    vec b = f.rhs(false, false);
     densemat v = b.getallvalues();
     const double* bv = v.getvalues();
     double s = 0;

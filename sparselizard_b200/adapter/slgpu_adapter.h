@@ -49,6 +49,10 @@ bool record_only(void);
 // Remembers the engine matrix handed to the last rawmat::process call.
 void set_last_processed(rawmat* m);
 
+// Forgets the DOF addresses shared by the contributions of the assembly that
+// is being processed (contribution.cpp); called by rawmat::process.
+void clear_address_cache(void);
+
 // Integral of a scalar expression over a physical region at a Gauss order
 // (what expression::integrate computes, src/expression/expression.cpp:808-889)
 // on the GPU: the expression is lowered to a coefficient program, evaluated

@@ -827,23 +827,6 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
         const uint32_t a0 = __shfl_sync(0xffffffffu, a_lo, rr), a1 = __shfl_sync(0xffffffffu, a_lo, rr + 1);
         const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
         const uint32_t k0 = __shfl_sync(0xffffffffu, i_lo, rr), k1 = __shfl_sync(0xffffffffu, i_lo, rr + 1);
-        // The next row's element-matrix rows and slots are requested into L2
-        // now (lane l: its first 32 incidences' runs), so that its loads,
-        // issued after this row's additions, wait on L2 rather than DRAM.
-        if (rr + 1 < nr) {
-            const uint32_t n0 = k1, n1 = __shfl_sync(0xffffffffu, i_lo, rr + 2);
-            if (lane < (int)min(32u, n1 - n0)) {
-                const unsigned long long pk = p.inc[n0 + lane];
-                const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-                const long long co = (long long)(pk & ((1ull << 40) - 1));
-                const char* v = reinterpret_cast<const char*>(p.vals + (sg.val_base + (co - sg.coo_base)));
-                const char* sl = reinterpret_cast<const char*>(p.slotmap + co);
-                const int vb = 8 * sg.width, sb = 2 * sg.width;
-                for (int off = 0; off < vb; off += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(v + off));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(v + vb - 8));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(sl));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(sl + sb - 2));
-            }
         }
         const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
         for (uint32_t kb = k0; kb < k1; kb += 32) {
