@@ -156,11 +156,11 @@ def peaks():
 # launch's group (traffic grows in proportion to the elements).  Summaries
 # and the commands that made them are under profiles/.
 TRAFFIC_PER_ELEMENT = {
-    # profiles/k_contract_split_elasticity_hex32.md, 32768 elements: a symmetric
-    # launch reads 59.91 MB and writes 138.28 MB, a paired one 70.26 + 338.40 MB;
-    # a step runs three of each, so a launch averages their mean.
-    ("c2", "contract_split"): ((59.910656e6 + 138.279168e6) + (70.263296e6 + 338.402048e6)) / 2 / 32768,
-    # profiles/k_row_values_elasticity_hex32.md: 2.859 GB read + 1.202 GB
+    # profiles/k_contract_split_elasticity_hex32.md, 32768 elements: the one
+    # launch of a step (all six contracted groups) reads 387.29 MB and writes
+    # 1798.11 MB.
+    ("c2", "contract_split"): (387.290624e6 + 1798.110e6) / 32768,
+    # profiles/k_row_values_elasticity_hex32.md: 2.858 GB read + 1.202 GB
     # written by the launch over all 9 groups of 32768 elements.
     ("c2", "row_values"): (2.858950e9 + 1.201917e9) / 32768,
 }
@@ -354,14 +354,14 @@ def roofline_of(stats, workload, n, int8_tops=None):
     if dom.startswith("contract_split"):
         if int8_tops:
             burst, sustained = int8_tops
-            peak = sustained
-            kind = ("measured INT8 dense, sustained (torch._int_mm 8192^3 back to back for 2 s, this run; the kernel "
-                    "is timed inside a long step); achieved counts INT8 ops")
+            kind = ("measured INT8 dense, burst (torch._int_mm 8192^3, best of 10, this run); achieved counts INT8 ops; "
+                    "peak_sustained: the same GEMM back to back for 2 s under the power cap")
         else:
-            burst = peak = 2.0 * bf16
+            burst = sustained = 2.0 * bf16
             kind = f"INT8 dense = 2 x {peak_kind} bf16 burst ({bf16:.0f} TFLOP/s); achieved counts INT8 ops"
-        roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_kind": kind, "frac": rate / 1e12 / peak, "peak_burst": burst, "frac_of_burst": rate / 1e12 / burst}
+        roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": burst, "unit": "TFLOP/s",
+                "peak_kind": kind, "frac": rate / 1e12 / burst, "peak_sustained": sustained,
+                "frac_of_sustained": rate / 1e12 / sustained}
     elif dom == "contract_fp64":
         roof = {"kernel": KERNEL_NAMES[dom], "bound": "tensor", "achieved": rate / 1e12, "peak": 40.0, "unit": "TFLOP/s",
                 "peak_kind": "nominal B200 FP64 40 TFLOP/s (FP64 vector and tensor rates are equal; not measured here)",
