@@ -120,6 +120,20 @@ def test_dropin_nonzero_dirichlet(ref_lib, gpu_lib, tmp, workload, kind, n, para
     P.check_rhs(ref, got["b"], TOL)
 
 
+def test_dropin_reassembly_after_order_change(ref_lib, gpu_lib, tmp):
+    """One formulation assembled at order 1, then its field raised to order 3
+    and assembled again: the second assembly's DOF numbering changes on the
+    same mesh and dofmanager, and the drop-in (which shares DOF addresses
+    between the contributions of an assembly) must match the reference."""
+    msh = str(tmp / "reorder.msh")
+    meshgen.workload_mesh("quad", 16, msh)
+    args = (W.POISSON_REORDER, msh, [3])
+    ref, got = P.reference(*args), P.gpu(*args)
+    P.check_pattern(ref, got)
+    P.check_values(ref, got, TOL)
+    P.check_rhs(ref, got["b"], TOL)
+
+
 @pytest.mark.parametrize("order", [1, 3])
 def test_gpu_integrate_matches_expression_integrate(ref_lib, gpu_lib, tmp, order):
     """Field interpolation and integration on the GPU: a field set by
