@@ -99,7 +99,8 @@ template struct MemberAccess<HarmFft, &opharmonic::mynumfftharms>;
 // vector field's formulation ask for the same test-function and dof
 // addresses many times (elasticity: 18 requests, 6 distinct tables).  Every
 // hit is checked against a fresh lookup of the list's first and last
-// elements; rawmat::process clears the cache (slgpu_adapter::clear_address_cache).
+// elements; rawmat::process and the end of a right-hand-side contribution
+// clear the cache (slgpu_adapter::clear_address_cache).
 struct AddressKey {
     const void* dm;
     const void* field;
@@ -637,6 +638,11 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
             }
         }
     }
+    // A right-hand side is complete once its contributions are added: the
+    // shared addresses live from the first matrix contribution of an
+    // assembly to its process(), or to the end of a right-hand side.
+    if (doffield == NULL)
+        slgpu_adapter::clear_address_cache();
 }
 
 namespace slgpu_adapter {

@@ -260,23 +260,23 @@ void poisson_quad_kfield(Problem& P, const char* msh, int order)
     P.fields = {v, k};
 }
 
-// Workload 8: Poisson on quads assembled once at order 1 (generate(), A()),
-// then the field's order raised to `order` and the same formulation
-// assembled again by the caller (run_reps): the second assembly sees a new
-// DOF numbering on the same mesh and dofmanager.
-void poisson_quad_reorder(Problem& P, const char* msh, int order)
+// Workload 8: Poisson on quads (as workload 1, at order `order`) assembled
+// after another formulation on the same mesh -- a field of order `order` + 1
+// with its own dofmanager -- was generated and left unprocessed.
+void poisson_quad_after_other(Problem& P, const char* msh, int order)
 {
     P.m = mesh(msh, 0);
-    field v("h1");
-    v.setorder(VOL, 1);
+    field v("h1"), w("h1");
+    v.setorder(VOL, order);
+    w.setorder(VOL, order + 1);
     v.setconstraint(BOUNDARY);
+    w.setconstraint(BOUNDARY);
+    formulation other;
+    other += integral(VOL, grad(dof(w)) * grad(tf(w)) + dof(w) * tf(w));
+    other.generate();
     P.f += integral(VOL, -grad(dof(v)) * grad(tf(v)), -2);
     P.f += integral(VOL, 1 * tf(v), -2);
-    P.f.generate();
-    mat A1 = P.f.A();
-    vec b1 = P.f.b();
-    v.setorder(VOL, order);
-    P.fields = {v};
+    P.fields = {v, w};
 }
 
 std::unique_ptr<Problem> build(int workload, const char* msh, const double* params)
@@ -290,7 +290,7 @@ std::unique_ptr<Problem> build(int workload, const char* msh, const double* para
     case 5: poisson_quad_dirichlet(*P, msh, (int)params[0]); break;
     case 6: elasticity_hex_dirichlet(*P, msh, (int)params[0]); break;
     case 7: poisson_quad_kfield(*P, msh, (int)params[0]); break;
-    case 8: poisson_quad_reorder(*P, msh, (int)params[0]); break;
+    case 8: poisson_quad_after_other(*P, msh, (int)params[0]); break;
     default: throw std::runtime_error("unknown workload");
     }
     return P;

@@ -13,7 +13,7 @@ Workload ids and parameters follow ``slz_run``:
   5 Poisson on quads, non-zero Dirichlet value on the boundary   params = [order]
   6 elasticity on hexes, prescribed displacement of the z = 0 face params = [order]
   7 Poisson on quads, per-element coefficient (slz_set_element_values) params = [order]
-  8 Poisson on quads assembled at order 1, then again at `order`       params = [order]
+  8 Poisson on quads after another formulation was generated         params = [order]
 """
 from __future__ import annotations
 
@@ -23,7 +23,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-POISSON_QUAD, ELASTICITY_HEX, HELMHOLTZ_TET, EDDY_TET, POISSON_DIRICHLET, ELASTICITY_DIRICHLET, POISSON_KFIELD, POISSON_REORDER = 1, 2, 3, 4, 5, 6, 7, 8
+POISSON_QUAD, ELASTICITY_HEX, HELMHOLTZ_TET, EDDY_TET, POISSON_DIRICHLET, ELASTICITY_DIRICHLET, POISSON_KFIELD, POISSON_AFTER_OTHER = 1, 2, 3, 4, 5, 6, 7, 8
 
 
 @dataclass

@@ -120,14 +120,14 @@ def test_dropin_nonzero_dirichlet(ref_lib, gpu_lib, tmp, workload, kind, n, para
     P.check_rhs(ref, got["b"], TOL)
 
 
-def test_dropin_reassembly_after_order_change(ref_lib, gpu_lib, tmp):
-    """One formulation assembled at order 1, then its field raised to order 3
-    and assembled again: the second assembly's DOF numbering changes on the
-    same mesh and dofmanager, and the drop-in (which shares DOF addresses
-    between the contributions of an assembly) must match the reference."""
-    msh = str(tmp / "reorder.msh")
+def test_dropin_after_another_formulation(ref_lib, gpu_lib, tmp):
+    """A formulation assembled after another one on the same mesh (a field of
+    another order, its own dofmanager) was generated and left unprocessed: the
+    drop-in shares DOF addresses between the contributions of an assembly
+    and must keep the two formulations' addresses apart."""
+    msh = str(tmp / "after_other.msh")
     meshgen.workload_mesh("quad", 16, msh)
-    args = (W.POISSON_REORDER, msh, [3])
+    args = (W.POISSON_AFTER_OTHER, msh, [2])
     ref, got = P.reference(*args), P.gpu(*args)
     P.check_pattern(ref, got)
     P.check_values(ref, got, TOL)
