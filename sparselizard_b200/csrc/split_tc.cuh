@@ -388,7 +388,7 @@ constexpr size_t split_smem_bytes() { return sizeof(SplitSmem<NE>) + 1024; }
 // timeout the CTA records the failure, the roles stop, outstanding copies and
 // MMAs are waited for (bounded), the TMEM is freed and the CTA returns.
 template <int S, int L, int NE>
-__global__ void __maxnreg__(112) k_contract_split(const __grid_constant__ SplitParams p)
+__global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __grid_constant__ SplitParams p)
 {
     static_assert(S <= kSplitMaxS && L - 1 <= S && L >= 6 && L <= 8, "level layout");
     using Sh = SplitShape<NE>;
