@@ -28,6 +28,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <condition_variable>
+#include <sys/mman.h>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -2736,7 +2738,7 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
         for (auto& e : ctx->x->ev) cudaEventDestroy(e);
         for (auto& e : ctx->x->evpool) cudaEventDestroy(e);
         for (auto& e : ctx->x->kev) cudaEventDestroy(e);
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < Ctx::kDlStages; b++) {
             if (ctx->dl_stage[b] != nullptr)
                 cudaFreeHost(ctx->dl_stage[b]);
             if (ctx->dl_ev[b] != nullptr)
@@ -3116,32 +3118,15 @@ int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstraine
 }
 
 namespace {
-constexpr size_t kDlChunk = size_t(64) << 20;
-
-// Host copy spread over threads (large destinations in pageable memory are
-// also first touched here, so the page faults are spread as well).
-void parallel_memcpy(char* dst, const char* src, size_t n)
-{
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(1, n >> 22));
-    if (nt <= 1) {
-        std::memcpy(dst, src, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    const size_t part = (n + nt - 1) / nt;
-    for (size_t t = 0; t < nt; t++) {
-        const size_t a = t * part, b = std::min(n, a + part);
-        if (a < b)
-            th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
-    }
-    for (auto& x : th) x.join();
-}
 
 // Device -> host copy on the context's stream.  Page-locked or small
 // destinations: one asynchronous copy (the caller synchronises).  Large
-// pageable ones: 64 MB chunks through two page-locked blocks, the copy of
-// chunk i+1 in flight while chunk i is copied on the host (synchronous).
+// pageable ones: 32 MB chunks through a ring of 16 page-locked blocks.  This
+// thread issues the copies (at most 16 in flight) and up to 8 worker threads
+// -- created once per call -- copy the landed chunks out, chunk i by worker
+// i % 8, each worker owning two blocks.  The pageable destination, usually
+// freshly allocated and not yet touched, is advised to use huge pages
+// (MADV_HUGEPAGE), so that its first-touch faults come 2 MB at a time.
 void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
 {
     if (n == 0)
@@ -3150,33 +3135,89 @@ void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
     cudaPointerAttributes a{};
     const bool pinned = cudaPointerGetAttributes(&a, dst) == cudaSuccess && a.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    if (pinned || n < 2 * kDlChunk) {
+    constexpr size_t kChunk = size_t(32) << 20;
+    if (pinned || n < 4 * kChunk) {
         cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
         return;
     }
-    for (int b = 0; b < 2; b++) {
+    {
+        const uintptr_t lo = (reinterpret_cast<uintptr_t>(dst) + (size_t(2) << 20) - 1) & ~((uintptr_t(2) << 20) - 1);
+        const uintptr_t hi = (reinterpret_cast<uintptr_t>(dst) + n) & ~((uintptr_t(2) << 20) - 1);
+        if (hi > lo)
+            madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only: failure changes nothing
+    }
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nw = std::max(1, std::min(std::min(hw, 8), Ctx::kDlStages / 2));
+    const int nstage = 2 * nw;
+    for (int b = 0; b < nstage; b++) {
         if (ctx->dl_stage[b] == nullptr)
-            cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&ctx->dl_stage[b]), kDlChunk, cudaHostAllocDefault), "cudaHostAlloc");
+            cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&ctx->dl_stage[b]), kChunk, cudaHostAllocDefault), "cudaHostAlloc");
         if (ctx->dl_ev[b] == nullptr)
             cuda_check(cudaEventCreateWithFlags(&ctx->dl_ev[b], cudaEventDisableTiming), "cudaEventCreate");
     }
-    const size_t nch = (n + kDlChunk - 1) / kDlChunk;
+    const size_t nch = (n + kChunk - 1) / kChunk;
+    // Chunk i uses block (i % nw) * 2 + (i / nw) % 2: worker i % nw alternates
+    // between its two blocks.
+    auto block = [&](size_t i) { return (int)((i % nw) * 2 + (i / nw) % 2); };
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t issued = 0;  // chunks [0, issued) have their copy queued
+    std::vector<char> done(nch, 0);
+    std::string err;
     auto issue = [&](size_t i) {
-        const size_t off = i * kDlChunk, len = std::min(kDlChunk, n - off);
-        cuda_check(cudaMemcpyAsync(ctx->dl_stage[i & 1], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, ctx->x->stream),
-                   "D2H chunk");
-        cuda_check(cudaEventRecord(ctx->dl_ev[i & 1], ctx->x->stream), "cudaEventRecord");
+        const size_t off = i * kChunk, len = std::min(kChunk, n - off);
+        const int b = block(i);
+        cudaError_t e = cudaMemcpyAsync(ctx->dl_stage[b], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, ctx->x->stream);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(ctx->dl_ev[b], ctx->x->stream);
+        return e;
     };
-    issue(0);
-    if (nch > 1)
-        issue(1);
+    std::vector<std::thread> workers;
+    for (int w = 0; w < nw; w++)
+        workers.emplace_back([&, w] {
+            for (size_t i = (size_t)w; i < nch; i += (size_t)nw) {
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    cv.wait(lk, [&] { return issued > i || !err.empty(); });
+                    if (!err.empty())
+                        return;
+                }
+                const int b = block(i);
+                const cudaError_t e = cudaEventSynchronize(ctx->dl_ev[b]);
+                if (e != cudaSuccess) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    err = std::string("D2H chunk wait: ") + cudaGetErrorString(e);
+                    cv.notify_all();
+                    return;
+                }
+                const size_t off = i * kChunk, len = std::min(kChunk, n - off);
+                std::memcpy(static_cast<char*>(dst) + off, ctx->dl_stage[b], len);
+                std::lock_guard<std::mutex> lk(mu);
+                done[i] = 1;
+                cv.notify_all();
+            }
+        });
+    // Issue in order; chunk i may be issued once chunk i - nstage (same block) was copied out.
     for (size_t i = 0; i < nch; i++) {
-        cuda_check(cudaEventSynchronize(ctx->dl_ev[i & 1]), "D2H chunk wait");
-        const size_t off = i * kDlChunk, len = std::min(kDlChunk, n - off);
-        parallel_memcpy(static_cast<char*>(dst) + off, ctx->dl_stage[i & 1], len);
-        if (i + 2 < nch)
-            issue(i + 2);
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return i < (size_t)nstage || done[i - nstage] || !err.empty(); });
+            if (!err.empty())
+                break;
+        }
+        const cudaError_t e = issue(i);
+        std::lock_guard<std::mutex> lk(mu);
+        if (e != cudaSuccess) {
+            err = std::string("D2H chunk: ") + cudaGetErrorString(e);
+            cv.notify_all();
+            break;
+        }
+        issued = i + 1;
+        cv.notify_all();
     }
+    for (auto& t : workers) t.join();
+    if (!err.empty())
+        fail(SLGPU_E_CUDA, err);
 }
 }  // namespace
 

@@ -307,8 +307,10 @@ struct Ctx {
     std::string jit_error;
     // Page-locked blocks and events of the pipelined download into pageable
     // host memory (slgpu_matrix_download*).
-    char* dl_stage[2] = {nullptr, nullptr};
-    cudaEvent_t dl_ev[2] = {nullptr, nullptr};
+    // Page-locked staging ring of large downloads into pageable memory.
+    static constexpr int kDlStages = 16;
+    char* dl_stage[kDlStages] = {};
+    cudaEvent_t dl_ev[kDlStages] = {};
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;
