@@ -114,7 +114,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -575,11 +575,12 @@ def run_ours(args, spec):
     for _ in range(args.warmup):
         process()
     phase = np.zeros(5)
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        phase += process()
-        kernel_stats(lib, ctx, stats)
+    with ClockSampler(local) as clk_k:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            phase += process()
+            kernel_stats(lib, ctx, stats)
     if "fp64" in tiers:
         st64 = {}
         for _ in range(min(args.warmup, 2)):
@@ -660,6 +661,7 @@ def run_ours(args, spec):
             "parity": parity,
             "per_config": per_config,
             "clocks": clk.summary(),
+            "clocks_kernel_steps": clk_k.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -823,51 +823,6 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
     }
     __syncwarp();
     constexpr int kGeneric = 1 << 17, kSerial = 1 << 16;
-    // Lane l's decoded incidence of the current block of 32, and the
-    // element-matrix row entries of one batch (lane j holds entry j of each).
-    uint32_t voff = 0, coo = 0;
-    double mult = 0.0;
-    int info = 0;  // width | kSerial | kGeneric
-    double val[kRowBatch];
-    int slot[kRowBatch];
-    // Lane l decodes incidence kb + l.  Value and COO offsets fit 32 bits
-    // (fewer than 2^32 COO entries per matrix).
-    auto decode = [&](uint32_t kb, int nkb) {
-        voff = 0;
-        coo = 0;
-        mult = 0.0;
-        info = 0;
-        if (lane < nkb) {
-            const unsigned long long pk = p.inc[kb + lane];
-            const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
-            coo = (uint32_t)(pk & ((1ull << 40) - 1));
-            voff = (uint32_t)(sg.val_base + ((long long)coo - sg.coo_base));
-            mult = sg.mult;
-            const bool serial = (pk >> 63) != 0;
-            info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
-        }
-    };
-    // Loads of incidences u .. u + kRowBatch - 1 of the block, all issued
-    // before any addition.
-    auto load_batch = [&](int u, int nkb) {
-#pragma unroll
-        for (int x = 0; x < kRowBatch; x++) {
-            const int src = (u + x) & 31;
-            const uint32_t vo = __shfl_sync(0xffffffffu, voff, src);
-            const uint32_t co = __shfl_sync(0xffffffffu, coo, src);
-            const int inf = __shfl_sync(0xffffffffu, info, src);
-            slot[x] = -1;
-            val[x] = 0.0;
-            if (u + x < nkb && lane < (inf & 0xffff)) {
-                slot[x] = p.slotmap[(uint64_t)co + lane];
-                val[x] = p.vals[(uint64_t)vo + lane];
-            }
-        }
-    };
-    // `pre`: the current row's first block is decoded and its first batch
-    // loaded (issued before the previous row's write-back, so that their
-    // latency overlaps it).
-    bool pre = false;
     for (int rr = 0; rr < nr; rr++) {
         const uint32_t a0 = __shfl_sync(0xffffffffu, a_lo, rr), a1 = __shfl_sync(0xffffffffu, a_lo, rr + 1);
         const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
@@ -875,13 +830,39 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
         const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
         for (uint32_t kb = k0; kb < k1; kb += 32) {
             const int nkb = (int)min(32u, k1 - kb);
-            const bool first = pre && kb == k0;
-            if (!first)
-                decode(kb, nkb);
+            // Lane l decodes incidence kb + l.  Value and COO offsets fit 32
+            // bits (fewer than 2^32 COO entries per matrix).
+            uint32_t voff = 0, coo = 0;
+            double mult = 0.0;
+            int info = 0;  // width | kSerial | kGeneric
+            if (lane < nkb) {
+                const unsigned long long pk = p.inc[kb + lane];
+                const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
+                coo = (uint32_t)(pk & ((1ull << 40) - 1));
+                voff = (uint32_t)(sg.val_base + ((long long)coo - sg.coo_base));
+                mult = sg.mult;
+                const bool serial = (pk >> 63) != 0;
+                info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
+            }
             if (!__any_sync(0xffffffffu, (info & kGeneric) != 0)) {
+                // Batches of kRowBatch incidences: every load issued before
+                // the ordered additions.
                 for (int u = 0; u < nkb; u += kRowBatch) {
-                    if (!(first && u == 0))
-                        load_batch(u, nkb);
+                    double val[kRowBatch];
+                    int slot[kRowBatch];
+#pragma unroll
+                    for (int x = 0; x < kRowBatch; x++) {
+                        const int src = (u + x) & 31;
+                        const uint32_t vo = __shfl_sync(0xffffffffu, voff, src);
+                        const uint32_t co = __shfl_sync(0xffffffffu, coo, src);
+                        const int inf = __shfl_sync(0xffffffffu, info, src);
+                        slot[x] = -1;
+                        val[x] = 0.0;
+                        if (u + x < nkb && lane < (inf & 0xffff)) {
+                            slot[x] = p.slotmap[(uint64_t)co + lane];
+                            val[x] = p.vals[(uint64_t)vo + lane];
+                        }
+                    }
 #pragma unroll
                     for (int x = 0; x < kRowBatch; x++) {
                         if (u + x < nkb) {
@@ -900,19 +881,6 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
                     const int inf = __shfl_sync(0xffffffffu, info, x);
                     row_add_generic(buf, inf & 0xffff, m, p.vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
                     __syncwarp();
-                }
-            }
-        }
-        // The next row's first block and batch, ahead of this row's write-back.
-        pre = false;
-        if (rr + 1 < nr) {
-            const uint32_t n1 = __shfl_sync(0xffffffffu, i_lo, rr + 2);
-            if (n1 > k1) {
-                const int nkb = (int)min(32u, n1 - k1);
-                decode(k1, nkb);
-                if (!__any_sync(0xffffffffu, (info & kGeneric) != 0)) {
-                    load_batch(0, nkb);
-                    pre = true;
                 }
             }
         }

@@ -549,19 +549,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
             const Tile unit = split_unit<NE>(G.tiles, u);
             if (unit.ne <= 0)
                 continue;
-            // This tile's row exponent, row map entry and column exponents
-            // are requested into L1 now, so that the recombination after the
-            // accumulator wait does not stall on their global loads.
-            {
-                const int pe = pt * kSplitM + quarter * 32 + lane;
-                if (pe < G.nrows) {
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(G.rowexp + (int64_t)unit.orient * G.Ppad + pe));
-                    if (G.rowmap != nullptr)
-                        asm volatile("prefetch.global.L1 [%0];" ::"l"(G.rowmap + pe));
-                }
-                if (lane == 0)
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(G.colexp + u * NE + c0));
-            }
             const int buf = (int)(i % Sh::kBufs);
             if (!mbar_wait(&sm.tmem_full[buf], (uint32_t)((i / Sh::kBufs) & 1), failed)) {
                 *failed = 1;
