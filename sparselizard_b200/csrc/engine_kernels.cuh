@@ -735,7 +735,7 @@ struct RowParams {
 // the additions still run in incidence order.  Incidences flagged serial
 // (duplicate addresses) or wider than a warp are added by their own loop at
 // their place in the order.
-constexpr int kRowBatch = 6;
+constexpr int kRowBatch = 8;
 
 __device__ __forceinline__ void row_add_generic(double* buf, int width, double mult, const double* v, const int16_t* sm, bool serial,
                                                 int lane)
@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
 // Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
 constexpr int kRowsPerWarp = 31;
 
-__global__ void __launch_bounds__(256, 5) k_row_values(RowParams p)
+__global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
 {
     extern __shared__ double rowbuf[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
