@@ -1448,6 +1448,7 @@ static void launch_split(Ctx* ctx, const SplitParams& p)
         attr = true;
     }
     const int64_t grid = std::min<int64_t>(p.nwork, std::max(ctx->nsm, 1));
+    cuda_check(cudaMemsetAsync(p.next, 0, sizeof(unsigned long long), ctx->x->stream), "memset");
     k_contract_split<S, L, NE><<<(unsigned)grid, kSplitThreads, smem, ctx->x->stream>>>(p);
 }
 
@@ -1569,6 +1570,7 @@ static void run_split_jobs(Ctx* ctx, const std::vector<SplitJob>& jobs, int NE)
             cexp += split_exp_bytes(g) / 4;
         }
         sp.error = ctx->x->split_error.as<unsigned int>();
+        sp.next = reinterpret_cast<unsigned long long*>(ctx->x->split_error.as<char>() + 16);
         const int kt = kstat_start(ctx, "slice_cols", slice_bytes);
         if (S == 7 && NE == 64)
             launch_slices<7, 64>(ctx, cs);
@@ -2016,7 +2018,7 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
     if (precision != SLGPU_PREC_FP64) {
         if (ctx->x->split_error.empty()) {
             ArenaPause keep(*ctx->x);
-            ctx->x->split_error.alloc(ctx, 16);
+            ctx->x->split_error.alloc(ctx, 32);
         }
         cuda_check(cudaMemsetAsync(ctx->x->split_error.as<void>(), 0, 16, ctx->x->stream), "memset");
     }
@@ -2338,7 +2340,7 @@ void prepare_value_path(Ctx* ctx, const Matrix& M, int precision)
     if (x.split_colexp.bytes() < expbytes)
         x.split_colexp.alloc(ctx, expbytes);
     if (x.split_error.empty())
-        x.split_error.alloc(ctx, 16);
+        x.split_error.alloc(ctx, 32);
 }
 
 ValueGraph::~ValueGraph()

@@ -251,7 +251,7 @@ struct Exec {
     std::vector<std::pair<std::string, double>> kev_tag;   // family, work of each pair
     std::map<std::string, KernelStat> kstats;
     DevBuf split_cols, split_colexp;   // split precision: column slices of the current group
-    DevBuf split_error;                // device flag set by a timed-out wait
+    DevBuf split_error;                // bytes 0-15: flags set by a timed-out wait; 16-23: split work counter
     // Page-locked staging for the small uploads of one call (kernel argument
     // arrays), so that they never wait for the stream: reset at the start of
     // each call on this execution state (the previous call has completed).

@@ -80,7 +80,11 @@ struct SplitParams {
     int ngroups;
     int64_t nwork;          // sum of the groups' work items
     unsigned int* error;    // set on a timed-out wait
+    unsigned long long* next;  // work items handed out after each CTA's first; zero at launch
 };
+
+// Work items passed from a CTA's producer to its MMA and epilogue roles.
+constexpr int kSplitItems = 8;
 
 // Group of work item w, advanced from the group of the CTA's previous item
 // (a CTA's items increase, so each role walks the groups once).
@@ -367,6 +371,8 @@ struct SplitSmem {
     alignas(8) uint64_t full[kSt];
     uint64_t empty[kSt];
     uint64_t tmem_full[2], tmem_empty[2], drain;
+    uint64_t item_full[kSplitItems], item_empty[kSplitItems];
+    int64_t items[kSplitItems];
     uint32_t tmem;
     int failed;
 };
@@ -374,10 +380,15 @@ template <int NE>
 constexpr size_t split_smem_bytes() { return sizeof(SplitSmem<NE>) + 1024; }
 
 // Persistent, warp-specialised kernel; one CTA per SM holds all 512 TMEM
-// columns.  Work item w = (row tile w % ntp, element unit w / ntp), so the
-// CTAs working at the same time share element units (B is read from L2 once
-// per unit).  Empty units (past the end of a short tile) are skipped by every
-// role alike.
+// columns.  Work item w = (row tile w % ntp, element unit w / ntp).  Each
+// CTA's first item is its index; later ones come from a global counter, so
+// the items are taken in order and the CTAs working at the same time always
+// hold neighbouring items: they share element units (B is read from L2 once
+// per unit), and the 32-byte sectors that neighbouring row tiles' mirrored
+// stores share are completed while they are still in L2.  (Handed out
+// round-robin, the CTAs drift apart over a long launch.)  The producer skips
+// empty units (past the end of a short tile) and passes each item to the MMA
+// and epilogue roles through a ring of kSplitItems slots; -1 ends the CTA.
 //   warp 0 (one thread): bulk copies of each K step into the stage ring;
 //   warp 1 (one thread): MMAs; owns the TMEM allocation;
 //   warps 2-17: epilogue; warp w reads TMEM lanes 32(w%4) .. 32(w%4)+31 and
@@ -414,6 +425,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
             mbar_init(&sm.tmem_full[b], 1);
             mbar_init(&sm.tmem_empty[b], NE / 4);  // epilogue warps with columns
         }
+        for (int k = 0; k < kSplitItems; k++) {
+            mbar_init(&sm.item_full[k], 1);
+            mbar_init(&sm.item_empty[k], 1 + NE / 4);  // MMA issuer and epilogue warps
+        }
         mbar_init(&sm.drain, 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -431,15 +446,33 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
         uint32_t used = 0, last_parity = 0;  // per-stage bit sets
         bool ok = true;
         int gi = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
-            gi = split_group_of(p, gi, w);
+        int64_t w = blockIdx.x;
+        for (uint32_t k = 0; ok; k++) {
+            // The next non-empty work item, or -1 at the end.
+            int64_t item = -1;
+            while (w < p.nwork) {
+                gi = split_group_of(p, gi, w);
+                if (split_unit<NE>(p.g[gi].tiles, (w - p.g[gi].w0) / p.g[gi].ntp).ne > 0) {
+                    item = w;
+                    break;
+                }
+                w = (int64_t)atomicAdd(p.next, 1ull) + gridDim.x;
+            }
+            const int slot = (int)(k % kSplitItems);
+            if (!mbar_wait(&sm.item_empty[slot], ((k / kSplitItems) & 1) ^ 1, failed)) {
+                ok = false;
+                break;
+            }
+            sm.items[slot] = item;
+            mbar_arrive(&sm.item_full[slot]);
+            if (item < 0)
+                break;
+            w = (int64_t)atomicAdd(p.next, 1ull) + gridDim.x;  // in flight during this item's copies
             const SplitGroup& G = p.g[gi];
-            const int64_t v = w - G.w0;
+            const int64_t v = item - G.w0;
             const int pt = (int)(v % G.ntp);
             const int64_t u = v / G.ntp;
             const Tile unit = split_unit<NE>(G.tiles, u);
-            if (unit.ne <= 0)
-                continue;
             const int8_t* srcA = G.A + ((int64_t)unit.orient * G.ntp + pt) * G.nk * kABytes;
             const int8_t* srcB = G.B + u * G.nk * kBBytes;
             const int nk = G.nk;
@@ -476,11 +509,18 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
         bool ok = true;
         int64_t i = 0;  // units processed by this CTA
         int gi = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork && ok; w += gridDim.x) {
+        for (uint32_t k = 0; ok; k++) {
+            const int slot = (int)(k % kSplitItems);
+            if (!mbar_wait(&sm.item_full[slot], (k / kSplitItems) & 1, failed)) {
+                ok = false;
+                break;
+            }
+            const int64_t w = sm.items[slot];
+            mbar_arrive(&sm.item_empty[slot]);
+            if (w < 0)
+                break;
             gi = split_group_of(p, gi, w);
             const SplitGroup& G = p.g[gi];
-            if (split_unit<NE>(G.tiles, (w - G.w0) / G.ntp).ne <= 0)
-                continue;
             const int nk = G.nk;
             const int buf = (int)(i % Sh::kBufs);
             const int64_t use = i / Sh::kBufs;
@@ -540,15 +580,25 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         int64_t i = 0;
         int gi = 0;
-        for (int64_t w = blockIdx.x; w < p.nwork && c0 < NE; w += gridDim.x) {
+        for (uint32_t k = 0; c0 < NE; k++) {
+            const int slot = (int)(k % kSplitItems);
+            if (!mbar_wait(&sm.item_full[slot], (k / kSplitItems) & 1, failed)) {
+                *failed = 1;
+                atomicOr(p.error, 1u);
+                break;
+            }
+            const int64_t w = sm.items[slot];
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(&sm.item_empty[slot]);
+            if (w < 0)
+                break;
             gi = split_group_of(p, gi, w);
             const SplitGroup& G = p.g[gi];
             const int64_t v = w - G.w0;
             const int pt = (int)(v % G.ntp);
             const int64_t u = v / G.ntp;
             const Tile unit = split_unit<NE>(G.tiles, u);
-            if (unit.ne <= 0)
-                continue;
             const int buf = (int)(i % Sh::kBufs);
             if (!mbar_wait(&sm.tmem_full[buf], (uint32_t)((i / Sh::kBufs) & 1), failed)) {
                 *failed = 1;
