@@ -12,7 +12,9 @@ value  : device throughput, inputs already in HBM (CUDA events on the engine's
 e2e    : the same metric through sparselizard's own API with the drop-in:
          warm generate() + A() + b() on the resident problem (host lowering,
          DOF addresses, uploads, assembly on the resident pattern and the
-         download of the CSR arrays into the rawmat that PETSc borrows).
+         download of the CSR values into the new rawmat that PETSc borrows;
+         the rawmat shares the row pointers and column indices that an earlier
+         download of the same pattern brought to the host).
 --impl reference times stock sparselizard (built from its sources, CPU, all
 host threads) on a bounded sample of the same workload (the same config).
 
@@ -624,8 +626,9 @@ def run_ours(args, spec):
            "h2d_bytes_per_step": int((h2d2.value - h2d1.value) / e2e_reps),
            "d2h_bytes_per_step": int((d2h2.value - d2h1.value) / e2e_reps),
            "what": "warm generate()+A()+b() through sparselizard's API with the drop-in: host lowering and DOF "
-                   "addresses, uploads, assembly on the resident pattern, download of the CSR arrays into the rawmat "
-                   "(one untimed warm repetition first)"}
+                   "addresses, uploads, assembly on the resident pattern, download of the CSR values into a new "
+                   "rawmat, which shares the row pointers and column indices downloaded for the same pattern before "
+                   "(one untimed warm repetition first; first_assembly downloads all CSR arrays)"}
     lib.slz_bench_release()
     del flush
     torch.cuda.empty_cache()

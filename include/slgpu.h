@@ -239,6 +239,13 @@ int slgpu_matrix_download(slgpu_ctx* ctx, int handle, int32_t* Arows, int32_t* A
                           int32_t* Drows, int32_t* Dcols, double* Dvals);
 /* Copies only the values (pattern unchanged since the last download). */
 int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, double* Dvals);
+/* Serial number of the CSR pattern that the matrix's last process() used (0
+ * before the first).  Every pattern the context builds gets a new serial, so
+ * two process() calls that report the same serial produced the same
+ * Arows/Acols/Drows/Dcols (rawmat.cpp:127-299 for the same addresses and
+ * constraints): a caller that kept the host copies of those arrays can
+ * download the values alone. */
+int slgpu_matrix_pattern_serial(slgpu_ctx* ctx, int handle, uint64_t* serial);
 /* Device pointers to the processed CSR arrays (valid until the next process/destroy). */
 int slgpu_matrix_device_csr(slgpu_ctx* ctx, int handle, const int32_t** Arows, const int32_t** Acols, const double** Avals,
                             const int32_t** Drows, const int32_t** Dcols, const double** Dvals);

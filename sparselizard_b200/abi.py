@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint8, c_uint, c_size_t, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint8, c_uint, c_uint64, c_size_t, c_void_p
 
 import numpy as np
 
@@ -127,6 +127,7 @@ SIGNATURES = {
     "slgpu_matrix_download": (c_int, [c_void_p, c_int, POINTER(c_int32), POINTER(c_int32), POINTER(c_double),
                                       POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),
     "slgpu_matrix_download_values": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double)]),
+    "slgpu_matrix_pattern_serial": (c_int, [c_void_p, c_int, POINTER(c_uint64)]),
     "slgpu_matrix_device_csr": (c_int, [c_void_p, c_int] + [POINTER(c_void_p)] * 6),
     "slgpu_matrix_eliminate": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "slgpu_rhs_assemble": (c_int, [c_void_p, POINTER(Group), c_int64, c_int, POINTER(c_double)]),

@@ -11,6 +11,26 @@
 #include <cstdint>
 #include <vector>
 
+namespace {
+
+// Row pointers and column indices of A and D from the last full download,
+// with the engine pattern they came from.  indexmat storage is reference
+// counted, so the rawmats filled from them share these arrays (PETSc only
+// reads them: MatCreateSeqAIJWithArrays borrows them as the structure of a
+// matrix whose nonzeros cannot change).  A process() on the same pattern --
+// the same serial means the same addresses and constraints -- takes them
+// over and downloads the values alone.
+struct StructureCache {
+    uint64_t serial = 0;
+    long long nA = -1, nnzA = -1, nnzD = -1;
+    indexmat Arows, Acols, Drows, Dcols;
+};
+StructureCache g_structure;
+
+}  // namespace
+
+void slgpu_adapter::release_structure_cache(void) { g_structure = StructureCache(); }
+
 rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr)
 {
     mydofmanager = dofmngr;
@@ -84,15 +104,36 @@ void rawmat::process(std::vector<bool>& isconstrained)
     nnzA = info.nnzA;
     nnzD = info.nnzD;
 
-    Arows = indexmat(Ainds.count() + 1, 1);
-    Acols = indexmat(nnzA, 1);
+    uint64_t serial = 0;
+    slgpu_adapter::check(slgpu_matrix_pattern_serial(ctx, handle, &serial), "slgpu_matrix_pattern_serial");
     Avals = densemat(nnzA, 1);
-    Drows = indexmat(Ainds.count() + 1, 1);
-    Dcols = indexmat(nnzD, 1);
     Dvals = densemat(nnzD, 1);
-    slgpu_adapter::check(slgpu_matrix_download(ctx, handle, Arows.getvalues(), Acols.getvalues(), Avals.getvalues(), Drows.getvalues(),
-                                               Dcols.getvalues(), Dvals.getvalues()),
-                         "slgpu_matrix_download");
+    StructureCache& sc = g_structure;
+    if (serial != 0 && sc.serial == serial && sc.nA == Ainds.count() && sc.nnzA == nnzA && sc.nnzD == nnzD) {
+        Arows = sc.Arows;
+        Acols = sc.Acols;
+        Drows = sc.Drows;
+        Dcols = sc.Dcols;
+        slgpu_adapter::check(slgpu_matrix_download_values(ctx, handle, Avals.getvalues(), Dvals.getvalues()),
+                             "slgpu_matrix_download_values");
+    } else {
+        Arows = indexmat(Ainds.count() + 1, 1);
+        Acols = indexmat(nnzA, 1);
+        Drows = indexmat(Ainds.count() + 1, 1);
+        Dcols = indexmat(nnzD, 1);
+        slgpu_adapter::check(slgpu_matrix_download(ctx, handle, Arows.getvalues(), Acols.getvalues(), Avals.getvalues(),
+                                                   Drows.getvalues(), Dcols.getvalues(), Dvals.getvalues()),
+                             "slgpu_matrix_download");
+        sc = StructureCache();
+        sc.serial = serial;
+        sc.nA = Ainds.count();
+        sc.nnzA = nnzA;
+        sc.nnzD = nnzD;
+        sc.Arows = Arows;
+        sc.Acols = Acols;
+        sc.Drows = Drows;
+        sc.Dcols = Dcols;
+    }
 
     MatCreateSeqAIJWithArrays(PETSC_COMM_SELF, Ainds.count(), Ainds.count(), Arows.getvalues(), Acols.getvalues(), Avals.getvalues(), &Amat);
     MatAssemblyBegin(Amat, MAT_FINAL_ASSEMBLY);

@@ -53,6 +53,12 @@ void set_last_processed(rawmat* m);
 // is being processed (contribution.cpp); called by rawmat::process.
 void clear_address_cache(void);
 
+// rawmat::process keeps the host CSR structure (Arows, Acols, Drows, Dcols)
+// of the last pattern it downloaded and shares it with the next rawmat
+// processed on the same engine pattern, which then downloads only values.
+// This frees the kept copy (the rawmats using it keep theirs).
+void release_structure_cache(void);
+
 // Integral of a scalar expression over a physical region at a Gauss order
 // (what expression::integrate computes, src/expression/expression.cpp:808-889)
 // on the GPU: the expression is lowered to a coefficient program, evaluated

@@ -945,6 +945,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     auto P = std::make_shared<Pattern>();
     P->key[0] = key0;
     P->key[1] = key1;
+    P->serial = ++ctx->pattern_serial;
     P->ndofs = M.ndofs;
     const int64_t ncoo = segs.empty() ? 0 : segs.back().coo_base + segs.back().count;
     P->ncoo = ncoo;
@@ -3251,6 +3252,16 @@ int slgpu_matrix_download_values(slgpu_ctx* ctx, int handle, double* Avals, doub
         d2h(ctx, Avals, M.Avals.as<void>(), P.nnzA * 8);
         d2h(ctx, Dvals, M.Dvals.as<void>(), P.nnzD * 8);
         cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync download");
+    });
+}
+
+int slgpu_matrix_pattern_serial(slgpu_ctx* ctx, int handle, uint64_t* serial)
+{
+    return guarded(ctx, [&] {
+        if (serial == nullptr)
+            fail(SLGPU_E_ARG, "null serial");
+        Matrix& M = get_matrix(ctx, handle);
+        *serial = M.pattern ? M.pattern->serial : 0;
     });
 }
 

@@ -166,6 +166,7 @@ struct FragmentDev {
 // the per-row incidence lists and the slot map.
 struct Pattern {
     uint64_t key[2] = {0, 0};
+    uint64_t serial = 0;   // unique per pattern built by the context
     int64_t ndofs = 0, nA = 0, nD = 0, nnzA = 0, nnzD = 0, ncoo = 0, nvalid = 0, ninc = 0;
     int lmax = 0;          // longest row (A and D entries)
     int row_kernel = -1;   // CSR value kernel chosen by timing: 0 streaming warps, 1 warp per row, -1 not yet
@@ -291,6 +292,7 @@ struct Ctx {
     int next_handle = 1;
     std::vector<std::shared_ptr<Pattern>> patterns;  // resident pattern cache
     uint64_t use_clock = 0;
+    uint64_t pattern_serial = 0;  // serials handed to the patterns built so far
     DevBuf scratch;  // reusable temporary storage (sort, scans)
     DevBuf hash_acc;
     std::vector<uint8_t> constr_host;  // last constraint array seen by process()
