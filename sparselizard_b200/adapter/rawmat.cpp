@@ -27,9 +27,62 @@ struct StructureCache {
 };
 StructureCache g_structure;
 
+// Value arrays of A lent to rawmats and taken back when a rawmat is destroyed
+// or processed again (only the rawmat uses its Avals; PETSc borrows the
+// pointer until the rawmat's destructor).  A buffer that comes back keeps its
+// pages, so the next download into it does not fault them in again: on a
+// fresh array the first touches, not the link, bound the copy.  Arrays of at
+// least kPooledValues entries are lent; at most kPoolBuffers are kept.
+struct ValueBuffer {
+    densemat storage;
+    long long capacity = 0;
+    const rawmat* user = nullptr;
+};
+constexpr long long kPooledValues = (long long)1 << 21;
+constexpr size_t kPoolBuffers = 2;
+std::vector<ValueBuffer> g_values;
+
+densemat lend_values(const rawmat* user, long long n)
+{
+    if (n < kPooledValues)
+        return densemat(n, 1);
+    for (ValueBuffer& b : g_values)
+        if (b.user == nullptr && b.capacity >= n) {
+            b.user = user;
+            return b.storage.getresized(n, 1);
+        }
+    // A free buffer that is too small is replaced; otherwise one is added
+    // while below the limit.
+    for (ValueBuffer& b : g_values)
+        if (b.user == nullptr) {
+            b = ValueBuffer{densemat(n, 1), n, user};
+            return b.storage;
+        }
+    if (g_values.size() < kPoolBuffers) {
+        g_values.push_back(ValueBuffer{densemat(n, 1), n, user});
+        return g_values.back().storage;
+    }
+    return densemat(n, 1);
+}
+
+void return_values(const rawmat* user)
+{
+    for (ValueBuffer& b : g_values)
+        if (b.user == user)
+            b.user = nullptr;
+}
+
 }  // namespace
 
-void slgpu_adapter::release_structure_cache(void) { g_structure = StructureCache(); }
+void slgpu_adapter::release_structure_cache(void)
+{
+    g_structure = StructureCache();
+    std::vector<ValueBuffer> kept;
+    for (ValueBuffer& b : g_values)
+        if (b.user != nullptr)
+            kept.push_back(b);
+    g_values = kept;
+}
 
 rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr)
 {
@@ -50,6 +103,7 @@ rawmat::rawmat(std::shared_ptr<dofmanager> dofmngr, Mat inA, Mat inD, indexmat i
 rawmat::~rawmat(void)
 {
     slgpu_adapter::forget_matrix(this);
+    return_values(this);
     // PETSc objects may only be destroyed before PetscFinalize.
     PetscBool ispetscinitialized;
     PetscInitialized(&ispetscinitialized);
@@ -106,7 +160,8 @@ void rawmat::process(std::vector<bool>& isconstrained)
 
     uint64_t serial = 0;
     slgpu_adapter::check(slgpu_matrix_pattern_serial(ctx, handle, &serial), "slgpu_matrix_pattern_serial");
-    Avals = densemat(nnzA, 1);
+    return_values(this);
+    Avals = lend_values(this, nnzA);
     Dvals = densemat(nnzD, 1);
     StructureCache& sc = g_structure;
     if (serial != 0 && sc.serial == serial && sc.nA == Ainds.count() && sc.nnzA == nnzA && sc.nnzD == nnzD) {

