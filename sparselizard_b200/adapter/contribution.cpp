@@ -26,8 +26,10 @@
 #include "opharmonic.h"
 #include "slgpu_adapter.h"
 
+#include <algorithm>
 #include <cmath>
 #include <map>
+#include <memory>
 #include <tuple>
 #include <sstream>
 #include <typeinfo>
@@ -95,49 +97,75 @@ template struct MemberAccess<HarmDest, &opharmonic::mydestharms>;
 template struct MemberAccess<HarmFft, &opharmonic::mynumfftharms>;
 
 // DOF addresses of one (dofmanager, field, order, element type, element list,
-// region), shared by the contributions of one assembly: the slices of a
-// vector field's formulation ask for the same test-function and dof
-// addresses many times (elasticity: 18 requests, 6 distinct tables).  Every
-// hit is checked against a fresh lookup of the list's first and last
-// elements; rawmat::process and the end of a right-hand-side contribution
-// clear the cache (slgpu_adapter::clear_address_cache).
+// region), kept across assemblies: the slices of a vector field's formulation
+// ask for the same test-function and dof addresses many times (elasticity: 18
+// requests, 6 distinct tables), and a repeated generate() asks for them again.
+// The addresses depend on the dofmanager's numbering, which changes only when
+// the mesh number changes or a field is added (dofmanager.cpp:4-33, ndofs
+// changes then), and on the field's interpolation order on each disjoint
+// region.  An entry therefore holds the dofmanager and field themselves (weak
+// references: a destroyed object never matches a new one at the same address),
+// its key holds the mesh number, ndofs, the element list's hash and the
+// field's orders, and every hit is still checked against a fresh lookup of 64
+// elements spread over the list.
 struct AddressKey {
     const void* dm;
     const void* field;
     int order, elemtype, physreg, meshnumber;
     long long ndofs;
     size_t n;
-    unsigned long long hash;
+    unsigned long long hash, orders;
     bool operator<(const AddressKey& o) const
     {
-        return std::tie(dm, field, order, elemtype, physreg, meshnumber, ndofs, n, hash) <
-               std::tie(o.dm, o.field, o.order, o.elemtype, o.physreg, o.meshnumber, o.ndofs, o.n, o.hash);
+        return std::tie(dm, field, order, elemtype, physreg, meshnumber, ndofs, n, hash, orders) <
+               std::tie(o.dm, o.field, o.order, o.elemtype, o.physreg, o.meshnumber, o.ndofs, o.n, o.hash, o.orders);
     }
 };
-std::map<AddressKey, indexmat> g_address_cache;
+struct AddressEntry {
+    std::weak_ptr<dofmanager> dm;
+    std::weak_ptr<rawfield> field;
+    indexmat addresses;
+};
+std::map<AddressKey, AddressEntry> g_address_cache;
+constexpr size_t kAddressEntries = 64;
+constexpr int kAddressProbe = 64;
 
 indexmat cached_addresses(const std::shared_ptr<dofmanager>& dm, const std::shared_ptr<rawfield>& f, int order, int elemtype,
                           std::vector<int>& elems, int physreg)
 {
     unsigned long long h = 1469598103934665603ull;
     for (int e : elems) h = (h ^ (unsigned long long)(unsigned)e) * 1099511628211ull;
+    unsigned long long orders = 1469598103934665603ull;
+    for (int d : universe::getrawmesh()->getphysicalregions()->get(physreg)->getdisjointregions(-1))
+        orders = (orders ^ ((unsigned long long)(unsigned)d << 8 | (unsigned)f->getinterpolationorder(d))) * 1099511628211ull;
     const AddressKey key{dm.get(), f.get(), order, elemtype, physreg, universe::getrawmesh()->getmeshnumber(), dm->countdofs(),
-                         elems.size(), h};
+                         elems.size(), h, orders};
     auto it = g_address_cache.find(key);
     if (it != g_address_cache.end() && !elems.empty()) {
-        std::vector<int> probe{elems.front(), elems.back()};
-        indexmat fresh = dm->getaddresses(f, order, elemtype, probe, physreg);
-        indexmat c = it->second;
-        const long long rows = c.countrows(), n = c.countcolumns();
-        bool same = fresh.countrows() == rows;
-        for (long long r = 0; same && r < rows; r++)
-            same = fresh.getvalues()[r * 2] == c.getvalues()[r * n] && fresh.getvalues()[r * 2 + 1] == c.getvalues()[r * n + n - 1];
+        bool same = it->second.dm.lock() == dm && it->second.field.lock() == f;
+        if (same) {
+            const long long n = (long long)elems.size(), np = std::min<long long>(n, kAddressProbe);
+            std::vector<int> probe(np);
+            std::vector<long long> col(np);
+            for (long long i = 0; i < np; i++) {
+                col[i] = np > 1 ? i * (n - 1) / (np - 1) : 0;
+                probe[i] = elems[col[i]];
+            }
+            indexmat fresh = dm->getaddresses(f, order, elemtype, probe, physreg);
+            indexmat c = it->second.addresses;
+            const long long rows = c.countrows();
+            same = fresh.countrows() == rows && c.countcolumns() == n;
+            for (long long r = 0; same && r < rows; r++)
+                for (long long i = 0; same && i < np; i++) same = fresh.getvalues()[r * np + i] == c.getvalues()[r * n + col[i]];
+        }
         if (same)
-            return c;
+            return it->second.addresses;
         g_address_cache.erase(it);
     }
     indexmat a = dm->getaddresses(f, order, elemtype, elems, physreg);
-    g_address_cache[key] = a;
+    if (g_address_cache.size() >= kAddressEntries)
+        g_address_cache.clear();
+    g_address_cache[key] = AddressEntry{dm, f, a};
     return a;
 }
 
@@ -638,11 +666,6 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
             }
         }
     }
-    // A right-hand side is complete once its contributions are added: the
-    // shared addresses live from the first matrix contribution of an
-    // assembly to its process(), or to the end of a right-hand side.
-    if (doffield == NULL)
-        slgpu_adapter::clear_address_cache();
 }
 
 namespace slgpu_adapter {

@@ -135,7 +135,6 @@ void rawmat::accumulate(indexmat rowadresses, indexmat coladresses, densemat val
 void rawmat::process(std::vector<bool>& isconstrained)
 {
     const long long ndofs = countrows();
-    slgpu_adapter::clear_address_cache();
 
     std::vector<int> renumtolocalindex;
     gentools::findtruefalse(isconstrained, Dinds, Ainds, renumtolocalindex);

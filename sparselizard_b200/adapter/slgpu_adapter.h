@@ -49,8 +49,8 @@ bool record_only(void);
 // Remembers the engine matrix handed to the last rawmat::process call.
 void set_last_processed(rawmat* m);
 
-// Forgets the DOF addresses shared by the contributions of the assembly that
-// is being processed (contribution.cpp); called by rawmat::process.
+// Forgets the DOF addresses kept for the contributions of later assemblies
+// (contribution.cpp).
 void clear_address_cache(void);
 
 // rawmat::process keeps the host CSR structure (Arows, Acols, Drows, Dcols)
