@@ -116,14 +116,72 @@ void DevBuf::release()
     arena_ = false;
 }
 
+// Host -> device copy of a large pageable array on the context's stream:
+// 4 MB chunks through a ring of page-locked blocks.  Up to 8 worker threads
+// (created per call), worker w taking chunks w, w + 8, ... into its two
+// blocks: it waits for the block's previous copy, copies the chunk in, queues
+// the copy to the device and records the block's event.  The source has been
+// read when this returns; the device copies complete in stream order.  (A
+// pageable cudaMemcpyAsync is staged by the driver on the calling thread.)
+static void h2d_pageable(Ctx* ctx, void* dst, const void* src, size_t n)
+{
+    constexpr size_t kChunk = size_t(4) << 20;
+    std::lock_guard<std::mutex> lk(ctx->ul_mu);
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nw = std::max(1, std::min(std::min(hw, 8), Ctx::kUlStages / 2));
+    for (int b = 0; b < 2 * nw; b++) {
+        if (ctx->ul_stage[b] == nullptr)
+            cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&ctx->ul_stage[b]), kChunk, cudaHostAllocDefault), "cudaHostAlloc");
+        if (ctx->ul_ev[b] == nullptr)
+            cuda_check(cudaEventCreateWithFlags(&ctx->ul_ev[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    const size_t nch = (n + kChunk - 1) / kChunk;
+    std::mutex emu;
+    std::string err;
+    std::vector<std::thread> workers;
+    for (int w = 0; w < nw; w++)
+        workers.emplace_back([&, w] {
+            int use = 0;
+            for (size_t i = (size_t)w; i < nch; i += (size_t)nw, use ^= 1) {
+                const int b = 2 * w + use;
+                const size_t off = i * kChunk, len = std::min(kChunk, n - off);
+                cudaError_t e = cudaEventSynchronize(ctx->ul_ev[b]);
+                if (e == cudaSuccess) {
+                    std::memcpy(ctx->ul_stage[b], static_cast<const char*>(src) + off, len);
+                    e = cudaMemcpyAsync(static_cast<char*>(dst) + off, ctx->ul_stage[b], len, cudaMemcpyHostToDevice, ctx->x->stream);
+                }
+                if (e == cudaSuccess)
+                    e = cudaEventRecord(ctx->ul_ev[b], ctx->x->stream);
+                if (e != cudaSuccess) {
+                    std::lock_guard<std::mutex> g(emu);
+                    err = std::string("H2D chunk: ") + cudaGetErrorString(e);
+                    return;
+                }
+            }
+        });
+    for (auto& t : workers) t.join();
+    if (!err.empty())
+        fail(SLGPU_E_CUDA, err);
+}
+
 template <class T>
 static void upload(Ctx* ctx, DevBuf& buf, const T* src, size_t count)
 {
     buf.alloc(ctx, count * sizeof(T));
-    ctx->bytes_h2d += (int64_t)(count * sizeof(T));
-    if (count > 0)
-        cuda_check(cudaMemcpyAsync(buf.as<void>(), src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->x->stream),
-                   "cudaMemcpyAsync H2D");
+    const size_t bytes = count * sizeof(T);
+    ctx->bytes_h2d += (int64_t)bytes;
+    if (count == 0)
+        return;
+    if (bytes >= (size_t(8) << 20) && !ctx->x->capturing) {
+        cudaPointerAttributes a{};
+        const bool pinned = cudaPointerGetAttributes(&a, src) == cudaSuccess && a.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (!pinned) {
+            h2d_pageable(ctx, buf.as<void>(), src, bytes);
+            return;
+        }
+    }
+    cuda_check(cudaMemcpyAsync(buf.as<void>(), src, bytes, cudaMemcpyHostToDevice, ctx->x->stream), "cudaMemcpyAsync H2D");
 }
 
 template <class T>
@@ -244,6 +302,30 @@ static std::vector<Instr> compile_program(const slgpu_group& g, int nterms)
 }
 
 // ------------------------------------------------------------ hashing
+// Hashes of several device arrays (data[i], n[i] entries, salt[i]) into
+// out[2 i], out[2 i + 1], with one read-back.
+static void hash_device_many(Ctx* ctx, const std::vector<const int32_t*>& data, const std::vector<int64_t>& n,
+                             const std::vector<uint64_t>& salt, uint64_t* out)
+{
+    const size_t m = data.size();
+    if (m == 0)
+        return;
+    if (ctx->hash_acc.bytes() < 2 * m * sizeof(unsigned long long))
+        ctx->hash_acc.alloc(ctx, 2 * m * sizeof(unsigned long long));
+    unsigned long long* acc = ctx->hash_acc.as<unsigned long long>();
+    cuda_check(cudaMemsetAsync(acc, 0, 2 * m * sizeof(unsigned long long), ctx->x->stream), "memset");
+    for (size_t i = 0; i < m; i++)
+        if (n[i] > 0) {
+            unsigned blocks = (unsigned)std::min<int64_t>(148 * 8, grid_for(n[i], 256));
+            k_hash_i32<<<blocks, 256, 0, ctx->x->stream>>>(data[i], n[i], salt[i], acc + 2 * i);
+            cuda_check(cudaGetLastError(), "k_hash_i32");
+        }
+    std::vector<unsigned long long> h(2 * m);
+    cuda_check(cudaMemcpyAsync(h.data(), acc, 2 * m * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->x->stream), "D2H hash");
+    cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync hash");
+    for (size_t i = 0; i < 2 * m; i++) out[i] = h[i];
+}
+
 static void hash_device(Ctx* ctx, const int32_t* data, int64_t n, uint64_t salt, uint64_t out[2])
 {
     if (ctx->hash_acc.empty())
@@ -445,15 +527,28 @@ static GroupDev::Key key_mix(GroupDev::Key k, uint64_t v)
     return {mix64(k.a ^ v), mix64(k.b + (v ^ 0xD6E8FEB86659FD93ull) * 0x9E3779B97F4A7C15ull)};
 }
 
+// Key of an array: four interleaved chains (entry i goes to chain i % 4, so
+// their multiplies overlap), combined at the end with the length.
 static GroupDev::Key key_of(const double* v, size_t n, uint64_t tag)
 {
-    GroupDev::Key k{tag, ~tag};
-    k = key_mix(k, n);
-    for (size_t i = 0; i < n; i++) {
+    GroupDev::Key c[4];
+    for (int j = 0; j < 4; j++) c[j] = GroupDev::Key{tag + (uint64_t)j, ~tag - (uint64_t)j};
+    size_t i = 0;
+    for (; i + 4 <= n; i += 4) {
+        uint64_t w[4];
+        std::memcpy(w, &v[i], 32);
+        c[0] = key_mix(c[0], w[0]);
+        c[1] = key_mix(c[1], w[1]);
+        c[2] = key_mix(c[2], w[2]);
+        c[3] = key_mix(c[3], w[3]);
+    }
+    for (; i < n; i++) {
         uint64_t w;
         std::memcpy(&w, &v[i], 8);
-        k = key_mix(k, w);
+        c[i % 4] = key_mix(c[i % 4], w);
     }
+    GroupDev::Key k = key_mix(GroupDev::Key{tag, ~tag}, n);
+    for (int j = 0; j < 4; j++) k = key_mix(key_mix(k, c[j].a), c[j].b);
     return k;
 }
 
@@ -561,7 +656,18 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
         uint64_t h = mix64((uint64_t)g.mesh ^ (uint64_t)g.elemtype << 8 ^ (uint64_t)g.ngp << 16 ^ (uint64_t)g.ncurvednodes << 32 ^
                            (uint64_t)g.problemdim << 48);
         h = mix64(h ^ (uint64_t)g.nelem ^ (uint64_t)(uint32_t)g.mesh << 40 ^ (uint64_t)(uint32_t)g.elemtype << 56);
-        for (int64_t e = 0; e < g.nelem; e++) h = mix64(h ^ ((uint64_t)(uint32_t)g.elems[e] << 8 | (uint64_t)(uint32_t)g.orient[e] << 40));
+        // Elements and orientations in four interleaved chains (e % 4).
+        auto word = [&](int64_t e) { return (uint64_t)(uint32_t)g.elems[e] << 8 | (uint64_t)(uint32_t)g.orient[e] << 40; };
+        uint64_t c0 = h, c1 = h + 1, c2 = h + 2, c3 = h + 3;
+        int64_t e = 0;
+        for (; e + 4 <= g.nelem; e += 4) {
+            c0 = mix64(c0 ^ word(e));
+            c1 = mix64(c1 ^ word(e + 1));
+            c2 = mix64(c2 ^ word(e + 2));
+            c3 = mix64(c3 ^ word(e + 3));
+        }
+        for (; e < g.nelem; e++) c0 = mix64(c0 ^ word(e) ^ (uint64_t)e);
+        h = mix64(mix64(mix64(mix64(h ^ c0) ^ c1) ^ c2) ^ c3);
         const size_t nl = (size_t)(1 + g.elemdim) * g.ncurvednodes * g.ngp;
         for (size_t k = 0; k < nl; k++) {
             uint64_t w;
@@ -696,19 +802,27 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     upload(ctx, gd->tiles_d, gd->tiles);
     gd->tfaddr.resize(g.ndests);
     gd->dofaddr.resize(g.ndests);
-    uint64_t h0 = 0, h1 = 0;
+    std::vector<const int32_t*> hdata;
+    std::vector<int64_t> hn;
+    std::vector<uint64_t> hsalt;
     for (int d = 0; d < g.ndests; d++) {
         upload(ctx, gd->tfaddr[d], g.dests[d].tfaddr, (size_t)g.ntf * g.nelem);
-        uint64_t h[2];
-        hash_device(ctx, gd->tfaddr[d].as<int32_t>(), (int64_t)g.ntf * g.nelem, 2 * d + 1, h);
-        h0 = mix64(h0 ^ h[0]);
-        h1 = mix64(h1 ^ h[1]);
+        hdata.push_back(gd->tfaddr[d].as<int32_t>());
+        hn.push_back((int64_t)g.ntf * g.nelem);
+        hsalt.push_back(2 * d + 1);
         if (!gd->rhs) {
             upload(ctx, gd->dofaddr[d], g.dests[d].dofaddr, (size_t)g.ndof * g.nelem);
-            hash_device(ctx, gd->dofaddr[d].as<int32_t>(), (int64_t)g.ndof * g.nelem, 2 * d + 2, h);
-            h0 = mix64(h0 ^ h[0]);
-            h1 = mix64(h1 ^ h[1]);
+            hdata.push_back(gd->dofaddr[d].as<int32_t>());
+            hn.push_back((int64_t)g.ndof * g.nelem);
+            hsalt.push_back(2 * d + 2);
         }
+    }
+    std::vector<uint64_t> hh(2 * hdata.size());
+    hash_device_many(ctx, hdata, hn, hsalt, hh.data());
+    uint64_t h0 = 0, h1 = 0;
+    for (size_t i = 0; i < hdata.size(); i++) {
+        h0 = mix64(h0 ^ hh[2 * i]);
+        h1 = mix64(h1 ^ hh[2 * i + 1]);
     }
     gd->addr_hash[0] = mix64(h0 ^ (uint64_t)g.ntf << 40 ^ (uint64_t)g.ndof << 20 ^ (uint64_t)g.nelem);
     gd->addr_hash[1] = mix64(h1 ^ (uint64_t)g.ndests << 32 ^ (uint64_t)gd->rhs);
@@ -2747,6 +2861,12 @@ void slgpu_ctx_destroy(slgpu_ctx* ctx)
             if (ctx->dl_ev[b] != nullptr)
                 cudaEventDestroy(ctx->dl_ev[b]);
         }
+        for (int b = 0; b < Ctx::kUlStages; b++) {
+            if (ctx->ul_stage[b] != nullptr)
+                cudaFreeHost(ctx->ul_stage[b]);
+            if (ctx->ul_ev[b] != nullptr)
+                cudaEventDestroy(ctx->ul_ev[b]);
+        }
         stage_free(ctx->main);
         cudaStreamDestroy(ctx->x->stream);
     }
@@ -3124,10 +3244,10 @@ namespace {
 
 // Device -> host copy on the context's stream.  Page-locked or small
 // destinations: one asynchronous copy (the caller synchronises).  Large
-// pageable ones: 32 MB chunks through a ring of 16 page-locked blocks.  This
-// thread issues the copies (at most 16 in flight) and up to 8 worker threads
+// pageable ones: 16 MB chunks through a ring of 32 page-locked blocks.  This
+// thread issues the copies (at most 32 in flight) and up to 16 worker threads
 // -- created once per call -- copy the landed chunks out, chunk i by worker
-// i % 8, each worker owning two blocks.  The pageable destination, usually
+// i % 16, each worker owning two blocks.  The pageable destination, often
 // freshly allocated and not yet touched, is advised to use huge pages
 // (MADV_HUGEPAGE), so that its first-touch faults come 2 MB at a time.
 void d2h(Ctx* ctx, void* dst, const void* src, size_t n)

@@ -312,6 +312,13 @@ struct Ctx {
     static constexpr int kDlStages = 32;
     char* dl_stage[kDlStages] = {};
     cudaEvent_t dl_ev[kDlStages] = {};
+    // Page-locked blocks (16 MB, two per copy thread) and events of the
+    // pipelined upload of large pageable arrays (group addresses); one upload
+    // at a time.
+    static constexpr int kUlStages = 16;
+    char* ul_stage[kUlStages] = {};
+    cudaEvent_t ul_ev[kUlStages] = {};
+    std::mutex ul_mu;
     // Record-only contexts: right-hand-side groups and their DOF counts.
     std::vector<std::shared_ptr<GroupDev>> rhs_record;
     std::vector<int64_t> rhs_record_ndofs;
