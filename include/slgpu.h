@@ -66,6 +66,14 @@ int64_t slgpu_bytes_in_use(const slgpu_ctx* ctx);
  * far (uploads of meshes, groups, data and constraints; downloads of CSR
  * arrays and values).  No counterpart in the reference (no device there). */
 int slgpu_transfer_bytes(const slgpu_ctx* ctx, int64_t* h2d, int64_t* d2h);
+/* Page-locks [ptr, ptr + bytes) of host memory for the context's device, so
+ * that downloads into it (slgpu_matrix_download*) and uploads from it go
+ * straight over the link instead of through page-locked staging blocks.
+ * Meant for buffers that receive many downloads; locking costs about as much
+ * as touching the pages once.  slgpu_host_unregister(ptr) undoes it, and must
+ * be called before the memory is freed.  No counterpart in the reference. */
+int slgpu_host_register(slgpu_ctx* ctx, void* ptr, size_t bytes);
+int slgpu_host_unregister(slgpu_ctx* ctx, void* ptr);
 /* The tile shapes the first-use tuner picked (one line each: kind, choice,
  * group shape ntf/ndof/ngp) and the CSR value kernel of each resident
  * pattern, as text.  No counterpart in the reference (a single fixed BLAS

@@ -24,6 +24,7 @@ struct StructureCache {
     uint64_t serial = 0;
     long long nA = -1, nnzA = -1, nnzD = -1;
     indexmat Arows, Acols, Drows, Dcols;
+    indexmat Ainds, Dinds;  // the same serial also means the same constraints
 };
 StructureCache g_structure;
 
@@ -31,13 +32,23 @@ StructureCache g_structure;
 // or processed again (only the rawmat uses its Avals; PETSc borrows the
 // pointer until the rawmat's destructor).  A buffer that comes back keeps its
 // pages, so the next download into it does not fault them in again: on a
-// fresh array the first touches, not the link, bound the copy.  Arrays of at
-// least kPooledValues entries are lent; at most kPoolBuffers are kept.
+// fresh array the first touches, not the link, bound the copy.  The second
+// time a buffer is lent it is page-locked (its pages are mapped by then), so
+// that downloads go straight into it over the link.  Arrays of at least
+// kPooledValues entries are lent; at most kPoolBuffers are kept.
 struct ValueBuffer {
     densemat storage;
     long long capacity = 0;
     const rawmat* user = nullptr;
+    bool locked = false;
 };
+
+void drop_buffer(ValueBuffer& b)
+{
+    if (b.locked)
+        slgpu_host_unregister(slgpu_adapter::context(), b.storage.getvalues());
+    b = ValueBuffer();
+}
 constexpr long long kPooledValues = (long long)1 << 21;
 constexpr size_t kPoolBuffers = 2;
 std::vector<ValueBuffer> g_values;
@@ -49,17 +60,21 @@ densemat lend_values(const rawmat* user, long long n)
     for (ValueBuffer& b : g_values)
         if (b.user == nullptr && b.capacity >= n) {
             b.user = user;
+            if (!b.locked)
+                b.locked = slgpu_host_register(slgpu_adapter::context(), b.storage.getvalues(), (size_t)b.capacity * sizeof(double)) ==
+                           SLGPU_OK;
             return b.storage.getresized(n, 1);
         }
     // A free buffer that is too small is replaced; otherwise one is added
     // while below the limit.
     for (ValueBuffer& b : g_values)
         if (b.user == nullptr) {
-            b = ValueBuffer{densemat(n, 1), n, user};
+            drop_buffer(b);
+            b = ValueBuffer{densemat(n, 1), n, user, false};
             return b.storage;
         }
     if (g_values.size() < kPoolBuffers) {
-        g_values.push_back(ValueBuffer{densemat(n, 1), n, user});
+        g_values.push_back(ValueBuffer{densemat(n, 1), n, user, false});
         return g_values.back().storage;
     }
     return densemat(n, 1);
@@ -78,9 +93,12 @@ void slgpu_adapter::release_structure_cache(void)
 {
     g_structure = StructureCache();
     std::vector<ValueBuffer> kept;
-    for (ValueBuffer& b : g_values)
+    for (ValueBuffer& b : g_values) {
         if (b.user != nullptr)
             kept.push_back(b);
+        else
+            drop_buffer(b);
+    }
     g_values = kept;
 }
 
@@ -136,9 +154,6 @@ void rawmat::process(std::vector<bool>& isconstrained)
 {
     const long long ndofs = countrows();
 
-    std::vector<int> renumtolocalindex;
-    gentools::findtruefalse(isconstrained, Dinds, Ainds, renumtolocalindex);
-
     slgpu_ctx* ctx = slgpu_adapter::context();
     int handle = slgpu_adapter::matrix_handle(this, ndofs);
     for (size_t i = 0; i < accumulatedvals.size(); i++) {
@@ -149,6 +164,7 @@ void rawmat::process(std::vector<bool>& isconstrained)
                              "slgpu_matrix_add_fragment");
     }
     std::vector<uint8_t> constr((size_t)ndofs);
+#pragma omp parallel for schedule(static) if (ndofs > (1 << 16))
     for (long long i = 0; i < ndofs; i++) constr[i] = isconstrained[i] ? 1 : 0;
 
     slgpu_csr_info info{};
@@ -163,7 +179,9 @@ void rawmat::process(std::vector<bool>& isconstrained)
     Avals = lend_values(this, nnzA);
     Dvals = densemat(nnzD, 1);
     StructureCache& sc = g_structure;
-    if (serial != 0 && sc.serial == serial && sc.nA == Ainds.count() && sc.nnzA == nnzA && sc.nnzD == nnzD) {
+    if (serial != 0 && sc.serial == serial && sc.nA == info.nA && sc.nnzA == nnzA && sc.nnzD == nnzD) {
+        Ainds = sc.Ainds;
+        Dinds = sc.Dinds;
         Arows = sc.Arows;
         Acols = sc.Acols;
         Drows = sc.Drows;
@@ -171,6 +189,8 @@ void rawmat::process(std::vector<bool>& isconstrained)
         slgpu_adapter::check(slgpu_matrix_download_values(ctx, handle, Avals.getvalues(), Dvals.getvalues()),
                              "slgpu_matrix_download_values");
     } else {
+        std::vector<int> renumtolocalindex;
+        gentools::findtruefalse(isconstrained, Dinds, Ainds, renumtolocalindex);
         Arows = indexmat(Ainds.count() + 1, 1);
         Acols = indexmat(nnzA, 1);
         Drows = indexmat(Ainds.count() + 1, 1);
@@ -187,6 +207,8 @@ void rawmat::process(std::vector<bool>& isconstrained)
         sc.Acols = Acols;
         sc.Drows = Drows;
         sc.Dcols = Dcols;
+        sc.Ainds = Ainds;
+        sc.Dinds = Dinds;
     }
 
     MatCreateSeqAIJWithArrays(PETSC_COMM_SELF, Ainds.count(), Ainds.count(), Arows.getvalues(), Acols.getvalues(), Avals.getvalues(), &Amat);

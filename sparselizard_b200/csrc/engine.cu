@@ -2911,6 +2911,28 @@ int slgpu_transfer_bytes(const slgpu_ctx* ctx, int64_t* h2d, int64_t* d2h)
     return SLGPU_OK;
 }
 
+int slgpu_host_register(slgpu_ctx* ctx, void* ptr, size_t bytes)
+{
+    return guarded(ctx, [&] {
+        if (ptr == nullptr || bytes == 0)
+            fail(SLGPU_E_ARG, "empty host range");
+        if (ctx->record_only)
+            fail(SLGPU_E_NODEVICE, "record-only context");
+        cuda_check(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault), "cudaHostRegister");
+    });
+}
+
+int slgpu_host_unregister(slgpu_ctx* ctx, void* ptr)
+{
+    return guarded(ctx, [&] {
+        if (ptr == nullptr)
+            fail(SLGPU_E_ARG, "null host pointer");
+        if (ctx->record_only)
+            fail(SLGPU_E_NODEVICE, "record-only context");
+        cuda_check(cudaHostUnregister(ptr), "cudaHostUnregister");
+    });
+}
+
 int slgpu_mesh_set_nodes(slgpu_ctx* ctx, int mesh, int64_t nnodes, const double* xyz)
 {
     return guarded(ctx, [&] {
