@@ -200,6 +200,15 @@ int slgpu_matrix_destroy(slgpu_ctx* ctx, int handle);
 int slgpu_matrix_clone(slgpu_ctx* ctx, int handle, int* new_handle);
 /* Adds a copy of `g`; returns its group index in *index (may be NULL). */
 int slgpu_matrix_add_group(slgpu_ctx* ctx, int handle, const slgpu_group* g, int* index);
+/* With `enable`, a destination address array (tfaddr or dofaddr) whose host
+ * pointer and length equal one given to an earlier slgpu_matrix_add_group of
+ * this matrix since its last process() is taken to hold the same values: its
+ * device copy and hash are reused instead of uploaded again.  The caller then
+ * keeps such arrays unchanged, and alive, until process().  The slices of a
+ * vector field's formulation pass the same address arrays many times
+ * (dofmanager::getaddresses per component, src/formulation/dofmanager.cpp:846);
+ * off by default. */
+int slgpu_matrix_share_addresses(slgpu_ctx* ctx, int handle, int enable);
 /* Raw fragment as stored by rawmat::accumulate (src/formulation/rawmat.cpp:57-65):
  * rows [ntr][nc], cols [ndr][nc], vals [nr][nc]; row r of vals uses rows[r/ndr]
  * and cols[r%ndr] when ntr or ndr differ from nr, else rows[r] and cols[r]. */

@@ -129,6 +129,7 @@ SIGNATURES = {
     "slgpu_matrix_download_values": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double)]),
     "slgpu_matrix_pattern_serial": (c_int, [c_void_p, c_int, POINTER(c_uint64)]),
     "slgpu_host_register": (c_int, [c_void_p, c_void_p, c_size_t]),
+    "slgpu_matrix_share_addresses": (c_int, [c_void_p, c_int, c_int]),
     "slgpu_host_unregister": (c_int, [c_void_p, c_void_p]),
     "slgpu_matrix_device_csr": (c_int, [c_void_p, c_int] + [POINTER(c_void_p)] * 6),
     "slgpu_matrix_eliminate": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),

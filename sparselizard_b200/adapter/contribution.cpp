@@ -653,6 +653,7 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
 
             if (doffield != NULL) {
                 int handle = slgpu_adapter::matrix_handle(mymat.get(), ndofs);
+                for (const indexmat& a : addrkeep) slgpu_adapter::keep_addresses(mymat.get(), a);
                 slgpu_adapter::check(slgpu_matrix_add_group(ctx, handle, &g, nullptr), "slgpu_matrix_add_group");
             } else {
                 // Right-hand side: b[addr] += -(element vectors), as

@@ -170,6 +170,7 @@ void rawmat::process(std::vector<bool>& isconstrained)
     slgpu_csr_info info{};
     slgpu_adapter::set_last_processed(this);
     slgpu_adapter::check(slgpu_matrix_process(ctx, handle, constr.data(), slgpu_adapter::precision(), &info), "slgpu_matrix_process");
+    slgpu_adapter::addresses_processed(this);
     nnzA = info.nnzA;
     nnzD = info.nnzD;
 

@@ -25,6 +25,11 @@ int g_last_handle = 0;
 
 struct MatEntry {
     int handle = 0;
+    // Address arrays given to the engine matrix since its last process(): the
+    // engine reuses the device copy of an array it has seen before (same host
+    // pointer and length), so none of them may be freed, and its address
+    // reused for other values, before process().
+    std::vector<indexmat> addresses;
     ~MatEntry()
     {
         if (handle != 0 && g_ctx != nullptr)
@@ -172,6 +177,7 @@ int matrix_handle(rawmat* m, long long ndofs)
     if (it == g_mats.end()) {
         auto e = std::make_shared<MatEntry>();
         check(slgpu_matrix_create(ctx, ndofs, &e->handle), "slgpu_matrix_create");
+        check(slgpu_matrix_share_addresses(ctx, e->handle, 1), "slgpu_matrix_share_addresses");
         g_mats[m] = e;
         return e->handle;
     }
@@ -179,9 +185,24 @@ int matrix_handle(rawmat* m, long long ndofs)
         // Shared with another rawmat (extractaccumulated): copy before writing.
         auto e = std::make_shared<MatEntry>();
         check(slgpu_matrix_clone(ctx, it->second->handle, &e->handle), "slgpu_matrix_clone");
+        e->addresses = it->second->addresses;
         it->second = e;
     }
     return it->second->handle;
+}
+
+void keep_addresses(rawmat* m, const indexmat& a)
+{
+    auto it = g_mats.find(m);
+    if (it != g_mats.end())
+        it->second->addresses.push_back(a);
+}
+
+void addresses_processed(rawmat* m)
+{
+    auto it = g_mats.find(m);
+    if (it != g_mats.end())
+        it->second->addresses.clear();
 }
 
 void share_matrix(rawmat* from, rawmat* to)

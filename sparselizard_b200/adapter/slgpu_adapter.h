@@ -8,6 +8,7 @@
 #define SLGPU_ADAPTER_H
 
 #include "slgpu.h"
+#include "indexmat.h"
 
 #include <memory>
 #include <string>
@@ -32,8 +33,14 @@ void check(int status, const char* what);
 // element type `elemtype` are resident; returns the engine mesh id.
 int ensure_mesh(int elemtype);
 
-// Engine matrix handle owned by a rawmat (created on first use).
+// Engine matrix handle owned by a rawmat (created on first use, with address
+// sharing on: slgpu_matrix_share_addresses).
 int matrix_handle(rawmat* m, long long ndofs);
+// Keeps an address array given to the rawmat's engine matrix alive until
+// addresses_processed(m), which rawmat::process calls after
+// slgpu_matrix_process (the engine may reuse its device copy until then).
+void keep_addresses(rawmat* m, const indexmat& a);
+void addresses_processed(rawmat* m);
 // Handle if any (0 = none).
 int find_matrix_handle(rawmat* m);
 // Moves/copies ownership of the engine matrix between rawmats.

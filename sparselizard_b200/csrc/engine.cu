@@ -622,7 +622,8 @@ static void content_keys(const slgpu_group& g, GroupDev& gd)
     for (int t = 0; t < g.nterms; t++) gd.term_keys.push_back({tk[g.terms[t].tf_table], tk[g.terms[t].dof_table], nk[g.terms[t].coef_node]});
 }
 
-static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
+static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g,
+                                            std::map<std::pair<const void*, int64_t>, Matrix::SharedAddresses>* shared = nullptr)
 {
     validate_group(g);
     auto gd = std::make_shared<GroupDev>();
@@ -800,29 +801,57 @@ static std::shared_ptr<GroupDev> make_group(Ctx* ctx, const slgpu_group& g)
     upload(ctx, gd->term_tf_d, gd->term_tf);
     upload(ctx, gd->term_dof_d, gd->term_dof);
     upload(ctx, gd->tiles_d, gd->tiles);
+    // Address arrays: uploaded and hashed by content, or, where the caller
+    // allows it, taken from an earlier group of the same matrix given the same
+    // host array.  The destination's place (salt) is mixed in on the host.
     gd->tfaddr.resize(g.ndests);
     gd->dofaddr.resize(g.ndests);
+    struct Part {
+        std::shared_ptr<DevBuf>* dst;
+        const int32_t* host;
+        int64_t n;
+        uint64_t salt;
+        uint64_t hash[2];
+    };
+    std::vector<Part> parts;
+    for (int d = 0; d < g.ndests; d++) {
+        parts.push_back(Part{&gd->tfaddr[d], g.dests[d].tfaddr, (int64_t)g.ntf * g.nelem, (uint64_t)(2 * d + 1), {0, 0}});
+        if (!gd->rhs)
+            parts.push_back(Part{&gd->dofaddr[d], g.dests[d].dofaddr, (int64_t)g.ndof * g.nelem, (uint64_t)(2 * d + 2), {0, 0}});
+    }
     std::vector<const int32_t*> hdata;
     std::vector<int64_t> hn;
-    std::vector<uint64_t> hsalt;
-    for (int d = 0; d < g.ndests; d++) {
-        upload(ctx, gd->tfaddr[d], g.dests[d].tfaddr, (size_t)g.ntf * g.nelem);
-        hdata.push_back(gd->tfaddr[d].as<int32_t>());
-        hn.push_back((int64_t)g.ntf * g.nelem);
-        hsalt.push_back(2 * d + 1);
-        if (!gd->rhs) {
-            upload(ctx, gd->dofaddr[d], g.dests[d].dofaddr, (size_t)g.ndof * g.nelem);
-            hdata.push_back(gd->dofaddr[d].as<int32_t>());
-            hn.push_back((int64_t)g.ndof * g.nelem);
-            hsalt.push_back(2 * d + 2);
+    std::vector<size_t> hpart;
+    for (size_t i = 0; i < parts.size(); i++) {
+        Part& pt = parts[i];
+        if (shared != nullptr) {
+            auto it = shared->find({pt.host, pt.n});
+            if (it != shared->end()) {
+                *pt.dst = it->second.buf;
+                pt.hash[0] = it->second.hash[0];
+                pt.hash[1] = it->second.hash[1];
+                continue;
+            }
         }
+        *pt.dst = std::make_shared<DevBuf>();
+        upload(ctx, **pt.dst, pt.host, (size_t)pt.n);
+        hdata.push_back((*pt.dst)->as<int32_t>());
+        hn.push_back(pt.n);
+        hpart.push_back(i);
     }
     std::vector<uint64_t> hh(2 * hdata.size());
-    hash_device_many(ctx, hdata, hn, hsalt, hh.data());
+    hash_device_many(ctx, hdata, hn, std::vector<uint64_t>(hdata.size(), 0), hh.data());
+    for (size_t k = 0; k < hpart.size(); k++) {
+        Part& pt = parts[hpart[k]];
+        pt.hash[0] = hh[2 * k];
+        pt.hash[1] = hh[2 * k + 1];
+        if (shared != nullptr)
+            (*shared)[{pt.host, pt.n}] = Matrix::SharedAddresses{*pt.dst, {pt.hash[0], pt.hash[1]}};
+    }
     uint64_t h0 = 0, h1 = 0;
-    for (size_t i = 0; i < hdata.size(); i++) {
-        h0 = mix64(h0 ^ hh[2 * i]);
-        h1 = mix64(h1 ^ hh[2 * i + 1]);
+    for (const Part& pt : parts) {
+        h0 = mix64(h0 ^ mix64(pt.hash[0] ^ pt.salt * 0x9E3779B97F4A7C15ull));
+        h1 = mix64(h1 ^ mix64(pt.hash[1] + pt.salt));
     }
     gd->addr_hash[0] = mix64(h0 ^ (uint64_t)g.ntf << 40 ^ (uint64_t)g.ndof << 20 ^ (uint64_t)g.nelem);
     gd->addr_hash[1] = mix64(h1 ^ (uint64_t)g.ndests << 32 ^ (uint64_t)gd->rhs);
@@ -1085,8 +1114,8 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
     for (auto& g : M.groups) {
         for (int d = 0; d < g->ndests; d++, si++) {
             KeyParams kp{};
-            kp.tfaddr = g->tfaddr[d].as<int32_t>();
-            kp.dofaddr = rhs ? nullptr : g->dofaddr[d].as<int32_t>();
+            kp.tfaddr = g->tfaddr[d]->as<int32_t>();
+            kp.dofaddr = rhs ? nullptr : g->dofaddr[d]->as<int32_t>();
             kp.ndof = g->ndof;
             kp.ntf = g->ntf;
             kp.nelem = g->nelem;
@@ -1326,7 +1355,7 @@ static std::shared_ptr<Pattern> get_pattern(Ctx* ctx, Matrix& M, const std::vect
             s.ntf = g->ntf;
             s.kind = 0;
             s.nelem = g->nelem;
-            s.rows = g->tfaddr[d].as<int32_t>();
+            s.rows = g->tfaddr[d]->as<int32_t>();
             isegs.push_back(s);
             ninc_total += s.count;
         }
@@ -3003,8 +3032,19 @@ int slgpu_matrix_clone(slgpu_ctx* ctx, int handle, int* new_handle)
         m->groups = M.groups;
         m->frags = M.frags;
         m->rec_constrained = M.rec_constrained;
+        m->share_addresses = M.share_addresses;
         *new_handle = ctx->next_handle++;
         ctx->matrices[*new_handle] = std::move(m);
+    });
+}
+
+int slgpu_matrix_share_addresses(slgpu_ctx* ctx, int handle, int enable)
+{
+    return guarded(ctx, [&] {
+        Matrix& M = get_matrix(ctx, handle);
+        M.share_addresses = enable != 0;
+        if (!M.share_addresses)
+            M.shared_addresses.clear();
     });
 }
 
@@ -3016,7 +3056,7 @@ int slgpu_matrix_add_group(slgpu_ctx* ctx, int handle, const slgpu_group* g, int
         Matrix& M = get_matrix(ctx, handle);
         if (g->terms == nullptr || g->nterms <= 0 || g->terms[0].dof_table < 0)
             fail(SLGPU_E_ARG, "matrix groups need dof tables (use slgpu_rhs_assemble for right-hand sides)");
-        M.groups.push_back(make_group(ctx, *g));
+        M.groups.push_back(make_group(ctx, *g, M.share_addresses ? &M.shared_addresses : nullptr));
         if (index)
             *index = (int)M.groups.size() - 1;
     });
@@ -3258,6 +3298,8 @@ int slgpu_matrix_process(slgpu_ctx* ctx, int handle, const uint8_t* isconstraine
         Matrix& M = get_matrix(ctx, handle);
         if (isconstrained == nullptr && M.ndofs > 0)
             fail(SLGPU_E_ARG, "null constraint array");
+        // Arrays given for sharing need to stay unchanged only until here.
+        M.shared_addresses.clear();
         process_matrix(ctx, M, isconstrained, precision, false, info);
     });
 }

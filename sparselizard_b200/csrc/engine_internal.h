@@ -108,7 +108,7 @@ struct GroupDev {
 
     DevBuf elems, orient, weights, lagrange, tables, consts, prog_d, elemdata, fielddata, field_off_d, field_rows_d,
         tab_off_d, tab_rows_d, term_scale_d, term_tf_d, term_dof_d, tiles_d;
-    std::vector<DevBuf> tfaddr, dofaddr;  // per destination
+    std::vector<std::shared_ptr<DevBuf>> tfaddr, dofaddr;  // per destination; shared by groups of one matrix when allowed
 
     // Mirror of each term for symmetric element matrices (empty: none), and
     // whether mirror coefficients are equal bit for bit; see mirror_terms in
@@ -231,6 +231,15 @@ struct Matrix {
     // updated in place when multipliers change.
     std::vector<RowSeg> rsegs_host;
     DevBuf rsegs_dev;
+    // slgpu_matrix_share_addresses: the device copies and content hashes of
+    // the address arrays given to add_group since the last process(), by host
+    // pointer and length.
+    struct SharedAddresses {
+        std::shared_ptr<DevBuf> buf;
+        uint64_t hash[2];
+    };
+    bool share_addresses = false;
+    std::map<std::pair<const void*, int64_t>, SharedAddresses> shared_addresses;
 };
 
 // Per kernel family: device time (CUDA events around each launch on the

@@ -215,3 +215,72 @@ def test_graph_replay_with_transposed_pair(ctx):
         assert np.all(np.isfinite(a)) and np.all(np.isfinite(d)), f"call {i}: non-finite values"
         assert np.array_equal(a, a0) and np.array_equal(d, d0), f"call {i}: graph != ungraphed"
     assert not np.array_equal(with_graph[1][0], with_graph[2][0])
+
+
+def test_pattern_serial_and_page_locked_downloads(ctx):
+    """slgpu_matrix_pattern_serial: unchanged across process() calls on the same
+    addresses and constraints, new when the constraints change.  Values
+    downloaded into page-locked host memory (slgpu_host_register) equal those
+    downloaded into pageable memory, and stay equal after unregistering."""
+    rng = np.random.Generator(np.random.PCG64(41))
+    t = _setup(ctx, rng, 31, 60, 9, 9, 4, 3, 3000)
+    L = ctx.lib
+    s = ctypes.c_uint64()
+    ctx.check(L.slgpu_matrix_pattern_serial(ctx.h, t["h"], ctypes.byref(s)))
+    assert s.value == 0
+    A0, D0 = _process(ctx, t, abi.PREC_FP64)
+    ctx.check(L.slgpu_matrix_pattern_serial(ctx.h, t["h"], ctypes.byref(s)))
+    s0 = s.value
+    assert s0 > 0
+    _process(ctx, t, abi.PREC_FP64)
+    ctx.check(L.slgpu_matrix_pattern_serial(ctx.h, t["h"], ctypes.byref(s)))
+    assert s.value == s0
+
+    buf = np.zeros(A0.size + 1024)
+    ctx.check(L.slgpu_host_register(ctx.h, buf.ctypes.data, buf.nbytes))
+    D = np.zeros(max(1, D0.size))
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, t["h"], abi.f64p(buf), abi.f64p(D)))
+    assert np.array_equal(buf[: A0.size], A0) and np.array_equal(D[: D0.size], D0)
+    ctx.check(L.slgpu_host_unregister(ctx.h, buf.ctypes.data))
+    buf[:] = 0
+    ctx.check(L.slgpu_matrix_download_values(ctx.h, t["h"], abi.f64p(buf), abi.f64p(D)))
+    assert np.array_equal(buf[: A0.size], A0)
+
+    t["con"] = t["con"].copy()
+    t["con"][::5] ^= 1
+    _process(ctx, t, abi.PREC_FP64)
+    ctx.check(L.slgpu_matrix_pattern_serial(ctx.h, t["h"], ctypes.byref(s)))
+    assert s.value != s0
+
+
+def test_shared_address_arrays(ctx):
+    """A group added twice with the same host address arrays (the second copy
+    with other term scales), with slgpu_matrix_share_addresses on and off:
+    the same CSR values bit for bit and the same pattern serial (addresses are
+    hashed by content either way)."""
+    rng = np.random.Generator(np.random.PCG64(43))
+    L = ctx.lib
+    gb, xyz, conn = S.group(rng, nelem_grid=40, ntf=9, ndof=9, nterms=4, ngp1=3, norient=2, ndests=2, ndofs=3000)
+    g1 = gb.g
+    g1.mesh = 33
+    ctx.check(L.slgpu_mesh_set_nodes(ctx.h, 33, xyz.size // 3, abi.f64p(xyz)))
+    ctx.check(L.slgpu_mesh_set_elements(ctx.h, 33, 3, 4, conn.size // 4, abi.i32p(conn)))
+    g2 = abi.Group.from_buffer_copy(g1)
+    terms2 = (abi.Term * g1.nterms)(*[abi.Term(g1.terms[t].tf_table, g1.terms[t].dof_table, g1.terms[t].coef_node, 0,
+                                               0.5 + t) for t in range(g1.nterms)])
+    g2.terms = terms2
+    con = (rng.random(3000) < 0.1).astype(np.uint8)
+    out = {}
+    for share in (0, 1):
+        h = ctypes.c_int()
+        ctx.check(L.slgpu_matrix_create(ctx.h, 3000, ctypes.byref(h)))
+        ctx.check(L.slgpu_matrix_share_addresses(ctx.h, h, share))
+        ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g1), None))
+        ctx.check(L.slgpu_matrix_add_group(ctx.h, h, ctypes.byref(g2), None))
+        A, D = _process(ctx, dict(h=h.value, con=con), abi.PREC_FP64)
+        s = ctypes.c_uint64()
+        ctx.check(L.slgpu_matrix_pattern_serial(ctx.h, h, ctypes.byref(s)))
+        out[share] = (A, D, s.value)
+        ctx.check(L.slgpu_matrix_destroy(ctx.h, h))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
