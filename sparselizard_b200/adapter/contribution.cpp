@@ -169,6 +169,29 @@ indexmat cached_addresses(const std::shared_ptr<dofmanager>& dm, const std::shar
     return a;
 }
 
+// Elements of a disjoint-region group in orientation groups (the lists that
+// elementselector hands out, concatenated, with each element's variant and the
+// variants' total orientations), kept per mesh and region list: they depend
+// only on the mesh's elements, which a mesh number change (adaptation)
+// renews.  Holds the rawmesh weakly, so that a new mesh at the address of a
+// destroyed one never matches.
+struct SelectorKey {
+    const void* mesh;
+    int meshnumber;
+    bool orientdep;
+    std::vector<int> disjregs;
+    bool operator<(const SelectorKey& o) const
+    {
+        return std::tie(mesh, meshnumber, orientdep, disjregs) < std::tie(o.mesh, o.meshnumber, o.orientdep, o.disjregs);
+    }
+};
+struct SelectorEntry {
+    std::weak_ptr<rawmesh> mesh;
+    std::vector<int> elems, variant, totalorients;
+};
+std::map<SelectorKey, SelectorEntry> g_selector_cache;
+constexpr size_t kSelectorEntries = 16;
+
 // Lowers coefficient operation trees of one disjoint-region group into an
 // slgpu coefficient program.  Shared subtrees (same operation object) become
 // one node.
@@ -470,26 +493,40 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
                 unsupported("a multiharmonic coefficient");
         }
 
-        elementselector myselector;
-        if (tfphysreg == integrationphysreg)
-            myselector = elementselector(mydisjregs, isorientationdependent);
-        else {
-            std::vector<int> activeelems = gentools::getactiveelements(mydisjregs, isnodeintfphysreg);
-            if (activeelems.size() > 0)
-                myselector = elementselector(mydisjregs, activeelems, isorientationdependent);
-        }
-        if (myselector.count() == 0)
-            continue;
-
         // Elements of all orientation groups, concatenated, with a variant index.
         std::vector<int> elems, variant, totalorients;
-        do {
-            std::vector<int> en = myselector.getelementnumbers();
-            int v = (int)totalorients.size();
-            totalorients.push_back(myselector.gettotalorientation());
-            elems.insert(elems.end(), en.begin(), en.end());
-            variant.insert(variant.end(), en.size(), v);
-        } while (myselector.next());
+        std::shared_ptr<rawmesh> rm = universe::getrawmesh();
+        const SelectorKey skey{rm.get(), rm->getmeshnumber(), isorientationdependent, mydisjregs};
+        auto sit = tfphysreg == integrationphysreg ? g_selector_cache.find(skey) : g_selector_cache.end();
+        if (sit != g_selector_cache.end() && sit->second.mesh.lock() == rm) {
+            elems = sit->second.elems;
+            variant = sit->second.variant;
+            totalorients = sit->second.totalorients;
+        } else {
+            elementselector myselector;
+            if (tfphysreg == integrationphysreg)
+                myselector = elementselector(mydisjregs, isorientationdependent);
+            else {
+                std::vector<int> activeelems = gentools::getactiveelements(mydisjregs, isnodeintfphysreg);
+                if (activeelems.size() > 0)
+                    myselector = elementselector(mydisjregs, activeelems, isorientationdependent);
+            }
+            if (myselector.count() > 0)
+                do {
+                    std::vector<int> en = myselector.getelementnumbers();
+                    int v = (int)totalorients.size();
+                    totalorients.push_back(myselector.gettotalorientation());
+                    elems.insert(elems.end(), en.begin(), en.end());
+                    variant.insert(variant.end(), en.size(), v);
+                } while (myselector.next());
+            if (tfphysreg == integrationphysreg) {
+                if (g_selector_cache.size() >= kSelectorEntries)
+                    g_selector_cache.clear();
+                g_selector_cache[skey] = SelectorEntry{rm, elems, variant, totalorients};
+            }
+        }
+        if (elems.empty())
+            continue;
         const int norient = (int)totalorients.size();
         const int nelem = (int)elems.size();
 

@@ -128,10 +128,21 @@ int ensure_mesh(int elemtype)
     nodes* nd = rm->getnodes();
     std::vector<double>* xyz = nd->getcoordinates();
     long long nn = (long long)xyz->size() / 3;
-    // Cheap content hash of the coordinates: meshes can move in place.
-    unsigned long long h = 1469598103934665603ull;
+    // Cheap content hash of the coordinates (meshes can move in place), in
+    // four interleaved chains so that their multiplies overlap.
     const unsigned long long* words = reinterpret_cast<const unsigned long long*>(xyz->data());
-    for (size_t i = 0; i < xyz->size(); i++) h = (h ^ words[i]) * 1099511628211ull;
+    const size_t nw = xyz->size();
+    unsigned long long c[4] = {1469598103934665603ull, 1099511628211ull, 0x9E3779B97F4A7C15ull, 0xD6E8FEB86659FD93ull};
+    size_t i = 0;
+    for (; i + 4 <= nw; i += 4) {
+        c[0] = (c[0] ^ words[i]) * 1099511628211ull;
+        c[1] = (c[1] ^ words[i + 1]) * 1099511628211ull;
+        c[2] = (c[2] ^ words[i + 2]) * 1099511628211ull;
+        c[3] = (c[3] ^ words[i + 3]) * 1099511628211ull;
+    }
+    for (; i < nw; i++) c[0] = (c[0] ^ words[i] ^ i) * 1099511628211ull;
+    unsigned long long h = 1469598103934665603ull;
+    for (int k = 0; k < 4; k++) h = (h ^ c[k]) * 1099511628211ull;
     const std::pair<const void*, int> key(rm.get(), rm->getmeshnumber());
     auto mit = g_meshes.find(key);
     if (mit == g_meshes.end()) {
