@@ -891,7 +891,7 @@ static CoefParams coef_params(Ctx* ctx, const GroupDev& g, double* C)
 }
 
 // Segments of the COO space: (group, destination) blocks then raw fragments.
-std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals)
+std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals, bool f32)
 {
     std::vector<Segment> segs;
     int64_t coo = 0, vb = 0;
@@ -903,7 +903,8 @@ std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group
             segs.push_back(Segment{coo, P * g->nelem, vb, g->dest_mult[d]});
             coo += P * g->nelem;
         }
-        vb += P * g->nelem;
+        // Float values take half as many doubles of the buffer.
+        vb += f32 ? (P * g->nelem + 1) / 2 : P * g->nelem;
     }
     for (auto& f : M.frags) {
         const int64_t n = (int64_t)f->nr * f->nc;
@@ -1620,6 +1621,7 @@ struct SplitJob {
     const int32_t* elemexp;
     double* out;
     double* out2;
+    bool f32;  // out and out2 hold floats
 };
 
 static std::array<int, 5> split_shape_key(const GroupDev& g, int tier) { return {0, tier, g.ntf, g.ndof, g.ngp}; }
@@ -1714,6 +1716,7 @@ static void run_split_jobs(Ctx* ctx, const std::vector<SplitJob>& jobs, int NE)
             cexp += split_exp_bytes(g) / 4;
         }
         sp.error = ctx->x->split_error.as<unsigned int>();
+        sp.f32 = jobs[b0].f32 ? 1 : 0;
         sp.next = reinterpret_cast<unsigned long long*>(ctx->x->split_error.as<char>() + 16);
         const int kt = kstat_start(ctx, "slice_cols", slice_bytes);
         if (S == 7 && NE == 64)
@@ -2146,8 +2149,18 @@ static void launch_coefficients(Ctx* ctx, const Matrix& M, double* C, const std:
 // Steps 1 and 2 on the current execution state's stream: coefficients of
 // every group (with per-group data overrides, if given), contraction of each
 // group into `vals` at the group's value base, fragment values after them.
+bool float_values(const Matrix& M, int precision)
+{
+    if (precision != SLGPU_PREC_FP32 || !M.frags.empty() || M.groups.empty())
+        return false;
+    for (auto& g : M.groups)
+        if (g->nelem > 0 && !uses_split(*g, precision))
+            return false;
+    return true;
+}
+
 void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::vector<int64_t>& gvb, double* vals,
-                         const std::vector<GroupData>* ov)
+                         const std::vector<GroupData>* ov, bool f32)
 {
     // Coefficients of every group coexist ([term][gp][element] per group) so
     // that groups sharing geometry are evaluated by one kernel.
@@ -2201,7 +2214,7 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
                 if (pair[gi] < 0 || pair[gi] > (int)gi)
                     split_jobs.push_back(SplitJob{g.get(), precision == SLGPU_PREC_SPLIT ? 0 : 1, pair[gi] > (int)gi, Cg,
                                                   E.as<int32_t>() + eoff[gi], vals + gvb[gi],
-                                                  pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr});
+                                                  pair[gi] > (int)gi ? vals + gvb[pair[gi]] : nullptr, f32});
                 gi++;
                 continue;
             }
@@ -2210,6 +2223,8 @@ void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::ve
                 gi++;
                 continue;
             }
+            if (f32)
+                fail(SLGPU_E_STATE, "float element values need every group contracted by the split kernels");
             const int64_t P = (int64_t)g->ntf * g->ndof;
             const size_t small_smem = small_kernel_smem(*g);
             if (uses_small_kernel(*g)) {
@@ -2275,12 +2290,12 @@ static int row_kernel_forced()
     return k;
 }
 
-std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs)
+std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs, bool f32)
 {
     std::vector<RowSeg> rsegs(segs.size());
     size_t s = 0;
     for (auto& g : M.groups)
-        for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, 0};
+        for (int d = 0; d < g->ndests; d++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, segs[s].mult, g->ndof, f32 ? 1 : 0};
     for (size_t f = 0; f < M.frags.size(); f++, s++) rsegs[s] = RowSeg{segs[s].coo_base, segs[s].val_base, 1.0, 1, 0};
     return rsegs;
 }
@@ -2349,15 +2364,18 @@ void launch_stream_rows(Ctx* ctx, const StreamLaunch& L)
     ctx->launches++;
 }
 
-void launch_thread_rows(Ctx* ctx, const RowParams& rp)
+void launch_thread_rows(Ctx* ctx, const RowParams& rp, bool f32)
 {
     const size_t smem = (size_t)rp.lmax * kThreadRows * 8;
-    k_row_thread<<<grid_for(rp.nrows, kThreadRows), kThreadRows, smem, ctx->x->stream>>>(rp);
+    if (f32)
+        k_row_thread<float><<<grid_for(rp.nrows, kThreadRows), kThreadRows, smem, ctx->x->stream>>>(rp);
+    else
+        k_row_thread<double><<<grid_for(rp.nrows, kThreadRows), kThreadRows, smem, ctx->x->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_row_thread");
     ctx->launches++;
 }
 
-void launch_warp_rows(Ctx* ctx, RowParams rp)
+void launch_warp_rows(Ctx* ctx, RowParams rp, bool f32)
 {
     // Consecutive rows per warp: up to kRowsPerWarp (the row buffer stays
     // clean between them), fewer when the rows are too few to fill the
@@ -2370,9 +2388,14 @@ void launch_warp_rows(Ctx* ctx, RowParams rp)
     if (smem > 48 * 1024) {
         if (smem > 227 * 1024)
             fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
-        cuda_check(cudaFuncSetAttribute(k_row_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
     }
-    k_row_values<<<grid_for((rp.nrows + rp.rows_per_warp - 1) / rp.rows_per_warp, wpb), 32 * wpb, smem, ctx->x->stream>>>(rp);
+    const unsigned grid = grid_for((rp.nrows + rp.rows_per_warp - 1) / rp.rows_per_warp, wpb);
+    if (f32)
+        k_row_values<float><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
+    else
+        k_row_values<double><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_row_values");
     ctx->launches++;
 }
@@ -2402,15 +2425,17 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
     rp.Avals = Avals;
     rp.Dvals = rhs ? nullptr : Dvals;
     rp.dense = rhs ? Avals : nullptr;
+    // Element values stored as floats (every segment alike, float_values()).
+    const bool f32 = !rsegs.empty() && rsegs[0].f32 != 0;
     // Bytes: kept element values and their slots, incidences, row
     // pointers read; A and D values written.
-    const double rbytes = 10.0 * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
+    const double rbytes = (f32 ? 6.0 : 10.0) * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);
     const StreamLaunch sl = stream_launch(ctx, rp, rsegs);
     const bool thread_ok = rp.lmax <= kThreadRowMax;
-    // Candidates: warp per row always, streaming warps and thread per row
-    // where their shapes allow.
+    // Candidates: warp per row always, streaming warps (double values) and
+    // thread per row where their shapes allow.
     std::vector<int> cand{1};
-    if (sl.ok)
+    if (sl.ok && !f32)
         cand.push_back(0);
     if (thread_ok)
         cand.push_back(2);
@@ -2418,15 +2443,17 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
         if (c == 0)
             launch_stream_rows(ctx, sl);
         else if (c == 2)
-            launch_thread_rows(ctx, rp);
+            launch_thread_rows(ctx, rp, f32);
         else
-            launch_warp_rows(ctx, rp);
+            launch_warp_rows(ctx, rp, f32);
     };
     int choice = row_kernel_forced();
-    if (choice >= 0 && std::find(cand.begin(), cand.end(), choice) == cand.end())
-        choice = 1;
     if (choice < 0)
         choice = P.row_kernel;
+    // A kernel this call cannot use (the streaming warps with float values):
+    // warp per row.
+    if (choice >= 0 && std::find(cand.begin(), cand.end(), choice) == cand.end())
+        choice = 1;
     if (choice < 0 && !ctx->x->capturing && ctx->x == &ctx->main) {
         // Every candidate timed on this call's data (their outputs are
         // identical), warp per row being the default.
@@ -2583,7 +2610,7 @@ static void capture_value_graph(Ctx* ctx, Matrix& M, int precision, bool rhs, co
     x.capturing = true;
     std::string err;
     try {
-        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
+        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr, float_values(M, precision));
         phase_event(ctx, ctx->x->ev[2]);
         launch_row_values(ctx, M, *M.pattern, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
     } catch (const std::exception& e) {
@@ -2639,7 +2666,10 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     ev_record(ctx, 0);
     std::vector<int64_t> gvb;
     int64_t total_vals = 0;
-    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
+    // FP32-level steps whose groups all go through the split kernels keep
+    // their element matrices as floats: half the element-value traffic.
+    const bool f32v = float_values(M, precision);
+    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals, f32v);
 
     // Constraints: device copy and content key, both reused while the array
     // is byte-identical to the previous call's.  A right-hand side uses an
@@ -2704,7 +2734,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
     // Resident segment array of the value kernels (updated in place while its
     // size is unchanged, so that captured graphs stay valid).
     {
-        std::vector<RowSeg> rsegs = row_segments(M, segs);
+        std::vector<RowSeg> rsegs = row_segments(M, segs, f32v);
         const size_t nb = rsegs.size() * sizeof(RowSeg);
         const bool same = rsegs.size() == M.rsegs_host.size() && std::memcmp(rsegs.data(), M.rsegs_host.data(), nb) == 0;
         if (!same || M.rsegs_dev.empty()) {
@@ -2742,7 +2772,7 @@ static void process_matrix(Ctx* ctx, Matrix& M, const uint8_t* isconstrained, in
         M.vsig_prev.clear();
     }
     if (!graphed) {
-        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr);
+        launch_contractions(ctx, M, precision, gvb, M.vals.as<double>(), nullptr, float_values(M, precision));
         phase_event(ctx, ctx->x->ev[2]);
         launch_row_values(ctx, M, P, M.rsegs_host, M.rsegs_dev.as<RowSeg>(), rhs, M.vals.as<double>(), Av, Dv);
     }

@@ -179,13 +179,15 @@ struct Pattern {
 };
 
 // Per COO segment, as the CSR value kernels read it: where its entries
-// values start in the element-value buffer, its destination multiplier and
-// the width of its incidences (ndof of a group, 1 for a raw fragment).
+// values start in the element-value buffer, its destination multiplier, the
+// width of its incidences (ndof of a group, 1 for a raw fragment) and whether
+// the values are stored as floats (FP32-level steps, float_values(): entry k
+// of the segment is float number 2 * val_base + k of the buffer).
 struct RowSeg {
     int64_t coo_base;
     int64_t val_base;
     double mult;
-    int32_t width, pad;
+    int32_t width, f32;
 };
 
 struct Segment {
@@ -346,10 +348,14 @@ struct GroupData {
 bool group_symmetric(const GroupDev& g);
 
 // Launch pieces of one assembly (engine.cu), issued on ctx->x's stream.
-std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals);
+// Whether a step of M at `precision` stores its element matrices as floats:
+// FP32-level steps whose groups are all contracted by the split kernels and
+// that have no raw fragments.
+bool float_values(const Matrix& M, int precision);
+std::vector<Segment> build_segments(const Matrix& M, std::vector<int64_t>* group_val_base, int64_t* total_vals, bool f32 = false);
 void launch_contractions(Ctx* ctx, const Matrix& M, int precision, const std::vector<int64_t>& gvb, double* vals,
-                         const std::vector<GroupData>* ov);
-std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs);
+                         const std::vector<GroupData>* ov, bool f32 = false);
+std::vector<RowSeg> row_segments(const Matrix& M, const std::vector<Segment>& segs, bool f32 = false);
 void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<RowSeg>& rsegs, const RowSeg* dsegs, bool rhs,
                        const double* vals, double* Avals, double* Dvals);
 // Copies `bytes` from host memory to a new device buffer through the current

@@ -737,7 +737,8 @@ struct RowParams {
 // their place in the order.
 constexpr int kRowBatch = 8;
 
-__device__ __forceinline__ void row_add_generic(double* buf, int width, double mult, const double* v, const int16_t* sm, bool serial,
+template <class V>
+__device__ __forceinline__ void row_add_generic(double* buf, int width, double mult, const V* v, const int16_t* sm, bool serial,
                                                 int lane)
 {
     if (serial) {
@@ -745,13 +746,13 @@ __device__ __forceinline__ void row_add_generic(double* buf, int width, double m
             for (int j = 0; j < width; j++) {
                 const int s = sm[j];
                 if (s >= 0)
-                    buf[s] = fma(v[j], mult, buf[s]);
+                    buf[s] = fma((double)v[j], mult, buf[s]);
             }
     } else {
         for (int j = lane; j < width; j += 32) {
             const int s = sm[j];
             if (s >= 0)
-                buf[s] = fma(v[j], mult, buf[s]);
+                buf[s] = fma((double)v[j], mult, buf[s]);
         }
     }
 }
@@ -764,8 +765,11 @@ __device__ __forceinline__ void row_add_generic(double* buf, int width, double m
 constexpr int kThreadRows = 128;
 constexpr int kThreadRowMax = 32;
 
+template <class V>
 __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
 {
+    const V* vals = reinterpret_cast<const V*>(p.vals);
+    constexpr int64_t kScale = sizeof(double) / sizeof(V);  // values of type V per double of the buffer
     extern __shared__ double tbuf[];
     const int64_t r = (int64_t)blockIdx.x * kThreadRows + threadIdx.x;
     if (r >= p.nrows)
@@ -780,12 +784,12 @@ __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
         const unsigned long long pk = p.inc[k];
         const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
         const long long co = (long long)(pk & ((1ull << 40) - 1));
-        const double* v = p.vals + (sg.val_base + (co - sg.coo_base));
+        const V* v = vals + (sg.val_base * kScale + (co - sg.coo_base));
         const int16_t* sl = p.slotmap + co;
         for (int j = 0; j < sg.width; j++) {
             const int s = sl[j];
             if (s >= 0)
-                buf[s * kThreadRows] = fma(v[j], sg.mult, buf[s * kThreadRows]);
+                buf[s * kThreadRows] = fma((double)v[j], sg.mult, buf[s * kThreadRows]);
         }
     }
     if (p.dense != nullptr) {
@@ -803,8 +807,11 @@ __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
 // Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
 constexpr int kRowsPerWarp = 31;
 
+template <class V>
 __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
 {
+    const V* vals = reinterpret_cast<const V*>(p.vals);
+    constexpr long long kScale = sizeof(double) / sizeof(V);  // values of type V per double of the buffer
     extern __shared__ double rowbuf[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * p.rows_per_warp;
@@ -839,7 +846,7 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
                 const unsigned long long pk = p.inc[kb + lane];
                 const RowSeg sg = p.segs[(pk >> 40) & ((1ull << 23) - 1)];
                 coo = (uint32_t)(pk & ((1ull << 40) - 1));
-                voff = (uint32_t)(sg.val_base + ((long long)coo - sg.coo_base));
+                voff = (uint32_t)(sg.val_base * kScale + ((long long)coo - sg.coo_base));
                 mult = sg.mult;
                 const bool serial = (pk >> 63) != 0;
                 info = sg.width | (serial ? kSerial : 0) | ((serial || sg.width > 32) ? kGeneric : 0);
@@ -860,7 +867,7 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
                         val[x] = 0.0;
                         if (u + x < nkb && lane < (inf & 0xffff)) {
                             slot[x] = p.slotmap[(uint64_t)co + lane];
-                            val[x] = p.vals[(uint64_t)vo + lane];
+                            val[x] = (double)vals[(uint64_t)vo + lane];
                         }
                     }
 #pragma unroll
@@ -879,7 +886,7 @@ __global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
                     const uint32_t co = __shfl_sync(0xffffffffu, coo, x);
                     const double m = __shfl_sync(0xffffffffu, mult, x);
                     const int inf = __shfl_sync(0xffffffffu, info, x);
-                    row_add_generic(buf, inf & 0xffff, m, p.vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
+                    row_add_generic(buf, inf & 0xffff, m, vals + vo, p.slotmap + co, (inf & kSerial) != 0, lane);
                     __syncwarp();
                 }
             }

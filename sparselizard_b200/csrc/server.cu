@@ -241,14 +241,17 @@ void launch(Server& S, Slot& s, Request& r)
     htrace_mark(ctx, "request: inputs");
     std::vector<int64_t> gvb;
     int64_t total_vals = 0;
-    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals);
+    // Element values stored as process() stores them (floats for FP32-level
+    // requests whose groups all go through the split kernels).
+    const bool f32v = float_values(M, r.precision);
+    std::vector<Segment> segs = build_segments(M, &gvb, &total_vals, f32v);
     r.vals.alloc(ctx, (size_t)std::max<int64_t>(total_vals, 1) * 8);
     ctx->x->kev_tag.clear();
-    launch_contractions(ctx, M, r.precision, gvb, r.vals.as<double>(), &ov);
+    launch_contractions(ctx, M, r.precision, gvb, r.vals.as<double>(), &ov, f32v);
     const double t2 = S.now();
     r.Avals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzA, 1) * 8);
     r.Dvals.alloc(ctx, (size_t)std::max<int64_t>(P.nnzD, 1) * 8);
-    std::vector<RowSeg> rsegs = row_segments(M, segs);
+    std::vector<RowSeg> rsegs = row_segments(M, segs, f32v);
     // Destination multipliers of the request's scale updates (segments are
     // the groups' destinations in order).
     if (!r.scales.empty()) {

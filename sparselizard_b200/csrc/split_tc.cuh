@@ -81,6 +81,7 @@ struct SplitParams {
     int64_t nwork;          // sum of the groups' work items
     unsigned int* error;    // set on a timed-out wait
     unsigned long long* next;  // work items handed out after each CTA's first; zero at launch
+    int f32;                // out and out2 hold floats (FP32-level steps): same entry order
 };
 
 // Work items passed from a CTA's producer to its MMA and epilogue roles.
@@ -655,9 +656,17 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
                         const double d = fma((double)Lo, 0x1p-21, (double)H[j + jj]);
                         if (j + jj < nj) {
                             const double v = scale2(d, rex + cx[jj]);
-                            outp[(int64_t)(j + jj) * P] = v;
-                            if (outm != nullptr)
-                                outm[(int64_t)(j + jj) * P] = v;
+                            if (p.f32) {
+                                // Entry k of a float matrix is float k of the same buffer.
+                                const int64_t o = (int64_t)(j + jj) * P;
+                                reinterpret_cast<float*>(G.out)[ebase + m.x + o] = (float)v;
+                                if (outm != nullptr)
+                                    reinterpret_cast<float*>(G.out2 != nullptr ? G.out2 : G.out)[ebase + m.y + o] = (float)v;
+                            } else {
+                                outp[(int64_t)(j + jj) * P] = v;
+                                if (outm != nullptr)
+                                    outm[(int64_t)(j + jj) * P] = v;
+                            }
                         }
                     }
                 }
