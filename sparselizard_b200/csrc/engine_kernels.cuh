@@ -735,7 +735,7 @@ struct RowParams {
 // the additions still run in incidence order.  Incidences flagged serial
 // (duplicate addresses) or wider than a warp are added by their own loop at
 // their place in the order.
-constexpr int kRowBatch = 8;
+constexpr int kRowBatch = 4;
 
 template <class V>
 __device__ __forceinline__ void row_add_generic(double* buf, int width, double mult, const V* v, const int16_t* sm, bool serial,
@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
 constexpr int kRowsPerWarp = 31;
 
 template <class V>
-__global__ void __launch_bounds__(256, 4) k_row_values(RowParams p)
+__global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
 {
     const V* vals = reinterpret_cast<const V*>(p.vals);
     constexpr long long kScale = sizeof(double) / sizeof(V);  // values of type V per double of the buffer
