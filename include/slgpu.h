@@ -281,6 +281,13 @@ int slgpu_matrix_eliminate(slgpu_ctx* ctx, int handle, const double* b, double* 
  * order.  b_accum is a host array of length ndofs.
  */
 int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int precision, double* b_accum);
+/* The same right-hand side, returned as the rows it reaches (ascending DOF
+ * numbers) and their values instead of added into a dense array: *count rows,
+ * at most `capacity` (ntf * nelem * ndests always suffices).  Rows it does not reach
+ * hold zero in the dense form.  For callers that add the result into a vector
+ * of their own (rawvec::setvalues with "add", src/formulation/rawvec.cpp:216-254). */
+int slgpu_rhs_assemble_rows(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int precision, int32_t* rows, double* vals,
+                            int64_t capacity, int64_t* count);
 
 /* Device time (ms) of the phases of the last process()/rhs call:
  * [0] geometry+coefficients, [1] contraction, [2] pattern (symbolic), [3] CSR values, [4] total. */

@@ -134,6 +134,8 @@ SIGNATURES = {
     "slgpu_matrix_device_csr": (c_int, [c_void_p, c_int] + [POINTER(c_void_p)] * 6),
     "slgpu_matrix_eliminate": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "slgpu_rhs_assemble": (c_int, [c_void_p, POINTER(Group), c_int64, c_int, POINTER(c_double)]),
+    "slgpu_rhs_assemble_rows": (c_int, [c_void_p, POINTER(Group), c_int64, c_int, POINTER(c_int32), POINTER(c_double), c_int64,
+                                        POINTER(c_int64)]),
     "slgpu_last_timings": (c_int, [c_void_p, POINTER(c_double)]),
     "slgpu_record_count": (c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
     "slgpu_record_group": (c_int, [c_void_p, c_int, c_int, POINTER(Group)]),

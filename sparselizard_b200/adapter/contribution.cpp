@@ -694,13 +694,23 @@ void contribution::generate(std::shared_ptr<rawvec> myvec, std::shared_ptr<rawma
                 slgpu_adapter::check(slgpu_matrix_add_group(ctx, handle, &g, nullptr), "slgpu_matrix_add_group");
             } else {
                 // Right-hand side: b[addr] += -(element vectors), as
-                // stiffnesses.minus() + rawvec::setvalues(..., "add").
-                densemat acc(1, (int)ndofs, 0.0);
-                int st = slgpu_rhs_assemble(ctx, &g, ndofs, prec, acc.getvalues());
+                // stiffnesses.minus() + rawvec::setvalues(..., "add"); only
+                // the rows the group reaches are added.
+                const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(ndofs, (int64_t)ntf * nelem * (int64_t)dests.size()));
+                std::vector<int32_t> rows((size_t)cap);
+                std::vector<double> vals((size_t)cap);
+                int64_t count = 0;
+                int st = slgpu_rhs_assemble_rows(ctx, &g, ndofs, prec, rows.data(), vals.data(), cap, &count);
                 if (st == SLGPU_E_NODEVICE && slgpu_adapter::record_only())
                     continue;  // recorded for inspection; nothing assembled
-                slgpu_adapter::check(st, "slgpu_rhs_assemble");
-                myvec->setvalues(indexmat((int)ndofs, 1, 0, 1), acc, "add");
+                slgpu_adapter::check(st, "slgpu_rhs_assemble_rows");
+                if (count > 0) {
+                    indexmat ri((long long)count, 1);
+                    densemat vi((long long)count, 1);
+                    std::copy(rows.begin(), rows.begin() + count, ri.getvalues());
+                    std::copy(vals.begin(), vals.begin() + count, vi.getvalues());
+                    myvec->setvalues(ri, vi, "add");
+                }
             }
         }
     }

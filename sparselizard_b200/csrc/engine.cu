@@ -3549,6 +3549,55 @@ int slgpu_rhs_assemble(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int 
     });
 }
 
+int slgpu_rhs_assemble_rows(slgpu_ctx* ctx, const slgpu_group* g, int64_t ndofs, int precision, int32_t* rows, double* vals,
+                            int64_t capacity, int64_t* count)
+{
+    return guarded(ctx, [&] {
+        if (g == nullptr || rows == nullptr || vals == nullptr || count == nullptr || capacity < 0)
+            fail(SLGPU_E_ARG, "null argument");
+        if (g->terms == nullptr || g->nterms <= 0 || g->terms[0].dof_table >= 0 || g->ndof != 1)
+            fail(SLGPU_E_ARG, "right-hand-side groups have no dof tables and ndof = 1");
+        Matrix M;
+        M.ndofs = ndofs;
+        M.groups.push_back(make_group(ctx, *g));
+        if (ctx->record_only) {
+            ctx->rhs_record.push_back(M.groups.back());
+            ctx->rhs_record_ndofs.push_back(ndofs);
+        }
+        process_matrix(ctx, M, nullptr, precision, true, nullptr);
+        Pattern& P = *M.pattern;
+        if (!P.rhs_rows_ready) {
+            // Every DOF is a row of a right-hand side; the rows with incidences
+            // are the ones an entry reaches.
+            std::vector<uint32_t> ip((size_t)P.nA + 1);
+            cuda_check(cudaMemcpyAsync(ip.data(), P.inc_ptr.as<void>(), ip.size() * 4, cudaMemcpyDeviceToHost, ctx->x->stream),
+                       "D2H incidence pointers");
+            cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync rhs rows");
+            P.rhs_rows.clear();
+            for (int64_t r = 0; r < P.nA; r++)
+                if (ip[r + 1] > ip[r])
+                    P.rhs_rows.push_back((int32_t)r);
+            upload(ctx, P.rhs_rows_d, P.rhs_rows);
+            P.rhs_rows_ready = true;
+        }
+        const int64_t n = (int64_t)P.rhs_rows.size();
+        if (n > capacity)
+            fail(SLGPU_E_ARG, "capacity smaller than the rows the right-hand side reaches");
+        *count = n;
+        if (n == 0)
+            return;
+        DevBuf out;
+        out.alloc(ctx, (size_t)n * 8);
+        k_gather_rows<<<grid_for(n, 256), 256, 0, ctx->x->stream>>>(M.Avals.as<double>(), P.rhs_rows_d.as<int32_t>(), n, out.as<double>());
+        cuda_check(cudaGetLastError(), "k_gather_rows");
+        ctx->launches++;
+        cuda_check(cudaMemcpyAsync(vals, out.as<void>(), (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->x->stream), "D2H rhs rows");
+        ctx->bytes_d2h += n * 8;
+        cuda_check(cudaStreamSynchronize(ctx->x->stream), "sync rhs");
+        std::memcpy(rows, P.rhs_rows.data(), (size_t)n * 4);
+    });
+}
+
 int slgpu_last_timings(const slgpu_ctx* ctx, double* ms5)
 {
     if (ctx == nullptr || ms5 == nullptr)

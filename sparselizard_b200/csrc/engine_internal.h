@@ -176,6 +176,11 @@ struct Pattern {
     DevBuf inc_ptr;        // uint32 [nA+1]: incidences of each row
     DevBuf inc;            // uint64 [ninc]: segment << 40 | COO index of the incidence's first entry
     uint64_t last_use = 0;
+    // Right-hand-side patterns: the rows (DOFs) that receive at least one
+    // entry, ascending, on the host and the device (built on first use).
+    bool rhs_rows_ready = false;
+    std::vector<int32_t> rhs_rows;
+    DevBuf rhs_rows_d;
 };
 
 // Per COO segment, as the CSR value kernels read it: where its entries

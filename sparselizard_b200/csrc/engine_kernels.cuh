@@ -695,6 +695,14 @@ __global__ void k_inc_finalize(const uint32_t* skeys, const uint32_t* sids, int6
     atomicAdd(&rowcount[renum[skeys[k]]], 1u);
 }
 
+// out[k] = v[rows[k]] for k < n.
+__global__ void k_gather_rows(const double* __restrict__ v, const int32_t* __restrict__ rows, int64_t n, double* __restrict__ out)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        out[k] = v[rows[k]];
+}
+
 __global__ void k_max_rowlen(const uint32_t* Arows, const uint32_t* Drows, int64_t nrows, unsigned long long* out)
 {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

@@ -274,6 +274,20 @@ def test_abi_rhs(ctx):
     ref = slref.rhs(gb.g, xyz, conn, ndofs)
     mag = slref.rhs(gb.g, xyz, conn, ndofs, absmode=True)
     assert np.max(np.abs(b - ref) / np.maximum(mag, 1e-300)) <= TOL
+    # The same right-hand side as reached rows and values (ndofs well above
+    # the rows reached): the dense result at those rows, zero elsewhere.
+    big = 5000
+    bd = np.zeros(big)
+    ctx.check(ctx.lib.slgpu_rhs_assemble(ctx.h, ctypes.byref(gb.g), big, abi.PREC_FP64, abi.f64p(bd)))
+    cap = gb.g.ntf * gb.g.nelem * gb.g.ndests
+    rows, vals, n = np.zeros(cap, np.int32), np.zeros(cap), ctypes.c_int64()
+    ctx.check(ctx.lib.slgpu_rhs_assemble_rows(ctx.h, ctypes.byref(gb.g), big, abi.PREC_FP64, abi.i32p(rows), abi.f64p(vals), cap,
+                                              ctypes.byref(n)))
+    rows, vals = rows[: n.value], vals[: n.value]
+    assert n.value > 0 and np.all(np.diff(rows) > 0)
+    dense = np.zeros(big)
+    dense[rows] = vals
+    assert np.array_equal(dense, bd)
 
 
 def test_abi_budget_error(ctx):
