@@ -839,10 +839,9 @@ __global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
     __syncwarp();
     constexpr int kGeneric = 1 << 17, kSerial = 1 << 16;
     for (int rr = 0; rr < nr; rr++) {
-        const uint32_t a0 = __shfl_sync(0xffffffffu, a_lo, rr), a1 = __shfl_sync(0xffffffffu, a_lo, rr + 1);
-        const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
+        // The CSR bounds are fetched after the incidences (only the
+        // write-back needs them): fewer registers live in the loop below.
         const uint32_t k0 = __shfl_sync(0xffffffffu, i_lo, rr), k1 = __shfl_sync(0xffffffffu, i_lo, rr + 1);
-        const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
         for (uint32_t kb = k0; kb < k1; kb += 32) {
             const int nkb = (int)min(32u, k1 - kb);
             // Lane l decodes incidence kb + l.  Value and COO offsets fit 32
@@ -899,6 +898,9 @@ __global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
                 }
             }
         }
+        const uint32_t a0 = __shfl_sync(0xffffffffu, a_lo, rr), a1 = __shfl_sync(0xffffffffu, a_lo, rr + 1);
+        const uint32_t d0 = __shfl_sync(0xffffffffu, d_lo, rr), d1 = __shfl_sync(0xffffffffu, d_lo, rr + 1);
+        const int la = (int)(a1 - a0), L = la + (int)(d1 - d0);
         const int64_t r = r0 + rr;
         if (p.dense != nullptr) {
             if (lane == 0)

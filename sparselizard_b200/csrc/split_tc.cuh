@@ -620,10 +620,31 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
                 for (int j = 0; j < 16; j++)
                     H[j] = (((long long)r[0][j] * 128 + r[1][j]) * 128 + r[2][j]) * 128 + r[3][j];
             }
-            int32_t r[L - 5][16];
+            // Levels 6..L: with three of them (L = 8) they are folded into
+            // int64 before the stores' addresses are live (32 registers held
+            // through the store loop instead of 48); with fewer the int32
+            // values are the smaller form and are kept.
+            constexpr int kLoLevels = L - 5;
+            constexpr bool kFoldLo = kLoLevels > 2;
+            int32_t r[kFoldLo ? 1 : kLoLevels][16];
+            long long Lo[kFoldLo ? 16 : 1];
+            if constexpr (kFoldLo) {
+                int32_t t[kLoLevels][16];
 #pragma unroll
-            for (int l = 0; l < L - 5; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), r[l]);
-            tmem_ld_wait();
+                for (int l = 0; l < kLoLevels; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), t[l]);
+                tmem_ld_wait();
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    long long lo = 0;
+#pragma unroll
+                    for (int l = 0; l < kLoLevels; l++) lo = lo * 128 + t[l][j];
+                    Lo[j] = lo << (7 * (8 - L));
+                }
+            } else {
+#pragma unroll
+                for (int l = 0; l < kLoLevels; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), r[l]);
+                tmem_ld_wait();
+            }
             // This warp's accumulators are in registers: release them.
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -649,11 +670,16 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
                     const int cx[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
                     for (int jj = 0; jj < 4; jj++) {
-                        long long Lo = 0;
+                        long long lo;
+                        if constexpr (kFoldLo) {
+                            lo = Lo[j + jj];
+                        } else {
+                            lo = 0;
 #pragma unroll
-                        for (int l = 0; l < L - 5; l++) Lo = Lo * 128 + r[l][j + jj];
-                        Lo <<= 7 * (8 - L);
-                        const double d = fma((double)Lo, 0x1p-21, (double)H[j + jj]);
+                            for (int l = 0; l < kLoLevels; l++) lo = lo * 128 + r[l][j + jj];
+                            lo <<= 7 * (8 - L);
+                        }
+                        const double d = fma((double)lo, 0x1p-21, (double)H[j + jj]);
                         if (j + jj < nj) {
                             const double v = scale2(d, rex + cx[jj]);
                             if (p.f32) {
