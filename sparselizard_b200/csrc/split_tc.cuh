@@ -360,6 +360,18 @@ __device__ __forceinline__ double scale2(double x, int s)
     return ldexp(x, s);
 }
 
+// Exact int64 -> double for |x| < 2^51 on the integer and FP64 pipes instead
+// of the conversion unit (which the epilogue's two conversions per output
+// saturate): x is added to the bit pattern of 1.5 * 2^52, whose mantissa ulp
+// is 1, so the pattern encodes 1.5 * 2^52 + x exactly; subtracting 1.5 * 2^52
+// is exact (both operands lie in [2^52, 2^53)).  The level sums meet the
+// bound: level l holds at most l - 1 pair products of at most K * 127^2
+// each, with K <= 16384, so |H| < 5.7e14 < 2^51 and |Lo| is smaller still.
+__device__ __forceinline__ double i64_to_f64_exact(long long x)
+{
+    return __longlong_as_double(0x4338000000000000LL + x) - 0x1.8p52;
+}
+
 // ---------------------------------------------------------------- contraction
 
 // Shared memory: pipeline stages, each one K step (32 bytes) of every A slice
@@ -620,30 +632,24 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
                 for (int j = 0; j < 16; j++)
                     H[j] = (((long long)r[0][j] * 128 + r[1][j]) * 128 + r[2][j]) * 128 + r[3][j];
             }
-            // Levels 6..L: with three of them (L = 8) they are folded into
-            // int64 before the stores' addresses are live (32 registers held
-            // through the store loop instead of 48); with fewer the int32
-            // values are the smaller form and are kept.
-            constexpr int kLoLevels = L - 5;
-            constexpr bool kFoldLo = kLoLevels > 2;
-            int32_t r[kFoldLo ? 1 : kLoLevels][16];
-            long long Lo[kFoldLo ? 16 : 1];
-            if constexpr (kFoldLo) {
-                int32_t t[kLoLevels][16];
+            // Levels 6..L give Lo; the recombined value (exact up to the one
+            // rounding of the fma) is formed before the stores' addresses are
+            // live, so the store loop holds 16 doubles instead of the level
+            // sums.
+            double d[16];
+            {
+                int32_t t[L - 5][16];
 #pragma unroll
-                for (int l = 0; l < kLoLevels; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), t[l]);
+                for (int l = 0; l < L - 5; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), t[l]);
                 tmem_ld_wait();
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     long long lo = 0;
 #pragma unroll
-                    for (int l = 0; l < kLoLevels; l++) lo = lo * 128 + t[l][j];
-                    Lo[j] = lo << (7 * (8 - L));
+                    for (int l = 0; l < L - 5; l++) lo = lo * 128 + t[l][j];
+                    lo <<= 7 * (8 - L);
+                    d[j] = fma(i64_to_f64_exact(lo), 0x1p-21, i64_to_f64_exact(H[j]));
                 }
-            } else {
-#pragma unroll
-                for (int l = 0; l < kLoLevels; l++) tmem_ld16_nowait(col + (uint32_t)((4 + l) * NE), r[l]);
-                tmem_ld_wait();
             }
             // This warp's accumulators are in registers: release them.
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -670,18 +676,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_contract_split(const __gri
                     const int cx[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
                     for (int jj = 0; jj < 4; jj++) {
-                        long long lo;
-                        if constexpr (kFoldLo) {
-                            lo = Lo[j + jj];
-                        } else {
-                            lo = 0;
-#pragma unroll
-                            for (int l = 0; l < kLoLevels; l++) lo = lo * 128 + r[l][j + jj];
-                            lo <<= 7 * (8 - L);
-                        }
-                        const double d = fma((double)lo, 0x1p-21, (double)H[j + jj]);
                         if (j + jj < nj) {
-                            const double v = scale2(d, rex + cx[jj]);
+                            const double v = scale2(d[j + jj], rex + cx[jj]);
                             if (p.f32) {
                                 // Entry k of a float matrix is float k of the same buffer.
                                 const int64_t o = (int64_t)(j + jj) * P;
