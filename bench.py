@@ -159,12 +159,12 @@ def peaks():
 # and the commands that made them are under profiles/.
 TRAFFIC_PER_ELEMENT = {
     # profiles/k_contract_split_elasticity_hex32.md, 32768 elements: the one
-    # launch of a step (all six contracted groups) reads 387.29 MB and writes
-    # 1798.11 MB.
-    ("c2", "contract_split"): (387.290624e6 + 1798.110e6) / 32768,
-    # profiles/k_row_values_elasticity_hex32.md: 3.211 GB read + 1.216 GB
+    # launch of a step (all six contracted groups) reads 417.57 MB and writes
+    # 1721.87 MB.
+    ("c2", "contract_split"): (417.574912e6 + 1721.872e6) / 32768,
+    # profiles/k_row_values_elasticity_hex32.md: 3.187 GB read + 1.199 GB
     # written by the launch over all 9 groups of 32768 elements.
-    ("c2", "row_values"): (3.211152e9 + 1.216269e9) / 32768,
+    ("c2", "row_values"): (3.186658e9 + 1.198509e9) / 32768,
 }
 
 
