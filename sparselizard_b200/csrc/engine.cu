@@ -2388,14 +2388,21 @@ void launch_warp_rows(Ctx* ctx, RowParams rp, bool f32)
     if (smem > 48 * 1024) {
         if (smem > 227 * 1024)
             fail(SLGPU_E_UNSUPPORTED, "a CSR row is too long for the shared-memory row buffer");
-        cuda_check(cudaFuncSetAttribute(k_row_values<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-        cuda_check(cudaFuncSetAttribute(k_row_values<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_row_values<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
     }
     const unsigned grid = grid_for((rp.nrows + rp.rows_per_warp - 1) / rp.rows_per_warp, wpb);
-    if (f32)
-        k_row_values<float><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
+    const bool U = rp.uniform_width > 0;
+    if (f32 && U)
+        k_row_values<float, true><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
+    else if (f32)
+        k_row_values<float, false><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
+    else if (U)
+        k_row_values<double, true><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
     else
-        k_row_values<double><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
+        k_row_values<double, false><<<grid, 32 * wpb, smem, ctx->x->stream>>>(rp);
     cuda_check(cudaGetLastError(), "k_row_values");
     ctx->launches++;
 }
@@ -2427,6 +2434,16 @@ void launch_row_values(Ctx* ctx, const Matrix& M, Pattern& P, const std::vector<
     rp.dense = rhs ? Avals : nullptr;
     // Element values stored as floats (every segment alike, float_values()).
     const bool f32 = !rsegs.empty() && rsegs[0].f32 != 0;
+    // Segments of one width (<= 32) with multiplier 1: the warp kernel takes
+    // both from the launch instead of from each incidence.
+    rp.uniform_width = 0;
+    if (!rsegs.empty() && rsegs[0].width >= 1 && rsegs[0].width <= 32) {
+        bool uni = true;
+        for (const RowSeg& sg : rsegs)
+            uni = uni && sg.width == rsegs[0].width && sg.mult == 1.0;
+        if (uni)
+            rp.uniform_width = rsegs[0].width;
+    }
     // Bytes: kept element values and their slots, incidences, row
     // pointers read; A and D values written.
     const double rbytes = (f32 ? 6.0 : 10.0) * P.nvalid + 8.0 * P.ninc + 4.0 * (P.nA + 1) + 8.0 * (rhs ? M.ndofs : P.nnzA + P.nnzD);

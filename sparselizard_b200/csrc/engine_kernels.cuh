@@ -728,6 +728,7 @@ struct RowParams {
     double* Dvals;
     double* dense;  // right-hand side: dense[row] = -value (Avals unused)
     int rows_per_warp;  // k_row_values: consecutive rows per warp (1 .. kRowsPerWarp)
+    int uniform_width;  // every segment this width (<= 32) with multiplier 1, else 0
 };
 
 // CSR values, one warp per row: the row's incidences are visited in a fixed
@@ -815,7 +816,7 @@ __global__ void __launch_bounds__(kThreadRows) k_row_thread(RowParams p)
 // Most rows per warp of k_row_values: their 32 row bounds fit one per lane.
 constexpr int kRowsPerWarp = 31;
 
-template <class V>
+template <class V, bool U>
 __global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
 {
     const V* vals = reinterpret_cast<const V*>(p.vals);
@@ -869,10 +870,10 @@ __global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
                         const int src = (u + x) & 31;
                         const uint32_t vo = __shfl_sync(0xffffffffu, voff, src);
                         const uint32_t co = __shfl_sync(0xffffffffu, coo, src);
-                        const int inf = __shfl_sync(0xffffffffu, info, src);
+                        const int w = U ? p.uniform_width : (__shfl_sync(0xffffffffu, info, src) & 0xffff);
                         slot[x] = -1;
                         val[x] = 0.0;
-                        if (u + x < nkb && lane < (inf & 0xffff)) {
+                        if (u + x < nkb && lane < w) {
                             slot[x] = p.slotmap[(uint64_t)co + lane];
                             val[x] = (double)vals[(uint64_t)vo + lane];
                         }
@@ -880,9 +881,15 @@ __global__ void __launch_bounds__(256, 6) k_row_values(RowParams p)
 #pragma unroll
                     for (int x = 0; x < kRowBatch; x++) {
                         if (u + x < nkb) {
-                            const double m = __shfl_sync(0xffffffffu, mult, (u + x) & 31);
-                            if (slot[x] >= 0)
-                                buf[slot[x]] = fma(val[x], m, buf[slot[x]]);
+                            if constexpr (U) {
+                                // Multiplier 1: val + buf is fma(val, 1, buf) bit for bit.
+                                if (slot[x] >= 0)
+                                    buf[slot[x]] = val[x] + buf[slot[x]];
+                            } else {
+                                const double m = __shfl_sync(0xffffffffu, mult, (u + x) & 31);
+                                if (slot[x] >= 0)
+                                    buf[slot[x]] = fma(val[x], m, buf[slot[x]]);
+                            }
                             __syncwarp();
                         }
                     }
