@@ -162,9 +162,9 @@ TRAFFIC_PER_ELEMENT = {
     # launch of a step (all six contracted groups) reads 417.57 MB and writes
     # 1721.87 MB.
     ("c2", "contract_split"): (417.574912e6 + 1721.872e6) / 32768,
-    # profiles/k_row_values_elasticity_hex32.md: 3.187 GB read + 1.199 GB
+    # profiles/k_row_values_elasticity_hex32.md: 3.140 GB read + 1.187 GB
     # written by the launch over all 9 groups of 32768 elements.
-    ("c2", "row_values"): (3.186658e9 + 1.198509e9) / 32768,
+    ("c2", "row_values"): (3.140404e9 + 1.187079e9) / 32768,
 }
 
 
